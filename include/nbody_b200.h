@@ -1,0 +1,204 @@
+/*
+ * nbody_b200.h -- C ABI of the B200 (sm_100a) Barnes-Hut step for the
+ * Milkyway@Home N-body client.
+ *
+ * The library (milkywayathome_client_b200/libnbody_b200.so) replaces the
+ * reference client's CPU step (nbody/src/nbody_grav.c, nbody_tree.c,
+ * nbody_plain.c, nbody_potential.c) and its OpenCL twin (nbody/src/nbody_cl.c +
+ * nbody/kernels/nbody_kernels.cl) on one GPU.  Every entry point takes plain
+ * pointers and sizes; nothing here depends on PyTorch or on the reference's
+ * headers.  The context and state the reference keeps in NBodyCtx / NBodyState
+ * (nbody/include/nbody_types.h:360-521) are passed as the flat NBodyCudaCtx
+ * below plus an opaque NBodyCudaState handle that owns the device copy of the
+ * bodies, the tree and the accelerations.
+ *
+ * Status values are the reference's NBodyStatus bit mask
+ * (nbody/include/nbody_types.h:541-583) with the same numeric values, so
+ * nbStatusIsFatal() from the reference applies unchanged.  CUDA runtime
+ * failures are reported as NBODY_CUDA_ERROR, which occupies the reference's
+ * NBODY_RESERVED_ERROR_1 bit.
+ *
+ * Threading: each NBodyCudaState is used from one host thread at a time, as the
+ * reference's NBodyState is (nbody/src/nbody.c:182-212).
+ */
+#ifndef NBODY_B200_H
+#define NBODY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status bits: values of NBodyStatus, nbody/include/nbody_types.h:541-583 ---- */
+#define NBODY_SUCCESS               0
+#define NBODY_ERROR                 (1 << 1)
+#define NBODY_TREE_STRUCTURE_ERROR  (1 << 3)
+#define NBODY_TREE_INCEST_FATAL     (1 << 4)
+#define NBODY_CAPABILITY_ERROR      (1 << 8)
+#define NBODY_UNIMPLEMENTED         (1 << 10)
+#define NBODY_UNSUPPORTED           (1 << 11)
+#define NBODY_USER_ERROR            (1 << 12)
+#define NBODY_MAX_DEPTH_ERROR       (1 << 16)
+#define NBODY_CELL_OVERFLOW_ERROR   (1 << 17)
+#define NBODY_CUDA_ERROR            (1 << 20)   /* NBODY_RESERVED_ERROR_1 */
+#define NBODY_TREE_INCEST_NONFATAL  (1 << 24)
+#define NBODY_STATUS_WARNINGS_MASK  0xFF000000u  /* NBODY_STATUS_ALL_WARNINGS */
+
+typedef int NBodyCudaStatus;
+
+/* ---- enumerations: same values as the reference's enums ---- */
+/* criterion_t, nbody/include/nbody_types.h:171-178 */
+enum { NBCUDA_TREECODE = 0, NBCUDA_SW93 = 1, NBCUDA_BH86 = 2, NBCUDA_EXACT = 3 };
+/* ExternalPotentialType, nbody/include/nbody_types.h:181-186 */
+enum { NBCUDA_POTENTIAL_DEFAULT = 0, NBCUDA_POTENTIAL_NONE = 1, NBCUDA_POTENTIAL_CUSTOM_LUA = 2 };
+/* spherical_t, disk_t, halo_t: nbody/include/nbody_potential_types.h:30-125 */
+enum { NBCUDA_NO_SPHERICAL = 0, NBCUDA_HERNQUIST_SPHERICAL = 1, NBCUDA_PLUMMER_SPHERICAL = 2 };
+enum { NBCUDA_NO_DISK = 0, NBCUDA_MIYAMOTO_NAGAI_DISK = 1, NBCUDA_FREEMAN_DISK = 2,
+       NBCUDA_DOUBLE_EXPONENTIAL_DISK = 3, NBCUDA_SECH2_EXPONENTIAL_DISK = 4,
+       NBCUDA_ORBITING_BAR = 5 };
+enum { NBCUDA_NO_HALO = 0, NBCUDA_LOGARITHMIC_HALO = 1, NBCUDA_NFW_HALO = 2,
+       NBCUDA_TRIAXIAL_HALO = 3, NBCUDA_CAUSTIC_HALO = 4, NBCUDA_ALLEN_SANTILLAN_HALO = 5,
+       NBCUDA_WILKINSON_EVANS_HALO = 6, NBCUDA_NFW_MASS_HALO = 7, NBCUDA_PLUMMER_HALO = 8,
+       NBCUDA_HERNQUIST_HALO = 9, NBCUDA_NINKOVIC_HALO = 10 };
+
+/* Arithmetic of the force walk. */
+enum {
+    NBCUDA_PRECISION_FP64  = 0,  /* drop-in: FP64, no FMA contraction, the reference's
+                                    per-body opening test and summation order */
+    NBCUDA_PRECISION_MIXED = 1   /* FP32 walk in leaf-cell-relative coordinates with FP64
+                                    accumulation; moments, potential and leapfrog stay FP64 */
+};
+
+/* Fields of Spherical / Disk / Halo (nbody/include/nbody_potential_types.h:40-156). */
+typedef struct { int type; double mass, scale; } NBodyCudaSpherical;
+typedef struct { int type; double mass, scaleLength, scaleHeight, patternSpeed, startAngle; } NBodyCudaDisk;
+typedef struct {
+    int type;
+    double vhalo, scaleLength, flattenZ, flattenY, flattenX, triaxAngle;
+    double c1, c2, c3, mass, gamma, lambda, rho0;
+} NBodyCudaHalo;
+/* Potential (nbody/include/nbody_potential_types.h:158-165) */
+typedef struct {
+    NBodyCudaSpherical sphere;
+    NBodyCudaDisk disk, disk2;
+    NBodyCudaHalo halo;
+} NBodyCudaPotential;
+
+/* The NBodyCtx fields the step reads (nbody/include/nbody_types.h:450-521). */
+typedef struct {
+    double eps2;          /* softening^2 */
+    double theta;         /* opening angle */
+    double timestep;      /* dt */
+    double treeRSize;     /* initial root size (power of two) */
+    int criterion;        /* NBCUDA_TREECODE .. NBCUDA_EXACT */
+    int useQuad;          /* quadrupole moments in the walk */
+    int allowIncest;      /* tree incest is a warning instead of fatal */
+    int potentialType;    /* NBCUDA_POTENTIAL_* */
+    int precision;        /* NBCUDA_PRECISION_* (no reference counterpart) */
+    int reserved;
+    NBodyCudaPotential pot;
+} NBodyCudaCtx;
+
+/* Layout of the reference's Body (nbody/include/nbody_types.h:103-125): pos is an
+ * mwvector {x,y,z,w} at offset 0, mass at 40, type (short) at 48, id at 52, vel
+ * (mwvector) at 64; sizeof(Body) == 96. */
+#define NBCUDA_BODY_STRIDE      96
+#define NBCUDA_BODY_POS_OFFSET   0
+#define NBCUDA_BODY_MASS_OFFSET 40
+#define NBCUDA_BODY_TYPE_OFFSET 48
+#define NBCUDA_BODY_ID_OFFSET   52
+#define NBCUDA_BODY_VEL_OFFSET  64
+/* mwvector stride of st->acctab (nbody/include/nbody_types.h:367) */
+#define NBCUDA_VECTOR_STRIDE    32
+
+/* Device-resident bodies, tree and accelerations: the CUDA counterpart of the
+ * st->ci / st->kernels / st->nbb slots of NBodyState (nbody_types.h:421-430). */
+typedef struct NBodyCudaState NBodyCudaState;
+
+/* Tree summary after the last tree build (NBodyTree, nbody_types.h:188-196). */
+typedef struct {
+    double rsize;          /* t->rsize: root side length after expandBox */
+    int nbody;             /* bodies in the state */
+    int nTreeBodies;       /* bodies with nonzero mass (inserted in the tree) */
+    int cellUsed;          /* t->cellUsed */
+    int maxDepth;          /* t->maxDepth: deepest body level */
+    int nNodes;            /* cells + tree bodies, in walk (preorder) order */
+    int step;              /* st->step */
+    int treeIncest;        /* st->treeIncest */
+} NBodyCudaTreeInfo;
+
+/* ---- lifecycle: replaces nbInitCL / nbInitNBodyStateCL (nbody/src/nbody_types.c:258-341)
+ * and destroyNBodyState's CL branch.  Allocates device buffers for nbody bodies. */
+NBodyCudaStatus nbInitCUDA(NBodyCudaState** st, int device, int nbody);
+void nbDestroyCUDA(NBodyCudaState* st);
+
+/* ---- marshalling: replaces nbMarshalBodies (nbody/src/nbody_cl.c:2211-2269).
+ * toDevice != 0 copies pos/vel/mass of the host Body[] (NBCUDA_BODY_STRIDE bytes apart)
+ * into the device state and resets st->step and the tree root size to treeRSize;
+ * toDevice == 0 writes pos and vel back into the host Body[]. */
+NBodyCudaStatus nbMarshalBodiesCUDA(NBodyCudaState* st, void* bodytab, int nbody,
+                                    int toDevice, double treeRSize);
+/* Plain SoA host arrays (pos/vel: x0,y0,z0,x1,...; mass: n) -- the same data as above. */
+NBodyCudaStatus nbSetBodiesCUDA(NBodyCudaState* st, const double* pos, const double* vel,
+                                const double* mass, int nbody, double treeRSize);
+NBodyCudaStatus nbGetBodiesCUDA(NBodyCudaState* st, double* pos, double* vel);
+/* st->acctab after the last force evaluation: 3 doubles per body in host memory. */
+NBodyCudaStatus nbGetAccelsCUDA(NBodyCudaState* st, double* acc);
+/* Device-pointer variants for callers that keep the bodies in their own device
+ * memory (x,y,z interleaved as above; all pointers on the state's device). */
+NBodyCudaStatus nbSetBodiesDeviceCUDA(NBodyCudaState* st, const double* dpos, const double* dvel,
+                                      const double* dmass, int nbody, double treeRSize);
+NBodyCudaStatus nbGetBodiesDeviceCUDA(NBodyCudaState* st, double* dpos, double* dvel, double* dacc);
+
+/* ---- the hot path ----
+ * nbGravMapCUDA replaces nbGravMap (nbody/src/nbody_grav.c:305-328): builds the tree
+ * (nbMakeTree, nbody/src/nbody_tree.c:429-460) unless criterion is Exact, then fills
+ * the accelerations with self-gravity + nbExtAcceleration (nbody/src/nbody_potential.c:627).
+ * nbStepSystemCUDA replaces nbStepSystem / nbStepSystemPlain (nbody/src/nbody.c:182-200,
+ * nbody/src/nbody_plain.c:329-364): one kick-drift-kick step, st->step += 1.
+ * nbRunStepsCUDA runs nsteps such steps back to back on the device and returns the OR of
+ * their statuses; it stops at the first fatal status as nbRunSystemPlain does
+ * (nbody/src/nbody_plain.c:410-446). */
+NBodyCudaStatus nbGravMapCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st);
+NBodyCudaStatus nbStepSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st);
+NBodyCudaStatus nbRunStepsCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, int nsteps);
+
+/* ---- tree introspection (parity checks of nbMakeTree) ---- */
+NBodyCudaStatus nbMakeTreeCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st);
+NBodyCudaStatus nbTreeInfoCUDA(NBodyCudaState* st, NBodyCudaTreeInfo* info);
+/* Nodes in walk (threadTree preorder) order, nNodes entries each: pos = CoM for cells,
+ * body position for bodies (3 doubles); mass; rcrit2 (0 for bodies); quad (6 doubles:
+ * xx,xy,xz,yy,yz,zz; 0 for bodies); next (index of Next(), nNodes for NULL); body (index
+ * of the body in the state for body nodes, -1 for cells); depth (cell level, root = 0;
+ * for bodies the level of their parent cell + 1).  Any pointer may be NULL. */
+NBodyCudaStatus nbGetTreeCUDA(NBodyCudaState* st, double* pos, double* mass, double* rcrit2,
+                              double* quad, int32_t* next, int32_t* body, int32_t* depth);
+
+/* ---- external potential alone: nbExtAcceleration (nbody/src/nbody_potential.c:627-762)
+ * at n host positions (3 doubles each) -> n host accelerations. */
+NBodyCudaStatus nbExtAccelerationCUDA(const NBodyCudaPotential* pot, const double* pos,
+                                      double* acc, int n, int device);
+
+/* Number of this library's kernel launches issued since load (a launch counter for
+ * benchmarks). */
+uint64_t nbKernelLaunchesCUDA(void);
+/* Milliseconds of device time of the force-walk kernels of the last nbGravMapCUDA /
+ * nbStepSystemCUDA / nbRunStepsCUDA call (CUDA events on the launch stream), and the
+ * number of walk launches they cover. */
+NBodyCudaStatus nbLastWalkTimeCUDA(NBodyCudaState* st, double* ms, int* launches);
+/* Interaction counts of the last force evaluation: body-body, body-cell interactions
+ * and node visits summed over all bodies (the algorithmic work of the walk). */
+NBodyCudaStatus nbInteractionCountsCUDA(NBodyCudaState* st, unsigned long long* nBodyBody,
+                                        unsigned long long* nBodyCell,
+                                        unsigned long long* nVisit);
+/* Enables (1) / disables (0) counting interactions in the walk (off by default). */
+NBodyCudaStatus nbSetCountingCUDA(NBodyCudaState* st, int enable);
+
+const char* nbLastErrorCUDA(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NBODY_B200_H */

@@ -1,0 +1,156 @@
+"""ctypes view of the C ABI in include/nbody_b200.h (libnbody_b200.so).
+
+The library is the product: every force evaluation and step runs in its sm_100a kernels.
+There is no CPU fallback -- if the shared library is missing or cannot be loaded, loading
+raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnbody_b200.so")
+
+# NBodyStatus bits (nbody/include/nbody_types.h:541-583)
+NBODY_SUCCESS = 0
+NBODY_ERROR = 1 << 1
+NBODY_TREE_STRUCTURE_ERROR = 1 << 3
+NBODY_TREE_INCEST_FATAL = 1 << 4
+NBODY_CAPABILITY_ERROR = 1 << 8
+NBODY_UNIMPLEMENTED = 1 << 10
+NBODY_UNSUPPORTED = 1 << 11
+NBODY_USER_ERROR = 1 << 12
+NBODY_MAX_DEPTH_ERROR = 1 << 16
+NBODY_CELL_OVERFLOW_ERROR = 1 << 17
+NBODY_CUDA_ERROR = 1 << 20
+NBODY_TREE_INCEST_NONFATAL = 1 << 24
+NBODY_STATUS_ALL_WARNINGS = 0xFF000000
+
+STATUS_NAMES = {
+    NBODY_ERROR: "NBODY_ERROR", NBODY_TREE_STRUCTURE_ERROR: "NBODY_TREE_STRUCTURE_ERROR",
+    NBODY_TREE_INCEST_FATAL: "NBODY_TREE_INCEST_FATAL",
+    NBODY_CAPABILITY_ERROR: "NBODY_CAPABILITY_ERROR", NBODY_UNIMPLEMENTED: "NBODY_UNIMPLEMENTED",
+    NBODY_UNSUPPORTED: "NBODY_UNSUPPORTED", NBODY_USER_ERROR: "NBODY_USER_ERROR",
+    NBODY_MAX_DEPTH_ERROR: "NBODY_MAX_DEPTH_ERROR",
+    NBODY_CELL_OVERFLOW_ERROR: "NBODY_CELL_OVERFLOW_ERROR", NBODY_CUDA_ERROR: "NBODY_CUDA_ERROR",
+    NBODY_TREE_INCEST_NONFATAL: "NBODY_TREE_INCEST_NONFATAL",
+}
+
+
+def status_is_fatal(rc):
+    """nbStatusIsFatal (nbody/include/nbody_types.h:582)."""
+    return (rc & ~NBODY_STATUS_ALL_WARNINGS & 0xFFFFFFFF) != 0
+
+
+def status_names(rc):
+    return [name for bit, name in sorted(STATUS_NAMES.items()) if rc & bit] or ["NBODY_SUCCESS"]
+
+
+# criterion_t (nbody/include/nbody_types.h:171-178)
+TREECODE, SW93, BH86, EXACT = 0, 1, 2, 3
+CRITERIA = {"treecode": TREECODE, "sw93": SW93, "bh86": BH86, "exact": EXACT}
+# ExternalPotentialType
+POTENTIAL_DEFAULT, POTENTIAL_NONE, POTENTIAL_CUSTOM_LUA = 0, 1, 2
+# spherical_t / disk_t / halo_t (nbody/include/nbody_potential_types.h)
+NO_SPHERICAL, HERNQUIST_SPHERICAL, PLUMMER_SPHERICAL = 0, 1, 2
+NO_DISK, MIYAMOTO_NAGAI_DISK = 0, 1
+NO_HALO, LOGARITHMIC_HALO, NFW_HALO = 0, 1, 2
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+
+
+class Spherical(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("mass", ctypes.c_double), ("scale", ctypes.c_double)]
+
+
+class Disk(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("mass", ctypes.c_double),
+                ("scaleLength", ctypes.c_double), ("scaleHeight", ctypes.c_double),
+                ("patternSpeed", ctypes.c_double), ("startAngle", ctypes.c_double)]
+
+
+class Halo(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int)] + [(f, ctypes.c_double) for f in (
+        "vhalo", "scaleLength", "flattenZ", "flattenY", "flattenX", "triaxAngle",
+        "c1", "c2", "c3", "mass", "gamma", "lambda_", "rho0")]
+
+
+class Potential(ctypes.Structure):
+    _fields_ = [("sphere", Spherical), ("disk", Disk), ("disk2", Disk), ("halo", Halo)]
+
+
+class Ctx(ctypes.Structure):
+    """NBodyCudaCtx: the NBodyCtx fields the step reads."""
+    _fields_ = [("eps2", ctypes.c_double), ("theta", ctypes.c_double),
+                ("timestep", ctypes.c_double), ("treeRSize", ctypes.c_double),
+                ("criterion", ctypes.c_int), ("useQuad", ctypes.c_int),
+                ("allowIncest", ctypes.c_int), ("potentialType", ctypes.c_int),
+                ("precision", ctypes.c_int), ("reserved", ctypes.c_int),
+                ("pot", Potential)]
+
+
+class TreeInfo(ctypes.Structure):
+    _fields_ = [("rsize", ctypes.c_double), ("nbody", ctypes.c_int),
+                ("nTreeBodies", ctypes.c_int), ("cellUsed", ctypes.c_int),
+                ("maxDepth", ctypes.c_int), ("nNodes", ctypes.c_int), ("step", ctypes.c_int),
+                ("treeIncest", ctypes.c_int)]
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_vp = ctypes.c_void_p
+_ull = ctypes.POINTER(ctypes.c_ulonglong)
+
+# (name, restype, argtypes) of every exported entry point
+SIGNATURES = [
+    ("nbInitCUDA", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int]),
+    ("nbDestroyCUDA", None, [_vp]),
+    ("nbMarshalBodiesCUDA", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
+    ("nbSetBodiesCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_double]),
+    ("nbGetBodiesCUDA", ctypes.c_int, [_vp, _vp, _vp]),
+    ("nbGetAccelsCUDA", ctypes.c_int, [_vp, _vp]),
+    ("nbSetBodiesDeviceCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_double]),
+    ("nbGetBodiesDeviceCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("nbGravMapCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp]),
+    ("nbStepSystemCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp]),
+    ("nbRunStepsCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, ctypes.c_int]),
+    ("nbMakeTreeCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp]),
+    ("nbTreeInfoCUDA", ctypes.c_int, [_vp, ctypes.POINTER(TreeInfo)]),
+    ("nbGetTreeCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("nbExtAccelerationCUDA", ctypes.c_int,
+     [ctypes.POINTER(Potential), _vp, _vp, ctypes.c_int, ctypes.c_int]),
+    ("nbKernelLaunchesCUDA", ctypes.c_uint64, []),
+    ("nbLastWalkTimeCUDA", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int)]),
+    ("nbInteractionCountsCUDA", ctypes.c_int, [_vp, _ull, _ull, _ull]),
+    ("nbSetCountingCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nbLastErrorCUDA", ctypes.c_char_p, []),
+]
+
+_lib = None
+
+
+def load(path=LIB_PATH):
+    """Load libnbody_b200.so (raises OSError/FileNotFoundError when it is absent)."""
+    global _lib
+    if _lib is not None and path == LIB_PATH:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            "%s is missing: build it with `python -m milkywayathome_client_b200.build`" % path)
+    lib = ctypes.CDLL(path)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path == LIB_PATH:
+        _lib = lib
+    return lib
+
+
+def last_error():
+    return load().nbLastErrorCUDA().decode(errors="replace")
+
+
+def ptr(a):
+    """Address of a numpy array's data (None passes NULL)."""
+    if a is None:
+        return None
+    return ctypes.c_void_p(a.ctypes.data)

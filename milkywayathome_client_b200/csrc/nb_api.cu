@@ -1,0 +1,697 @@
+// C ABI of the B200 step (include/nbody_b200.h): device state, marshalling and the
+// host-side sequencing of the kernels of nbGravMap / nbStepSystem.
+#include "nb_common.cuh"
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+// ---- kernels defined in the other translation units ----
+void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
+                         const double* nodeQuad, const unsigned* order, const double* px,
+                         const double* py, const double* pz, double* ax, double* ay, double* az,
+                         double* vx, double* vy, double* vz, const NbWalkParams& wp,
+                         const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s);
+void nb_launch_walk_mixed(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
+                          const double* nodeQuad, const unsigned* order, const double* px,
+                          const double* py, const double* pz, double* ax, double* ay, double* az,
+                          double* vx, double* vy, double* vz, const NbWalkParams& wp,
+                          const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s);
+void nb_launch_direct_fp64(const double* px, const double* py, const double* pz,
+                           const double* mass, double* ax, double* ay, double* az, double* vx,
+                           double* vy, double* vz, const NbWalkParams& wp, const NbPot& pot,
+                           NbScalars* sc, cudaStream_t s);
+void nb_launch_ext_only(const double* dpos, double* dacc, int n, const NbPot& pot, cudaStream_t s);
+
+static std::atomic<unsigned long long> g_launches{0};
+void nb_count_launch(int n) { g_launches.fetch_add((unsigned long long) n); }
+
+static thread_local std::string g_lastError;
+static NBodyCudaStatus nb_cuda_fail(cudaError_t e, const char* what)
+{
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+    g_lastError = buf;
+    return NBODY_CUDA_ERROR;
+}
+#define NB_CHECK(call)                                                        \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) return nb_cuda_fail(e_, #call);                \
+    } while (0)
+
+// ---- small kernels: SoA <-> interleaved / AoS Body ----
+__global__ void k_split_xyz(const double* __restrict__ in, double* __restrict__ x,
+                            double* __restrict__ y, double* __restrict__ z, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x[i] = in[3 * i]; y[i] = in[3 * i + 1]; z[i] = in[3 * i + 2];
+    }
+}
+__global__ void k_join_xyz(const double* __restrict__ x, const double* __restrict__ y,
+                           const double* __restrict__ z, double* __restrict__ out, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        out[3 * i] = x[i]; out[3 * i + 1] = y[i]; out[3 * i + 2] = z[i];
+    }
+}
+__global__ void k_from_bodies(const unsigned char* __restrict__ aos, double* px, double* py,
+                              double* pz, double* vx, double* vy, double* vz, double* mass, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double* b = reinterpret_cast<const double*>(aos + (size_t) i * NBCUDA_BODY_STRIDE);
+        px[i] = b[0]; py[i] = b[1]; pz[i] = b[2];
+        mass[i] = b[NBCUDA_BODY_MASS_OFFSET / 8];
+        vx[i] = b[NBCUDA_BODY_VEL_OFFSET / 8];
+        vy[i] = b[NBCUDA_BODY_VEL_OFFSET / 8 + 1];
+        vz[i] = b[NBCUDA_BODY_VEL_OFFSET / 8 + 2];
+    }
+}
+__global__ void k_to_bodies(unsigned char* __restrict__ aos, const double* px, const double* py,
+                            const double* pz, const double* vx, const double* vy,
+                            const double* vz, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double* b = reinterpret_cast<double*>(aos + (size_t) i * NBCUDA_BODY_STRIDE);
+        b[0] = px[i]; b[1] = py[i]; b[2] = pz[i];
+        b[NBCUDA_BODY_VEL_OFFSET / 8] = vx[i];
+        b[NBCUDA_BODY_VEL_OFFSET / 8 + 1] = vy[i];
+        b[NBCUDA_BODY_VEL_OFFSET / 8 + 2] = vz[i];
+    }
+}
+// advanceVelocities alone, for a step whose force evaluation failed (the reference still
+// kicks with the previous accelerations, nbody/src/nbody_plain.c:352-353).
+__global__ void k_kick(double* vx, double* vy, double* vz, const double* ax, const double* ay,
+                       const double* az, int n, double dtHalf)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        vx[i] = vx[i] + dtHalf * (ax[i] + 0.0);
+        vy[i] = vy[i] + dtHalf * (ay[i] + 0.0);
+        vz[i] = vz[i] + dtHalf * (az[i] + 0.0);
+    }
+}
+
+struct NBodyCudaState {
+    int device = 0;
+    int nbody = 0;
+    int capBodies = 0;
+    int numSMs = 148;
+    cudaStream_t stream = nullptr;
+    NbTreeBuffers b{};
+    int capNodes = 0;
+    NbScalars* scHost = nullptr;        // pinned mirror of the device scalars
+    double* stage = nullptr;            // device staging: 3 doubles per body
+    unsigned char* aos = nullptr;       // device staging for Body[] records
+    size_t aosBytes = 0;
+    double rsize = 4.0;                 // t->rsize carried between steps
+    int step = 0;
+    int treeIncest = 0;                 // st->treeIncest (sticky)
+    int counting = 0;
+    int haveTree = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float walkMs = 0.0f;
+    int walkLaunches = 0;
+    unsigned long long cBB = 0, cBC = 0, cVisit = 0;
+};
+
+template <typename T>
+static cudaError_t nb_alloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void**) p, count * sizeof(T));
+}
+
+static void nb_free_nodes(NBodyCudaState* st)
+{
+    NbTreeBuffers& b = st->b;
+    cudaFree(b.nodePM); cudaFree(b.nodeCrit); cudaFree(b.nodeLink); cudaFree(b.nodeQuad);
+    cudaFree(b.nodeDepth); cudaFree(b.parent); cudaFree(b.nchild); cudaFree(b.arrive);
+    b.nodePM = nullptr; b.nodeCrit = nullptr; b.nodeLink = nullptr; b.nodeQuad = nullptr;
+    b.nodeDepth = b.parent = b.nchild = b.arrive = nullptr;
+    st->capNodes = 0;
+}
+
+static NBodyCudaStatus nb_alloc_nodes(NBodyCudaState* st, int cap)
+{
+    nb_free_nodes(st);
+    NbTreeBuffers& b = st->b;
+    NB_CHECK(nb_alloc(&b.nodePM, cap));
+    NB_CHECK(nb_alloc(&b.nodeCrit, cap));
+    NB_CHECK(nb_alloc(&b.nodeLink, cap));
+    NB_CHECK(nb_alloc(&b.nodeQuad, 6 * (size_t) cap));
+    NB_CHECK(nb_alloc(&b.nodeDepth, cap));
+    NB_CHECK(nb_alloc(&b.parent, cap));
+    NB_CHECK(nb_alloc(&b.nchild, cap));
+    NB_CHECK(nb_alloc(&b.arrive, cap));
+    st->capNodes = cap;
+    return NBODY_SUCCESS;
+}
+
+static NBodyCudaStatus nb_alloc_bodies(NBodyCudaState* st, int n)
+{
+    NbTreeBuffers& b = st->b;
+    const size_t N = (size_t) (n > 0 ? n : 1);
+    NB_CHECK(nb_alloc(&b.px, N)); NB_CHECK(nb_alloc(&b.py, N)); NB_CHECK(nb_alloc(&b.pz, N));
+    NB_CHECK(nb_alloc(&b.vx, N)); NB_CHECK(nb_alloc(&b.vy, N)); NB_CHECK(nb_alloc(&b.vz, N));
+    NB_CHECK(nb_alloc(&b.ax, N)); NB_CHECK(nb_alloc(&b.ay, N)); NB_CHECK(nb_alloc(&b.az, N));
+    NB_CHECK(nb_alloc(&b.mass, N));
+    NB_CHECK(cudaMemsetAsync(b.ax, 0, N * sizeof(double), st->stream));
+    NB_CHECK(cudaMemsetAsync(b.ay, 0, N * sizeof(double), st->stream));
+    NB_CHECK(cudaMemsetAsync(b.az, 0, N * sizeof(double), st->stream));
+    NB_CHECK(nb_alloc(&b.sort.keyA, N)); NB_CHECK(nb_alloc(&b.sort.keyB, N));
+    NB_CHECK(nb_alloc(&b.sort.idxA, N)); NB_CHECK(nb_alloc(&b.sort.idxB, N));
+    const int tiles = (int) ((N + 2047) / 2048);
+    NB_CHECK(nb_alloc(&b.sort.hist, 256 * (size_t) tiles));
+    b.sort.capTiles = tiles;
+    NB_CHECK(nb_alloc(&b.gx, N)); NB_CHECK(nb_alloc(&b.gy, N)); NB_CHECK(nb_alloc(&b.gz, N));
+    NB_CHECK(nb_alloc(&b.delta, N)); NB_CHECK(nb_alloc(&b.cum, N));
+    NB_CHECK(nb_alloc(&b.scanTmp, (size_t) nb_scan_tmp_ints((int) N)));
+    NB_CHECK(nb_alloc(&b.bodyNode, N));
+    NB_CHECK(nb_alloc(&st->stage, 3 * N));
+    st->capBodies = (int) N;
+    return nb_alloc_nodes(st, 2 * (int) N + 64);
+}
+
+static void nb_free_all(NBodyCudaState* st)
+{
+    NbTreeBuffers& b = st->b;
+    double* d[] = {b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.ax, b.ay, b.az, b.mass, st->stage};
+    for (double* p : d) cudaFree(p);
+    cudaFree(b.sort.keyA); cudaFree(b.sort.keyB); cudaFree(b.sort.idxA); cudaFree(b.sort.idxB);
+    cudaFree(b.sort.hist);
+    cudaFree(b.gx); cudaFree(b.gy); cudaFree(b.gz);
+    cudaFree(b.delta); cudaFree(b.cum); cudaFree(b.scanTmp); cudaFree(b.bodyNode);
+    cudaFree(b.sc);
+    cudaFree(st->aos);
+    nb_free_nodes(st);
+    if (st->scHost) cudaFreeHost(st->scHost);
+    if (st->ev0) cudaEventDestroy(st->ev0);
+    if (st->ev1) cudaEventDestroy(st->ev1);
+    if (st->stream) cudaStreamDestroy(st->stream);
+}
+
+static NbPot nb_pot_from(const NBodyCudaCtx* c)
+{
+    NbPot p{};
+    p.enabled = c->potentialType == NBCUDA_POTENTIAL_DEFAULT;
+    p.sphType = c->pot.sphere.type; p.sphMass = c->pot.sphere.mass; p.sphScale = c->pot.sphere.scale;
+    p.diskType = c->pot.disk.type; p.diskMass = c->pot.disk.mass;
+    p.diskA = c->pot.disk.scaleLength; p.diskB = c->pot.disk.scaleHeight;
+    p.disk2Type = c->pot.disk2.type; p.disk2Mass = c->pot.disk2.mass;
+    p.disk2A = c->pot.disk2.scaleLength; p.disk2B = c->pot.disk2.scaleHeight;
+    p.haloType = c->pot.halo.type; p.haloV = c->pot.halo.vhalo;
+    p.haloA = c->pot.halo.scaleLength; p.haloQz = c->pot.halo.flattenZ;
+    return p;
+}
+
+static bool nb_pow2(double x)
+{
+    int e;
+    return x > 0.0 && std::isfinite(x) && std::frexp(x, &e) == 0.5;
+}
+
+// Options this implementation evaluates on the GPU; anything else is NBODY_UNSUPPORTED,
+// as the reference's OpenCL path does for a custom Lua potential (nbody_types.c:297-301).
+static NBodyCudaStatus nb_check_ctx(const NBodyCudaCtx* c, std::string& why)
+{
+    if (!c) { why = "null context"; return NBODY_USER_ERROR; }
+    if (c->criterion < NBCUDA_TREECODE || c->criterion > NBCUDA_EXACT) { why = "invalid criterion"; return NBODY_USER_ERROR; }
+    if (c->precision != NBCUDA_PRECISION_FP64 && c->precision != NBCUDA_PRECISION_MIXED) { why = "invalid precision"; return NBODY_USER_ERROR; }
+    if (c->potentialType == NBCUDA_POTENTIAL_CUSTOM_LUA) { why = "custom Lua potential"; return NBODY_UNSUPPORTED; }
+    if (c->potentialType == NBCUDA_POTENTIAL_DEFAULT) {
+        const NBodyCudaPotential& p = c->pot;
+        if (p.sphere.type != NBCUDA_NO_SPHERICAL && p.sphere.type != NBCUDA_HERNQUIST_SPHERICAL &&
+            p.sphere.type != NBCUDA_PLUMMER_SPHERICAL) { why = "bulge type"; return NBODY_UNSUPPORTED; }
+        if (p.disk.type != NBCUDA_NO_DISK && p.disk.type != NBCUDA_MIYAMOTO_NAGAI_DISK) { why = "disk type"; return NBODY_UNSUPPORTED; }
+        if (p.disk2.type != NBCUDA_NO_DISK && p.disk2.type != NBCUDA_MIYAMOTO_NAGAI_DISK) { why = "disk2 type"; return NBODY_UNSUPPORTED; }
+        if (p.halo.type != NBCUDA_NO_HALO && p.halo.type != NBCUDA_LOGARITHMIC_HALO &&
+            p.halo.type != NBCUDA_NFW_HALO) { why = "halo type"; return NBODY_UNSUPPORTED; }
+    }
+    return NBODY_SUCCESS;
+}
+
+static int nb_blocks(NBodyCudaState* st, int n)
+{
+    int g = (n + 255) / 256;
+    int cap = st->numSMs * 8;
+    if (g < 1) g = 1;
+    return g < cap ? g : cap;
+}
+
+// One force evaluation; drift/kick select the fused halves of the leapfrog.
+static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int drift, int kick)
+{
+    std::string why;
+    NBodyCudaStatus rc = nb_check_ctx(ctx, why);
+    if (rc) { g_lastError = why; return rc; }
+    if (ctx->criterion != NBCUDA_EXACT && !nb_pow2(st->rsize)) {
+        g_lastError = "root size must be a power of two";
+        return NBODY_UNSUPPORTED;
+    }
+    NB_CHECK(cudaSetDevice(st->device));
+    const int n = st->nbody;
+    const cudaStream_t s = st->stream;
+    NbTreeBuffers& b = st->b;
+    const NbPot pot = nb_pot_from(ctx);
+    NbWalkParams wp{};
+    wp.eps2 = ctx->eps2;
+    wp.dtHalf = 0.5 * ctx->timestep;
+    wp.useQuad = ctx->useQuad;
+    wp.kick = kick;
+    wp.n = n;
+    const bool mixed = ctx->precision == NBCUDA_PRECISION_MIXED;
+
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        // reset per-evaluation device scalars (keep rsize)
+        NbScalars init{};
+        init.rsize = st->rsize;
+        init.capNodes = st->capNodes;
+        NB_CHECK(cudaMemcpyAsync(b.sc, &init, sizeof init, cudaMemcpyHostToDevice, s));
+        st->walkLaunches = 0;
+        if (ctx->criterion == NBCUDA_EXACT) {
+            if (drift) {
+                // advancePosVel without the tree: reuse the bounding-box pass for the drift
+                nb_launch_drift_only(b, n, ctx->timestep, st->numSMs, s);
+            }
+            NB_CHECK(cudaEventRecord(st->ev0, s));
+            nb_launch_direct_fp64(b.px, b.py, b.pz, b.mass, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp,
+                                  pot, b.sc, s);
+            NB_CHECK(cudaEventRecord(st->ev1, s));
+            st->walkLaunches = 1;
+            st->haveTree = 0;
+        } else {
+            nb_build_tree(b, n, ctx->criterion, ctx->theta, ctx->useQuad, drift, ctx->timestep,
+                          st->numSMs, s);
+            nb_link_and_moments(b, n, st->capNodes, ctx->criterion, ctx->theta, ctx->useQuad, s);
+            NB_CHECK(cudaEventRecord(st->ev0, s));
+            if (mixed)
+                nb_launch_walk_mixed(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px,
+                                     b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
+                                     st->counting != 0, s);
+            else
+                nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px,
+                                    b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
+                                    st->counting != 0, s);
+            NB_CHECK(cudaEventRecord(st->ev1, s));
+            st->walkLaunches = 1;
+            st->haveTree = 1;
+        }
+        NB_CHECK(cudaGetLastError());
+        NB_CHECK(cudaMemcpyAsync(st->scHost, b.sc, sizeof(NbScalars), cudaMemcpyDeviceToHost, s));
+        NB_CHECK(cudaStreamSynchronize(s));
+        NbScalars& h = *st->scHost;
+        st->rsize = h.rsize;
+        if (h.status & NBODY_CELL_OVERFLOW_ERROR) {
+            // grow the node arrays and redo this evaluation (positions already drifted)
+            int need = h.neededNodes + h.neededNodes / 4 + 64;
+            rc = nb_alloc_nodes(st, need);
+            if (rc) return rc;
+            drift = 0;
+            continue;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, st->ev0, st->ev1);
+        st->walkMs = ms;
+        st->cBB = h.nBodyBody; st->cBC = h.nBodyCell; st->cVisit = h.nVisit;
+        NBodyCudaStatus out = h.status;
+        if ((out & ~(int) NBODY_STATUS_WARNINGS_MASK) == 0) {
+            if (h.incest) st->treeIncest = 1;
+        } else if (kick) {
+            // the failed evaluation left the accelerations untouched; the reference still
+            // applies advanceVelocities with them
+            k_kick<<<nb_blocks(st, n), 256, 0, s>>>(b.vx, b.vy, b.vz, b.ax, b.ay, b.az, n, wp.dtHalf);
+            nb_count_launch();
+            NB_CHECK(cudaStreamSynchronize(s));
+        }
+        if (st->treeIncest)
+            out |= ctx->allowIncest ? NBODY_TREE_INCEST_NONFATAL : NBODY_TREE_INCEST_FATAL;
+        return out;
+    }
+    g_lastError = "node capacity could not be grown";
+    return NBODY_CELL_OVERFLOW_ERROR;
+}
+
+extern "C" {
+
+NBodyCudaStatus nbInitCUDA(NBodyCudaState** out, int device, int nbody)
+{
+    if (!out || nbody < 0) return NBODY_USER_ERROR;
+    *out = nullptr;
+    int count = 0;
+    NB_CHECK(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) { g_lastError = "no such CUDA device"; return NBODY_CUDA_ERROR; }
+    NB_CHECK(cudaSetDevice(device));
+    NBodyCudaState* st = new NBodyCudaState();
+    st->device = device;
+    st->nbody = nbody;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) st->numSMs = prop.multiProcessorCount;
+    NBodyCudaStatus rc = NBODY_SUCCESS;
+    cudaError_t e = cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&st->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&st->ev1);
+    if (e == cudaSuccess) e = cudaMallocHost((void**) &st->scHost, sizeof(NbScalars));
+    if (e == cudaSuccess) e = cudaMalloc((void**) &st->b.sc, sizeof(NbScalars));
+    if (e != cudaSuccess) rc = nb_cuda_fail(e, "nbInitCUDA");
+    if (!rc) rc = nb_alloc_bodies(st, nbody);
+    if (rc) { nb_free_all(st); delete st; return rc; }
+    *out = st;
+    return NBODY_SUCCESS;
+}
+
+void nbDestroyCUDA(NBodyCudaState* st)
+{
+    if (!st) return;
+    cudaSetDevice(st->device);
+    if (st->stream) cudaStreamSynchronize(st->stream);
+    nb_free_all(st);
+    delete st;
+}
+
+static NBodyCudaStatus nb_reset_run(NBodyCudaState* st, double treeRSize)
+{
+    if (!(treeRSize > 0.0) || !nb_pow2(treeRSize)) {
+        g_lastError = "treeRSize must be a positive power of two";
+        return NBODY_UNSUPPORTED;
+    }
+    st->rsize = treeRSize;
+    st->step = 0;
+    st->treeIncest = 0;
+    st->haveTree = 0;
+    return NBODY_SUCCESS;
+}
+
+static bool nb_is_pinned(const void* p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    return a.type == cudaMemoryTypeHost;
+}
+
+NBodyCudaStatus nbMarshalBodiesCUDA(NBodyCudaState* st, void* bodytab, int nbody, int toDevice,
+                                    double treeRSize)
+{
+    if (!st || !bodytab || nbody != st->nbody) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    const size_t bytes = (size_t) nbody * NBCUDA_BODY_STRIDE;
+    if (st->aosBytes < bytes) {
+        cudaFree(st->aos);
+        st->aos = nullptr;
+        NB_CHECK(cudaMalloc((void**) &st->aos, bytes ? bytes : 1));
+        st->aosBytes = bytes;
+    }
+    NbTreeBuffers& b = st->b;
+    const cudaStream_t s = st->stream;
+    if (toDevice) {
+        NBodyCudaStatus rc = nb_reset_run(st, treeRSize);
+        if (rc) return rc;
+        if (nbody) {
+            NB_CHECK(cudaMemcpyAsync(st->aos, bodytab, bytes, cudaMemcpyHostToDevice, s));
+            k_from_bodies<<<nb_blocks(st, nbody), 256, 0, s>>>(st->aos, b.px, b.py, b.pz, b.vx, b.vy,
+                                                                b.vz, b.mass, nbody);
+            nb_count_launch();
+        }
+    } else if (nbody) {
+        k_to_bodies<<<nb_blocks(st, nbody), 256, 0, s>>>(st->aos, b.px, b.py, b.pz, b.vx, b.vy, b.vz,
+                                                          nbody);
+        nb_count_launch();
+        NB_CHECK(cudaMemcpyAsync(bodytab, st->aos, bytes, cudaMemcpyDeviceToHost, s));
+    }
+    NB_CHECK(cudaGetLastError());
+    NB_CHECK(cudaStreamSynchronize(s));
+    return NBODY_SUCCESS;
+}
+
+static NBodyCudaStatus nb_upload3(NBodyCudaState* st, const double* host, double* x, double* y,
+                                  double* z, int n)
+{
+    if (!n) return NBODY_SUCCESS;
+    const size_t bytes = 3 * (size_t) n * sizeof(double);
+    NB_CHECK(cudaMemcpyAsync(st->stage, host, bytes, cudaMemcpyHostToDevice, st->stream));
+    k_split_xyz<<<nb_blocks(st, n), 256, 0, st->stream>>>(st->stage, x, y, z, n);
+    nb_count_launch();
+    if (!nb_is_pinned(host)) NB_CHECK(cudaStreamSynchronize(st->stream));
+    return NBODY_SUCCESS;
+}
+
+static NBodyCudaStatus nb_download3(NBodyCudaState* st, double* host, const double* x,
+                                    const double* y, const double* z, int n)
+{
+    if (!n) return NBODY_SUCCESS;
+    k_join_xyz<<<nb_blocks(st, n), 256, 0, st->stream>>>(x, y, z, st->stage, n);
+    nb_count_launch();
+    NB_CHECK(cudaMemcpyAsync(host, st->stage, 3 * (size_t) n * sizeof(double),
+                             cudaMemcpyDeviceToHost, st->stream));
+    NB_CHECK(cudaStreamSynchronize(st->stream));
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbSetBodiesCUDA(NBodyCudaState* st, const double* pos, const double* vel,
+                                const double* mass, int nbody, double treeRSize)
+{
+    if (!st || nbody != st->nbody || (nbody && (!pos || !vel || !mass))) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    NBodyCudaStatus rc = nb_reset_run(st, treeRSize);
+    if (rc) return rc;
+    NbTreeBuffers& b = st->b;
+    rc = nb_upload3(st, pos, b.px, b.py, b.pz, nbody);
+    if (rc) return rc;
+    rc = nb_upload3(st, vel, b.vx, b.vy, b.vz, nbody);
+    if (rc) return rc;
+    if (nbody) NB_CHECK(cudaMemcpyAsync(b.mass, mass, (size_t) nbody * sizeof(double),
+                                        cudaMemcpyHostToDevice, st->stream));
+    NB_CHECK(cudaStreamSynchronize(st->stream));
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbGetBodiesCUDA(NBodyCudaState* st, double* pos, double* vel)
+{
+    if (!st) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    NbTreeBuffers& b = st->b;
+    NBodyCudaStatus rc = NBODY_SUCCESS;
+    if (pos) rc = nb_download3(st, pos, b.px, b.py, b.pz, st->nbody);
+    if (!rc && vel) rc = nb_download3(st, vel, b.vx, b.vy, b.vz, st->nbody);
+    return rc;
+}
+
+NBodyCudaStatus nbGetAccelsCUDA(NBodyCudaState* st, double* acc)
+{
+    if (!st || !acc) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    return nb_download3(st, acc, st->b.ax, st->b.ay, st->b.az, st->nbody);
+}
+
+NBodyCudaStatus nbSetBodiesDeviceCUDA(NBodyCudaState* st, const double* dpos, const double* dvel,
+                                      const double* dmass, int nbody, double treeRSize)
+{
+    if (!st || nbody != st->nbody) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    NBodyCudaStatus rc = nb_reset_run(st, treeRSize);
+    if (rc) return rc;
+    if (!nbody) return NBODY_SUCCESS;
+    NbTreeBuffers& b = st->b;
+    const cudaStream_t s = st->stream;
+    k_split_xyz<<<nb_blocks(st, nbody), 256, 0, s>>>(dpos, b.px, b.py, b.pz, nbody);
+    k_split_xyz<<<nb_blocks(st, nbody), 256, 0, s>>>(dvel, b.vx, b.vy, b.vz, nbody);
+    nb_count_launch(2);
+    NB_CHECK(cudaMemcpyAsync(b.mass, dmass, (size_t) nbody * sizeof(double),
+                             cudaMemcpyDeviceToDevice, s));
+    NB_CHECK(cudaGetLastError());
+    NB_CHECK(cudaStreamSynchronize(s));
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbGetBodiesDeviceCUDA(NBodyCudaState* st, double* dpos, double* dvel, double* dacc)
+{
+    if (!st) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    NbTreeBuffers& b = st->b;
+    const cudaStream_t s = st->stream;
+    const int n = st->nbody;
+    if (!n) return NBODY_SUCCESS;
+    if (dpos) k_join_xyz<<<nb_blocks(st, n), 256, 0, s>>>(b.px, b.py, b.pz, dpos, n);
+    if (dvel) k_join_xyz<<<nb_blocks(st, n), 256, 0, s>>>(b.vx, b.vy, b.vz, dvel, n);
+    if (dacc) k_join_xyz<<<nb_blocks(st, n), 256, 0, s>>>(b.ax, b.ay, b.az, dacc, n);
+    nb_count_launch((dpos != nullptr) + (dvel != nullptr) + (dacc != nullptr));
+    NB_CHECK(cudaGetLastError());
+    NB_CHECK(cudaStreamSynchronize(s));
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbGravMapCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st)
+{
+    if (!st) return NBODY_USER_ERROR;
+    return nb_force(ctx, st, 0, 0);
+}
+
+NBodyCudaStatus nbStepSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st)
+{
+    if (!st) return NBODY_USER_ERROR;
+    NBodyCudaStatus rc = nb_force(ctx, st, 1, 1);
+    if (!(rc & (NBODY_USER_ERROR | NBODY_UNSUPPORTED | NBODY_CUDA_ERROR))) st->step++;
+    return rc;
+}
+
+NBodyCudaStatus nbRunStepsCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, int nsteps)
+{
+    if (!st || nsteps < 0) return NBODY_USER_ERROR;
+    NBodyCudaStatus all = NBODY_SUCCESS;
+    float walkMs = 0.0f;
+    for (int k = 0; k < nsteps; ++k) {
+        NBodyCudaStatus rc = nbStepSystemCUDA(ctx, st);
+        walkMs += st->walkMs;
+        all |= rc;
+        if (rc & ~(int) NBODY_STATUS_WARNINGS_MASK) break;
+    }
+    st->walkMs = walkMs;
+    st->walkLaunches = nsteps;
+    return all;
+}
+
+NBodyCudaStatus nbMakeTreeCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st)
+{
+    if (!st) return NBODY_USER_ERROR;
+    std::string why;
+    NBodyCudaStatus rc = nb_check_ctx(ctx, why);
+    if (rc) { g_lastError = why; return rc; }
+    if (ctx->criterion == NBCUDA_EXACT) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    NbTreeBuffers& b = st->b;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        NbScalars init{};
+        init.rsize = st->rsize;
+        init.capNodes = st->capNodes;
+        NB_CHECK(cudaMemcpyAsync(b.sc, &init, sizeof init, cudaMemcpyHostToDevice, st->stream));
+        nb_build_tree(b, st->nbody, ctx->criterion, ctx->theta, ctx->useQuad, 0, 0.0, st->numSMs,
+                      st->stream);
+        nb_link_and_moments(b, st->nbody, st->capNodes, ctx->criterion, ctx->theta, ctx->useQuad,
+                            st->stream);
+        NB_CHECK(cudaGetLastError());
+        NB_CHECK(cudaMemcpyAsync(st->scHost, b.sc, sizeof(NbScalars), cudaMemcpyDeviceToHost,
+                                 st->stream));
+        NB_CHECK(cudaStreamSynchronize(st->stream));
+        st->rsize = st->scHost->rsize;
+        if (st->scHost->status & NBODY_CELL_OVERFLOW_ERROR) {
+            rc = nb_alloc_nodes(st, st->scHost->neededNodes + st->scHost->neededNodes / 4 + 64);
+            if (rc) return rc;
+            continue;
+        }
+        st->haveTree = 1;
+        return st->scHost->status;
+    }
+    return NBODY_CELL_OVERFLOW_ERROR;
+}
+
+NBodyCudaStatus nbTreeInfoCUDA(NBodyCudaState* st, NBodyCudaTreeInfo* info)
+{
+    if (!st || !info) return NBODY_USER_ERROR;
+    const NbScalars& h = *st->scHost;
+    info->rsize = st->rsize;
+    info->nbody = st->nbody;
+    info->nTreeBodies = st->haveTree ? h.nTree : 0;
+    info->cellUsed = st->haveTree ? h.nCells : 0;
+    info->maxDepth = st->haveTree ? h.maxDepth : 0;
+    info->nNodes = st->haveTree ? h.nNodes : 0;
+    info->step = st->step;
+    info->treeIncest = st->treeIncest;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbGetTreeCUDA(NBodyCudaState* st, double* pos, double* mass, double* rcrit2,
+                              double* quad, int32_t* next, int32_t* body, int32_t* depth)
+{
+    if (!st || !st->haveTree) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    const int nn = st->scHost->nNodes;
+    NbTreeBuffers& b = st->b;
+    const cudaStream_t s = st->stream;
+    if (pos || mass) {
+        double4* tmp = (double4*) malloc(sizeof(double4) * (size_t) (nn ? nn : 1));
+        NB_CHECK(cudaMemcpyAsync(tmp, b.nodePM, sizeof(double4) * (size_t) nn, cudaMemcpyDeviceToHost, s));
+        NB_CHECK(cudaStreamSynchronize(s));
+        for (int k = 0; k < nn; ++k) {
+            if (pos) { pos[3 * k] = tmp[k].x; pos[3 * k + 1] = tmp[k].y; pos[3 * k + 2] = tmp[k].z; }
+            if (mass) mass[k] = tmp[k].w;
+        }
+        free(tmp);
+    }
+    int2* lk = (int2*) malloc(sizeof(int2) * (size_t) (nn ? nn : 1));
+    NB_CHECK(cudaMemcpyAsync(lk, b.nodeLink, sizeof(int2) * (size_t) nn, cudaMemcpyDeviceToHost, s));
+    if (rcrit2) NB_CHECK(cudaMemcpyAsync(rcrit2, b.nodeCrit, sizeof(double) * (size_t) nn, cudaMemcpyDeviceToHost, s));
+    if (quad) NB_CHECK(cudaMemcpyAsync(quad, b.nodeQuad, 6 * sizeof(double) * (size_t) nn, cudaMemcpyDeviceToHost, s));
+    if (depth) NB_CHECK(cudaMemcpyAsync(depth, b.nodeDepth, sizeof(int) * (size_t) nn, cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaStreamSynchronize(s));
+    for (int k = 0; k < nn; ++k) {
+        if (next) next[k] = lk[k].x;
+        if (body) body[k] = lk[k].y;
+        if (lk[k].y >= 0) {
+            if (rcrit2) rcrit2[k] = 0.0;
+            if (quad) for (int c = 0; c < 6; ++c) quad[6 * (size_t) k + c] = 0.0;
+        }
+    }
+    free(lk);
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbExtAccelerationCUDA(const NBodyCudaPotential* pot, const double* pos,
+                                      double* acc, int n, int device)
+{
+    if (!pot || n < 0 || (n && (!pos || !acc))) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(device));
+    NBodyCudaCtx c{};
+    c.potentialType = NBCUDA_POTENTIAL_DEFAULT;
+    c.pot = *pot;
+    std::string why;
+    NBodyCudaStatus rc = nb_check_ctx(&c, why);
+    if (rc) { g_lastError = why; return rc; }
+    if (!n) return NBODY_SUCCESS;
+    double *dp = nullptr, *da = nullptr;
+    NB_CHECK(cudaMalloc((void**) &dp, 3 * sizeof(double) * (size_t) n));
+    cudaError_t e = cudaMalloc((void**) &da, 3 * sizeof(double) * (size_t) n);
+    if (e != cudaSuccess) { cudaFree(dp); return nb_cuda_fail(e, "cudaMalloc"); }
+    e = cudaMemcpy(dp, pos, 3 * sizeof(double) * (size_t) n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        nb_launch_ext_only(dp, da, n, nb_pot_from(&c), 0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(acc, da, 3 * sizeof(double) * (size_t) n, cudaMemcpyDeviceToHost);
+    cudaFree(dp);
+    cudaFree(da);
+    if (e != cudaSuccess) return nb_cuda_fail(e, "nbExtAccelerationCUDA");
+    return NBODY_SUCCESS;
+}
+
+uint64_t nbKernelLaunchesCUDA(void) { return g_launches.load(); }
+
+NBodyCudaStatus nbLastWalkTimeCUDA(NBodyCudaState* st, double* ms, int* launches)
+{
+    if (!st) return NBODY_USER_ERROR;
+    if (ms) *ms = st->walkMs;
+    if (launches) *launches = st->walkLaunches;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbInteractionCountsCUDA(NBodyCudaState* st, unsigned long long* nBodyBody,
+                                        unsigned long long* nBodyCell, unsigned long long* nVisit)
+{
+    if (!st) return NBODY_USER_ERROR;
+    if (nBodyBody) *nBodyBody = st->cBB;
+    if (nBodyCell) *nBodyCell = st->cBC;
+    if (nVisit) *nVisit = st->cVisit;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbSetCountingCUDA(NBodyCudaState* st, int enable)
+{
+    if (!st) return NBODY_USER_ERROR;
+    st->counting = enable != 0;
+    return NBODY_SUCCESS;
+}
+
+const char* nbLastErrorCUDA(void) { return g_lastError.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,136 @@
+// Shared declarations of the B200 Barnes-Hut step (sm_100a).
+//
+// Device data layout (all in HBM, one NBodyCudaState per simulation):
+//   bodies      SoA FP64 in the caller's order: px py pz vx vy vz ax ay az mass
+//   sort        63-bit Morton keys of the top 21 levels + body index (LSD radix sort),
+//               then 62-bit integer grid coordinates per axis of the sorted bodies
+//   tree        nodes in the reference's walk order (threadTree preorder,
+//               nbody/src/nbody_tree.c:127-150): for node k
+//                 nodePM[k]   = {x, y, z, mass}   (CoM for cells, position for bodies)
+//                 nodeCrit[k] = rcrit2            (cells only)
+//                 nodeLink[k] = {next, body}      (Next() index, body index or -1)
+//                 nodeQuad[k] = 6 quadrupole components (cells only)
+//   scalars     NbScalars below (root size, counts, status bits)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/nbody_b200.h"
+
+#define NB_FULL_MASK 0xffffffffu
+
+// Levels of the integer grid used for the octant decisions: coordinates are
+// floor(pos * 2^62 / rsize) + 2^61, so every cell midpoint of depth < 62 is an
+// integer on this grid and `mid <= pos` (nbody/src/nbody_tree.c:42-49) is an exact
+// integer comparison.
+#define NB_GRID_LEVELS 62
+#define NB_KEY_LEVELS 21          // levels in the 63-bit sort key
+#define NB_MASSLESS_KEY 0xffffffffffffffffull
+
+struct NbScalars {
+    unsigned long long xyzmaxBits;  // max |coordinate| over bodies (bit pattern, >= 0)
+    double rsize;                   // root side length (t->rsize), kept between steps
+    double gridScale;               // 2^62 / rsize
+    int depthEps;                   // first depth whose cell size is <= DBL_EPSILON
+    int nTree;                      // bodies with nonzero mass
+    int nCells;
+    int nNodes;
+    int maxDepth;                   // deepest parent level of a body (t->maxDepth)
+    int status;                     // NBodyStatus bits raised on the device
+    int incest;                     // a body did not meet itself in the walk
+    int capNodes;                   // node capacity of the allocation
+    int neededNodes;                // nodes the last build asked for (overflow recovery)
+    unsigned long long nBodyBody;   // interaction counters (counting build of the walk)
+    unsigned long long nBodyCell;
+    unsigned long long nVisit;
+};
+
+// Potential parameters in constant-friendly POD form.
+struct NbPot {
+    int sphType; double sphMass, sphScale;
+    int diskType; double diskMass, diskA, diskB;
+    int disk2Type; double disk2Mass, disk2A, disk2B;
+    int haloType; double haloV, haloA, haloQz;
+    int enabled;   // potentialType == DEFAULT
+};
+
+struct NbWalkParams {
+    double eps2;
+    double dtHalf;
+    int useQuad;
+    int kick;      // 1: v += (a + 0) * dtHalf after the force (advanceVelocities)
+    int n;
+};
+
+// ---- correctly rounded powers ------------------------------------------------------
+// The reference evaluates the disk/bulge terms with crlibm's correctly rounded pow_rn
+// (milkyway/include/milkyway_math_double.h:43-59).  x^2 and x^0.5 are correctly rounded
+// by one IEEE multiply / sqrt.  x^1.5 and x^3 are formed here as a double-double value
+// (error-free products via fma) and rounded once: the double-double carries ~104 bits,
+// so its rounding equals the correctly rounded result except for arguments whose exact
+// power lies within 2^-100 relative of a rounding boundary.
+__device__ __forceinline__ double nb_pow_1p5(double x)
+{
+    if (!(x > 0.0) || isinf(x)) {
+        if (x == 0.0) return 0.0;
+        return isinf(x) && x > 0.0 ? x : __longlong_as_double(0x7ff8000000000000ll);
+    }
+    double s = __dsqrt_rn(x);
+    double r = __fma_rn(-s, s, x);                 // x - s^2, exact
+    double t = __ddiv_rn(r, __dmul_rn(2.0, s));    // sqrt(x) = s + t (+ O(t^2/s))
+    double hi = __dmul_rn(x, s);
+    double lo = __fma_rn(x, s, -hi);               // x*s - hi, exact
+    lo = __dadd_rn(lo, __dmul_rn(x, t));
+    return __dadd_rn(hi, lo);
+}
+
+__device__ __forceinline__ double nb_pow_3(double x)
+{
+    double sq = __dmul_rn(x, x);
+    double e1 = __fma_rn(x, x, -sq);               // x^2 - sq, exact
+    double hi = __dmul_rn(sq, x);
+    double lo = __fma_rn(sq, x, -hi);              // sq*x - hi, exact
+    lo = __dadd_rn(lo, __dmul_rn(e1, x));
+    if (isinf(hi) || hi == 0.0) return hi;
+    return __dadd_rn(hi, lo);
+}
+
+// Device error checks produce NBodyStatus bits; kernels stop doing work once a fatal
+// bit is set so the state is left as it was at the failure point.
+__device__ __forceinline__ void nb_raise(NbScalars* sc, int bits) { atomicOr(&sc->status, bits); }
+__device__ __forceinline__ bool nb_failed(const NbScalars* sc)
+{
+    return (*(volatile const int*) &sc->status & ~(int) NBODY_STATUS_WARNINGS_MASK) != 0;
+}
+
+// Launch accounting (all launches of this library go through nb_count_launch).
+void nb_count_launch(int n = 1);
+
+// ---- kernels-facing host entry points (implemented in the .cu files) ----
+struct NbSortBuffers {
+    unsigned long long* keyA; unsigned long long* keyB;
+    unsigned int* idxA; unsigned int* idxB;
+    unsigned int* hist;    // 256 * nTiles
+    int capTiles;
+};
+// Sorts (keyA, idxA) by key in place (result in keyA/idxA); n items.
+void nb_radix_sort(NbSortBuffers& b, int n, cudaStream_t s);
+// Device buffers of one simulation.
+struct NbTreeBuffers {
+    double *px, *py, *pz, *vx, *vy, *vz, *ax, *ay, *az, *mass;
+    NbSortBuffers sort;
+    long long *gx, *gy, *gz;
+    int *delta, *cum, *scanTmp, *bodyNode;
+    double4* nodePM; double* nodeCrit; int2* nodeLink; double* nodeQuad;
+    int *nodeDepth, *parent, *nchild, *arrive;
+    NbScalars* sc;
+};
+
+void nb_build_tree(NbTreeBuffers& b, int n, int criterion, double theta, int useQuad, int drift,
+                   double dt, int numSMs, cudaStream_t s);
+void nb_link_and_moments(NbTreeBuffers& b, int n, int capNodes, int criterion, double theta,
+                         int useQuad, cudaStream_t s);
+void nb_launch_drift_only(NbTreeBuffers& b, int n, double dt, int numSMs, cudaStream_t s);
+
+// Inclusive prefix sum of n ints in place; tmp needs nb_scan_tmp_ints(n) ints.
+int nb_scan_tmp_ints(int n);
+void nb_inclusive_scan(int* data, int n, int* tmp, cudaStream_t s);

@@ -1,0 +1,97 @@
+// External Milky Way potential and the per-body force epilogue, shared by the walk kernels.
+// Included only by translation units compiled with -fmad=false, so the expressions keep the
+// reference's rounding.
+#pragma once
+#include "nb_common.cuh"
+
+// nbExtAcceleration (nbody/src/nbody_potential.c:627-762) for the supported components:
+// Miyamoto-Nagai disks (:173-194), logarithmic (:488-504) and NFW (:506-515) halos,
+// Hernquist (:157-162) and Plummer (:164-169) bulges.
+__device__ __forceinline__ void nb_ext_accel(const NbPot& p, double x, double y, double z,
+                                             double& ox, double& oy, double& oz)
+{
+    const double absv = sqrt(z * z + (y * y + x * x));
+    const double limit = 0.00390625;          // mw_pow(2.0, -8.0)
+    const double r = (double) (absv <= limit) * limit + (double) (absv > limit) * absv;
+    double axx = 0.0, ayy = 0.0, azz = 0.0;
+    if (p.diskType == NBCUDA_MIYAMOTO_NAGAI_DISK) {
+        const double zp = sqrt(z * z + p.diskB * p.diskB);
+        const double azp = p.diskA + zp;
+        const double rp = x * x + y * y + azp * azp;
+        const double rth = nb_pow_1p5(rp);
+        axx = -p.diskMass * x / rth;
+        ayy = -p.diskMass * y / rth;
+        azz = -p.diskMass * z * azp / (zp * rth);
+    }
+    {
+        double tx = 0.0, ty = 0.0, tz = 0.0;
+        if (p.disk2Type == NBCUDA_MIYAMOTO_NAGAI_DISK) {
+            const double zp = sqrt(z * z + p.disk2B * p.disk2B);
+            const double azp = p.disk2A + zp;
+            const double rp = x * x + y * y + azp * azp;
+            const double rth = nb_pow_1p5(rp);
+            tx = -p.disk2Mass * x / rth;
+            ty = -p.disk2Mass * y / rth;
+            tz = -p.disk2Mass * z * azp / (zp * rth);
+        }
+        axx = axx + tx; ayy = ayy + ty; azz = azz + tz;
+    }
+    {
+        double tx = 0.0, ty = 0.0, tz = 0.0;
+        if (p.haloType == NBCUDA_LOGARITHMIC_HALO) {
+            const double q = p.haloQz, d = p.haloA, v0 = p.haloV;
+            const double zq = z / q;
+            const double denom = d * d + x * x + y * y + zq * zq;
+            const double k = -2.0 * v0 * v0 / denom;
+            tx = k * x; ty = k * y; tz = k * z / (q * q);
+        } else if (p.haloType == NBCUDA_NFW_HALO) {
+            const double a = p.haloA;
+            const double M = p.haloV * p.haloV * a / 0.2162165954;
+            const double ar = a + r;
+            const double c = (-M / (r * r)) * (log(ar / a) / r - 1 / ar);
+            tx = c * x; ty = c * y; tz = c * z;
+        }
+        axx = axx + tx; ayy = ayy + ty; azz = azz + tz;
+    }
+    {
+        double tx = 0.0, ty = 0.0, tz = 0.0;
+        if (p.sphType == NBCUDA_HERNQUIST_SPHERICAL) {
+            const double tmp = p.sphScale + r;
+            const double c = -p.sphMass / (r * (tmp * tmp));
+            tx = c * x; ty = c * y; tz = c * z;
+        } else if (p.sphType == NBCUDA_PLUMMER_SPHERICAL) {
+            const double tmp = sqrt(p.sphScale * p.sphScale + r * r);
+            const double c = -p.sphMass / nb_pow_3(tmp);
+            tx = c * x; ty = c * y; tz = c * z;
+        }
+        axx = axx + tx; ayy = ayy + ty; azz = azz + tz;
+    }
+    ox = axx; oy = ayy; oz = azz;
+}
+
+// nbMapForceBody's epilogue (nbody/src/nbody_grav.c:167-176): a += nbExtAcceleration(pos)
+// + plummerAccel(pos, LMC at the origin, mass 0, scale 1), whose value is (0 - pos) * 0.
+__device__ __forceinline__ void nb_finish_body(const NbPot& pot, const NbWalkParams& wp, unsigned j,
+                                               double x0, double y0, double z0, double accx,
+                                               double accy, double accz, double* __restrict__ ax,
+                                               double* __restrict__ ay, double* __restrict__ az,
+                                               double* __restrict__ vx, double* __restrict__ vy,
+                                               double* __restrict__ vz)
+{
+    if (pot.enabled) {
+        double ex, ey, ez;
+        nb_ext_accel(pot, x0, y0, z0, ex, ey, ez);
+        ex = ex + (0.0 - x0) * 0.0;
+        ey = ey + (0.0 - y0) * 0.0;
+        ez = ez + (0.0 - z0) * 0.0;
+        accx = accx + ex; accy = accy + ey; accz = accz + ez;
+    }
+    ax[j] = accx; ay[j] = accy; az[j] = accz;
+    if (wp.kick) {
+        // advanceVelocities (nbody/src/nbody_plain.c:301-315): v += (a + acc_i1) * dtHalf
+        vx[j] = vx[j] + wp.dtHalf * (accx + 0.0);
+        vy[j] = vy[j] + wp.dtHalf * (accy + 0.0);
+        vz[j] = vz[j] + wp.dtHalf * (accz + 0.0);
+    }
+}
+

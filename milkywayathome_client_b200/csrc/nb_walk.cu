@@ -1,0 +1,183 @@
+// Force evaluation: FP64 Barnes-Hut walk, FP64 direct summation and the external Milky Way
+// potential.  Compiled with -fmad=false so every expression keeps the reference's rounding
+// (the reference CPU build uses SSE2 without FMA, milkyway/include/milkyway_math_double.h:128).
+//
+// Walk (nbGravity, nbody/src/nbody_grav.c:42-124).  One warp walks for 32 bodies that are
+// consecutive in octree-path order.  Every lane keeps its own position in the reference's
+// stackless walk: at node q it accepts (interacts, then jumps to Next(q)) if q is a body or
+// |dr|^2 >= rcrit2(q), otherwise it opens q (goes to More(q) = q + 1 in walk order).  The warp
+// visits the smallest pending node of its lanes, so each lane sees exactly the nodes of its
+// own CPU walk, in the CPU's order, and accumulates the same terms in the same order; the
+// node records are read once per warp visit (uniform address).  FP64-pipe bound: a monopole
+// interaction is 18 flops + sqrt + 2 divisions, a quadrupole cell adds 38 flops + 2 divisions.
+#include "nb_common.cuh"
+#include "nb_potential.cuh"
+
+constexpr int WALK_THREADS = 256;
+
+template <bool COUNT>
+__global__ void __launch_bounds__(WALK_THREADS)
+k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeCrit,
+            const int2* __restrict__ nodeLink, const double* __restrict__ nodeQuad,
+            const unsigned int* __restrict__ order, const double* __restrict__ px,
+            const double* __restrict__ py, const double* __restrict__ pz,
+            double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
+            double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
+            NbWalkParams wp, NbPot pot, NbScalars* __restrict__ sc)
+{
+    if (nb_failed(sc)) return;
+    const int end = sc->nNodes;
+    const int lane = threadIdx.x & 31;
+    const int i = (int) ((blockIdx.x * (unsigned) blockDim.x + threadIdx.x) >> 5) * 32 + lane;
+    const bool valid = i < wp.n;
+    const unsigned j = valid ? order[i] : 0u;
+    const double x0 = valid ? px[j] : 0.0, y0 = valid ? py[j] : 0.0, z0 = valid ? pz[j] : 0.0;
+    const double eps2 = wp.eps2;
+    const bool useQuad = wp.useQuad != 0;
+    int ptr = valid ? 0 : end;
+    double accx = 0.0, accy = 0.0, accz = 0.0;
+    bool metSelf = false;
+    unsigned long long cVisit = 0, cBB = 0, cBC = 0;
+    for (;;) {
+        const int q = __reduce_min_sync(NB_FULL_MASK, ptr);
+        if (q >= end) break;
+        if (ptr != q) continue;
+        const double4 nd = nodePM[q];
+        const int2 link = nodeLink[q];
+        const double dx = nd.x - x0, dy = nd.y - y0, dz = nd.z - z0;
+        double drSq = dz * dz + (dy * dy + dx * dx);
+        const bool isBody = link.y >= 0;
+        if (COUNT) ++cVisit;
+        if (isBody || drSq >= nodeCrit[q]) {
+            ptr = link.x;
+            if (isBody && (unsigned) link.y == j) { metSelf = true; continue; }
+            if (COUNT) { if (isBody) ++cBB; else ++cBC; }
+            drSq = drSq + eps2;
+            const double drab = sqrt(drSq);
+            const double phii = nd.w / drab;
+            const double mor3 = phii / drSq;
+            accx = accx + mor3 * dx;
+            accy = accy + mor3 * dy;
+            accz = accz + mor3 * dz;
+            if (useQuad && !isBody) {
+                const double2* Q2 = reinterpret_cast<const double2*>(nodeQuad + 6 * (size_t) q);
+                const double2 q01 = Q2[0], q23 = Q2[1], q45 = Q2[2];
+                const double qxx = q01.x, qxy = q01.y, qxz = q23.x, qyy = q23.y, qyz = q45.x, qzz = q45.y;
+                const double qdx = qxx * dx + qxy * dy + qxz * dz;
+                const double qdy = qxy * dx + qyy * dy + qyz * dz;
+                const double qdz = qxz * dx + qyz * dy + qzz * dz;
+                const double drQdr = qdx * dx + qdy * dy + qdz * dz;
+                const double dr5inv = 1.0 / ((drSq * drSq) * drab);
+                const double phiQ = 2.5 * (dr5inv * drQdr) / drSq;
+                accx = accx + phiQ * dx;
+                accy = accy + phiQ * dy;
+                accz = accz + phiQ * dz;
+                accx = accx - dr5inv * qdx;
+                accy = accy - dr5inv * qdy;
+                accz = accz - dr5inv * qdz;
+            }
+        } else {
+            ptr = q + 1;
+        }
+    }
+    if (COUNT) {
+        for (int o = 16; o > 0; o >>= 1) {
+            cVisit += __shfl_xor_sync(NB_FULL_MASK, cVisit, o);
+            cBB += __shfl_xor_sync(NB_FULL_MASK, cBB, o);
+            cBC += __shfl_xor_sync(NB_FULL_MASK, cBC, o);
+        }
+        if (lane == 0) {
+            atomicAdd(&sc->nVisit, cVisit);
+            atomicAdd(&sc->nBodyBody, cBB);
+            atomicAdd(&sc->nBodyCell, cBC);
+        }
+    }
+    if (!valid) return;
+    // a body that never meets itself is tree incest (nbody/src/nbody_grav.c:111-118)
+    if (!metSelf) atomicOr(&sc->incest, 1);
+    nb_finish_body(pot, wp, j, x0, y0, z0, accx, accy, accz, ax, ay, az, vx, vy, vz);
+}
+
+// nbGravity_Exact (nbody/src/nbody_grav.c:205-227): direct sum over all bodies in input
+// order (the self term contributes 0 * dr).  One thread per body; sources staged in tiles.
+constexpr int EXACT_TILE = 256;
+__global__ void __launch_bounds__(EXACT_TILE)
+k_direct_fp64(const double* __restrict__ px, const double* __restrict__ py,
+              const double* __restrict__ pz, const double* __restrict__ mass,
+              double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
+              double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
+              NbWalkParams wp, NbPot pot, NbScalars* __restrict__ sc)
+{
+    __shared__ double4 tile[EXACT_TILE];
+    const int n = wp.n;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const double x0 = valid ? px[i] : 0.0, y0 = valid ? py[i] : 0.0, z0 = valid ? pz[i] : 0.0;
+    const double eps2 = wp.eps2;
+    double accx = 0.0, accy = 0.0, accz = 0.0;
+    for (int base = 0; base < n; base += EXACT_TILE) {
+        const int k = base + threadIdx.x;
+        __syncthreads();
+        tile[threadIdx.x] = k < n ? make_double4(px[k], py[k], pz[k], mass[k]) : make_double4(0, 0, 0, 0);
+        __syncthreads();
+        const int lim = min(EXACT_TILE, n - base);
+        for (int t = 0; t < lim; ++t) {
+            const double4 b = tile[t];
+            const double dx = b.x - x0, dy = b.y - y0, dz = b.z - z0;
+            const double drSq = (dz * dz + (dy * dy + dx * dx)) + eps2;
+            const double drab = sqrt(drSq);
+            const double phii = b.w / drab;
+            const double mor3 = phii / drSq;
+            accx = accx + mor3 * dx;
+            accy = accy + mor3 * dy;
+            accz = accz + mor3 * dz;
+        }
+    }
+    if (valid) nb_finish_body(pot, wp, (unsigned) i, x0, y0, z0, accx, accy, accz, ax, ay, az, vx, vy, vz);
+}
+
+__global__ void k_ext_only(const double* __restrict__ pos, double* __restrict__ acc, int n, NbPot pot)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double ex, ey, ez;
+        nb_ext_accel(pot, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], ex, ey, ez);
+        acc[3 * i] = ex; acc[3 * i + 1] = ey; acc[3 * i + 2] = ez;
+    }
+}
+
+// ---- host launchers ----
+void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
+                         const double* nodeQuad, const unsigned* order, const double* px,
+                         const double* py, const double* pz, double* ax, double* ay, double* az,
+                         double* vx, double* vy, double* vz, const NbWalkParams& wp,
+                         const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s)
+{
+    const int warps = (wp.n + 31) / 32;
+    const int blocks = (warps * 32 + WALK_THREADS - 1) / WALK_THREADS;
+    if (blocks <= 0) return;
+    if (count)
+        k_walk_fp64<true><<<blocks, WALK_THREADS, 0, s>>>(nodePM, nodeCrit, nodeLink, nodeQuad, order,
+                                                          px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc);
+    else
+        k_walk_fp64<false><<<blocks, WALK_THREADS, 0, s>>>(nodePM, nodeCrit, nodeLink, nodeQuad, order,
+                                                           px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc);
+    nb_count_launch();
+}
+
+void nb_launch_direct_fp64(const double* px, const double* py, const double* pz,
+                           const double* mass, double* ax, double* ay, double* az, double* vx,
+                           double* vy, double* vz, const NbWalkParams& wp, const NbPot& pot,
+                           NbScalars* sc, cudaStream_t s)
+{
+    const int blocks = (wp.n + EXACT_TILE - 1) / EXACT_TILE;
+    if (blocks <= 0) return;
+    k_direct_fp64<<<blocks, EXACT_TILE, 0, s>>>(px, py, pz, mass, ax, ay, az, vx, vy, vz, wp, pot, sc);
+    nb_count_launch();
+}
+
+void nb_launch_ext_only(const double* dpos, double* dacc, int n, const NbPot& pot, cudaStream_t s)
+{
+    if (n <= 0) return;
+    k_ext_only<<<(n + 255) / 256, 256, 0, s>>>(dpos, dacc, n, pot);
+    nb_count_launch();
+}

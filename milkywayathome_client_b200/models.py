@@ -1,0 +1,143 @@
+"""Set-up helpers: the reference's timestep/softening formulas and a seeded synthetic
+two-component Plummer dwarf with the shapes and sizes of the reference's dwarf models.
+
+These run once per simulation on the host (they are the reference's Lua set-up, not the
+step).  The dwarf sampler is synthetic: positions follow each component's Plummer profile
+exactly; speeds are drawn from the isotropic Plummer distribution function
+f(E) ~ (-E)^{7/2} evaluated in the combined potential of both components, which keeps the
+dwarf close to equilibrium.  It is not the reference's Eddington-inversion sampler
+(nbGenerateMixedDwarfCore, nbody/src/nbody_mixeddwarf.c:765-1026) and does not reproduce
+its random stream; parity with the reference is established on identical input arrays.
+"""
+import math
+
+import numpy as np
+
+PI_4_3 = 4.0 * math.pi / 3.0
+SUN_GC_DIST = 8.0   # ctx.sunGCDist default (nbody/include/nbody_defaults.h)
+
+
+def calculate_timestep(mass, r0):
+    """calculateTimestep (nbody/src/nbody_lua_models.c:139-142)."""
+    return (1.0 / 10.0) ** 2 * math.sqrt((PI_4_3 * r0 ** 3) / mass)
+
+
+def two_component_timestep(mass_l, rscale_l, mass_d, rscale_d):
+    """get_timestep of the two-component sample workunit
+    (nbody/sample_workunits/for_developers.lua:165-199)."""
+    mass_enc_d = mass_d * rscale_l ** 3 * (rscale_l ** 2 + rscale_d ** 2) ** (-1.5)
+    mass_enc_l = mass_l * rscale_d ** 3 * (rscale_l ** 2 + rscale_d ** 2) ** (-1.5)
+    s1 = rscale_l ** 3 / (mass_enc_d + mass_l)
+    s2 = rscale_d ** 3 / (mass_enc_l + mass_d)
+    return (1.0 / 100.0) * math.sqrt(PI_4_3 * min(s1, s2))
+
+
+def calculate_virial(a_b, a_d, M_b, M_d, n=100000):
+    """nbCalculateVirial (nbody/src/nbody_virial.c:38-103): 5-point Gauss-Legendre on n
+    panels out to 1000 scale radii."""
+    w = np.array([0.2369268850561891, 0.4786286704993665, 0.5688888888888889,
+                  0.4786286704993665, 0.2369268850561891])
+    x = np.array([-0.9061798459386640, -0.5384693101056831, 0.0, 0.5384693101056831,
+                  0.9061798459386640])
+    upper = 1000.0 * max(a_b, a_d)
+    width = upper / n
+    a1 = np.arange(n) * width
+    r = (width * x[None, :] / 2.0 + (a1[:, None] + a1[:, None] + width) / 2.0)
+    dens = 3.0 / 4.0 / math.pi * (M_b / a_b ** 3 * (1.0 + r * r / a_b / a_b) ** -2.5 +
+                                  M_d / a_d ** 3 * (1.0 + r * r / a_d / a_d) ** -2.5)
+    integ = 1.0 / 4.0 / math.pi * (M_b / a_b * r * r * (1.0 + r * r / a_b / a_b) ** -0.5 +
+                                   M_d / a_d * r * r * (1.0 + r * r / a_d / a_d) ** -0.5)
+    integral = float(np.sum(w[None, :] * dens * integ * width / 2.0))
+    M_tot = M_b + M_d
+    return M_tot * M_tot / 16.0 / math.pi / math.pi / integral
+
+
+def calculate_eps2(nbody, a_b, a_d, M_b, M_d):
+    """calculateEps2 (nbody/src/nbody_lua_models.c:158-169)."""
+    eps = calculate_virial(a_b, a_d, M_b, M_d) * 0.98 * nbody ** -0.26
+    return max(eps * eps, np.finfo(np.float64).eps)
+
+
+def lbr_to_cartesian(l_deg, b_deg, r, sun_gc_dist=SUN_GC_DIST):
+    """lbrToCartesian with the Sun at (-sunGCDist, 0, 0)."""
+    l, b = math.radians(l_deg), math.radians(b_deg)
+    return np.array([r * math.cos(b) * math.cos(l) - sun_gc_dist,
+                     r * math.cos(b) * math.sin(l), r * math.sin(b)])
+
+
+def _plummer_radii(rng, n, a, rmax_factor=50.0):
+    umax = (1.0 + 1.0 / rmax_factor ** 2) ** -1.5     # mass fraction inside rmax
+    u = rng.uniform(1e-12, umax, n)
+    return a / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+
+
+def _unit_vectors(rng, n):
+    z = rng.uniform(-1.0, 1.0, n)
+    phi = rng.uniform(0.0, 2.0 * math.pi, n)
+    s = np.sqrt(1.0 - z * z)
+    return np.stack([s * np.cos(phi), s * np.sin(phi), z], axis=1)
+
+
+def _df_speed_fraction(rng, n):
+    """q = v / v_esc with density q^2 (1 - q^2)^{7/2} (rejection, Aarseth et al. 1974)."""
+    out = np.empty(n)
+    filled = 0
+    while filled < n:
+        k = max(2 * (n - filled), 1024)
+        q = rng.uniform(0.0, 1.0, k)
+        y = rng.uniform(0.0, 0.1, k)
+        q = q[y < q * q * (1.0 - q * q) ** 3.5]
+        take = min(len(q), n - filled)
+        out[filled:filled + take] = q[:take]
+        filled += take
+    return out
+
+
+def plummer_plummer_dwarf(nbody, seed=0, mass_l=12.0, rscale_l=0.2, light_r_ratio=0.2,
+                          light_mass_ratio=0.2, n_baryon=None, position=None, velocity=None):
+    """Seeded two-component Plummer+Plummer dwarf (baryons first, then dark matter).
+
+    Parameters follow the sample workunit (for_developers.lua:460-478): the dark component
+    has radius rscale_l/light_r_ratio*(1-light_r_ratio) and mass
+    mass_l/light_mass_ratio*(1-light_mass_ratio).  Returns pos (n,3), vel (n,3), mass (n,),
+    type (n,) with +1 for baryons and -1 for dark matter (the reference's ignore flag)."""
+    rng = np.random.default_rng(seed)
+    if n_baryon is None:
+        n_baryon = nbody // 2
+    n_dark = nbody - n_baryon
+    dwarf_mass = mass_l / light_mass_ratio
+    rscale_t = rscale_l / light_r_ratio
+    rscale_d = rscale_t * (1.0 - light_r_ratio)
+    mass_d = dwarf_mass * (1.0 - light_mass_ratio)
+    r = np.concatenate([_plummer_radii(rng, n_baryon, rscale_l), _plummer_radii(rng, n_dark, rscale_d)])
+    pos = r[:, None] * _unit_vectors(rng, nbody)
+    phi = -(mass_l / np.sqrt(r * r + rscale_l ** 2)) - (mass_d / np.sqrt(r * r + rscale_d ** 2))
+    v = _df_speed_fraction(rng, nbody) * np.sqrt(-2.0 * phi)
+    vel = v[:, None] * _unit_vectors(rng, nbody)
+    mass = np.concatenate([np.full(n_baryon, mass_l / max(n_baryon, 1)),
+                           np.full(n_dark, mass_d / max(n_dark, 1))])
+    typ = np.concatenate([np.ones(n_baryon, np.int32), -np.ones(n_dark, np.int32)])
+    # centre the sample, then place it on the orbit
+    cm = (mass[:, None] * pos).sum(0) / mass.sum()
+    cv = (mass[:, None] * vel).sum(0) / mass.sum()
+    pos -= cm
+    vel -= cv
+    if position is None:
+        position = lbr_to_cartesian(218.0, 53.5, 28.6)
+    if velocity is None:
+        velocity = np.array([-156.0, 79.0, 107.0])
+    pos += np.asarray(position, dtype=np.float64)
+    vel += np.asarray(velocity, dtype=np.float64)
+    return pos, vel, mass, typ
+
+
+def dwarf_config(nbody, theta=1.0, criterion="TreeCode", useQuad=True, mass_l=12.0,
+                 rscale_l=0.2, light_r_ratio=0.2, light_mass_ratio=0.2):
+    """Context settings of the two-component sample workunit at nbody bodies: dt from the
+    two-component formula, eps2 from calculateEps2."""
+    rscale_d = rscale_l / light_r_ratio * (1.0 - light_r_ratio)
+    mass_d = mass_l / light_mass_ratio * (1.0 - light_mass_ratio)
+    dt = two_component_timestep(mass_l, rscale_l, mass_d, rscale_d)
+    eps2 = calculate_eps2(nbody, rscale_l, rscale_d, mass_l, mass_d)
+    return dict(timestep=dt, eps2=eps2, theta=theta, criterion=criterion, useQuad=useQuad,
+                treeRSize=4.0)

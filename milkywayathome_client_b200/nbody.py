@@ -1,0 +1,291 @@
+"""Host-side mirror of the reference's N-body step interface, running on the B200 library.
+
+Names, argument meaning and error behaviour follow the reference's own plugin seam for the
+step -- the Lua types and methods the reference's tests drive (NBodyCtx.create,
+Potential.create with Spherical/Disk/Halo, NBodyState.create, state:step;
+nbody/src/nbody_lua_types/*.c) and the C entry points behind them (nbGravMap,
+nbStepSystem, nbRunSystem; nbody/src/nbody_grav.c:305, nbody/src/nbody.c:182-212).
+Statuses are the reference's NBodyStatus bit masks.  All arithmetic happens in the CUDA
+library (libnbody_b200.so); this module only marshals numpy arrays through the C ABI.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import (CRITERIA, PRECISION_FP64, PRECISION_MIXED, POTENTIAL_DEFAULT, POTENTIAL_NONE,
+                   status_is_fatal, status_names)
+
+
+class NBodyError(RuntimeError):
+    """A fatal NBodyStatus returned by the library."""
+
+    def __init__(self, what, status):
+        detail = _lib.last_error() if status & _lib.NBODY_CUDA_ERROR else ""
+        super().__init__("%s failed: %s%s" % (what, "|".join(status_names(status)),
+                                              (" (" + detail + ")") if detail else ""))
+        self.status = status
+
+
+# ---- potential components (nbody/src/nbody_lua_types/nbody_lua_{spherical,disk,halo}.c) ----
+class Spherical:
+    @staticmethod
+    def hernquist(mass, scale):
+        return _lib.Spherical(_lib.HERNQUIST_SPHERICAL, mass, scale)
+
+    @staticmethod
+    def plummer(mass, scale):
+        return _lib.Spherical(_lib.PLUMMER_SPHERICAL, mass, scale)
+
+    @staticmethod
+    def none(mass=0.0):
+        return _lib.Spherical(_lib.NO_SPHERICAL, mass, 0.0)
+
+
+class Disk:
+    @staticmethod
+    def miyamotoNagai(mass, scaleLength, scaleHeight):
+        return _lib.Disk(_lib.MIYAMOTO_NAGAI_DISK, mass, scaleLength, scaleHeight, 0.0, 0.0)
+
+    @staticmethod
+    def none(mass=0.0):
+        return _lib.Disk(_lib.NO_DISK, mass, 0.0, 0.0, 0.0, 0.0)
+
+
+class Halo:
+    @staticmethod
+    def logarithmic(vhalo, scaleLength, flattenZ):
+        h = _lib.Halo()
+        h.type, h.vhalo, h.scaleLength, h.flattenZ = _lib.LOGARITHMIC_HALO, vhalo, scaleLength, flattenZ
+        return h
+
+    @staticmethod
+    def nfw(vhalo, scaleLength):
+        h = _lib.Halo()
+        h.type, h.vhalo, h.scaleLength = _lib.NFW_HALO, vhalo, scaleLength
+        return h
+
+    @staticmethod
+    def none(mass=0.0):
+        h = _lib.Halo()
+        h.type, h.mass = _lib.NO_HALO, mass
+        return h
+
+
+class Potential:
+    """Potential.create{spherical, disk, disk2, halo} (nbody_lua_potential.c)."""
+
+    @staticmethod
+    def create(spherical=None, disk=None, disk2=None, halo=None):
+        p = _lib.Potential()
+        p.sphere = spherical if spherical is not None else Spherical.none()
+        p.disk = disk if disk is not None else Disk.none()
+        p.disk2 = disk2 if disk2 is not None else Disk.none()
+        p.halo = halo if halo is not None else Halo.none()
+        return p
+
+
+def milky_way_potential(vhalo=73.0):
+    """The Miyamoto-Nagai + Hernquist + logarithmic-halo potential of the sample workunits
+    (nbody/sample_workunits/for_developers.lua:150-162)."""
+    return Potential.create(
+        spherical=Spherical.hernquist(mass=1.52954402e5, scale=0.7),
+        disk=Disk.miyamotoNagai(mass=4.45865888e5, scaleLength=6.5, scaleHeight=0.26),
+        disk2=Disk.none(mass=3.0e5),
+        halo=Halo.logarithmic(vhalo=vhalo, scaleLength=12.0, flattenZ=1.0))
+
+
+class NBodyCtx:
+    """NBodyCtx.create{...} (nbody/src/nbody_lua_types/nbody_lua_nbodyctx.c:84-221): the
+    settings of a run.  nStep = ceil(timeEvolve / timestep) and the timestep is corrected to
+    timeEvolve / nStep as the reference does (nbCorrectTimestep, nbody/src/nbody_util.c:26-30)."""
+
+    def __init__(self, timestep, eps2, theta=0.0, criterion="TreeCode", useQuad=True,
+                 timeEvolve=None, treeRSize=4.0, allowIncest=False, potential=None,
+                 precision="fp64"):
+        crit = CRITERIA[criterion.lower()] if isinstance(criterion, str) else int(criterion)
+        self.nStep = 0
+        if timeEvolve is not None and timeEvolve > 0.0:
+            self.nStep = int(math.ceil(timeEvolve / timestep))
+            timestep = timeEvolve / self.nStep
+        self.timeEvolve = timeEvolve
+        c = _lib.Ctx()
+        c.eps2, c.theta, c.timestep, c.treeRSize = eps2, theta, timestep, treeRSize
+        c.criterion, c.useQuad, c.allowIncest = crit, int(bool(useQuad)), int(bool(allowIncest))
+        if potential is None:
+            c.potentialType = POTENTIAL_NONE
+        else:
+            c.potentialType = POTENTIAL_DEFAULT
+            c.pot = potential
+        c.precision = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}[precision]
+        self._c = c
+
+    @classmethod
+    def from_struct(cls, c, nStep=0):
+        self = cls.__new__(cls)
+        self._c = _lib.Ctx()
+        ctypes.pointer(self._c)[0] = c
+        self.nStep = nStep
+        self.timeEvolve = c.timestep * nStep if nStep else None
+        return self
+
+    def with_precision(self, precision):
+        other = NBodyCtx.from_struct(self._c, self.nStep)
+        other._c.precision = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}[precision]
+        return other
+
+    def __getattr__(self, name):
+        c = self.__dict__.get("_c")
+        if c is not None and name in dict(_lib.Ctx._fields_):
+            return getattr(c, name)
+        raise AttributeError(name)
+
+    @property
+    def struct(self):
+        return self._c
+
+
+class NBodyState:
+    """Device-resident N-body state: NBodyState.create(ctx, bodies) and state:step(ctx)
+    (nbody/src/nbody_lua_types/nbody_lua_nbodystate.c:60-147) over the CUDA library.
+
+    Bodies are given as arrays: pos (n,3), vel (n,3), mass (n,), float64.  Like the reference
+    binding, create() evaluates the initial accelerations (nbGravMap) so that step() is a full
+    kick-drift-kick."""
+
+    def __init__(self, nbody, device=0):
+        self.lib = _lib.load()
+        self.nbody = int(nbody)
+        self.device = device
+        h = ctypes.c_void_p()
+        rc = self.lib.nbInitCUDA(ctypes.byref(h), device, self.nbody)
+        if rc:
+            raise NBodyError("nbInitCUDA", rc)
+        self._h = h
+
+    @classmethod
+    def create(cls, ctx, pos, vel, mass, device=0, gravmap=True):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        vel = np.ascontiguousarray(vel, dtype=np.float64).reshape(-1, 3)
+        mass = np.ascontiguousarray(mass, dtype=np.float64).reshape(-1)
+        st = cls(len(mass), device)
+        st.set_bodies(pos, vel, mass, ctx.treeRSize)
+        if gravmap:
+            st.check("nbGravMap", st.gravMap(ctx))
+        return st
+
+    # -- lifecycle --
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.nbDestroyCUDA(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @staticmethod
+    def check(what, rc):
+        if status_is_fatal(rc):
+            raise NBodyError(what, rc)
+        return rc
+
+    # -- marshalling (nbMarshalBodies) --
+    def set_bodies(self, pos, vel, mass, treeRSize=4.0):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        vel = np.ascontiguousarray(vel, dtype=np.float64)
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        rc = self.lib.nbSetBodiesCUDA(self._h, _lib.ptr(pos), _lib.ptr(vel), _lib.ptr(mass),
+                                      self.nbody, float(treeRSize))
+        self.check("nbSetBodiesCUDA", rc)
+
+    def marshal_bodies(self, bodytab, to_device, treeRSize=4.0):
+        """bodytab: a writable buffer of n reference Body records (96 bytes each)."""
+        buf = (ctypes.c_char * (96 * self.nbody)).from_buffer(bodytab)
+        rc = self.lib.nbMarshalBodiesCUDA(self._h, ctypes.addressof(buf), self.nbody,
+                                          int(bool(to_device)), float(treeRSize))
+        self.check("nbMarshalBodiesCUDA", rc)
+
+    def bodies(self):
+        pos = np.empty((self.nbody, 3))
+        vel = np.empty((self.nbody, 3))
+        self.check("nbGetBodiesCUDA", self.lib.nbGetBodiesCUDA(self._h, _lib.ptr(pos), _lib.ptr(vel)))
+        return pos, vel
+
+    def accels(self):
+        acc = np.empty((self.nbody, 3))
+        self.check("nbGetAccelsCUDA", self.lib.nbGetAccelsCUDA(self._h, _lib.ptr(acc)))
+        return acc
+
+    # -- the step (nbGravMap / nbStepSystem / run loop) --
+    def gravMap(self, ctx):
+        return self.lib.nbGravMapCUDA(ctypes.byref(ctx.struct), self._h)
+
+    def step(self, ctx):
+        return self.lib.nbStepSystemCUDA(ctypes.byref(ctx.struct), self._h)
+
+    def run_steps(self, ctx, nsteps):
+        return self.lib.nbRunStepsCUDA(ctypes.byref(ctx.struct), self._h, int(nsteps))
+
+    def makeTree(self, ctx):
+        return self.lib.nbMakeTreeCUDA(ctypes.byref(ctx.struct), self._h)
+
+    # -- introspection --
+    def tree_info(self):
+        info = _lib.TreeInfo()
+        self.check("nbTreeInfoCUDA", self.lib.nbTreeInfoCUDA(self._h, ctypes.byref(info)))
+        return info
+
+    def tree(self):
+        n = self.tree_info().nNodes
+        out = {"pos": np.empty((n, 3)), "mass": np.empty(n), "rcrit2": np.empty(n),
+               "quad": np.empty((n, 6)), "next": np.empty(n, np.int32),
+               "body": np.empty(n, np.int32), "depth": np.empty(n, np.int32)}
+        rc = self.lib.nbGetTreeCUDA(self._h, *[_lib.ptr(out[k]) for k in
+                                               ("pos", "mass", "rcrit2", "quad", "next", "body",
+                                                "depth")])
+        self.check("nbGetTreeCUDA", rc)
+        return out
+
+    @property
+    def step_count(self):
+        return self.tree_info().step
+
+    def walk_time_ms(self):
+        ms = ctypes.c_double()
+        n = ctypes.c_int()
+        self.lib.nbLastWalkTimeCUDA(self._h, ctypes.byref(ms), ctypes.byref(n))
+        return ms.value, n.value
+
+    def set_counting(self, enable):
+        self.lib.nbSetCountingCUDA(self._h, int(bool(enable)))
+
+    def interaction_counts(self):
+        a, b, c = ctypes.c_ulonglong(), ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        self.lib.nbInteractionCountsCUDA(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return a.value, b.value, c.value
+
+
+def ext_acceleration(potential, pos, device=0):
+    """nbExtAcceleration (nbody/src/nbody_potential.c:627) at many positions, on the GPU."""
+    lib = _lib.load()
+    pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+    acc = np.empty_like(pos)
+    rc = lib.nbExtAccelerationCUDA(ctypes.byref(potential), _lib.ptr(pos), _lib.ptr(acc),
+                                   len(pos), device)
+    NBodyState.check("nbExtAccelerationCUDA", rc)
+    return acc
+
+
+def kernel_launches():
+    """Kernel launches issued by libnbody_b200.so since it was loaded."""
+    return int(_lib.load().nbKernelLaunchesCUDA())

@@ -1,0 +1,456 @@
+/*
+ * ref_shim.c -- ctypes entry points into the reference N-body client's own CPU code.
+ *
+ * Test infrastructure only (the checker, never the product).  Compiled by oracle/ref.mk
+ * together with the reference sources into oracle/_ref/libnbref.so; it includes the
+ * reference's headers and calls its public functions unchanged:
+ *   nbGravMap (nbody/src/nbody_grav.c:305), nbStepSystem (nbody/src/nbody.c:182),
+ *   nbMakeTree (nbody/src/nbody_tree.c:429), nbExtAcceleration
+ *   (nbody/src/nbody_potential.c:627), nbSetup (nbody/src/nbody_lua.c:612),
+ *   nbCreateHistogram / nbReadHistogram / nbSystemLikelihood (nbody/src/nbody.c:217-397).
+ * The mapping between the reference's NBodyCtx and the flat NBodyCudaCtx of
+ * include/nbody_b200.h below is the same code a maintainer adds to the reference to call
+ * the CUDA library.
+ */
+#include "nbody_priv.h"
+#include "nbody.h"
+#include "nbody_lua.h"
+#include "nbody_grav.h"
+#include "nbody_tree.h"
+#include "nbody_potential.h"
+#include "nbody_histogram.h"
+#include "nbody_likelihood.h"
+#include "nbody_defaults.h"
+#include "milkyway_util.h"
+#include <crlibm.h>
+#include <stddef.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../include/nbody_b200.h"
+
+typedef struct {
+    NBodyCtx ctx;
+    NBodyState st;
+    NBodyFlags nbf;
+    int fromLua;
+} RefHandle;
+
+/* ---- layout facts of the reference ABI ---- */
+int nbref_layout(long* out, int n)
+{
+    long v[] = { (long) sizeof(Body), (long) offsetof(Body, bodynode.pos),
+                 (long) offsetof(Body, bodynode.mass), (long) offsetof(Body, bodynode.type),
+                 (long) offsetof(Body, bodynode.id), (long) offsetof(Body, vel),
+                 (long) sizeof(mwvector), (long) sizeof(NBodyCell) };
+    int k, m = (int) (sizeof v / sizeof v[0]);
+    for (k = 0; k < n && k < m; ++k) out[k] = v[k];
+    return m;
+}
+
+/* ---- NBodyCtx <-> NBodyCudaCtx ---- */
+void nbref_ctx_from_flat(NBodyCtx* ctx, const NBodyCudaCtx* c)
+{
+    static const NBodyCtx empty = EMPTY_NBODYCTX;
+    *ctx = empty;
+    ctx->eps2 = c->eps2;
+    ctx->theta = c->theta;
+    ctx->timestep = c->timestep;
+    ctx->treeRSize = c->treeRSize;
+    ctx->criterion = (criterion_t) c->criterion;
+    ctx->useQuad = (mwbool) c->useQuad;
+    ctx->allowIncest = (mwbool) c->allowIncest;
+    ctx->quietErrors = TRUE;
+    ctx->potentialType = (ExternalPotentialType) c->potentialType;
+    ctx->pot.sphere[0].type = (spherical_t) c->pot.sphere.type;
+    ctx->pot.sphere[0].mass = c->pot.sphere.mass;
+    ctx->pot.sphere[0].scale = c->pot.sphere.scale;
+    ctx->pot.disk.type = (disk_t) c->pot.disk.type;
+    ctx->pot.disk.mass = c->pot.disk.mass;
+    ctx->pot.disk.scaleLength = c->pot.disk.scaleLength;
+    ctx->pot.disk.scaleHeight = c->pot.disk.scaleHeight;
+    ctx->pot.disk.patternSpeed = c->pot.disk.patternSpeed;
+    ctx->pot.disk.startAngle = c->pot.disk.startAngle;
+    ctx->pot.disk2.type = (disk_t) c->pot.disk2.type;
+    ctx->pot.disk2.mass = c->pot.disk2.mass;
+    ctx->pot.disk2.scaleLength = c->pot.disk2.scaleLength;
+    ctx->pot.disk2.scaleHeight = c->pot.disk2.scaleHeight;
+    ctx->pot.disk2.patternSpeed = c->pot.disk2.patternSpeed;
+    ctx->pot.disk2.startAngle = c->pot.disk2.startAngle;
+    ctx->pot.halo.type = (halo_t) c->pot.halo.type;
+    ctx->pot.halo.vhalo = c->pot.halo.vhalo;
+    ctx->pot.halo.scaleLength = c->pot.halo.scaleLength;
+    ctx->pot.halo.flattenZ = c->pot.halo.flattenZ;
+    ctx->pot.halo.flattenY = c->pot.halo.flattenY;
+    ctx->pot.halo.flattenX = c->pot.halo.flattenX;
+    ctx->pot.halo.triaxAngle = c->pot.halo.triaxAngle;
+    ctx->pot.halo.c1 = c->pot.halo.c1;
+    ctx->pot.halo.c2 = c->pot.halo.c2;
+    ctx->pot.halo.c3 = c->pot.halo.c3;
+    ctx->pot.halo.mass = c->pot.halo.mass;
+    ctx->pot.halo.gamma = c->pot.halo.gamma;
+    ctx->pot.halo.lambda = c->pot.halo.lambda;
+    ctx->pot.halo.rho0 = c->pot.halo.rho0;
+}
+
+void nbref_ctx_to_flat(NBodyCudaCtx* c, const NBodyCtx* ctx)
+{
+    memset(c, 0, sizeof *c);
+    c->eps2 = ctx->eps2;
+    c->theta = ctx->theta;
+    c->timestep = ctx->timestep;
+    c->treeRSize = ctx->treeRSize;
+    c->criterion = (int) ctx->criterion;
+    c->useQuad = ctx->useQuad;
+    c->allowIncest = ctx->allowIncest;
+    c->potentialType = (int) ctx->potentialType;
+    c->precision = NBCUDA_PRECISION_FP64;
+    c->pot.sphere.type = ctx->pot.sphere[0].type;
+    c->pot.sphere.mass = ctx->pot.sphere[0].mass;
+    c->pot.sphere.scale = ctx->pot.sphere[0].scale;
+    c->pot.disk.type = ctx->pot.disk.type;
+    c->pot.disk.mass = ctx->pot.disk.mass;
+    c->pot.disk.scaleLength = ctx->pot.disk.scaleLength;
+    c->pot.disk.scaleHeight = ctx->pot.disk.scaleHeight;
+    c->pot.disk.patternSpeed = ctx->pot.disk.patternSpeed;
+    c->pot.disk.startAngle = ctx->pot.disk.startAngle;
+    c->pot.disk2.type = ctx->pot.disk2.type;
+    c->pot.disk2.mass = ctx->pot.disk2.mass;
+    c->pot.disk2.scaleLength = ctx->pot.disk2.scaleLength;
+    c->pot.disk2.scaleHeight = ctx->pot.disk2.scaleHeight;
+    c->pot.disk2.patternSpeed = ctx->pot.disk2.patternSpeed;
+    c->pot.disk2.startAngle = ctx->pot.disk2.startAngle;
+    c->pot.halo.type = ctx->pot.halo.type;
+    c->pot.halo.vhalo = ctx->pot.halo.vhalo;
+    c->pot.halo.scaleLength = ctx->pot.halo.scaleLength;
+    c->pot.halo.flattenZ = ctx->pot.halo.flattenZ;
+    c->pot.halo.flattenY = ctx->pot.halo.flattenY;
+    c->pot.halo.flattenX = ctx->pot.halo.flattenX;
+    c->pot.halo.triaxAngle = ctx->pot.halo.triaxAngle;
+    c->pot.halo.c1 = ctx->pot.halo.c1;
+    c->pot.halo.c2 = ctx->pot.halo.c2;
+    c->pot.halo.c3 = ctx->pot.halo.c3;
+    c->pot.halo.mass = ctx->pot.halo.mass;
+    c->pot.halo.gamma = ctx->pot.halo.gamma;
+    c->pot.halo.lambda = ctx->pot.halo.lambda;
+    c->pot.halo.rho0 = ctx->pot.halo.rho0;
+}
+
+/* ---- states built from arrays ---- */
+void* nbref_state_new(const NBodyCudaCtx* c, const double* pos, const double* vel,
+                      const double* mass, const int* type, int n)
+{
+    static const NBodyState emptyState = EMPTY_NBODYSTATE;
+    RefHandle* h = (RefHandle*) calloc(1, sizeof(RefHandle));
+    Body* bodies;
+    int i;
+    nbref_ctx_from_flat(&h->ctx, c);
+    h->ctx.nStep = 0;
+    h->st = emptyState;
+    bodies = (Body*) mwMallocA((n > 0 ? n : 1) * sizeof(Body));
+    memset(bodies, 0, (n > 0 ? n : 1) * sizeof(Body));
+    for (i = 0; i < n; ++i) {
+        SET_VECTOR(Pos(&bodies[i]), pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        SET_VECTOR(Vel(&bodies[i]), vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+        Mass(&bodies[i]) = mass[i];
+        Type(&bodies[i]) = (body_t) (type ? type[i] : 1);
+        idBody(&bodies[i]) = (unsigned int) i;
+    }
+    setInitialNBodyState(&h->st, &h->ctx, bodies, n);
+    return h;
+}
+
+int nbref_state_gravmap(void* hv)
+{
+    RefHandle* h = (RefHandle*) hv;
+    return (int) nbGravMap(&h->ctx, &h->st);
+}
+
+int nbref_state_maketree(void* hv)
+{
+    RefHandle* h = (RefHandle*) hv;
+    return (int) nbMakeTree(&h->ctx, &h->st);
+}
+
+/* nsteps of nbStepSystem; stops at the first fatal status as nbRunSystemPlain does. */
+int nbref_state_step(void* hv, int nsteps)
+{
+    RefHandle* h = (RefHandle*) hv;
+    int k, all = 0;
+    for (k = 0; k < nsteps; ++k) {
+        NBodyStatus rc = nbStepSystem(&h->ctx, &h->st);
+        all |= (int) rc;
+        if (nbStatusIsFatal(rc)) break;
+    }
+    return all;
+}
+
+void nbref_state_get(void* hv, double* pos, double* vel, double* acc, double* rsize, int* step,
+                     int* incest)
+{
+    RefHandle* h = (RefHandle*) hv;
+    int i;
+    for (i = 0; i < h->st.nbody; ++i) {
+        const Body* b = &h->st.bodytab[i];
+        if (pos) { pos[3 * i] = X(Pos(b)); pos[3 * i + 1] = Y(Pos(b)); pos[3 * i + 2] = Z(Pos(b)); }
+        if (vel) { vel[3 * i] = X(Vel(b)); vel[3 * i + 1] = Y(Vel(b)); vel[3 * i + 2] = Z(Vel(b)); }
+        if (acc) {
+            acc[3 * i] = X(h->st.acctab[i]);
+            acc[3 * i + 1] = Y(h->st.acctab[i]);
+            acc[3 * i + 2] = Z(h->st.acctab[i]);
+        }
+    }
+    if (rsize) *rsize = h->st.tree.rsize;
+    if (step) *step = (int) h->st.step;
+    if (incest) *incest = h->st.treeIncest;
+}
+
+/* Masses and types of the bodies (Lua-built states). */
+void nbref_state_masses(void* hv, double* mass, int* type)
+{
+    RefHandle* h = (RefHandle*) hv;
+    int i;
+    for (i = 0; i < h->st.nbody; ++i) {
+        if (mass) mass[i] = Mass(&h->st.bodytab[i]);
+        if (type) type[i] = Type(&h->st.bodytab[i]);
+    }
+}
+
+void nbref_state_set(void* hv, const double* pos, const double* vel)
+{
+    RefHandle* h = (RefHandle*) hv;
+    int i;
+    for (i = 0; i < h->st.nbody; ++i) {
+        Body* b = &h->st.bodytab[i];
+        if (pos) SET_VECTOR(Pos(b), pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        if (vel) SET_VECTOR(Vel(b), vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+    }
+}
+
+int nbref_state_nbody(void* hv) { return ((RefHandle*) hv)->st.nbody; }
+
+static int cmp_ptr(const void* a, const void* b)
+{
+    const char* x = *(const char* const*) a;
+    const char* y = *(const char* const*) b;
+    return x < y ? -1 : (x > y);
+}
+
+static int ptr_index(const void** sorted, const int* idx, int n, const void* p)
+{
+    int lo = 0, hi = n - 1;
+    while (lo <= hi) {
+        int mid = (lo + hi) / 2;
+        if ((const char*) sorted[mid] == (const char*) p) return idx[mid];
+        if ((const char*) sorted[mid] < (const char*) p) lo = mid + 1; else hi = mid - 1;
+    }
+    return -1;
+}
+
+/* Tree of the last nbMakeTree in walk (Next/More preorder) order; returns the node count.
+ * Arrays as in nbGetTreeCUDA (include/nbody_b200.h); any may be NULL; cap = their length. */
+int nbref_state_tree(void* hv, int cap, double* pos, double* mass, double* rcrit2, double* quad,
+                     int* next, int* body, int* depth)
+{
+    RefHandle* h = (RefHandle*) hv;
+    const NBodyNode* p;
+    const void** ptrs;
+    const void** sorted;
+    int* order;
+    int* idx;
+    int n = 0, k;
+    for (p = (const NBodyNode*) h->st.tree.root; p; p = isCell(p) ? More(p) : Next(p)) ++n;
+    if (n > cap) return -n;
+    ptrs = (const void**) malloc(sizeof(void*) * (n + 1));
+    sorted = (const void**) malloc(sizeof(void*) * (n + 1));
+    order = (int*) malloc(sizeof(int) * (n + 1));
+    idx = (int*) malloc(sizeof(int) * (n + 1));
+    k = 0;
+    for (p = (const NBodyNode*) h->st.tree.root; p; p = isCell(p) ? More(p) : Next(p)) ptrs[k++] = p;
+    {   /* sort pointers to map them back to walk indices */
+        const void** tmp = (const void**) malloc(sizeof(void*) * (n + 1));
+        for (k = 0; k < n; ++k) tmp[k] = ptrs[k];
+        qsort(tmp, (size_t) n, sizeof(void*), cmp_ptr);
+        for (k = 0; k < n; ++k) sorted[k] = tmp[k];
+        free(tmp);
+        for (k = 0; k < n; ++k) {
+            int lo = 0, hi = n - 1;
+            while (lo <= hi) {
+                int mid = (lo + hi) / 2;
+                if (sorted[mid] == ptrs[k]) { idx[mid] = k; break; }
+                if ((const char*) sorted[mid] < (const char*) ptrs[k]) lo = mid + 1; else hi = mid - 1;
+            }
+        }
+    }
+    {
+        /* depth by walking: a cell's children are More(c), then Next() until Next(c) */
+        int* dep = (int*) calloc((size_t) n + 1, sizeof(int));
+        for (k = 0; k < n; ++k) {
+            const NBodyNode* q = (const NBodyNode*) ptrs[k];
+            if (isCell(q)) {
+                const NBodyNode* c = More(q);
+                const NBodyNode* stop = Next(q);
+                while (c && c != stop) {
+                    int ci = ptr_index(sorted, idx, n, c);
+                    if (ci >= 0) dep[ci] = dep[k] + 1;
+                    c = Next(c);
+                }
+            }
+        }
+        for (k = 0; k < n; ++k) {
+            const NBodyNode* q = (const NBodyNode*) ptrs[k];
+            const NBodyNode* nx = Next(q);
+            if (pos) { pos[3 * k] = X(Pos(q)); pos[3 * k + 1] = Y(Pos(q)); pos[3 * k + 2] = Z(Pos(q)); }
+            if (mass) mass[k] = Mass(q);
+            if (next) next[k] = nx ? ptr_index(sorted, idx, n, nx) : n;
+            if (depth) depth[k] = dep[k];
+            if (isCell(q)) {
+                if (rcrit2) rcrit2[k] = Rcrit2(q);
+                if (quad) {
+                    if (h->ctx.useQuad) {
+                        quad[6 * k + 0] = Quad(q).xx; quad[6 * k + 1] = Quad(q).xy;
+                        quad[6 * k + 2] = Quad(q).xz; quad[6 * k + 3] = Quad(q).yy;
+                        quad[6 * k + 4] = Quad(q).yz; quad[6 * k + 5] = Quad(q).zz;
+                    } else memset(quad + 6 * k, 0, 6 * sizeof(double));
+                }
+                if (body) body[k] = -1;
+            } else {
+                if (rcrit2) rcrit2[k] = 0.0;
+                if (quad) memset(quad + 6 * k, 0, 6 * sizeof(double));
+                if (body) body[k] = (int) ((const Body*) q - h->st.bodytab);
+            }
+        }
+        free(dep);
+    }
+    free(ptrs); free(sorted); free(order); free(idx);
+    return n;
+}
+
+void nbref_state_tree_info(void* hv, double* rsize, int* cellUsed, int* maxDepth)
+{
+    RefHandle* h = (RefHandle*) hv;
+    if (rsize) *rsize = h->st.tree.rsize;
+    if (cellUsed) *cellUsed = (int) h->st.tree.cellUsed;
+    if (maxDepth) *maxDepth = (int) h->st.tree.maxDepth;
+}
+
+void nbref_state_free(void* hv)
+{
+    RefHandle* h = (RefHandle*) hv;
+    if (!h) return;
+    destroyNBodyState(&h->st);
+    if (h->fromLua) {
+        free(h->nbf.inputFile);
+        free(h->nbf.histogramFileName);
+        if (h->nbf.forwardedArgs) {
+            unsigned int k;
+            for (k = 0; k < h->nbf.numForwardedArgs; ++k) free((void*) h->nbf.forwardedArgs[k]);
+            free((void*) h->nbf.forwardedArgs);
+        }
+    }
+    free(h);
+}
+
+/* ---- Lua-described runs (nbSetup, nbody/src/nbody_lua.c:612) ---- */
+void* nbref_open_lua(const char* luaFile, const char* histFile, unsigned int seed,
+                     const char* const* args, int nargs)
+{
+    static const NBodyState emptyState = EMPTY_NBODYSTATE;
+    static const NBodyCtx emptyCtx = EMPTY_NBODYCTX;
+    static const NBodyFlags emptyFlags = EMPTY_NBODY_FLAGS;
+    RefHandle* h = (RefHandle*) calloc(1, sizeof(RefHandle));
+    int k;
+    h->ctx = emptyCtx;
+    h->st = emptyState;
+    h->nbf = emptyFlags;
+    h->fromLua = 1;
+    h->nbf.inputFile = strdup(luaFile);
+    h->nbf.histogramFileName = histFile ? strdup(histFile) : NULL;
+    h->nbf.setSeed = 1;
+    h->nbf.seed = seed;
+    h->nbf.ignoreCheckpoint = 1;
+    h->nbf.numForwardedArgs = (unsigned int) nargs;
+    h->nbf.forwardedArgs = (const char**) calloc((size_t) (nargs > 0 ? nargs : 1), sizeof(char*));
+    for (k = 0; k < nargs; ++k) h->nbf.forwardedArgs[k] = strdup(args[k]);
+    if (nbSetup(&h->ctx, &h->st, &h->nbf)) {
+        nbref_state_free(h);
+        return NULL;
+    }
+    h->ctx.quietErrors = TRUE;
+    h->st.previousForwardTime = h->ctx.timeEvolve;
+    return h;
+}
+
+void nbref_handle_ctx(void* hv, NBodyCudaCtx* out, int* nStep, double* timeEvolve)
+{
+    RefHandle* h = (RefHandle*) hv;
+    nbref_ctx_to_flat(out, &h->ctx);
+    if (nStep) *nStep = (int) h->ctx.nStep;
+    if (timeEvolve) *timeEvolve = h->ctx.timeEvolve;
+}
+
+/* The reference's run loop without checkpoints / best-likelihood tracking:
+ * nbGravMap once, then nStep x nbStepSystem (nbody/src/nbody_plain.c:366-446). */
+int nbref_run(void* hv)
+{
+    RefHandle* h = (RefHandle*) hv;
+    NBodyStatus rc = nbGravMap(&h->ctx, &h->st);
+    if (nbStatusIsFatal(rc)) return (int) rc;
+    while (h->st.step < h->ctx.nStep) {
+        rc |= nbStepSystem(&h->ctx, &h->st);
+        if (nbStatusIsFatal(rc)) break;
+    }
+    return (int) rc;
+}
+
+/* Final likelihood as nbReportResults computes it (nbody/src/nbody.c:217-397); out[0..9] =
+ * likelihood, EMD, mass, beta, vel, betaAvg, velAvg, dist, pm_dec, pm_ra (not negated). */
+int nbref_likelihood(void* hv, double* out)
+{
+    RefHandle* h = (RefHandle*) hv;
+    HistogramParams hp;
+    NBodyLikelihoodMethod method;
+    MainStruct* histogram;
+    MainStruct* data;
+    real* arr;
+    int k;
+    if (!h->nbf.histogramFileName) return -1;
+    if (nbGetLikelihoodInfo(&h->nbf, &hp, &method) || method == NBODY_INVALID_METHOD) return -2;
+    histogram = nbCreateHistogram(&h->ctx, &h->st, &hp);
+    if (!histogram) return -3;
+    data = nbReadHistogram(h->nbf.histogramFileName);
+    if (!data) { free(histogram); return -4; }
+    arr = nbSystemLikelihood(&h->st, data, histogram, method);
+    for (k = 0; k < 10; ++k) out[k] = arr[k];
+    if (out[0] > DEFAULT_WORST_CASE || out[0] < -DEFAULT_WORST_CASE) out[0] = DEFAULT_WORST_CASE;
+    else if (out[0] == 0.0) out[0] = DEFAULT_BEST_CASE;
+    if (isnan(out[0])) out[0] = DEFAULT_WORST_CASE;
+    for (k = 0; k < 8; ++k) {
+        free(histogram->histograms[k]);
+        free(data->histograms[k]);
+    }
+    free(histogram);
+    free(data);
+    return 0;
+}
+
+/* ---- math pins ---- */
+double nbref_pow_rn(double x, double y) { return pow_rn(x, y); }
+double nbref_log_rn(double x) { return log_rn(x); }
+
+void nbref_ext_accel(const NBodyCudaPotential* p, const double* pos, double* acc, int n)
+{
+    NBodyCudaCtx c;
+    NBodyCtx ctx;
+    int i;
+    memset(&c, 0, sizeof c);
+    c.pot = *p;
+    nbref_ctx_from_flat(&ctx, &c);
+    for (i = 0; i < n; ++i) {
+        mwvector v, a;
+        SET_VECTOR(v, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        v.w = 0.0;
+        a = nbExtAcceleration(&ctx.pot, v, 0.0);
+        acc[3 * i] = X(a); acc[3 * i + 1] = Y(a); acc[3 * i + 2] = Z(a);
+    }
+}
