@@ -188,11 +188,26 @@ uint64_t nbKernelLaunchesCUDA(void);
  * nbStepSystemCUDA / nbRunStepsCUDA call (CUDA events on the launch stream), and the
  * number of walk launches they cover. */
 NBodyCudaStatus nbLastWalkTimeCUDA(NBodyCudaState* st, double* ms, int* launches);
-/* Interaction counts of the last force evaluation: body-body, body-cell interactions
- * and node visits summed over all bodies (the algorithmic work of the walk). */
+/* Milliseconds of device time of the whole last nbGravMapCUDA / nbStepSystemCUDA call (tree
+ * build, walk and leapfrog; CUDA events on the state's stream); for nbRunStepsCUDA the sum
+ * over its steps. */
+NBodyCudaStatus nbLastStepTimeCUDA(NBodyCudaState* st, double* ms);
+/* FP64 direct-summation self-gravity (the arithmetic of nbGravity_Exact,
+ * nbody/src/nbody_grav.c:205-227) at `count` target bodies of the state, over all its bodies:
+ * the accuracy oracle for the tree forms.  targets: host indices; acc: 3 doubles per target. */
+NBodyCudaStatus nbDirectSampleCUDA(NBodyCudaState* st, double eps2, const int32_t* targets,
+                                   int count, double* acc);
+/* Measured FMA throughput of the device in TFLOP/s (fp64 != 0: DFMA, else FFMA; 2 flops per
+ * FMA): the pipe roofline the walk kernels are reported against. */
+NBodyCudaStatus nbPeakFmaCUDA(int device, int fp64, double* tflops);
+/* Interaction counts of the last force evaluation (counting enabled): body-body and
+ * body-cell interactions and node visits summed over all bodies (the algorithmic work of
+ * the walk), and walk iterations summed over warps (32 x nWarpSteps / nVisit is the
+ * fraction of lanes busy in a visit). */
 NBodyCudaStatus nbInteractionCountsCUDA(NBodyCudaState* st, unsigned long long* nBodyBody,
                                         unsigned long long* nBodyCell,
-                                        unsigned long long* nVisit);
+                                        unsigned long long* nVisit,
+                                        unsigned long long* nWarpSteps);
 /* Enables (1) / disables (0) counting interactions in the walk (off by default). */
 NBodyCudaStatus nbSetCountingCUDA(NBodyCudaState* st, int enable);
 

@@ -119,7 +119,10 @@ SIGNATURES = [
      [ctypes.POINTER(Potential), _vp, _vp, ctypes.c_int, ctypes.c_int]),
     ("nbKernelLaunchesCUDA", ctypes.c_uint64, []),
     ("nbLastWalkTimeCUDA", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int)]),
-    ("nbInteractionCountsCUDA", ctypes.c_int, [_vp, _ull, _ull, _ull]),
+    ("nbLastStepTimeCUDA", ctypes.c_int, [_vp, _dp]),
+    ("nbDirectSampleCUDA", ctypes.c_int, [_vp, ctypes.c_double, _vp, ctypes.c_int, _vp]),
+    ("nbPeakFmaCUDA", ctypes.c_int, [ctypes.c_int, ctypes.c_int, _dp]),
+    ("nbInteractionCountsCUDA", ctypes.c_int, [_vp, _ull, _ull, _ull, _ull]),
     ("nbSetCountingCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbLastErrorCUDA", ctypes.c_char_p, []),
 ]

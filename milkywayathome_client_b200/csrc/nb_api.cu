@@ -14,11 +14,13 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
                          const double* py, const double* pz, double* ax, double* ay, double* az,
                          double* vx, double* vy, double* vz, const NbWalkParams& wp,
                          const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s);
-void nb_launch_walk_mixed(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
-                          const double* nodeQuad, const unsigned* order, const double* px,
-                          const double* py, const double* pz, double* ax, double* ay, double* az,
-                          double* vx, double* vy, double* vz, const NbWalkParams& wp,
-                          const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s);
+void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int capNodes,
+                          const NbWalkParams& wp, const NbPot& pot, bool count, int numSMs,
+                          cudaStream_t s);
+void nb_launch_direct_sample(const double* px, const double* py, const double* pz,
+                             const double* mass, int n, const int* targets, int count,
+                             double eps2, double* out, cudaStream_t s);
+double nb_fma_probe(int fp64, int numSMs, cudaStream_t s);
 void nb_launch_direct_fp64(const double* px, const double* py, const double* pz,
                            const double* mass, double* ax, double* ay, double* az, double* vx,
                            double* vy, double* vz, const NbWalkParams& wp, const NbPot& pot,
@@ -100,6 +102,7 @@ struct NBodyCudaState {
     int numSMs = 148;
     cudaStream_t stream = nullptr;
     NbTreeBuffers b{};
+    NbMixedBuffers mx{};
     int capNodes = 0;
     NbScalars* scHost = nullptr;        // pinned mirror of the device scalars
     double* stage = nullptr;            // device staging: 3 doubles per body
@@ -110,10 +113,12 @@ struct NBodyCudaState {
     int treeIncest = 0;                 // st->treeIncest (sticky)
     int counting = 0;
     int haveTree = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;    // around the walk kernel
+    cudaEvent_t evS = nullptr, evE = nullptr;    // around a whole force evaluation / step
     float walkMs = 0.0f;
+    float stepMs = 0.0f;
     int walkLaunches = 0;
-    unsigned long long cBB = 0, cBC = 0, cVisit = 0;
+    unsigned long long cBB = 0, cBC = 0, cVisit = 0, cWarpSteps = 0;
 };
 
 template <typename T>
@@ -129,8 +134,10 @@ static void nb_free_nodes(NBodyCudaState* st)
     NbTreeBuffers& b = st->b;
     cudaFree(b.nodePM); cudaFree(b.nodeCrit); cudaFree(b.nodeLink); cudaFree(b.nodeQuad);
     cudaFree(b.nodeDepth); cudaFree(b.parent); cudaFree(b.nchild); cudaFree(b.arrive);
+    cudaFree(st->mx.hi); cudaFree(st->mx.lo); cudaFree(st->mx.q32);
     b.nodePM = nullptr; b.nodeCrit = nullptr; b.nodeLink = nullptr; b.nodeQuad = nullptr;
     b.nodeDepth = b.parent = b.nchild = b.arrive = nullptr;
+    st->mx = NbMixedBuffers{};
     st->capNodes = 0;
 }
 
@@ -146,6 +153,9 @@ static NBodyCudaStatus nb_alloc_nodes(NBodyCudaState* st, int cap)
     NB_CHECK(nb_alloc(&b.parent, cap));
     NB_CHECK(nb_alloc(&b.nchild, cap));
     NB_CHECK(nb_alloc(&b.arrive, cap));
+    NB_CHECK(nb_alloc(&st->mx.hi, cap));
+    NB_CHECK(nb_alloc(&st->mx.lo, cap));
+    NB_CHECK(nb_alloc(&st->mx.q32, 2 * (size_t) cap));
     st->capNodes = cap;
     return NBODY_SUCCESS;
 }
@@ -190,6 +200,8 @@ static void nb_free_all(NBodyCudaState* st)
     if (st->scHost) cudaFreeHost(st->scHost);
     if (st->ev0) cudaEventDestroy(st->ev0);
     if (st->ev1) cudaEventDestroy(st->ev1);
+    if (st->evS) cudaEventDestroy(st->evS);
+    if (st->evE) cudaEventDestroy(st->evE);
     if (st->stream) cudaStreamDestroy(st->stream);
 }
 
@@ -270,6 +282,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
         init.rsize = st->rsize;
         init.capNodes = st->capNodes;
         NB_CHECK(cudaMemcpyAsync(b.sc, &init, sizeof init, cudaMemcpyHostToDevice, s));
+        NB_CHECK(cudaEventRecord(st->evS, s));
         st->walkLaunches = 0;
         if (ctx->criterion == NBCUDA_EXACT) {
             if (drift) {
@@ -288,9 +301,8 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
             nb_link_and_moments(b, n, st->capNodes, ctx->criterion, ctx->theta, ctx->useQuad, s);
             NB_CHECK(cudaEventRecord(st->ev0, s));
             if (mixed)
-                nb_launch_walk_mixed(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px,
-                                     b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
-                                     st->counting != 0, s);
+                nb_launch_walk_mixed(b, st->mx, st->capNodes, wp, pot, st->counting != 0,
+                                     st->numSMs, s);
             else
                 nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px,
                                     b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
@@ -299,6 +311,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
             st->walkLaunches = 1;
             st->haveTree = 1;
         }
+        NB_CHECK(cudaEventRecord(st->evE, s));
         NB_CHECK(cudaGetLastError());
         NB_CHECK(cudaMemcpyAsync(st->scHost, b.sc, sizeof(NbScalars), cudaMemcpyDeviceToHost, s));
         NB_CHECK(cudaStreamSynchronize(s));
@@ -315,7 +328,11 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, st->ev0, st->ev1);
         st->walkMs = ms;
+        ms = 0.0f;
+        cudaEventElapsedTime(&ms, st->evS, st->evE);
+        st->stepMs = ms;
         st->cBB = h.nBodyBody; st->cBC = h.nBodyCell; st->cVisit = h.nVisit;
+        st->cWarpSteps = h.nWarpSteps;
         NBodyCudaStatus out = h.status;
         if ((out & ~(int) NBODY_STATUS_WARNINGS_MASK) == 0) {
             if (h.incest) st->treeIncest = 1;
@@ -353,6 +370,8 @@ NBodyCudaStatus nbInitCUDA(NBodyCudaState** out, int device, int nbody)
     cudaError_t e = cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&st->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&st->ev1);
+    if (e == cudaSuccess) e = cudaEventCreate(&st->evS);
+    if (e == cudaSuccess) e = cudaEventCreate(&st->evE);
     if (e == cudaSuccess) e = cudaMallocHost((void**) &st->scHost, sizeof(NbScalars));
     if (e == cudaSuccess) e = cudaMalloc((void**) &st->b.sc, sizeof(NbScalars));
     if (e != cudaSuccess) rc = nb_cuda_fail(e, "nbInitCUDA");
@@ -540,14 +559,16 @@ NBodyCudaStatus nbRunStepsCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, int 
 {
     if (!st || nsteps < 0) return NBODY_USER_ERROR;
     NBodyCudaStatus all = NBODY_SUCCESS;
-    float walkMs = 0.0f;
+    float walkMs = 0.0f, stepMs = 0.0f;
     for (int k = 0; k < nsteps; ++k) {
         NBodyCudaStatus rc = nbStepSystemCUDA(ctx, st);
         walkMs += st->walkMs;
+        stepMs += st->stepMs;
         all |= rc;
         if (rc & ~(int) NBODY_STATUS_WARNINGS_MASK) break;
     }
     st->walkMs = walkMs;
+    st->stepMs = stepMs;
     st->walkLaunches = nsteps;
     return all;
 }
@@ -675,10 +696,58 @@ NBodyCudaStatus nbLastWalkTimeCUDA(NBodyCudaState* st, double* ms, int* launches
     return NBODY_SUCCESS;
 }
 
+NBodyCudaStatus nbLastStepTimeCUDA(NBodyCudaState* st, double* ms)
+{
+    if (!st || !ms) return NBODY_USER_ERROR;
+    *ms = st->stepMs;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbDirectSampleCUDA(NBodyCudaState* st, double eps2, const int32_t* targets,
+                                   int count, double* acc)
+{
+    if (!st || count < 0 || (count && (!targets || !acc))) return NBODY_USER_ERROR;
+    for (int k = 0; k < count; ++k)
+        if (targets[k] < 0 || targets[k] >= st->nbody) return NBODY_USER_ERROR;
+    if (!count) return NBODY_SUCCESS;
+    NB_CHECK(cudaSetDevice(st->device));
+    int* dt = nullptr;
+    double* da = nullptr;
+    NB_CHECK(cudaMalloc((void**) &dt, sizeof(int) * (size_t) count));
+    cudaError_t e = cudaMalloc((void**) &da, 3 * sizeof(double) * (size_t) count);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dt, targets, sizeof(int) * (size_t) count, cudaMemcpyHostToDevice, st->stream);
+    if (e == cudaSuccess) {
+        nb_launch_direct_sample(st->b.px, st->b.py, st->b.pz, st->b.mass, st->nbody, dt, count,
+                                eps2, da, st->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(acc, da, 3 * sizeof(double) * (size_t) count, cudaMemcpyDeviceToHost, st->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st->stream);
+    cudaFree(dt);
+    cudaFree(da);
+    if (e != cudaSuccess) return nb_cuda_fail(e, "nbDirectSampleCUDA");
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbPeakFmaCUDA(int device, int fp64, double* tflops)
+{
+    if (!tflops) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    NB_CHECK(cudaGetDeviceProperties(&prop, device));
+    *tflops = nb_fma_probe(fp64, prop.multiProcessorCount, 0);
+    NB_CHECK(cudaGetLastError());
+    return NBODY_SUCCESS;
+}
+
 NBodyCudaStatus nbInteractionCountsCUDA(NBodyCudaState* st, unsigned long long* nBodyBody,
-                                        unsigned long long* nBodyCell, unsigned long long* nVisit)
+                                        unsigned long long* nBodyCell, unsigned long long* nVisit,
+                                        unsigned long long* nWarpSteps)
 {
     if (!st) return NBODY_USER_ERROR;
+    if (nWarpSteps) *nWarpSteps = st->cWarpSteps;
     if (nBodyBody) *nBodyBody = st->cBB;
     if (nBodyCell) *nBodyCell = st->cBC;
     if (nVisit) *nVisit = st->cVisit;

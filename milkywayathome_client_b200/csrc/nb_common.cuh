@@ -42,6 +42,7 @@ struct NbScalars {
     unsigned long long nBodyBody;   // interaction counters (counting build of the walk)
     unsigned long long nBodyCell;
     unsigned long long nVisit;
+    unsigned long long nWarpSteps;  // walk iterations summed over warps (SIMT utilisation)
 };
 
 // Potential parameters in constant-friendly POD form.
@@ -123,6 +124,13 @@ struct NbTreeBuffers {
     double4* nodePM; double* nodeCrit; int2* nodeLink; double* nodeQuad;
     int *nodeDepth, *parent, *nchild, *arrive;
     NbScalars* sc;
+};
+
+// FP32 node records of the mixed-precision walk.
+struct NbMixedBuffers {
+    float4* hi;    // {hi.x, hi.y, hi.z, rcrit2 (-inf for bodies)}
+    float4* lo;    // {lo.x, lo.y, lo.z, mass}
+    float4* q32;   // 2 per node: {xx, xy, xz, yy}, {yz, zz, 0, 0}
 };
 
 void nb_build_tree(NbTreeBuffers& b, int n, int criterion, double theta, int useQuad, int drift,

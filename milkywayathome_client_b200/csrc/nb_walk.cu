@@ -37,10 +37,11 @@ k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeC
     int ptr = valid ? 0 : end;
     double accx = 0.0, accy = 0.0, accz = 0.0;
     bool metSelf = false;
-    unsigned long long cVisit = 0, cBB = 0, cBC = 0;
+    unsigned long long cVisit = 0, cBB = 0, cBC = 0, cSteps = 0;
     for (;;) {
         const int q = __reduce_min_sync(NB_FULL_MASK, ptr);
         if (q >= end) break;
+        if (COUNT) ++cSteps;
         if (ptr != q) continue;
         const double4 nd = nodePM[q];
         const int2 link = nodeLink[q];
@@ -87,6 +88,7 @@ k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeC
             cBC += __shfl_xor_sync(NB_FULL_MASK, cBC, o);
         }
         if (lane == 0) {
+            atomicAdd(&sc->nWarpSteps, cSteps);
             atomicAdd(&sc->nVisit, cVisit);
             atomicAdd(&sc->nBodyBody, cBB);
             atomicAdd(&sc->nBodyCell, cBC);
@@ -136,6 +138,56 @@ k_direct_fp64(const double* __restrict__ px, const double* __restrict__ py,
     if (valid) nb_finish_body(pot, wp, (unsigned) i, x0, y0, z0, accx, accy, accz, ax, ay, az, vx, vy, vz);
 }
 
+// Direct FP64 sums (nbGravity_Exact arithmetic) for a sample of target bodies: the accuracy
+// oracle of the walk forms.  Self-gravity only.
+__global__ void __launch_bounds__(EXACT_TILE)
+k_direct_sample(const double* __restrict__ px, const double* __restrict__ py,
+                const double* __restrict__ pz, const double* __restrict__ mass, int n,
+                const int* __restrict__ targets, int count, double eps2, double* __restrict__ out)
+{
+    __shared__ double4 tile[EXACT_TILE];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = t < count;
+    const int i = valid ? targets[t] : 0;
+    const double x0 = px[i], y0 = py[i], z0 = pz[i];
+    double accx = 0.0, accy = 0.0, accz = 0.0;
+    for (int base = 0; base < n; base += EXACT_TILE) {
+        const int k = base + threadIdx.x;
+        __syncthreads();
+        tile[threadIdx.x] = k < n ? make_double4(px[k], py[k], pz[k], mass[k]) : make_double4(0, 0, 0, 0);
+        __syncthreads();
+        const int lim = min(EXACT_TILE, n - base);
+        for (int s = 0; s < lim; ++s) {
+            const double4 b = tile[s];
+            const double dx = b.x - x0, dy = b.y - y0, dz = b.z - z0;
+            const double drSq = (dz * dz + (dy * dy + dx * dx)) + eps2;
+            const double drab = sqrt(drSq);
+            const double phii = b.w / drab;
+            const double mor3 = phii / drSq;
+            accx = accx + mor3 * dx;
+            accy = accy + mor3 * dy;
+            accz = accz + mor3 * dz;
+        }
+    }
+    if (valid) { out[3 * t] = accx; out[3 * t + 1] = accy; out[3 * t + 2] = accz; }
+}
+
+// FMA throughput probe: independent FMA chains per thread (the denominator of the walk's
+// pipe roofline).  fp64 selects DFMA or FFMA.
+template <typename T>
+__global__ void k_fma_probe(T* out, int iters, T seed)
+{
+    T a0 = seed + (T) threadIdx.x, a1 = a0 + (T) 1, a2 = a0 + (T) 2, a3 = a0 + (T) 3;
+    T a4 = a0 + (T) 4, a5 = a0 + (T) 5, a6 = a0 + (T) 6, a7 = a0 + (T) 7;
+    const T m = (T) 0.999999, c = (T) 1e-7;
+    for (int k = 0; k < iters; ++k) {
+        a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+        a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+    }
+    const T s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+    if (s == (T) -1) out[0] = s;   // keeps the chains live
+}
+
 __global__ void k_ext_only(const double* __restrict__ pos, double* __restrict__ acc, int n, NbPot pot)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -180,4 +232,42 @@ void nb_launch_ext_only(const double* dpos, double* dacc, int n, const NbPot& po
     if (n <= 0) return;
     k_ext_only<<<(n + 255) / 256, 256, 0, s>>>(dpos, dacc, n, pot);
     nb_count_launch();
+}
+
+void nb_launch_direct_sample(const double* px, const double* py, const double* pz,
+                             const double* mass, int n, const int* targets, int count,
+                             double eps2, double* out, cudaStream_t s)
+{
+    if (count <= 0) return;
+    k_direct_sample<<<(count + EXACT_TILE - 1) / EXACT_TILE, EXACT_TILE, 0, s>>>(
+        px, py, pz, mass, n, targets, count, eps2, out);
+    nb_count_launch();
+}
+
+// Returns the achieved FMA rate in TFLOP/s (2 flops per FMA) over blocks x 256 threads.
+double nb_fma_probe(int fp64, int numSMs, cudaStream_t s)
+{
+    const int threads = 256, blocks = numSMs * 8, iters = 1 << 14;
+    void* out = nullptr;
+    cudaMalloc(&out, 16);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 0.0;
+    for (int rep = 0; rep < 3; ++rep) {
+        cudaEventRecord(e0, s);
+        if (fp64) k_fma_probe<double><<<blocks, threads, 0, s>>>((double*) out, iters, 1.0);
+        else k_fma_probe<float><<<blocks, threads, 0, s>>>((float*) out, iters, 1.0f);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double flops = 2.0 * 8.0 * (double) iters * threads * (double) blocks;
+        if (ms > 0.f) best = fmax(best, flops / (ms * 1e-3) / 1e12);
+    }
+    nb_count_launch(3);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    return best;
 }

@@ -266,13 +266,33 @@ class NBodyState:
         self.lib.nbLastWalkTimeCUDA(self._h, ctypes.byref(ms), ctypes.byref(n))
         return ms.value, n.value
 
+    def step_time_ms(self):
+        """Device time of the whole last gravMap / step / run_steps call."""
+        ms = ctypes.c_double()
+        self.lib.nbLastStepTimeCUDA(self._h, ctypes.byref(ms))
+        return ms.value
+
+    def direct_sample(self, eps2, targets):
+        """FP64 direct-sum self-gravity at the given body indices (accuracy oracle)."""
+        targets = np.ascontiguousarray(targets, dtype=np.int32)
+        acc = np.empty((len(targets), 3))
+        rc = self.lib.nbDirectSampleCUDA(self._h, float(eps2), _lib.ptr(targets), len(targets),
+                                         _lib.ptr(acc))
+        self.check("nbDirectSampleCUDA", rc)
+        return acc
+
     def set_counting(self, enable):
         self.lib.nbSetCountingCUDA(self._h, int(bool(enable)))
 
     def interaction_counts(self):
-        a, b, c = ctypes.c_ulonglong(), ctypes.c_ulonglong(), ctypes.c_ulonglong()
-        self.lib.nbInteractionCountsCUDA(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
-        return a.value, b.value, c.value
+        """(body-body, body-cell, visits) of the last force evaluation with counting on."""
+        return self.walk_stats()[:3]
+
+    def walk_stats(self):
+        """(body-body, body-cell, visits, warp iterations) of the last counted evaluation."""
+        v = [ctypes.c_ulonglong() for _ in range(4)]
+        self.lib.nbInteractionCountsCUDA(self._h, *[ctypes.byref(x) for x in v])
+        return tuple(x.value for x in v)
 
 
 def ext_acceleration(potential, pos, device=0):
@@ -284,6 +304,14 @@ def ext_acceleration(potential, pos, device=0):
                                    len(pos), device)
     NBodyState.check("nbExtAccelerationCUDA", rc)
     return acc
+
+
+def peak_fma_tflops(fp64=True, device=0):
+    """Measured DFMA (fp64) or FFMA throughput of the device, TFLOP/s."""
+    out = ctypes.c_double()
+    rc = _lib.load().nbPeakFmaCUDA(device, int(bool(fp64)), ctypes.byref(out))
+    NBodyState.check("nbPeakFmaCUDA", rc)
+    return out.value
 
 
 def kernel_launches():

@@ -52,6 +52,10 @@ def oracle():
         lib.or_ext_accel.argtypes = [_vp, _vp, _vp, ctypes.c_int]
         lib.or_pow_1p5.restype = ctypes.c_double
         lib.or_pow_1p5.argtypes = [ctypes.c_double]
+        lib.or_sample_step.restype = ctypes.c_int
+        lib.or_sample_step.argtypes = [_vp, _vp, _vp, ctypes.c_int, _dp, _vp, ctypes.c_int, _vp, _dp, _dp]
+        lib.or_threads.restype = ctypes.c_int
+        lib.or_threads.argtypes = []
         lib.or_pow_3.restype = ctypes.c_double
         lib.or_pow_3.argtypes = [ctypes.c_double]
         _oracle = lib
@@ -90,6 +94,8 @@ def ref():
             "nbref_pow_rn": (ctypes.c_double, [ctypes.c_double, ctypes.c_double]),
             "nbref_log_rn": (ctypes.c_double, [ctypes.c_double]),
             "nbref_ext_accel": (None, [_vp, _vp, _vp, ctypes.c_int]),
+            "nbref_sample_step": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _dp, _dp]),
+            "nbref_threads": (ctypes.c_int, []),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -153,6 +159,19 @@ def tree(ctx, pos, mass, rsize):
         res = {k: v[:n] for k, v in out.items()}
         res.update(status=st.value, rsize=rs.value, maxDepth=md.value, nNodes=n)
         return res
+
+
+def sample_step(ctx, pos, mass, rsize, idx):
+    """or_sample_step: (status, t_tree, t_walk, acc_of_sample)."""
+    lib = oracle()
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    mass = np.ascontiguousarray(mass, dtype=np.float64)
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    acc = np.zeros((len(idx), 3))
+    rs, tt, tw = ctypes.c_double(rsize), ctypes.c_double(), ctypes.c_double()
+    rc = lib.or_sample_step(ctypes.byref(ctx), _p(pos), _p(mass), len(mass), ctypes.byref(rs),
+                            _p(idx), len(idx), _p(acc), ctypes.byref(tt), ctypes.byref(tw))
+    return rc, tt.value, tw.value, acc
 
 
 def ext_accel(potential, pos):
@@ -253,6 +272,13 @@ class RefState:
             self.lib.nbref_state_tree_info(self.h, ctypes.byref(rs), ctypes.byref(cu), ctypes.byref(md))
             res.update(rsize=rs.value, cellUsed=cu.value, maxDepth=md.value, nNodes=n)
             return res
+
+    def sample_step(self, idx):
+        """nbMakeTree + the walk for the bodies in idx; returns (status, t_tree, t_walk) s."""
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        tt, tw = ctypes.c_double(), ctypes.c_double()
+        rc = self.lib.nbref_sample_step(self.h, _p(idx), len(idx), ctypes.byref(tt), ctypes.byref(tw))
+        return rc, tt.value, tw.value
 
     def ctx(self, ctx_type):
         c = ctx_type()

@@ -533,3 +533,39 @@ int or_tree(const NBodyCudaCtx* ctx, const double* pos, const double* mass, int 
     free(bodyNext); free(t.cells); free(cellIdx); free(bodyIdx);
     return count;
 }
+
+/* A bounded sample of one step for the CPU baseline (the restatement's counterpart of
+ * nbref_sample_step): the whole tree, then the walk + external potential for `count` bodies.
+ * Times in seconds (omp_get_wtime). */
+#include <omp.h>
+int or_sample_step(const NBodyCudaCtx* ctx, const double* pos, const double* mass, int n,
+                   double* rsize, const int* idx, int count, double* acc, double* tTree,
+                   double* tWalk)
+{
+    OrTree t;
+    int* bodyNext = (int*) malloc(sizeof(int) * (size_t) (n > 0 ? n : 1));
+    double t0, t1, t2;
+    int k, rc;
+    memset(&t, 0, sizeof t);
+    t.rsize = *rsize;
+    t0 = omp_get_wtime();
+    rc = or_make_tree(ctx, &t, pos, mass, n, bodyNext);
+    t1 = omp_get_wtime();
+    *rsize = t.rsize;
+    if (rc == NBODY_SUCCESS) {
+#pragma omp parallel for schedule(dynamic, 64)
+        for (k = 0; k < count; ++k) {
+            int met;
+            or_gravity(ctx, &t, pos, mass, bodyNext, idx[k], acc + 3 * k, &met, NULL);
+            or_add_external(ctx, pos + 3 * idx[k], acc + 3 * k);
+        }
+    }
+    t2 = omp_get_wtime();
+    *tTree = t1 - t0;
+    *tWalk = t2 - t1;
+    free(bodyNext);
+    free(t.cells);
+    return rc;
+}
+
+int or_threads(void) { return omp_get_max_threads(); }

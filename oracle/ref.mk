@@ -116,14 +116,16 @@ $(OBJ)/nbody/%.o: $(REF)/nbody/src/%.c $(GEN)/.stamp
 	@mkdir -p $(dir $@)
 	$(CC) $(CFLAGS) -c $< -o $@
 
-$(OBJ)/local/%.o: oracle/%.c $(GEN)/.stamp
+$(OBJ)/local/%.o: oracle/%.c oracle/ref.mk $(GEN)/.stamp
 	@mkdir -p $(dir $@)
-	$(CC) $(CFLAGS) -c $< -o $@
+	$(CC) $(CFLAGS) -I$(REF)/nbody/src -c $< -o $@
 
 $(OUT)/milkyway_nbody: $(OBJ)/nbody/main.o $(OBJS)
 	$(CXX) -fopenmp -o $@ $^ -lm -lrt -lpthread -ldl
 
-$(OUT)/libnbref.so: $(OBJ)/local/ref_shim.o $(OBJS)
+# ref_shim.c compiles nbody_grav.c itself (for its file-static walk), so the library takes
+# every reference object except nbody_grav.o
+$(OUT)/libnbref.so: $(OBJ)/local/ref_shim.o $(filter-out $(OBJ)/nbody/nbody_grav.o,$(OBJS))
 	$(CXX) -shared -fopenmp -o $@ $^ -lm -lrt -lpthread -ldl
 
 .PHONY: all

@@ -29,6 +29,12 @@
 
 #include "../include/nbody_b200.h"
 
+/* The reference's force walk itself (nbGravity and nbMapForceBody are file-static in
+ * nbody/src/nbody_grav.c): compiled here from that source so that a bounded sample of the
+ * walk can be timed; oracle/ref.mk leaves nbody_grav.o out of libnbref.so accordingly. */
+#include "nbody_grav.c"
+#include <omp.h>
+
 typedef struct {
     NBodyCtx ctx;
     NBodyState st;
@@ -454,3 +460,40 @@ void nbref_ext_accel(const NBodyCudaPotential* p, const double* pos, double* acc
         acc[3 * i] = X(a); acc[3 * i + 1] = Y(a); acc[3 * i + 2] = Z(a);
     }
 }
+
+/* A bounded sample of one reference step for the CPU baseline: nbMakeTree on the whole
+ * system, then nbGravity + nbExtAcceleration (nbMapForceBody's per-body work,
+ * nbody/src/nbody_grav.c:126-176) for `count` of its bodies on all OpenMP threads.
+ * Returns the tree status; times in seconds. */
+int nbref_sample_step(void* hv, const int* idx, int count, double* tTree, double* tWalk)
+{
+    RefHandle* h = (RefHandle*) hv;
+    double t0, t1, t2;
+    int k;
+    NBodyStatus rc;
+    t0 = omp_get_wtime();
+    rc = nbMakeTree(&h->ctx, &h->st);
+    t1 = omp_get_wtime();
+    if (!nbStatusIsFatal(rc)) {
+        const Body* bodies = h->st.bodytab;
+        mwvector* accels = h->st.acctab;
+        mwvector zero;
+        SET_VECTOR(zero, 0.0, 0.0, 0.0);
+        zero.w = 0.0;
+#pragma omp parallel for schedule(dynamic, 64)
+        for (k = 0; k < count; ++k) {
+            const Body* b = &bodies[idx[k]];
+            mwvector a = nbGravity(&h->ctx, &h->st, b);
+            mwvector e = mw_addv(nbExtAcceleration(&h->ctx.pot, Pos(b), 0.0),
+                                 plummerAccel(Pos(b), zero, 0.0, 1.0));
+            mw_incaddv(a, e);
+            accels[idx[k]] = a;
+        }
+    }
+    t2 = omp_get_wtime();
+    *tTree = t1 - t0;
+    *tWalk = t2 - t1;
+    return (int) rc;
+}
+
+int nbref_threads(void) { return omp_get_max_threads(); }
