@@ -384,6 +384,13 @@ void* nbref_open_lua(const char* luaFile, const char* histFile, unsigned int see
     }
     h->ctx.quietErrors = TRUE;
     h->st.previousForwardTime = h->ctx.timeEvolve;
+    /* the comparison switches nbMain copies into the state before the run (nbody.c:485-490) */
+    h->st.useVelDisp = h->ctx.useVelDisp;
+    h->st.useBetaDisp = h->ctx.useBetaDisp;
+    h->st.useBetaComp = h->ctx.useBetaComp;
+    h->st.useVlos = h->ctx.useVlos;
+    h->st.useDist = h->ctx.useDist;
+    h->st.usePropMot = h->ctx.usePropMot;
     return h;
 }
 
