@@ -181,6 +181,19 @@ NBodyCudaStatus nbGetTreeCUDA(NBodyCudaState* st, double* pos, double* mass, dou
 NBodyCudaStatus nbExtAccelerationCUDA(const NBodyCudaPotential* pot, const double* pos,
                                       double* acc, int n, int device);
 
+/* nbExtAcceleration at n host positions with no device allocation (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc/cudaFree -- cudaFree waits for the
+ * whole device, cudaMalloc can fail under a fixed memory budget -- such as an orbit
+ * integrator evaluating a few points per step, or a process sharing the GPU with a running
+ * simulation.  Positions and results go through one fixed static device array of
+ * NB_NOALLOC_MAX_POINTS (65536) points (3 MiB, held by every device that loads the library
+ * until exit); larger n is rejected with NBODY_USER_ERROR.  The first call on a device looks
+ * up the array's address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race.  Same results as
+ * nbExtAccelerationCUDA. */
+NBodyCudaStatus nbExtAccelerationNoAllocCUDA(const NBodyCudaPotential* pot, const double* pos,
+                                             double* acc, int n, int device);
+
 /* Number of this library's kernel launches issued since load (a launch counter for
  * benchmarks). */
 uint64_t nbKernelLaunchesCUDA(void);

@@ -117,6 +117,8 @@ SIGNATURES = [
     ("nbGetTreeCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("nbExtAccelerationCUDA", ctypes.c_int,
      [ctypes.POINTER(Potential), _vp, _vp, ctypes.c_int, ctypes.c_int]),
+    ("nbExtAccelerationNoAllocCUDA", ctypes.c_int,
+     [ctypes.POINTER(Potential), _vp, _vp, ctypes.c_int, ctypes.c_int]),
     ("nbKernelLaunchesCUDA", ctypes.c_uint64, []),
     ("nbLastWalkTimeCUDA", ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int)]),
     ("nbLastStepTimeCUDA", ctypes.c_int, [_vp, _dp]),

@@ -30,7 +30,7 @@ void nb_launch_ext_only(const double* dpos, double* dacc, int n, const NbPot& po
 static std::atomic<unsigned long long> g_launches{0};
 void nb_count_launch(int n) { g_launches.fetch_add((unsigned long long) n); }
 
-static thread_local std::string g_lastError;
+thread_local std::string g_lastError;
 static NBodyCudaStatus nb_cuda_fail(cudaError_t e, const char* what)
 {
     char buf[256];
@@ -205,7 +205,7 @@ static void nb_free_all(NBodyCudaState* st)
     if (st->stream) cudaStreamDestroy(st->stream);
 }
 
-static NbPot nb_pot_from(const NBodyCudaCtx* c)
+NbPot nb_pot_from(const NBodyCudaCtx* c)
 {
     NbPot p{};
     p.enabled = c->potentialType == NBCUDA_POTENTIAL_DEFAULT;
@@ -227,7 +227,7 @@ static bool nb_pow2(double x)
 
 // Options this implementation evaluates on the GPU; anything else is NBODY_UNSUPPORTED,
 // as the reference's OpenCL path does for a custom Lua potential (nbody_types.c:297-301).
-static NBodyCudaStatus nb_check_ctx(const NBodyCudaCtx* c, std::string& why)
+NBodyCudaStatus nb_check_ctx(const NBodyCudaCtx* c, std::string& why)
 {
     if (!c) { why = "null context"; return NBODY_USER_ERROR; }
     if (c->criterion < NBCUDA_TREECODE || c->criterion > NBCUDA_EXACT) { why = "invalid criterion"; return NBODY_USER_ERROR; }
