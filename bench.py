@@ -56,6 +56,9 @@ def parse_args():
     ap.add_argument("--theta", type=float, default=THETA_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--adjoint-n", type=int, default=131072,
+                    help="bodies of the adjoint-cost measurement (0 skips it)")
+    ap.add_argument("--adjoint-steps", type=int, default=64)
     ap.add_argument("--profile", choices=["fp64", "mixed"],
                     help="profiling entry: build the dwarf, run two force evaluations, exit")
     return ap.parse_args()
@@ -63,46 +66,71 @@ def parse_args():
 
 # ---------------------------------------------------------------------------------------
 class Dist:
-    """torch.distributed plumbing (barrier, max over ranks); single process without it."""
+    """torch.distributed plumbing (barrier, max/sum over ranks); a single process without it.
+    NCCL between GPUs; gloo when no GPU is present (the CPU tests of the replica logic)."""
 
-    def __init__(self):
+    def __init__(self, backend=None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.cuda = False
         if self.world > 1:
             import datetime
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+            self.cuda = torch.cuda.is_available() if backend is None else backend == "nccl"
+            if self.cuda:
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend or ("nccl" if self.cuda else "gloo"),
+                                    timeout=datetime.timedelta(seconds=180))
             self.pg = dist
+        else:
+            try:
+                import torch
+                self.cuda = torch.cuda.is_available()
+            except ImportError:
+                self.cuda = False
+
+    def _tensor(self, x):
+        import torch
+        dev = "cuda:%d" % self.local if self.cuda else "cpu"
+        return torch.tensor([float(x)], device=dev, dtype=torch.float64)
 
     def barrier(self):
-        import torch
         if self.pg:
-            self.pg.barrier(device_ids=[self.local])
-        torch.cuda.synchronize()
+            if self.cuda:
+                self.pg.barrier(device_ids=[self.local])
+            else:
+                self.pg.barrier()
+        if self.cuda:
+            import torch
+            torch.cuda.synchronize()
 
     def max(self, x):
         if not self.pg:
             return x
-        import torch
-        t = torch.tensor([float(x)], device="cuda:%d" % self.local, dtype=torch.float64)
+        t = self._tensor(x)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
     def sum(self, x):
         if not self.pg:
             return x
-        import torch
-        t = torch.tensor([float(x)], device="cuda:%d" % self.local, dtype=torch.float64)
+        t = self._tensor(x)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
         return float(t.item())
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
+
+
+def replica_throughput(dist, n_per_rank, steps, seconds_this_rank):
+    """Whole-job body-updates/s of independent replicas: all ranks' updates over the slowest
+    rank's time (max over ranks)."""
+    t = dist.max(seconds_this_rank)
+    return dist.world * n_per_rank * steps / t, t
 
 
 class ClockSampler:
@@ -209,6 +237,34 @@ def cpu_baseline_sample(ctx, pos, mass, seconds):
             "status": int(rc), "step_seconds_estimate": step_s}
 
 
+def adjoint_ratio(n, steps, dev):
+    """Adjoint step / forward step time of the FP64 step with the tree frozen per step, on the
+    two-component dwarf at n bodies (checkpoints every 32 steps, recomputation between them).
+    Both passes are timed the same way (CUDA events on torch's stream around the whole pass,
+    host sequencing included)."""
+    import torch
+    from milkywayathome_client_b200 import adjoint, models
+    from milkywayathome_client_b200.nbody import NBodyCtx, milky_way_potential
+    pos, vel, mass, _ = models.plummer_plummer_dwarf(n, seed=4242)
+    ctx = NBodyCtx(potential=milky_way_potential(), **models.dwarf_config(n, theta=0.5))
+    device = torch.device("cuda:%d" % dev)
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device=device)
+    x0, v0, m = t(pos).requires_grad_(True), t(vel).requires_grad_(True), t(mass).requires_grad_(True)
+    dt = t(ctx.timestep).requires_grad_(True)
+    w = torch.randn((n, 3), dtype=torch.float64, device=device, generator=torch.Generator(device=device).manual_seed(0))
+    stats = {}
+    xN, vN = adjoint.run(ctx, x0, v0, m, dt, steps, every=32, stats=stats)
+    ((xN * w).sum() + (vN * w).sum()).backward()
+    return {"n_bodies": n, "steps": steps, "checkpoint_every": 32,
+            "forward_step_ms": stats["forward_step_ms"], "adjoint_step_ms": stats["adjoint_step_ms"],
+            "ratio": stats["adjoint_step_ms"] / stats["forward_step_ms"],
+            "parts_device_ms": {k: stats[k] for k in ("forward_step_device_ms",
+                                                      "recompute_step_device_ms", "vjp_device_ms",
+                                                      "vjp_walk_device_ms")},
+            "how": "tree frozen per step; backward = segment recomputation + tree rebuild + "
+                   "force VJP per step; both passes timed with CUDA events around the pass"}
+
+
 def run_reference(args, dist):
     """--impl reference: bounded reference samples on the host, rank 0 only."""
     if dist.rank != 0:
@@ -293,8 +349,7 @@ def run_ours(args, dist):
 
     # ---- FP64 drop-in (headline) ----
     st, counts, step_ms, walk_ms, launches, clk, info = timed_run(ctx)
-    t_dev = dist.max(sum(step_ms) / 1e3)
-    value = dist.world * n * K / t_dev
+    value, t_dev = replica_throughput(dist, n, K, sum(step_ms) / 1e3)
     flops_per_walk = walk_flops(counts)
     mean_walk = float(np.mean(walk_ms))
 
@@ -340,8 +395,8 @@ def run_ours(args, dist):
         hp[:] = p
         hv[:] = v
     dist.barrier()
-    t_e2e = dist.max(time.perf_counter() - t0)
-    e2e = {"value": dist.world * n * K / t_e2e, "unit": UNIT,
+    e2e_value, t_e2e = replica_throughput(dist, n, K, time.perf_counter() - t0)
+    e2e = {"value": e2e_value, "unit": UNIT,
            "h2d_bytes_per_step": int(n * (3 + 3 + 1) * 8), "d2h_bytes_per_step": int(n * 6 * 8),
            "how": ("per step: nbSetBodiesCUDA (pinned pos/vel/mass -> HBM), nbStepSystemCUDA, "
                    "nbGetBodiesCUDA (HBM -> pinned pos/vel); host wall clock, max over ranks")}
@@ -350,8 +405,8 @@ def run_ours(args, dist):
     # ---- mixed form ----
     stm, counts_m, step_ms_m, walk_ms_m, launches_m, clk_m, _ = timed_run(ctx_mixed)
     stm.close()
-    t_mixed = dist.max(sum(step_ms_m) / 1e3)
-    mixed = {"value": dist.world * n * K / t_mixed, "unit": UNIT,
+    mixed_value, t_mixed = replica_throughput(dist, n, K, sum(step_ms_m) / 1e3)
+    mixed = {"value": mixed_value, "unit": UNIT,
              "ms_per_step": 1e3 * t_mixed / K, "walk_ms": float(np.mean(walk_ms_m)),
              "speedup_vs_fp64": t_dev / t_mixed}
 
@@ -383,6 +438,14 @@ def run_ours(args, dist):
     mixed["roofline"]["frac"] = mixed["roofline"]["achieved"] / peak32
     mixed["roofline"]["lane_utilisation"] = counts_m[2] / (32.0 * max(counts_m[3], 1))
 
+    # ---- adjoint step cost (the adjoint configuration's dwarf) ----
+    adj = None
+    if args.adjoint_n > 0:
+        try:
+            adj = adjoint_ratio(args.adjoint_n, args.adjoint_steps, dev)
+        except Exception as e:
+            notes.append("adjoint measurement failed: %r" % (e,))
+
     # ---- CPU baseline (rank 0, single GPU only) ----
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
@@ -404,7 +467,7 @@ def run_ours(args, dist):
                        "l2": "inputs larger than L2: %d tree nodes (~%.0f MB) + bodies (~%.0f MB) per step"
                              % (info.nNodes, info.nNodes * 176 / 1e6, n * 120 / 1e6)},
             "roofline": roofline, "mixed": mixed, "accuracy": accuracy, "e2e": e2e,
-            "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk,
+            "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk, "adjoint": adj,
             "tree": {"nodes": info.nNodes, "cells": info.cellUsed, "max_depth": info.maxDepth,
                      "rsize": info.rsize},
         }

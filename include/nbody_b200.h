@@ -165,6 +165,18 @@ NBodyCudaStatus nbGravMapCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st);
 NBodyCudaStatus nbStepSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st);
 NBodyCudaStatus nbRunStepsCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, int nsteps);
 
+/* ---- adjoint (no counterpart in the reference) ----
+ * Vector-Jacobian product of the last force evaluation with its tree frozen: given the
+ * adjoint abar of every body's acceleration (device pointer, 3 doubles per body in the
+ * state's body order), writes xbar_j = sum_i abar_i . d a_i / d x_j (device, 3 per body) and,
+ * if dMbar is not NULL, mbar_j = sum_i abar_i . d a_i / d m_j (device, 1 per body).  Every
+ * opening decision of that evaluation is kept; the accelerations depend on the bodies
+ * through the cells' centres of mass, masses and quadrupoles, which the adjoint follows.
+ * Call it right after nbGravMapCUDA / nbStepSystemCUDA at the positions it was evaluated
+ * at, with the same context (FP64 precision). */
+NBodyCudaStatus nbGravVJPCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, const double* dAbar,
+                              double* dXbar, double* dMbar);
+
 /* ---- tree introspection (parity checks of nbMakeTree) ---- */
 NBodyCudaStatus nbMakeTreeCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st);
 NBodyCudaStatus nbTreeInfoCUDA(NBodyCudaState* st, NBodyCudaTreeInfo* info);

@@ -113,6 +113,7 @@ SIGNATURES = [
     ("nbStepSystemCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp]),
     ("nbRunStepsCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, ctypes.c_int]),
     ("nbMakeTreeCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp]),
+    ("nbGravVJPCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, _vp, _vp, _vp]),
     ("nbTreeInfoCUDA", ctypes.c_int, [_vp, ctypes.POINTER(TreeInfo)]),
     ("nbGetTreeCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("nbExtAccelerationCUDA", ctypes.c_int,

@@ -21,6 +21,10 @@ void nb_launch_direct_sample(const double* px, const double* py, const double* p
                              const double* mass, int n, const int* targets, int count,
                              double eps2, double* out, cudaStream_t s);
 double nb_fma_probe(int fp64, int numSMs, cudaStream_t s);
+void nb_launch_vjp(NbTreeBuffers& b, double* nodeBar, int capNodes, int maxDepth, int criterion,
+                   const NbWalkParams& wp, const NbPot& pot, const double* abar, double* xbar,
+                   double* mbar, int numSMs, cudaEvent_t walkStart, cudaEvent_t walkEnd,
+                   cudaStream_t s);
 void nb_launch_direct_fp64(const double* px, const double* py, const double* pz,
                            const double* mass, double* ax, double* ay, double* az, double* vx,
                            double* vy, double* vz, const NbWalkParams& wp, const NbPot& pot,
@@ -119,6 +123,9 @@ struct NBodyCudaState {
     float stepMs = 0.0f;
     int walkLaunches = 0;
     unsigned long long cBB = 0, cBC = 0, cVisit = 0, cWarpSteps = 0;
+    double* nodeBar = nullptr;          // adjoint: 10 doubles per node
+    int nodeBarCap = 0;
+    int lastCriterion = -1;             // criterion of the last force evaluation
 };
 
 template <typename T>
@@ -134,10 +141,16 @@ static void nb_free_nodes(NBodyCudaState* st)
     NbTreeBuffers& b = st->b;
     cudaFree(b.nodePM); cudaFree(b.nodeCrit); cudaFree(b.nodeLink); cudaFree(b.nodeQuad);
     cudaFree(b.nodeDepth); cudaFree(b.parent); cudaFree(b.nchild); cudaFree(b.arrive);
-    cudaFree(st->mx.hi); cudaFree(st->mx.lo); cudaFree(st->mx.q32);
+    cudaFree(b.nodeRange); b.nodeRange = nullptr;
+    cudaFree(st->mx.groups);
+    cudaFree(st->mx.hi); cudaFree(st->mx.lo); cudaFree(st->mx.q32); cudaFree(st->mx.child8);
     b.nodePM = nullptr; b.nodeCrit = nullptr; b.nodeLink = nullptr; b.nodeQuad = nullptr;
     b.nodeDepth = b.parent = b.nchild = b.arrive = nullptr;
+    int* stacks = st->mx.stacks;
+    const int wb = st->mx.walkBlocks;
     st->mx = NbMixedBuffers{};
+    st->mx.stacks = stacks;          // the walk stacks do not depend on the node count
+    st->mx.walkBlocks = wb;
     st->capNodes = 0;
 }
 
@@ -153,9 +166,12 @@ static NBodyCudaStatus nb_alloc_nodes(NBodyCudaState* st, int cap)
     NB_CHECK(nb_alloc(&b.parent, cap));
     NB_CHECK(nb_alloc(&b.nchild, cap));
     NB_CHECK(nb_alloc(&b.arrive, cap));
+    NB_CHECK(nb_alloc(&b.nodeRange, cap));
+    NB_CHECK(nb_alloc(&st->mx.groups, cap));
     NB_CHECK(nb_alloc(&st->mx.hi, cap));
     NB_CHECK(nb_alloc(&st->mx.lo, cap));
     NB_CHECK(nb_alloc(&st->mx.q32, 2 * (size_t) cap));
+    NB_CHECK(nb_alloc(&st->mx.child8, 2 * (size_t) cap));
     st->capNodes = cap;
     return NBODY_SUCCESS;
 }
@@ -175,6 +191,7 @@ static NBodyCudaStatus nb_alloc_bodies(NBodyCudaState* st, int n)
     NB_CHECK(nb_alloc(&b.sort.idxA, N)); NB_CHECK(nb_alloc(&b.sort.idxB, N));
     const int tiles = (int) ((N + 2047) / 2048);
     NB_CHECK(nb_alloc(&b.sort.hist, 256 * (size_t) tiles));
+    NB_CHECK(nb_alloc(&b.sort.histTmp, (size_t) nb_scan_tmp_ints(256 * tiles)));
     b.sort.capTiles = tiles;
     NB_CHECK(nb_alloc(&b.gx, N)); NB_CHECK(nb_alloc(&b.gy, N)); NB_CHECK(nb_alloc(&b.gz, N));
     NB_CHECK(nb_alloc(&b.delta, N)); NB_CHECK(nb_alloc(&b.cum, N));
@@ -191,12 +208,16 @@ static void nb_free_all(NBodyCudaState* st)
     double* d[] = {b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.ax, b.ay, b.az, b.mass, st->stage};
     for (double* p : d) cudaFree(p);
     cudaFree(b.sort.keyA); cudaFree(b.sort.keyB); cudaFree(b.sort.idxA); cudaFree(b.sort.idxB);
-    cudaFree(b.sort.hist);
+    cudaFree(b.sort.hist); cudaFree(b.sort.histTmp);
     cudaFree(b.gx); cudaFree(b.gy); cudaFree(b.gz);
     cudaFree(b.delta); cudaFree(b.cum); cudaFree(b.scanTmp); cudaFree(b.bodyNode);
     cudaFree(b.sc);
     cudaFree(st->aos);
     nb_free_nodes(st);
+    cudaFree(st->mx.stacks);
+    st->mx.stacks = nullptr;
+    cudaFree(st->nodeBar);
+    st->nodeBar = nullptr;
     if (st->scHost) cudaFreeHost(st->scHost);
     if (st->ev0) cudaEventDestroy(st->ev0);
     if (st->ev1) cudaEventDestroy(st->ev1);
@@ -300,9 +321,14 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
                           st->numSMs, s);
             nb_link_and_moments(b, n, st->capNodes, ctx->criterion, ctx->theta, ctx->useQuad, s);
             NB_CHECK(cudaEventRecord(st->ev0, s));
-            if (mixed)
+            if (mixed) {
+                if (!st->mx.stacks) {
+                    st->mx.walkBlocks = nb_mixed_walk_blocks(st->numSMs);
+                    NB_CHECK(nb_alloc(&st->mx.stacks, nb_mixed_stack_ints(st->mx.walkBlocks)));
+                }
                 nb_launch_walk_mixed(b, st->mx, st->capNodes, wp, pot, st->counting != 0,
                                      st->numSMs, s);
+            }
             else
                 nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px,
                                     b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
@@ -345,6 +371,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
         }
         if (st->treeIncest)
             out |= ctx->allowIncest ? NBODY_TREE_INCEST_NONFATAL : NBODY_TREE_INCEST_FATAL;
+        st->lastCriterion = ctx->criterion;
         return out;
     }
     g_lastError = "node capacity could not be grown";
@@ -602,6 +629,7 @@ NBodyCudaStatus nbMakeTreeCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st)
             continue;
         }
         st->haveTree = 1;
+        st->lastCriterion = ctx->criterion;
         return st->scHost->status;
     }
     return NBODY_CELL_OVERFLOW_ERROR;
@@ -728,6 +756,48 @@ NBodyCudaStatus nbDirectSampleCUDA(NBodyCudaState* st, double eps2, const int32_
     cudaFree(dt);
     cudaFree(da);
     if (e != cudaSuccess) return nb_cuda_fail(e, "nbDirectSampleCUDA");
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbGravVJPCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, const double* dAbar,
+                              double* dXbar, double* dMbar)
+{
+    if (!st || !dAbar || !dXbar) return NBODY_USER_ERROR;
+    std::string why;
+    NBodyCudaStatus rc = nb_check_ctx(ctx, why);
+    if (rc) { g_lastError = why; return rc; }
+    if (ctx->precision != NBCUDA_PRECISION_FP64) {
+        g_lastError = "the adjoint follows the FP64 walk";
+        return NBODY_UNSUPPORTED;
+    }
+    if (ctx->criterion != st->lastCriterion || (ctx->criterion != NBCUDA_EXACT && !st->haveTree)) {
+        g_lastError = "nbGravVJPCUDA needs a force evaluation with the same context first";
+        return NBODY_USER_ERROR;
+    }
+    NB_CHECK(cudaSetDevice(st->device));
+    if (ctx->criterion != NBCUDA_EXACT && st->nodeBarCap < st->capNodes) {
+        cudaFree(st->nodeBar);
+        st->nodeBar = nullptr;
+        NB_CHECK(cudaMalloc((void**) &st->nodeBar, 10 * sizeof(double) * (size_t) st->capNodes));
+        st->nodeBarCap = st->capNodes;
+    }
+    NbWalkParams wp{};
+    wp.eps2 = ctx->eps2;
+    wp.useQuad = ctx->useQuad;
+    wp.n = st->nbody;
+    NB_CHECK(cudaEventRecord(st->evS, st->stream));
+    nb_launch_vjp(st->b, st->nodeBar, st->capNodes, st->scHost->maxDepth, ctx->criterion, wp,
+                  nb_pot_from(ctx), dAbar, dXbar, dMbar, st->numSMs, st->ev0, st->ev1, st->stream);
+    NB_CHECK(cudaEventRecord(st->evE, st->stream));
+    NB_CHECK(cudaGetLastError());
+    NB_CHECK(cudaStreamSynchronize(st->stream));
+    // timings of the adjoint: walk = the walk-side kernel, step = the whole product
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, st->ev0, st->ev1);
+    st->walkMs = ms;
+    ms = 0.0f;
+    cudaEventElapsedTime(&ms, st->evS, st->evE);
+    st->stepMs = ms;
     return NBODY_SUCCESS;
 }
 

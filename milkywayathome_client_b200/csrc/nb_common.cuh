@@ -43,6 +43,8 @@ struct NbScalars {
     unsigned long long nBodyCell;
     unsigned long long nVisit;
     unsigned long long nWarpSteps;  // walk iterations summed over warps (SIMT utilisation)
+    int groupNext;                  // next group for the persistent group walk
+    int nGroups;                    // walk groups formed for the mixed walk
 };
 
 // Potential parameters in constant-friendly POD form.
@@ -111,6 +113,7 @@ struct NbSortBuffers {
     unsigned long long* keyA; unsigned long long* keyB;
     unsigned int* idxA; unsigned int* idxB;
     unsigned int* hist;    // 256 * nTiles
+    int* histTmp;          // tile sums of the scan over hist
     int capTiles;
 };
 // Sorts (keyA, idxA) by key in place (result in keyA/idxA); n items.
@@ -123,6 +126,7 @@ struct NbTreeBuffers {
     int *delta, *cum, *scanTmp, *bodyNode;
     double4* nodePM; double* nodeCrit; int2* nodeLink; double* nodeQuad;
     int *nodeDepth, *parent, *nchild, *arrive;
+    int2* nodeRange;   // first and last sorted body of every node's subtree
     NbScalars* sc;
 };
 
@@ -131,7 +135,13 @@ struct NbMixedBuffers {
     float4* hi;    // {hi.x, hi.y, hi.z, rcrit2 (-inf for bodies)}
     float4* lo;    // {lo.x, lo.y, lo.z, mass}
     float4* q32;   // 2 per node: {xx, xy, xz, yy}, {yz, zz, 0, 0}
+    int4* child8;  // 2 per node: up to 8 child indices of a cell (-1 = none)
+    int* stacks;   // per resident warp: the group walk's depth-first stack
+    int2* groups;  // walk groups: first sorted body, body count (<= 32)
+    int walkBlocks;
 };
+int nb_mixed_walk_blocks(int numSMs);
+size_t nb_mixed_stack_ints(int blocks);
 
 void nb_build_tree(NbTreeBuffers& b, int n, int criterion, double theta, int useQuad, int drift,
                    double dt, int numSMs, cudaStream_t s);

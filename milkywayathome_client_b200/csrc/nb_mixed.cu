@@ -16,8 +16,6 @@
 #include "nb_common.cuh"
 #include "nb_potential.cuh"
 
-constexpr int MIXED_THREADS = 256;
-constexpr int NB_MIXED_FLUSH = 16;
 
 __device__ __forceinline__ void nb_split(double v, float& hi, float& lo)
 {
@@ -29,7 +27,8 @@ __device__ __forceinline__ void nb_split(double v, float& hi, float& lo)
 __global__ void k_pack_f32(const double4* __restrict__ nodePM, const double* __restrict__ nodeCrit,
                            const int2* __restrict__ nodeLink, const double* __restrict__ nodeQuad,
                            float4* __restrict__ nodeHi, float4* __restrict__ nodeLo,
-                           float4* __restrict__ nodeQ32, const NbScalars* __restrict__ sc)
+                           float4* __restrict__ nodeQ32, int4* __restrict__ child8,
+                           const NbScalars* __restrict__ sc)
 {
     if (nb_failed(sc)) return;
     const int nNodes = sc->nNodes;
@@ -45,6 +44,15 @@ __global__ void k_pack_f32(const double4* __restrict__ nodePM, const double* __r
         const float crit = isBody ? __int_as_float(0xff800000) : __double2float_rn(nodeCrit[k]);
         nodeHi[k] = make_float4(hx, hy, hz, crit);
         nodeLo[k] = make_float4(lx, ly, lz, __double2float_rn(p.w));
+        if (!isBody) {
+            // the children of a cell: k+1, then Next() up to Next(k) (threadTree order)
+            int ch[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+            const int stop = nodeLink[k].x;
+            int c = k + 1;
+            for (int m = 0; m < 8 && c < stop; ++m) { ch[m] = c; c = nodeLink[c].x; }
+            child8[2 * (size_t) k] = make_int4(ch[0], ch[1], ch[2], ch[3]);
+            child8[2 * (size_t) k + 1] = make_int4(ch[4], ch[5], ch[6], ch[7]);
+        }
         const double* Q = nodeQuad + 6 * (size_t) k;
         if (isBody) {
             nodeQ32[2 * (size_t) k] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -57,102 +65,281 @@ __global__ void k_pack_f32(const double4* __restrict__ nodePM, const double* __r
     }
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(MIXED_THREADS)
-k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeLo,
-             const float4* __restrict__ nodeQ32, const int2* __restrict__ nodeLink,
-             const double4* __restrict__ nodePM,
-             const unsigned int* __restrict__ order, const double* __restrict__ px,
-             const double* __restrict__ py, const double* __restrict__ pz,
-             double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
-             double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
-             NbWalkParams wp, NbPot pot, NbScalars* __restrict__ sc)
+// ---- group walk -------------------------------------------------------------------------
+// A warp walks for a group of <= 32 bodies of one compact cell (k_groups).  Cells are tested
+// against the group's bounding box: a cell is accepted when |CoM - box|^2 >= rcrit2, which
+// implies the reference's per-body test |CoM - x|^2 >= rcrit2 (nbody/src/nbody_grav.c:58) for
+// every body x of the group, so the group opens every cell any of its bodies would open.
+//
+// Walk: warp-parallel depth-first traversal.  Each step pops up to 32 nodes from the warp's
+// stack (one per lane), tests them at once, appends visited bodies and accepted cells to two
+// per-warp interaction lists in shared memory and pushes the children of opened cells
+// (explicit child lists built by k_pack_f32).  Popping from the top keeps the stack sorted by
+// depth, so at most 8 x 32 nodes of any one depth are ever on it: 256 x 63 levels bounds it
+// (NB_GROUP_STACK).  A full list is evaluated by all 32 lanes at once (each lane for its own
+// body, entries read as shared-memory broadcasts), FP32 with FMA and rsqrtf; partial sums go
+// into FP64 accumulators after every list.  Persistent warps take groups from a counter.
+constexpr int GROUP_WARPS = 4;
+constexpr int GROUP_THREADS = 32 * GROUP_WARPS;
+constexpr int LIST_CAP = 64;
+constexpr int NB_GROUP_STACK = 16384;     // >= 256 x 63 + 32
+
+// Interaction lists in shared memory, one float4 array per field so that the 32 lanes'
+// appends hit consecutive 16-byte slots (no bank conflicts) while the evaluation reads each
+// entry as broadcasts.  Cell entry: {hi, mass} {lo, qxx} {qxy, qxz, qyy, qyz} {qzz, -, -, -};
+// body entry: {hi, mass} {lo, -}.
+struct CellList { float4 a[LIST_CAP], b[LIST_CAP], c[LIST_CAP], d[LIST_CAP]; };
+struct BodyList { float4 a[LIST_CAP], b[LIST_CAP]; };
+
+__device__ __forceinline__ void nb_eval_bodies(const BodyList& list, int n, float bhx, float bhy,
+                                               float bhz, float blx, float bly, float blz,
+                                               float eps2, float& fx, float& fy, float& fz)
+{
+    for (int e = 0; e < n; ++e) {
+        const float4 a = list.a[e], b = list.b[e];
+        const float dx = (a.x - bhx) + (b.x - blx);
+        const float dy = (a.y - bhy) + (b.y - bly);
+        const float dz = (a.z - bhz) + (b.z - blz);
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+        const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
+        const float mor3 = a.w * rinv * rinv * rinv;
+        fx = fmaf(mor3, dx, fx);
+        fy = fmaf(mor3, dy, fy);
+        fz = fmaf(mor3, dz, fz);
+    }
+}
+
+__device__ __forceinline__ void nb_eval_cells(const CellList& list, int n, float bhx, float bhy,
+                                              float bhz, float blx, float bly, float blz,
+                                              float eps2, bool useQuad, float& fx, float& fy,
+                                              float& fz)
+{
+    for (int e = 0; e < n; ++e) {
+        const float4 a = list.a[e], b = list.b[e];
+        const float dx = (a.x - bhx) + (b.x - blx);
+        const float dy = (a.y - bhy) + (b.y - bly);
+        const float dz = (a.z - bhz) + (b.z - blz);
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+        const float rinv = rsqrtf(r2);
+        const float rinv2 = rinv * rinv;
+        const float mor3 = a.w * rinv * rinv2;
+        fx = fmaf(mor3, dx, fx);
+        fy = fmaf(mor3, dy, fy);
+        fz = fmaf(mor3, dz, fz);
+        if (useQuad) {
+            const float4 c = list.c[e], d = list.d[e];
+            const float qxx = b.w, qxy = c.x, qxz = c.y, qyy = c.z, qyz = c.w, qzz = d.x;
+            const float qdx = fmaf(qxz, dz, fmaf(qxy, dy, qxx * dx));
+            const float qdy = fmaf(qyz, dz, fmaf(qyy, dy, qxy * dx));
+            const float qdz = fmaf(qzz, dz, fmaf(qyz, dy, qxz * dx));
+            const float drQdr = fmaf(qdz, dz, fmaf(qdy, dy, qdx * dx));
+            const float dr5inv = rinv2 * rinv2 * rinv;
+            const float phiQ = 2.5f * dr5inv * drQdr * rinv2;
+            fx = fmaf(phiQ, dx, fmaf(-dr5inv, qdx, fx));
+            fy = fmaf(phiQ, dy, fmaf(-dr5inv, qdy, fy));
+            fz = fmaf(phiQ, dz, fmaf(-dr5inv, qdz, fz));
+        }
+    }
+}
+
+// Walk groups: contiguous runs of <= 32 sorted bodies that share a compact cell.  Every cell
+// with more than 32 bodies lays out its direct children in octant order and packs the
+// consecutive ones holding <= 32 bodies (cells or single bodies) into groups of <= 32; a
+// root with <= 32 bodies is one group; test particles (not in the tree, sorted last) form
+// groups of 32 consecutive bodies.  The groups partition the sorted bodies.
+__global__ void k_groups(const int2* __restrict__ nodeLink, const int2* __restrict__ nodeRange,
+                         int2* __restrict__ groups, int n, NbScalars* __restrict__ sc)
 {
     if (nb_failed(sc)) return;
-    const int end = sc->nNodes;
-    const int lane = threadIdx.x & 31;
-    const int i = (int) ((blockIdx.x * (unsigned) blockDim.x + threadIdx.x) >> 5) * 32 + lane;
-    const bool valid = i < wp.n;
-    const unsigned j = valid ? order[i] : 0u;
-    const double x0 = valid ? px[j] : 0.0, y0 = valid ? py[j] : 0.0, z0 = valid ? pz[j] : 0.0;
+    const int nNodes = sc->nNodes, m = sc->nTree;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = gridDim.x * blockDim.x;
+    for (int c = tid; c < nNodes; c += stride) {
+        const int2 l = nodeLink[c];
+        if (l.y >= 0) continue;                              // bodies are handled by parents
+        const int2 r = nodeRange[c];
+        const int cnt = r.y - r.x + 1;
+        if (cnt <= 32) {
+            if (c == 0 && cnt > 0) groups[atomicAdd(&sc->nGroups, 1)] = make_int2(r.x, cnt);
+            continue;
+        }
+        int gFirst = -1, gCount = 0;
+        for (int k = c + 1; k < l.x; k = nodeLink[k].x) {
+            const int2 rk = nodeRange[k];
+            const int ck = rk.y - rk.x + 1;
+            if (ck > 32) {                                   // descended by its own thread
+                if (gCount) groups[atomicAdd(&sc->nGroups, 1)] = make_int2(gFirst, gCount);
+                gCount = 0;
+                continue;
+            }
+            if (gCount && gCount + ck > 32) {
+                groups[atomicAdd(&sc->nGroups, 1)] = make_int2(gFirst, gCount);
+                gCount = 0;
+            }
+            if (!gCount) gFirst = rk.x;
+            gCount += ck;
+        }
+        if (gCount) groups[atomicAdd(&sc->nGroups, 1)] = make_int2(gFirst, gCount);
+    }
+    for (int t = tid; m + 32 * t < n; t += stride)
+        groups[atomicAdd(&sc->nGroups, 1)] = make_int2(m + 32 * t, min(32, n - m - 32 * t));
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(GROUP_THREADS)
+k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeLo,
+             const float4* __restrict__ nodeQ32, const int4* __restrict__ child8,
+             const double4* __restrict__ nodePM, const unsigned int* __restrict__ order,
+             const double* __restrict__ px, const double* __restrict__ py,
+             const double* __restrict__ pz, const double* __restrict__ mass,
+             double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
+             double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
+             int* __restrict__ stacks, const int2* __restrict__ groups, NbWalkParams wp,
+             NbPot pot, NbScalars* __restrict__ sc)
+{
+    __shared__ CellList sCells[GROUP_WARPS];
+    __shared__ BodyList sBodies[GROUP_WARPS];
+    if (nb_failed(sc)) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    CellList& cells = sCells[warp];
+    BodyList& bodies = sBodies[warp];
+    int* stack = stacks + (size_t) (blockIdx.x * GROUP_WARPS + warp) * NB_GROUP_STACK;
+    const unsigned ltMask = (1u << lane) - 1u;
+    const int nGroups = sc->nGroups;
     const double4 root = nodePM[0];
-    float bhx, bhy, bhz, blx, bly, blz;
-    nb_split(x0 - root.x, bhx, blx);
-    nb_split(y0 - root.y, bhy, bly);
-    nb_split(z0 - root.z, bhz, blz);
     const float eps2 = (float) wp.eps2;
     const bool useQuad = wp.useQuad != 0;
-    int ptr = valid ? 0 : end;
-    double accx = 0.0, accy = 0.0, accz = 0.0;
-    float fx = 0.f, fy = 0.f, fz = 0.f;
-    int pending = 0;
-    bool metSelf = false;
+    const float inf = __int_as_float(0x7f800000);
     unsigned long long cVisit = 0, cBB = 0, cBC = 0, cSteps = 0;
+
     for (;;) {
-        const int q = __reduce_min_sync(NB_FULL_MASK, ptr);
-        if (q >= end) break;
-        if (COUNT) ++cSteps;
-        if (ptr != q) continue;
-        const float4 hi = nodeHi[q];
-        const float4 lo = nodeLo[q];
-        const int2 link = nodeLink[q];
-        const float dx = (hi.x - bhx) + (lo.x - blx);
-        const float dy = (hi.y - bhy) + (lo.y - bly);
-        const float dz = (hi.z - bhz) + (lo.z - blz);
-        float drSq = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-        if (COUNT) ++cVisit;
-        if (drSq >= hi.w) {        // bodies carry -inf: always accepted
-            ptr = link.x;
-            const bool isBody = link.y >= 0;
-            if (isBody && (unsigned) link.y == j) { metSelf = true; continue; }
-            if (COUNT) { if (isBody) ++cBB; else ++cBC; }
-            drSq += eps2;
-            const float rinv = rsqrtf(drSq);
-            const float rinv2 = rinv * rinv;
-            const float mor3 = lo.w * rinv * rinv2;
-            fx = fmaf(mor3, dx, fx);
-            fy = fmaf(mor3, dy, fy);
-            fz = fmaf(mor3, dz, fz);
-            if (useQuad && !isBody) {
-                const float4 qa = nodeQ32[2 * (size_t) q];
-                const float4 qb = nodeQ32[2 * (size_t) q + 1];
-                const float qxx = qa.x, qxy = qa.y, qxz = qa.z, qyy = qa.w, qyz = qb.x, qzz = qb.y;
-                const float qdx = fmaf(qxz, dz, fmaf(qxy, dy, qxx * dx));
-                const float qdy = fmaf(qyz, dz, fmaf(qyy, dy, qxy * dx));
-                const float qdz = fmaf(qzz, dz, fmaf(qyz, dy, qxz * dx));
-                const float drQdr = fmaf(qdz, dz, fmaf(qdy, dy, qdx * dx));
-                const float dr5inv = rinv2 * rinv2 * rinv;
-                const float phiQ = 2.5f * dr5inv * drQdr * rinv2;
-                fx = fmaf(phiQ, dx, fmaf(-dr5inv, qdx, fx));
-                fy = fmaf(phiQ, dy, fmaf(-dr5inv, qdy, fy));
-                fz = fmaf(phiQ, dz, fmaf(-dr5inv, qdz, fz));
+        int g = 0;
+        if (lane == 0) g = atomicAdd(&sc->groupNext, 1);
+        g = __shfl_sync(NB_FULL_MASK, g, 0);
+        if (g >= nGroups) break;
+        const int2 grp = groups[g];
+        const int i = grp.x + lane;
+        const bool valid = lane < grp.y;
+        const unsigned j = valid ? order[i] : 0u;
+        const double x0 = valid ? px[j] : 0.0, y0 = valid ? py[j] : 0.0, z0 = valid ? pz[j] : 0.0;
+        float bhx, bhy, bhz, blx, bly, blz;
+        nb_split(x0 - root.x, bhx, blx);
+        nb_split(y0 - root.y, bhy, bly);
+        nb_split(z0 - root.z, bhz, blz);
+        float mnx = valid ? bhx + blx : inf, mny = valid ? bhy + bly : inf, mnz = valid ? bhz + blz : inf;
+        float mxx = valid ? bhx + blx : -inf, mxy = valid ? bhy + bly : -inf, mxz = valid ? bhz + blz : -inf;
+        for (int o = 16; o > 0; o >>= 1) {
+            mnx = fminf(mnx, __shfl_xor_sync(NB_FULL_MASK, mnx, o));
+            mny = fminf(mny, __shfl_xor_sync(NB_FULL_MASK, mny, o));
+            mnz = fminf(mnz, __shfl_xor_sync(NB_FULL_MASK, mnz, o));
+            mxx = fmaxf(mxx, __shfl_xor_sync(NB_FULL_MASK, mxx, o));
+            mxy = fmaxf(mxy, __shfl_xor_sync(NB_FULL_MASK, mxy, o));
+            mxz = fmaxf(mxz, __shfl_xor_sync(NB_FULL_MASK, mxz, o));
+        }
+        const float cx = 0.5f * (mnx + mxx), cy = 0.5f * (mny + mxy), cz = 0.5f * (mnz + mxz);
+        const float hx = 0.5f * (mxx - mnx), hy = 0.5f * (mxy - mny), hz = 0.5f * (mxz - mnz);
+        double accx = 0.0, accy = 0.0, accz = 0.0;
+        float fx = 0.f, fy = 0.f, fz = 0.f;
+        int nC = 0, nB = 0;
+        if (lane == 0) stack[0] = 0;      // the root
+        int top = 1;
+        __syncwarp();
+        while (top > 0) {
+            const int take = min(32, top);
+            const int base = top - take;
+            const int k = lane < take ? stack[base + lane] : -1;
+            top = base;
+            float4 hi = make_float4(0.f, 0.f, 0.f, 0.f), lo = hi;
+            bool isBody = false, accCell = false, openCell = false;
+            if (k >= 0) {
+                hi = nodeHi[k];
+                lo = nodeLo[k];
+                isBody = hi.w == -inf;          // bodies carry rcrit2 = -inf
+                if (!isBody) {
+                    const float ddx = fmaxf(fabsf((hi.x + lo.x) - cx) - hx, 0.f);
+                    const float ddy = fmaxf(fabsf((hi.y + lo.y) - cy) - hy, 0.f);
+                    const float ddz = fmaxf(fabsf((hi.z + lo.z) - cz) - hz, 0.f);
+                    const float d2 = fmaf(ddz, ddz, fmaf(ddy, ddy, ddx * ddx));
+                    accCell = d2 >= hi.w;
+                    openCell = !accCell;
+                }
             }
-            if (++pending == NB_MIXED_FLUSH) {
+            int4 c0 = make_int4(-1, -1, -1, -1), c1 = c0;
+            if (openCell) { c0 = child8[2 * (size_t) k]; c1 = child8[2 * (size_t) k + 1]; }
+            const unsigned bodyMask = __ballot_sync(NB_FULL_MASK, isBody);
+            const unsigned cellMask = __ballot_sync(NB_FULL_MASK, accCell);
+            if (COUNT) {
+                ++cSteps;
+                cVisit += 32ull * (unsigned) __popc(__ballot_sync(NB_FULL_MASK, k >= 0));
+                cBB += 32ull * __popc(bodyMask);
+                cBC += 32ull * __popc(cellMask);
+            }
+            if (nB + __popc(bodyMask) > LIST_CAP) {
+                nb_eval_bodies(bodies, nB, bhx, bhy, bhz, blx, bly, blz, eps2, fx, fy, fz);
+                nB = 0;
+                __syncwarp();
+            }
+            if (nC + __popc(cellMask) > LIST_CAP) {
+                nb_eval_cells(cells, nC, bhx, bhy, bhz, blx, bly, blz, eps2, useQuad, fx, fy, fz);
+                nC = 0;
+                __syncwarp();
                 accx += (double) fx; accy += (double) fy; accz += (double) fz;
                 fx = fy = fz = 0.f;
-                pending = 0;
             }
-        } else {
-            ptr = q + 1;
+            if (isBody) {
+                const int e = nB + __popc(bodyMask & ltMask);
+                bodies.a[e] = make_float4(hi.x, hi.y, hi.z, lo.w);
+                bodies.b[e] = make_float4(lo.x, lo.y, lo.z, 0.f);
+            }
+            if (accCell) {
+                const int e = nC + __popc(cellMask & ltMask);
+                const float4 qa = nodeQ32[2 * (size_t) k], qb = nodeQ32[2 * (size_t) k + 1];
+                cells.a[e] = make_float4(hi.x, hi.y, hi.z, lo.w);
+                cells.b[e] = make_float4(lo.x, lo.y, lo.z, qa.x);
+                cells.c[e] = make_float4(qa.y, qa.z, qa.w, qb.x);
+                cells.d[e] = make_float4(qb.y, 0.f, 0.f, 0.f);
+            }
+            nB += __popc(bodyMask);
+            nC += __popc(cellMask);
+            // push the children of opened cells (warp prefix sum of their counts)
+            const int nch = (c0.x >= 0) + (c0.y >= 0) + (c0.z >= 0) + (c0.w >= 0) +
+                            (c1.x >= 0) + (c1.y >= 0) + (c1.z >= 0) + (c1.w >= 0);
+            int incl = nch;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(NB_FULL_MASK, incl, o);
+                if (lane >= o) incl += u;
+            }
+            const int total = __shfl_sync(NB_FULL_MASK, incl, 31);
+            if (top + total > NB_GROUP_STACK) {      // cannot happen (depth-sorted stack bound)
+                if (lane == 0) nb_raise(sc, NBODY_CAPABILITY_ERROR);
+                top = 0;
+                break;
+            }
+            int w = top + incl - nch;
+            const int cl[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+            for (int m = 0; m < 8; ++m)
+                if (cl[m] >= 0) stack[w++] = cl[m];
+            top += total;
+            __syncwarp();
+        }
+        __syncwarp();
+        nb_eval_bodies(bodies, nB, bhx, bhy, bhz, blx, bly, blz, eps2, fx, fy, fz);
+        nb_eval_cells(cells, nC, bhx, bhy, bhz, blx, bly, blz, eps2, useQuad, fx, fy, fz);
+        __syncwarp();
+        accx += (double) fx; accy += (double) fy; accz += (double) fz;
+        if (valid) {
+            // test particles are not in the tree and never meet themselves (nbody_grav.c:111-118)
+            if (mass[j] == 0.0) atomicOr(&sc->incest, 1);
+            nb_finish_body(pot, wp, j, x0, y0, z0, accx, accy, accz, ax, ay, az, vx, vy, vz);
         }
     }
-    accx += (double) fx; accy += (double) fy; accz += (double) fz;
-    if (COUNT) {
-        for (int o = 16; o > 0; o >>= 1) {
-            cVisit += __shfl_xor_sync(NB_FULL_MASK, cVisit, o);
-            cBB += __shfl_xor_sync(NB_FULL_MASK, cBB, o);
-            cBC += __shfl_xor_sync(NB_FULL_MASK, cBC, o);
-        }
-        if (lane == 0) {
-            atomicAdd(&sc->nWarpSteps, cSteps);
-            atomicAdd(&sc->nVisit, cVisit);
-            atomicAdd(&sc->nBodyBody, cBB);
-            atomicAdd(&sc->nBodyCell, cBC);
-        }
+    if (COUNT && lane == 0) {
+        atomicAdd(&sc->nWarpSteps, cSteps);
+        atomicAdd(&sc->nVisit, cVisit);
+        atomicAdd(&sc->nBodyBody, cBB);
+        atomicAdd(&sc->nBodyCell, cBC);
     }
-    if (!valid) return;
-    if (!metSelf) atomicOr(&sc->incest, 1);
-    nb_finish_body(pot, wp, j, x0, y0, z0, accx, accy, accz, ax, ay, az, vx, vy, vz);
 }
 
 void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int capNodes,
@@ -160,18 +347,33 @@ void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int c
                           cudaStream_t s)
 {
     k_pack_f32<<<min((capNodes + 255) / 256, numSMs * 16), 256, 0, s>>>(
-        b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, m.hi, m.lo, m.q32, b.sc);
-    nb_count_launch();
-    const int warps = (wp.n + 31) / 32;
-    const int blocks = (warps * 32 + MIXED_THREADS - 1) / MIXED_THREADS;
-    if (blocks <= 0) return;
+        b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, m.hi, m.lo, m.q32, m.child8, b.sc);
+    k_groups<<<min((capNodes + 255) / 256, numSMs * 16), 256, 0, s>>>(b.nodeLink, b.nodeRange,
+                                                                       m.groups, wp.n, b.sc);
+    nb_count_launch(2);
+    if (wp.n <= 0) return;
+    const int blocks = m.walkBlocks;
     if (count)
-        k_walk_mixed<true><<<blocks, MIXED_THREADS, 0, s>>>(m.hi, m.lo, m.q32, b.nodeLink, b.nodePM,
-                                                            b.sort.idxA, b.px, b.py, b.pz, b.ax, b.ay,
-                                                            b.az, b.vx, b.vy, b.vz, wp, pot, b.sc);
+        k_walk_mixed<true><<<blocks, GROUP_THREADS, 0, s>>>(m.hi, m.lo, m.q32, m.child8, b.nodePM,
+                                                            b.sort.idxA, b.px, b.py, b.pz, b.mass,
+                                                            b.ax, b.ay, b.az, b.vx, b.vy, b.vz,
+                                                            m.stacks, m.groups, wp, pot, b.sc);
     else
-        k_walk_mixed<false><<<blocks, MIXED_THREADS, 0, s>>>(m.hi, m.lo, m.q32, b.nodeLink, b.nodePM,
-                                                             b.sort.idxA, b.px, b.py, b.pz, b.ax, b.ay,
-                                                             b.az, b.vx, b.vy, b.vz, wp, pot, b.sc);
+        k_walk_mixed<false><<<blocks, GROUP_THREADS, 0, s>>>(m.hi, m.lo, m.q32, m.child8, b.nodePM,
+                                                             b.sort.idxA, b.px, b.py, b.pz, b.mass,
+                                                             b.ax, b.ay, b.az, b.vx, b.vy, b.vz,
+                                                             m.stacks, m.groups, wp, pot, b.sc);
     nb_count_launch();
 }
+
+// Persistent grid of the group walk: as many blocks as fit on the device at once.
+int nb_mixed_walk_blocks(int numSMs)
+{
+    int perSM = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_walk_mixed<false>, GROUP_THREADS, 0)
+            != cudaSuccess || perSM < 1)
+        perSM = 1;
+    return perSM * numSMs;
+}
+
+size_t nb_mixed_stack_ints(int blocks) { return (size_t) blocks * GROUP_WARPS * NB_GROUP_STACK; }

@@ -4,9 +4,9 @@
 // (nbody/kernels/nbody_kernels.cl:898-1159): bodies are ordered by octree path once and
 // the tree is derived from the sorted order without locks or spin-waits.
 //
-// Each of the 8 passes sorts by one 8-bit digit in three kernels: per-tile digit
-// histograms, one exclusive scan over the (digit, tile) table, and a stable scatter that
-// ranks keys inside a tile with warp match/ballot.  HBM-bound: a pass reads and writes
+// Each of the 8 passes sorts by one 8-bit digit: per-tile digit histograms, an exclusive
+// scan of the (digit, tile) table (three coalesced phases), and a stable scatter that ranks
+// keys inside a tile with warp match/ballot.  HBM-bound: a pass reads and writes
 // 12 bytes per key.
 #include "nb_common.cuh"
 
@@ -32,33 +32,6 @@ k_rs_hist(const unsigned long long* __restrict__ keys, int n, int shift,
     }
     __syncthreads();
     hist[threadIdx.x * nTiles + blockIdx.x] = cnt[threadIdx.x];
-}
-
-// Exclusive scan of hist (len entries, digit-major) in place by one block.
-constexpr int SC_THREADS = 1024;
-__global__ void __launch_bounds__(SC_THREADS)
-k_rs_scan(unsigned int* __restrict__ hist, int len)
-{
-    __shared__ unsigned int part[SC_THREADS];
-    const int per = (len + SC_THREADS - 1) / SC_THREADS;
-    const int lo = threadIdx.x * per;
-    const int hi = min(lo + per, len);
-    unsigned int s = 0;
-    for (int i = lo; i < hi; ++i) s += hist[i];
-    part[threadIdx.x] = s;
-    __syncthreads();
-    for (int off = 1; off < SC_THREADS; off <<= 1) {
-        unsigned int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
-    }
-    unsigned int run = part[threadIdx.x] - s;    // exclusive prefix of this chunk
-    for (int i = lo; i < hi; ++i) {
-        unsigned int v = hist[i];
-        hist[i] = run;
-        run += v;
-    }
 }
 
 __global__ void __launch_bounds__(RS_THREADS)
@@ -137,6 +110,7 @@ __device__ __forceinline__ int block_inclusive_scan(int v, int* sh)
     return r;
 }
 
+template <bool EXCLUSIVE>
 __global__ void __launch_bounds__(PS_THREADS)
 k_ps_tile(int* __restrict__ data, int n, int* __restrict__ tileSums)
 {
@@ -146,9 +120,9 @@ k_ps_tile(int* __restrict__ data, int n, int* __restrict__ tileSums)
     int s = 0;
 #pragma unroll
     for (int k = 0; k < PS_ITEMS; ++k) {
-        v[k] = base + k < n ? data[base + k] : 0;
-        s += v[k];
-        v[k] = s;
+        const int x = base + k < n ? data[base + k] : 0;
+        v[k] = EXCLUSIVE ? s : s + x;
+        s += x;
     }
     int incl = block_inclusive_scan(s, sh);
     int excl = incl - s;
@@ -199,9 +173,14 @@ void nb_radix_sort(NbSortBuffers& b, int n, cudaStream_t s)
     for (int pass = 0; pass < 8; ++pass) {
         const int shift = pass * 8;
         k_rs_hist<<<nTiles, RS_THREADS, 0, s>>>(kin, n, shift, b.hist, nTiles);
-        k_rs_scan<<<1, SC_THREADS, 0, s>>>(b.hist, 256 * nTiles);
+        // exclusive scan of the (digit, tile) table, three coalesced phases
+        const int len = 256 * nTiles;
+        const int scanTiles = (len + PS_TILE - 1) / PS_TILE;
+        k_ps_tile<true><<<scanTiles, PS_THREADS, 0, s>>>((int*) b.hist, len, b.histTmp);
+        k_ps_top<<<1, PS_THREADS, 0, s>>>(b.histTmp, scanTiles);
+        k_ps_apply<<<scanTiles, PS_THREADS, 0, s>>>((int*) b.hist, len, b.histTmp);
         k_rs_scatter<<<nTiles, RS_THREADS, 0, s>>>(kin, iin, kout, iout, n, shift, b.hist, nTiles);
-        nb_count_launch(3);
+        nb_count_launch(5);
         unsigned long long* tk = kin; kin = kout; kout = tk;
         unsigned int* ti = iin; iin = iout; iout = ti;
     }
@@ -214,7 +193,7 @@ void nb_inclusive_scan(int* data, int n, int* tmp, cudaStream_t s)
 {
     if (n <= 0) return;
     const int nTiles = (n + PS_TILE - 1) / PS_TILE;
-    k_ps_tile<<<nTiles, PS_THREADS, 0, s>>>(data, n, tmp);
+    k_ps_tile<false><<<nTiles, PS_THREADS, 0, s>>>(data, n, tmp);
     k_ps_top<<<1, PS_THREADS, 0, s>>>(tmp, nTiles);
     k_ps_apply<<<nTiles, PS_THREADS, 0, s>>>(data, n, tmp);
     nb_count_launch(3);

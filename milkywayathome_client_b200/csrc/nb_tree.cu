@@ -272,7 +272,7 @@ __global__ void k_emit_bodies(const double* __restrict__ px, const double* __res
                               const int* __restrict__ cum, double4* __restrict__ nodePM,
                               double* __restrict__ nodeCrit, int2* __restrict__ nodeLink,
                               int* __restrict__ nodeDepth, int* __restrict__ bodyNode,
-                              NbScalars* __restrict__ sc)
+                              int2* __restrict__ nodeRange, NbScalars* __restrict__ sc)
 {
     if (nb_failed(sc)) return;
     const int m = sc->nTree;
@@ -283,6 +283,7 @@ __global__ void k_emit_bodies(const double* __restrict__ px, const double* __res
         nodePM[p] = make_double4(px[j], py[j], pz[j], mass[j]);
         nodeCrit[p] = 0.0;
         nodeLink[p] = make_int2(p + 1, (int) j);
+        nodeRange[p] = make_int2(i, i);
         const int lev = max(0, max(nb_delta_or(delta, i - 1, m), nb_delta_or(delta, i, m)));
         nodeDepth[p] = lev + 1;
         bodyNode[i] = p;
@@ -354,7 +355,8 @@ __global__ void k_emit_cells(const long long* __restrict__ gx, const long long* 
                              const int* __restrict__ cum, double4* __restrict__ nodePM,
                              double* __restrict__ nodeCrit, int2* __restrict__ nodeLink,
                              int* __restrict__ nodeDepth, double* __restrict__ nodeQuad,
-                             int criterion, double theta, NbScalars* __restrict__ sc)
+                             int2* __restrict__ nodeRange, int criterion, double theta,
+                             NbScalars* __restrict__ sc)
 {
     if (nb_failed(sc)) return;
     const int m = sc->nTree;
@@ -379,12 +381,13 @@ __global__ void k_emit_cells(const long long* __restrict__ gx, const long long* 
         }
         for (int D = dPrev + 1; D <= dHere; ++D) {
             const int p = a + cellsBefore + (D - dPrev - 1);
-            int next;
-            if (m <= 1) next = m + 1;
+            int next, last;
+            if (m <= 1) { next = m + 1; last = m - 1; }
             else {
-                const int b = nb_range_end(gx, gy, gz, a, D, m);
-                next = b + nb_cells_before_body(cum, b, m) + 1;
+                last = nb_range_end(gx, gy, gz, a, D, m);
+                next = last + nb_cells_before_body(cum, last, m) + 1;
             }
+            nodeRange[p] = make_int2(a, last);
             nodePM[p] = make_double4(cx, cy, cz, 0.0);
             nodeCrit[p] = 0.0;
             nodeLink[p] = make_int2(next, -1);
@@ -549,9 +552,10 @@ void nb_build_tree(NbTreeBuffers& b, int n, int criterion, double theta, int use
     if (n > 1) nb_inclusive_scan(b.cum, n - 1, b.scanTmp, s);
     k_count_nodes<<<1, 1, 0, s>>>(b.cum, b.sc);
     k_emit_bodies<<<g, T, 0, s>>>(b.px, b.py, b.pz, b.mass, b.sort.idxA, b.delta, b.cum, b.nodePM,
-                                  b.nodeCrit, b.nodeLink, b.nodeDepth, b.bodyNode, b.sc);
+                                  b.nodeCrit, b.nodeLink, b.nodeDepth, b.bodyNode, b.nodeRange, b.sc);
     k_emit_cells<<<g, T, 0, s>>>(b.gx, b.gy, b.gz, b.delta, b.cum, b.nodePM, b.nodeCrit,
-                                 b.nodeLink, b.nodeDepth, b.nodeQuad, criterion, theta, b.sc);
+                                 b.nodeLink, b.nodeDepth, b.nodeQuad, b.nodeRange, criterion, theta,
+                                 b.sc);
     nb_count_launch(3);
 }
 

@@ -13,7 +13,7 @@
 #include "nb_common.cuh"
 #include "nb_potential.cuh"
 
-constexpr int WALK_THREADS = 256;
+constexpr int WALK_THREADS = 128;
 
 template <bool COUNT>
 __global__ void __launch_bounds__(WALK_THREADS)

@@ -276,17 +276,54 @@ def test_marshal_reference_body_records(dwarf_small):
     assert np.array_equal(rec["id"], np.arange(n)) and bits_equal(rec["mass"], mass)
 
 
-def test_mixed_precision_close_to_fp64(dwarf_small):
-    """The mixed form walks the same tree in FP32 with FP64 accumulation: its accelerations
-    stay within 1e-5 relative (median 1e-7) of the FP64 walk."""
+def test_mixed_precision_error_vs_direct_summation(dwarf_small):
+    """The mixed form (FP32 group walk, FP64 accumulation) adds at most 1 % to the FP64
+    Barnes-Hut walk's acceleration error against FP64 direct summation (median and 99th
+    percentile over all bodies).  Its group test opens a superset of the cells the per-body
+    test opens, so its error is usually below the FP64 walk's."""
     from milkywayathome_client_b200 import NBodyState
     pos, vel, mass, _ = dwarf_small
     ctx = make_ctx(len(mass), theta=0.5, potential=None)
     ctxm = ctx.with_precision("mixed")
     with _gpu_state(ctx, pos, vel, mass) as st:
+        direct = st.direct_sample(ctx.eps2, np.arange(len(mass)))
         assert st.gravMap(ctx) == 0
         a64 = st.accels()
         assert st.gravMap(ctxm) == 0
         a32 = st.accels()
-    rel = np.linalg.norm(a32 - a64, axis=1) / np.linalg.norm(a64, axis=1)
-    assert np.median(rel) < 1e-6 and rel.max() < 1e-4
+    norm = np.linalg.norm(direct, axis=1)
+    e64 = np.linalg.norm(a64 - direct, axis=1) / norm
+    e32 = np.linalg.norm(a32 - direct, axis=1) / norm
+    for q in (50, 90, 99):
+        assert np.percentile(e32, q) <= 1.01 * np.percentile(e64, q), q
+    # the group test opens a superset of cells, but individual bodies can lose some of the
+    # cancellation between cell errors that the coarser per-body choice had: the tail is
+    # bounded, not identical
+    assert e32.max() < 3e-2
+
+
+def test_mixed_precision_step_runs_and_stays_close(dwarf_small):
+    """Ten mixed-precision steps track the FP64 trajectory closely (positions within 1e-5
+    of the dwarf's size after ten steps: the two forms differ by the Barnes-Hut error, not
+    by a systematic drift)."""
+    from milkywayathome_client_b200 import NBodyState
+    pos, vel, mass, _ = dwarf_small
+    ctx = make_ctx(len(mass), theta=0.5)
+    ctxm = ctx.with_precision("mixed")
+    with NBodyState.create(ctx, pos, vel, mass) as s64, NBodyState.create(ctxm, pos, vel, mass) as s32:
+        assert s64.run_steps(ctx, 10) == 0
+        assert s32.run_steps(ctxm, 10) == 0
+        p64, _ = s64.bodies()
+        p32, _ = s32.bodies()
+    scale = np.abs(pos - pos.mean(0)).max()
+    assert np.abs(p32 - p64).max() < 1e-5 * scale
+
+
+def test_mixed_flags_test_particles_as_incest():
+    from milkywayathome_client_b200 import models
+    pos, vel, mass, _ = models.plummer_plummer_dwarf(1000, seed=2)
+    mass = mass.copy()
+    mass[::9] = 0.0
+    ctx = make_ctx(len(mass), theta=0.6, allowIncest=True, precision="mixed")
+    with _gpu_state(ctx, pos, vel, mass) as st:
+        assert st.gravMap(ctx) == (1 << 24)
