@@ -59,7 +59,7 @@ def parse_args():
     ap.add_argument("--adjoint-n", type=int, default=131072,
                     help="bodies of the adjoint-cost measurement (0 skips it)")
     ap.add_argument("--adjoint-steps", type=int, default=64)
-    ap.add_argument("--profile", choices=["fp64", "mixed"],
+    ap.add_argument("--profile", choices=["fp64", "mixed", "adjoint"],
                     help="profiling entry: build the dwarf, run two force evaluations, exit")
     return ap.parse_args()
 
@@ -259,10 +259,13 @@ def adjoint_ratio(n, steps, dev):
             "forward_step_ms": stats["forward_step_ms"], "adjoint_step_ms": stats["adjoint_step_ms"],
             "ratio": stats["adjoint_step_ms"] / stats["forward_step_ms"],
             "parts_device_ms": {k: stats[k] for k in ("forward_step_device_ms",
-                                                      "recompute_step_device_ms", "vjp_device_ms",
+                                                      "recompute_step_device_ms",
+                                                      "reverse_step_device_ms",
                                                       "vjp_walk_device_ms")},
-            "how": "tree frozen per step; backward = segment recomputation + tree rebuild + "
-                   "force VJP per step; both passes timed with CUDA events around the pass"}
+            "how": "tree frozen per step; backward = segment recomputation (saving each step's "
+                   "bodies and tree in HBM) + reverse step (nbStepAdjointCUDA: force VJP on the "
+                   "saved tree and reverse leapfrog) per step; both passes timed with CUDA "
+                   "events around the pass"}
 
 
 def run_reference(args, dist):
@@ -478,8 +481,29 @@ def run_ours(args, dist):
 
 
 def run_profile(args):
-    """Small committed entry for ncu: the dwarf, one warm-up and one profiled gravMap."""
+    """Small committed entry for ncu: the dwarf, one warm-up and one profiled gravMap (or, for
+    --profile adjoint, one force evaluation followed by one force VJP at --adjoint-n bodies)."""
     from milkywayathome_client_b200 import models
+    if args.profile == "adjoint":
+        import torch
+        from milkywayathome_client_b200.adjoint import DeviceState
+        from milkywayathome_client_b200.nbody import NBodyCtx, milky_way_potential
+        n = args.adjoint_n
+        pos, vel, mass, _ = models.plummer_plummer_dwarf(n, seed=4242)
+        ctx = NBodyCtx(potential=milky_way_potential(), **models.dwarf_config(n, theta=args.theta))
+        dev = torch.device("cuda:0")
+        t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+        ds = DeviceState(n, dev)
+        ds.set(t(pos), t(vel), t(mass), ctx.treeRSize)
+        ds.gravmap(ctx)
+        fwd_walk = ds.st.walk_time_ms()[0]
+        abar = torch.randn((n, 3), dtype=torch.float64, device=dev,
+                           generator=torch.Generator(device=dev).manual_seed(0))
+        ds.vjp(ctx, abar)
+        print(json.dumps({"profile": "adjoint", "n": n, "forward_walk_ms": fwd_walk,
+                          "vjp_walk_ms": ds.st.walk_time_ms()[0], "vjp_ms": ds.st.step_time_ms()}))
+        ds.close()
+        return 0
     from milkywayathome_client_b200.nbody import NBodyCtx, NBodyState, milky_way_potential
     pos, vel, mass, _ = models.plummer_plummer_dwarf(args.n, seed=1000)
     ctx = NBodyCtx(potential=milky_way_potential(), precision=args.profile,

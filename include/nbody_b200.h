@@ -177,6 +177,32 @@ NBodyCudaStatus nbRunStepsCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, int 
 NBodyCudaStatus nbGravVJPCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, const double* dAbar,
                               double* dXbar, double* dMbar);
 
+/* Saved force evaluations for the reverse pass (no reference counterpart).  nbSaveStateCUDA
+ * copies, device to device, the bodies (positions, velocities, accelerations, masses) and the
+ * tree of the last force evaluation into slot `slot` (0 <= slot < 65536; storage grows on
+ * demand and is kept until nbReleaseStatesCUDA or nbDestroyCUDA); nbRestoreStateCUDA makes a
+ * saved evaluation the current one again, tree included, so nbGravVJPCUDA and
+ * nbStepAdjointCUDA can follow it without rebuilding the tree. */
+NBodyCudaStatus nbSaveStateCUDA(NBodyCudaState* st, int slot);
+NBodyCudaStatus nbRestoreStateCUDA(NBodyCudaState* st, int slot);
+NBodyCudaStatus nbReleaseStatesCUDA(NBodyCudaState* st);
+
+/* Reverse of one kick-drift-kick step (the step of nbStepSystemPlain,
+ * nbody/src/nbody_plain.c:329-364), no reference counterpart.  The current evaluation must be
+ * the step's end state x1, v1, a1 = A(x1) (right after nbStepSystemCUDA, or restored).  With
+ * h = timestep / 2, dAk the accelerations a0 at the step's start (device, 3 per body) and the
+ * adjoints, all device arrays of 3 doubles per body except dMbar (1 per body) and dDtbar (one
+ * double):
+ *     abar = h vbar + abarNext;  (gx, gm) = nbGravVJP(abar)
+ *     xbar += gx;  mbar += gm  (skipped if dMbar is NULL)
+ *     dtbar += vbar.a1/2 + xbar.vh + (vbar + dt xbar).a0/2   (vh = v1 - h a1; skipped if NULL)
+ *     vbar += dt xbar;  abarNext = h vbar
+ * so that after it (xbar, vbar) are the adjoints of the step's start state and abarNext the
+ * adjoint of a0 for the reverse of the step before.  Everything stays on the device. */
+NBodyCudaStatus nbStepAdjointCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, const double* dAk,
+                                  double* dXbar, double* dVbar, double* dMbar, double* dAbarNext,
+                                  double* dDtbar);
+
 /* ---- tree introspection (parity checks of nbMakeTree) ---- */
 NBodyCudaStatus nbMakeTreeCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st);
 NBodyCudaStatus nbTreeInfoCUDA(NBodyCudaState* st, NBodyCudaTreeInfo* info);

@@ -114,6 +114,10 @@ SIGNATURES = [
     ("nbRunStepsCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, ctypes.c_int]),
     ("nbMakeTreeCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp]),
     ("nbGravVJPCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, _vp, _vp, _vp]),
+    ("nbSaveStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nbRestoreStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nbReleaseStatesCUDA", ctypes.c_int, [_vp]),
+    ("nbStepAdjointCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("nbTreeInfoCUDA", ctypes.c_int, [_vp, ctypes.POINTER(TreeInfo)]),
     ("nbGetTreeCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("nbExtAccelerationCUDA", ctypes.c_int,

@@ -3,10 +3,11 @@
 No counterpart in the reference (it has no adjoint).  The forward pass runs nsteps
 kick-drift-kick steps of the FP64 drop-in step on the GPU (nbStepSystemCUDA), keeping a
 checkpoint (positions, velocities, root size) every K steps.  The backward pass walks the
-segments in reverse: it recomputes the states of one segment from its checkpoint, then
-runs the reverse leapfrog step by step, with the vector-Jacobian product of the forces at
-each state taken with that state's tree frozen (nbMakeTreeCUDA + nbGravVJPCUDA: tidal
-tensor of the walk, the cells' moment adjoints, the external potential's Jacobian).
+segments in reverse: it recomputes the states of one segment from its checkpoint, saving
+each state's bodies and tree in HBM (nbSaveStateCUDA), then runs the reverse leapfrog step
+by step on the device (nbRestoreStateCUDA + nbStepAdjointCUDA: the vector-Jacobian product
+of the forces with that state's tree frozen -- tidal tensor of the walk, the cells' moment
+adjoints, the external potential's Jacobian -- and the reverse kicks and drift).
 
 Around it, torch code that is differentiable end to end:
   * dwarf_ics       -- a seeded two-component Plummer dwarf as a function of the 6 dwarf
@@ -78,6 +79,26 @@ class DeviceState:
             return 0
         return NBodyState.check("nbMakeTree", self.st.makeTree(ctx))
 
+    def accel(self):
+        a = torch.empty((self.n, 3), dtype=torch.float64, device=self.device)
+        rc = self.lib.nbGetBodiesDeviceCUDA(self.st._h, None, None, _ptr(a))
+        NBodyState.check("nbGetBodiesDeviceCUDA", rc)
+        return a
+
+    def save(self, slot):
+        NBodyState.check("nbSaveStateCUDA", self.lib.nbSaveStateCUDA(self.st._h, slot))
+
+    def restore(self, slot):
+        NBodyState.check("nbRestoreStateCUDA", self.lib.nbRestoreStateCUDA(self.st._h, slot))
+
+    def step_adjoint(self, ctx, ak, xbar, vbar, mbar, abar_next, dtbar):
+        """Reverse of the step whose end state is current (nbStepAdjointCUDA); updates the
+        adjoint tensors in place."""
+        _sync()
+        rc = self.lib.nbStepAdjointCUDA(ctypes.byref(ctx.struct), self.st._h, _ptr(ak), _ptr(xbar),
+                                        _ptr(vbar), _ptr(mbar), _ptr(abar_next), _ptr(dtbar))
+        NBodyState.check("nbStepAdjointCUDA", rc)
+
     def vjp(self, ctx, abar):
         abar = abar.contiguous()
         xbar = torch.empty((self.n, 3), dtype=torch.float64, device=self.device)
@@ -132,52 +153,40 @@ class _Run(torch.autograd.Function):
         (m,) = fctx.saved_tensors
         ds, ctx, ckpts = fctx.ds, fctx.ctx, fctx.ckpts
         nsteps, every = fctx.nsteps, fctx.every
-        dt = ctx.struct.timestep
-        h = 0.5 * dt
-        xbar = gx.detach().clone() if gx is not None else torch.zeros_like(ckpts[0][0])
-        vbar = gv.detach().clone() if gv is not None else torch.zeros_like(ckpts[0][0])
+        like = ckpts[0][0]
+        xbar = gx.detach().clone().contiguous() if gx is not None else torch.zeros_like(like)
+        vbar = gv.detach().clone().contiguous() if gv is not None else torch.zeros_like(like)
         mbar = torch.zeros_like(m)
         dtbar = torch.zeros((), dtype=torch.float64, device=m.device)
-        abar_next = torch.zeros_like(xbar)        # adjoint of a_{k+1} from the step after it
+        abar_next = torch.zeros_like(like)        # adjoint of a_{k+1} from the step after it
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         _sync()
         ev0.record()
-        vjp_calls = 0
-        rec_ms = vjp_ms = vjp_walk_ms = 0.0       # device times of the parts, summed
+        rev_calls = 0
+        rec_ms = rev_ms = rev_walk_ms = 0.0       # device times of the parts, summed
         for s in range(len(ckpts) - 1, -1, -1):
             k0 = s * every
             k1 = min(k0 + every, nsteps)
             x0, v0, rs0 = ckpts[s]
-            # recompute the states x_k, v_k, a_k and root sizes of this segment
+            # recompute the segment; slot j keeps the evaluation (bodies + tree) of state k0 + j
             ds.set(x0, v0, m, rs0)
             ds.gravmap(ctx)
-            states = [ds.get() + (ds.rsize(),)]
-            for _ in range(k0, k1):
+            ds.save(0)
+            acc = [ds.accel()]
+            for j in range(k0, k1):
                 ds.step(ctx)
                 rec_ms += ds.st.step_time_ms()
-                states.append(ds.get() + (ds.rsize(),))
+                ds.save(j - k0 + 1)
+                acc.append(ds.accel())
+            # reverse steps k1-1 .. k0 on the saved trees (nbStepAdjointCUDA)
             for k in range(k1 - 1, k0 - 1, -1):
-                x1, v1, a1, rs1 = states[k - k0 + 1]
-                xk, vk, ak, _ = states[k - k0]
-                # forward: vh = vk + h ak; x1 = xk + dt vh; a1 = A(x1); v1 = vh + h a1
-                abar1 = h * vbar + abar_next
-                ds.set(x1, v1, m, rs1)
-                ds.maketree(ctx)
-                gx1, gm1 = ds.vjp(ctx, abar1)
-                vjp_ms += ds.st.step_time_ms()
-                vjp_walk_ms += ds.st.walk_time_ms()[0]
-                vjp_calls += 1
-                vh = vk + h * ak
-                xbar = xbar + gx1                 # total adjoint of x_{k+1}
-                mbar = mbar + gm1
-                dtbar = dtbar + 0.5 * (vbar * a1).sum() + (xbar * vh).sum()
-                vbar = vbar + dt * xbar           # adjoint of vh (and of v_k)
-                dtbar = dtbar + 0.5 * (vbar * ak).sum()
-                abar_next = h * vbar              # adjoint of a_k, used by the step before
-        # a_0 = A(x_0) feeds the first kick
-        x0, v0, rs0 = ckpts[0]
-        ds.set(x0, v0, m, rs0)
-        ds.maketree(ctx)
+                ds.restore(k - k0 + 1)
+                ds.step_adjoint(ctx, acc[k - k0], xbar, vbar, mbar, abar_next, dtbar)
+                rev_ms += ds.st.step_time_ms()
+                rev_walk_ms += ds.st.walk_time_ms()[0]
+                rev_calls += 1
+        # a_0 = A(x_0) feeds the first kick: slot 0 of the first segment holds it
+        ds.restore(0)
         gx0, gm0 = ds.vjp(ctx, abar_next)
         xbar = xbar + gx0
         mbar = mbar + gm0
@@ -185,10 +194,10 @@ class _Run(torch.autograd.Function):
         ev1.synchronize()
         if fctx.stats is not None:
             fctx.stats["adjoint_step_ms"] = ev0.elapsed_time(ev1) / max(nsteps, 1)
-            fctx.stats["vjp_calls"] = vjp_calls + 1
+            fctx.stats["vjp_calls"] = rev_calls + 1
             fctx.stats["recompute_step_device_ms"] = rec_ms / max(nsteps, 1)
-            fctx.stats["vjp_device_ms"] = vjp_ms / max(vjp_calls, 1)
-            fctx.stats["vjp_walk_device_ms"] = vjp_walk_ms / max(vjp_calls, 1)
+            fctx.stats["reverse_step_device_ms"] = rev_ms / max(rev_calls, 1)
+            fctx.stats["vjp_walk_device_ms"] = rev_walk_ms / max(rev_calls, 1)
         ds.close()
         return xbar, vbar, mbar, dtbar, None, None, None, None
 

@@ -2,7 +2,8 @@
 
 Every translation unit is compiled by nvcc for sm_100a only, with -fmad=false so the FP64
 code keeps the reference CPU build's rounding (no FMA contraction); FP32 code that wants a
-fused multiply-add spells out fmaf().
+fused multiply-add spells out fmaf().  The adjoint kernels (nb_adjoint.cu) have no reference
+rounding to keep and are compiled with contraction on.
 
     python -m milkywayathome_client_b200.build [--force] [--verbose]
 """
@@ -18,8 +19,9 @@ SOURCES = ["nb_sort.cu", "nb_tree.cu", "nb_walk.cu", "nb_mixed.cu", "nb_api.cu",
 HEADERS = ["nb_common.cuh", "nb_potential.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
-         "-Xcompiler", "-O3", "-Xptxas", "-v"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+         "-Xptxas", "-v"]
+FMAD_ON = {"nb_adjoint.cu"}          # everything else: -fmad=false (reference rounding)
 
 
 def _newer(target, deps):
@@ -39,7 +41,8 @@ def build(force=False, verbose=False):
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _newer(o, [s] + hdrs):
-            cmd = [NVCC] + ARCH + FLAGS + ["-I", inc, "-c", s, "-o", o]
+            fmad = ["-fmad=true"] if src in FMAD_ON else ["-fmad=false"]
+            cmd = [NVCC] + ARCH + FLAGS + fmad + ["-I", inc, "-c", s, "-o", o]
             r = subprocess.run(cmd, capture_output=True, text=True)
             log = os.path.join(BUILD, src.replace(".cu", ".ptxas.txt"))
             with open(log, "w") as f:

@@ -115,8 +115,9 @@ __device__ __forceinline__ Vjp1 nb_interaction_vjp(double dx, double dy, double 
 {
     Vjp1 o;
     const double s = dx * dx + dy * dy + dz * dz + eps2;
-    const double is = 1.0 / s;
-    const double r3 = is * sqrt(is);          // s^-3/2
+    const double rs = rsqrt(s);               // s^-1/2 (within 1 ulp)
+    const double is = rs * rs;
+    const double r3 = is * rs;                // s^-3/2
     const double r5 = r3 * is;                // s^-5/2
     const double al = dx * abx + dy * aby + dz * abz;
     o.rx = m * (abx * r3 - 3.0 * dx * al * r5);
@@ -173,7 +174,7 @@ __device__ __forceinline__ double nb_warp_sum_transposed(double (&r)[V], int lan
 }
 
 // Node adjoints: nodeBar[k*10 + 0..2] = CoM, [3] = mass, [4..9] = quadrupole.
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 5)
 k_walk_vjp(const double4* __restrict__ nodePM, const double* __restrict__ nodeCrit,
            const int2* __restrict__ nodeLink, const double* __restrict__ nodeQuad,
            const unsigned int* __restrict__ order, const double* __restrict__ px,
@@ -389,4 +390,81 @@ void nb_launch_vjp(NbTreeBuffers& b, double* nodeBar, int capNodes, int maxDepth
     k_vjp_finish<<<min((n + 255) / 256, numSMs * 8), 256, 0, s>>>(b.bodyNode, b.sort.idxA, nodeBar,
                                                                     xbar, mbar, b.sc, n);
     nb_count_launch(3 + maxDepth);
+}
+
+// ---- reverse leapfrog step ----
+// The forward step k (nbody/src/nbody_plain.c:329-364 with the kicks of
+// nbody/src/nbody_grav.c:296-303): vh = v_k + h a_k, x_{k+1} = x_k + dt vh,
+// a_{k+1} = A(x_{k+1}), v_{k+1} = vh + h a_{k+1}, h = dt / 2.  Given the adjoints (xbar, vbar)
+// of (x_{k+1}, v_{k+1}) and abarNext, the adjoint a_{k+1} receives from step k+1's first kick,
+// the reverse step is
+//   abar = h vbar + abarNext;  (gx, gm) = VJP of A at x_{k+1} applied to abar
+//   xbar += gx;  mbar += gm
+//   dtbar += vbar . a_{k+1} / 2 + xbar . vh + (vbar + dt xbar) . a_k / 2
+//   vbar += dt xbar;  abarNext = h vbar
+__global__ void k_adj_pre(const double* __restrict__ vbar, const double* __restrict__ abarNext,
+                          double* __restrict__ abar, double h, int n3)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
+        abar[i] = h * vbar[i] + abarNext[i];
+}
+
+__global__ void __launch_bounds__(256)
+k_adj_post(const double* __restrict__ ax, const double* __restrict__ ay,
+           const double* __restrict__ az, const double* __restrict__ vx,
+           const double* __restrict__ vy, const double* __restrict__ vz,
+           const double* __restrict__ ak, const double* __restrict__ gx,
+           const double* __restrict__ gm, double* __restrict__ xbar, double* __restrict__ vbar,
+           double* __restrict__ mbar, double* __restrict__ abarNext, double* __restrict__ dtbar,
+           double dt, int n)
+{
+    const double h = 0.5 * dt;
+    double part = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double a1[3] = {ax[i], ay[i], az[i]};
+        const double v1[3] = {vx[i], vy[i], vz[i]};
+        for (int c = 0; c < 3; ++c) {
+            const int k = 3 * i + c;
+            const double vh = v1[c] - h * a1[c];
+            const double xb = xbar[k] + gx[k];
+            double vb = vbar[k];
+            part += 0.5 * vb * a1[c] + xb * vh;
+            vb += dt * xb;
+            part += 0.5 * vb * ak[k];
+            xbar[k] = xb;
+            vbar[k] = vb;
+            abarNext[k] = h * vb;
+        }
+        if (mbar) mbar[i] += gm[i];
+    }
+    // block sum of the time-step adjoint, one atomic per block
+    __shared__ double red[8];
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(NB_FULL_MASK, part, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        part = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(NB_FULL_MASK, part, o);
+        if (threadIdx.x == 0 && dtbar) atomicAdd(dtbar, part);
+    }
+}
+
+void nb_launch_step_adjoint(NbTreeBuffers& b, double* nodeBar, int capNodes, int maxDepth,
+                            int criterion, const NbWalkParams& wp, const NbPot& pot, double dt,
+                            const double* ak, double* xbar, double* vbar, double* mbar,
+                            double* abarNext, double* dtbar, double* scratch, int numSMs,
+                            cudaEvent_t walkStart, cudaEvent_t walkEnd, cudaStream_t s)
+{
+    const int n = wp.n;
+    if (n <= 0) return;
+    double* abar = scratch;                    // 3 n
+    double* gx = scratch + 3 * (size_t) n;     // 3 n
+    double* gm = scratch + 6 * (size_t) n;     // n
+    const int blocks = min((3 * n + 255) / 256, numSMs * 8);
+    k_adj_pre<<<blocks, 256, 0, s>>>(vbar, abarNext, abar, 0.5 * dt, 3 * n);
+    nb_launch_vjp(b, nodeBar, capNodes, maxDepth, criterion, wp, pot, abar, gx, gm, numSMs,
+                  walkStart, walkEnd, s);
+    k_adj_post<<<min((n + 255) / 256, numSMs * 8), 256, 0, s>>>(
+        b.ax, b.ay, b.az, b.vx, b.vy, b.vz, ak, gx, gm, xbar, vbar, mbar, abarNext, dtbar, dt, n);
+    nb_count_launch(2);
 }

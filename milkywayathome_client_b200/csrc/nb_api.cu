@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 
 // ---- kernels defined in the other translation units ----
 void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
@@ -25,6 +26,11 @@ void nb_launch_vjp(NbTreeBuffers& b, double* nodeBar, int capNodes, int maxDepth
                    const NbWalkParams& wp, const NbPot& pot, const double* abar, double* xbar,
                    double* mbar, int numSMs, cudaEvent_t walkStart, cudaEvent_t walkEnd,
                    cudaStream_t s);
+void nb_launch_step_adjoint(NbTreeBuffers& b, double* nodeBar, int capNodes, int maxDepth,
+                            int criterion, const NbWalkParams& wp, const NbPot& pot, double dt,
+                            const double* ak, double* xbar, double* vbar, double* mbar,
+                            double* abarNext, double* dtbar, double* scratch, int numSMs,
+                            cudaEvent_t walkStart, cudaEvent_t walkEnd, cudaStream_t s);
 void nb_launch_direct_fp64(const double* px, const double* py, const double* pz,
                            const double* mass, double* ax, double* ay, double* az, double* vx,
                            double* vy, double* vz, const NbWalkParams& wp, const NbPot& pot,
@@ -99,6 +105,24 @@ __global__ void k_kick(double* vx, double* vy, double* vz, const double* ax, con
     }
 }
 
+// A saved force evaluation: the bodies (positions, velocities, accelerations, masses) and the
+// tree the accelerations were computed with, for the reverse pass of the adjoint.
+struct NbSlot {
+    char* mem = nullptr;
+    size_t bytes = 0;
+    double* body = nullptr;             // 10 arrays of n: px py pz vx vy vz ax ay az mass
+    unsigned* order = nullptr;          // sorted body order
+    int* bodyNode = nullptr;
+    double4* nodePM = nullptr;
+    double* nodeCrit = nullptr;
+    int2* nodeLink = nullptr;
+    double* nodeQuad = nullptr;
+    int* nodeDepth = nullptr;
+    NbScalars sc{};
+    double rsize = 0.0;
+    int haveTree = 0, criterion = -1, step = 0, treeIncest = 0, valid = 0;
+};
+
 struct NBodyCudaState {
     int device = 0;
     int nbody = 0;
@@ -126,6 +150,8 @@ struct NBodyCudaState {
     double* nodeBar = nullptr;          // adjoint: 10 doubles per node
     int nodeBarCap = 0;
     int lastCriterion = -1;             // criterion of the last force evaluation
+    std::vector<NbSlot> slots;          // saved evaluations (nbSaveStateCUDA)
+    double* adjScratch = nullptr;       // reverse step: 7 doubles per body
 };
 
 template <typename T>
@@ -218,6 +244,10 @@ static void nb_free_all(NBodyCudaState* st)
     st->mx.stacks = nullptr;
     cudaFree(st->nodeBar);
     st->nodeBar = nullptr;
+    for (NbSlot& sl : st->slots) cudaFree(sl.mem);
+    st->slots.clear();
+    cudaFree(st->adjScratch);
+    st->adjScratch = nullptr;
     if (st->scHost) cudaFreeHost(st->scHost);
     if (st->ev0) cudaEventDestroy(st->ev0);
     if (st->ev1) cudaEventDestroy(st->ev1);
@@ -792,6 +822,157 @@ NBodyCudaStatus nbGravVJPCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, const
     NB_CHECK(cudaGetLastError());
     NB_CHECK(cudaStreamSynchronize(st->stream));
     // timings of the adjoint: walk = the walk-side kernel, step = the whole product
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, st->ev0, st->ev1);
+    st->walkMs = ms;
+    ms = 0.0f;
+    cudaEventElapsedTime(&ms, st->evS, st->evE);
+    st->stepMs = ms;
+    return NBODY_SUCCESS;
+}
+
+static size_t nb_align256(size_t x) { return (x + 255) & ~(size_t) 255; }
+
+NBodyCudaStatus nbSaveStateCUDA(NBodyCudaState* st, int slot)
+{
+    if (!st || slot < 0 || slot >= (1 << 16)) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    if ((int) st->slots.size() <= slot) st->slots.resize(slot + 1);
+    NbSlot& sl = st->slots[slot];
+    const size_t n = (size_t) st->nbody;
+    const size_t nodes = st->haveTree ? (size_t) st->scHost->nNodes : 0;
+    const size_t need = nb_align256(10 * n * sizeof(double)) + 2 * nb_align256(n * sizeof(int)) +
+                        nb_align256(nodes * sizeof(double4)) + nb_align256(nodes * sizeof(double)) +
+                        nb_align256(nodes * sizeof(int2)) + nb_align256(6 * nodes * sizeof(double)) +
+                        nb_align256(nodes * sizeof(int)) + 256;
+    if (sl.bytes < need) {
+        cudaFree(sl.mem);
+        sl.mem = nullptr;
+        sl.bytes = 0;
+        NB_CHECK(cudaMalloc((void**) &sl.mem, need));
+        sl.bytes = need;
+    }
+    char* p = sl.mem;
+    auto carve = [&p](size_t bytes) { char* q = p; p += nb_align256(bytes); return q; };
+    sl.body = (double*) carve(10 * n * sizeof(double));
+    sl.order = (unsigned*) carve(n * sizeof(int));
+    sl.bodyNode = (int*) carve(n * sizeof(int));
+    sl.nodePM = (double4*) carve(nodes * sizeof(double4));
+    sl.nodeCrit = (double*) carve(nodes * sizeof(double));
+    sl.nodeLink = (int2*) carve(nodes * sizeof(int2));
+    sl.nodeQuad = (double*) carve(6 * nodes * sizeof(double));
+    sl.nodeDepth = (int*) carve(nodes * sizeof(int));
+    NbTreeBuffers& b = st->b;
+    const cudaStream_t s = st->stream;
+    const double* src[10] = {b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.ax, b.ay, b.az, b.mass};
+    for (int k = 0; k < 10; ++k)
+        NB_CHECK(cudaMemcpyAsync(sl.body + k * n, src[k], n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (nodes) {
+        NB_CHECK(cudaMemcpyAsync(sl.order, b.sort.idxA, n * sizeof(int), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(sl.bodyNode, b.bodyNode, n * sizeof(int), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(sl.nodePM, b.nodePM, nodes * sizeof(double4), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(sl.nodeCrit, b.nodeCrit, nodes * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(sl.nodeLink, b.nodeLink, nodes * sizeof(int2), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(sl.nodeQuad, b.nodeQuad, 6 * nodes * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(sl.nodeDepth, b.nodeDepth, nodes * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    }
+    NB_CHECK(cudaStreamSynchronize(s));
+    sl.sc = *st->scHost;
+    sl.rsize = st->rsize;
+    sl.haveTree = st->haveTree;
+    sl.criterion = st->lastCriterion;
+    sl.step = st->step;
+    sl.treeIncest = st->treeIncest;
+    sl.valid = 1;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbRestoreStateCUDA(NBodyCudaState* st, int slot)
+{
+    if (!st || slot < 0 || slot >= (int) st->slots.size() || !st->slots[slot].valid) {
+        g_lastError = "nbRestoreStateCUDA: no state saved in this slot";
+        return NBODY_USER_ERROR;
+    }
+    NB_CHECK(cudaSetDevice(st->device));
+    NbSlot& sl = st->slots[slot];
+    const size_t n = (size_t) st->nbody;
+    const size_t nodes = sl.haveTree ? (size_t) sl.sc.nNodes : 0;
+    if (sl.haveTree && st->capNodes < sl.sc.nNodes) {
+        NBodyCudaStatus rc = nb_alloc_nodes(st, sl.sc.nNodes);
+        if (rc) return rc;
+    }
+    NbTreeBuffers& b = st->b;
+    const cudaStream_t s = st->stream;
+    double* dst[10] = {b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.ax, b.ay, b.az, b.mass};
+    for (int k = 0; k < 10; ++k)
+        NB_CHECK(cudaMemcpyAsync(dst[k], sl.body + k * n, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (nodes) {
+        NB_CHECK(cudaMemcpyAsync(b.sort.idxA, sl.order, n * sizeof(int), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(b.bodyNode, sl.bodyNode, n * sizeof(int), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(b.nodePM, sl.nodePM, nodes * sizeof(double4), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(b.nodeCrit, sl.nodeCrit, nodes * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(b.nodeLink, sl.nodeLink, nodes * sizeof(int2), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(b.nodeQuad, sl.nodeQuad, 6 * nodes * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(b.nodeDepth, sl.nodeDepth, nodes * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    }
+    *st->scHost = sl.sc;
+    st->scHost->capNodes = st->capNodes;
+    NB_CHECK(cudaMemcpyAsync(b.sc, st->scHost, sizeof(NbScalars), cudaMemcpyHostToDevice, s));
+    NB_CHECK(cudaStreamSynchronize(s));
+    st->rsize = sl.rsize;
+    st->haveTree = sl.haveTree;
+    st->lastCriterion = sl.criterion;
+    st->step = sl.step;
+    st->treeIncest = sl.treeIncest;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbReleaseStatesCUDA(NBodyCudaState* st)
+{
+    if (!st) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    for (NbSlot& sl : st->slots) cudaFree(sl.mem);
+    st->slots.clear();
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbStepAdjointCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, const double* dAk,
+                                  double* dXbar, double* dVbar, double* dMbar, double* dAbarNext,
+                                  double* dDtbar)
+{
+    if (!st || !dAk || !dXbar || !dVbar || !dAbarNext) return NBODY_USER_ERROR;
+    std::string why;
+    NBodyCudaStatus rc = nb_check_ctx(ctx, why);
+    if (rc) { g_lastError = why; return rc; }
+    if (ctx->precision != NBCUDA_PRECISION_FP64) {
+        g_lastError = "the adjoint follows the FP64 walk";
+        return NBODY_UNSUPPORTED;
+    }
+    if (ctx->criterion != st->lastCriterion || (ctx->criterion != NBCUDA_EXACT && !st->haveTree)) {
+        g_lastError = "nbStepAdjointCUDA needs the force evaluation of the step's end state first";
+        return NBODY_USER_ERROR;
+    }
+    NB_CHECK(cudaSetDevice(st->device));
+    if (ctx->criterion != NBCUDA_EXACT && st->nodeBarCap < st->capNodes) {
+        cudaFree(st->nodeBar);
+        st->nodeBar = nullptr;
+        NB_CHECK(cudaMalloc((void**) &st->nodeBar, 10 * sizeof(double) * (size_t) st->capNodes));
+        st->nodeBarCap = st->capNodes;
+    }
+    if (!st->adjScratch)
+        NB_CHECK(nb_alloc(&st->adjScratch, 7 * (size_t) st->capBodies));
+    NbWalkParams wp{};
+    wp.eps2 = ctx->eps2;
+    wp.useQuad = ctx->useQuad;
+    wp.n = st->nbody;
+    NB_CHECK(cudaEventRecord(st->evS, st->stream));
+    nb_launch_step_adjoint(st->b, st->nodeBar, st->capNodes, st->scHost->maxDepth, ctx->criterion,
+                           wp, nb_pot_from(ctx), ctx->timestep, dAk, dXbar, dVbar, dMbar,
+                           dAbarNext, dDtbar, st->adjScratch, st->numSMs, st->ev0, st->ev1,
+                           st->stream);
+    NB_CHECK(cudaEventRecord(st->evE, st->stream));
+    NB_CHECK(cudaGetLastError());
+    NB_CHECK(cudaStreamSynchronize(st->stream));
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, st->ev0, st->ev1);
     st->walkMs = ms;
