@@ -59,6 +59,10 @@ def parse_args():
     ap.add_argument("--adjoint-n", type=int, default=131072,
                     help="bodies of the adjoint-cost measurement (0 skips it)")
     ap.add_argument("--adjoint-steps", type=int, default=64)
+    ap.add_argument("--energy-steps", type=int, default=100,
+                    help="steps of the energy-drift run of both forms (0: skip)")
+    ap.add_argument("--theta2", type=float, default=1.0,
+                    help="second opening angle measured for both forms (0: skip)")
     ap.add_argument("--profile", choices=["fp64", "mixed", "adjoint"],
                     help="profiling entry: build the dwarf, run two force evaluations, exit")
     return ap.parse_args()
@@ -357,28 +361,28 @@ def run_ours(args, dist):
     mean_walk = float(np.mean(walk_ms))
 
     # ---- accuracy against FP64 direct summation on a seeded 4,096-body sample ----
-    ctx_self = NBodyCtx(potential=None, **cfg)
     rng = np.random.default_rng(4096)
     sample = np.sort(rng.choice(n, size=min(4096, n), replace=False)).astype(np.int32)
-    acc_form = {}
-    with NBodyState.create(ctx_self, pos, vel, mass, device=dev, gravmap=False) as sa:
-        direct = sa.direct_sample(cfg["eps2"], sample)
-        for name, c in (("fp64", ctx_self), ("mixed", ctx_self.with_precision("mixed"))):
-            sa.check("nbGravMap", sa.gravMap(c))
-            a = sa.accels()[sample]
-            rel = np.linalg.norm(a - direct, axis=1) / np.linalg.norm(direct, axis=1)
-            acc_form[name] = rel
-    accuracy = {
-        "sample": "4,096 seeded bodies, self-gravity only, vs FP64 direct summation",
-        "fp64": {p: float(np.percentile(acc_form["fp64"], q)) for p, q in
-                 (("p50", 50), ("p90", 90), ("p99", 99), ("max", 100))},
-        "mixed": {p: float(np.percentile(acc_form["mixed"], q)) for p, q in
-                  (("p50", 50), ("p90", 90), ("p99", 99), ("max", 100))},
-    }
-    accuracy["mixed_added_error_p50_pct"] = 100.0 * (
-        accuracy["mixed"]["p50"] - accuracy["fp64"]["p50"]) / accuracy["fp64"]["p50"]
-    accuracy["mixed_added_error_p99_pct"] = 100.0 * (
-        accuracy["mixed"]["p99"] - accuracy["fp64"]["p99"]) / accuracy["fp64"]["p99"]
+
+    def form_accuracy(c_cfg):
+        c_self = NBodyCtx(potential=None, **c_cfg)
+        rel = {}
+        with NBodyState.create(c_self, pos, vel, mass, device=dev, gravmap=False) as sa:
+            direct = sa.direct_sample(c_cfg["eps2"], sample)
+            for name, c in (("fp64", c_self), ("mixed", c_self.with_precision("mixed"))):
+                sa.check("nbGravMap", sa.gravMap(c))
+                a = sa.accels()[sample]
+                rel[name] = np.linalg.norm(a - direct, axis=1) / np.linalg.norm(direct, axis=1)
+        out = {"sample": "4,096 seeded bodies, self-gravity only, vs FP64 direct summation"}
+        for name in ("fp64", "mixed"):
+            out[name] = {p: float(np.percentile(rel[name], q)) for p, q in
+                         (("p50", 50), ("p90", 90), ("p99", 99), ("max", 100))}
+        for p in ("p50", "p99"):
+            out["mixed_added_error_%s_pct" % p] = 100.0 * (
+                out["mixed"][p] - out["fp64"][p]) / out["fp64"][p]
+        return out
+
+    accuracy = form_accuracy(cfg)
 
     # ---- e2e through the C ABI with pinned host buffers ----
     hp = pinned_array((n, 3)); hv = pinned_array((n, 3)); hm = pinned_array((n,))
@@ -412,6 +416,44 @@ def run_ours(args, dist):
     mixed = {"value": mixed_value, "unit": UNIT,
              "ms_per_step": 1e3 * t_mixed / K, "walk_ms": float(np.mean(walk_ms_m)),
              "speedup_vs_fp64": t_dev / t_mixed}
+
+    # ---- energy drift of both forms over the configuration's step count ----
+    energy = None
+    if args.energy_steps > 0:
+        energy = {"steps": args.energy_steps,
+                  "how": "total energy (kinetic + softened self-gravity + external potential) "
+                         "by FP64 direct summation on the GPU (nbEnergyCUDA) before and after "
+                         "the run; rel_drift = (E1 - E0) / |E0|; the external potential "
+                         "dominates E, so the drift is also given over |W0|, the dwarf's "
+                         "self-gravity energy"}
+        for name, c in (("fp64", ctx), ("mixed", ctx_mixed)):
+            with NBodyState.create(c, pos, vel, mass, device=dev) as se:
+                e0 = se.energy(c)
+                se.check("nbRunSteps", se.run_steps(c, args.energy_steps))
+                e1 = se.energy(c)
+            energy[name] = {"E0": sum(e0), "E1": sum(e1),
+                            "rel_drift": (sum(e1) - sum(e0)) / abs(sum(e0)),
+                            "drift_over_self_energy": (sum(e1) - sum(e0)) / abs(e0[1]),
+                            "components_E0": list(e0)}
+
+    # ---- the configuration's second opening angle: both forms, speed and accuracy ----
+    theta2 = None
+    if args.theta2 > 0:
+        cfg2 = models.dwarf_config(n, theta=args.theta2)
+        ctx2 = NBodyCtx(potential=milky_way_potential(), **cfg2)
+        theta2 = {"theta": args.theta2}
+        for name, c in (("fp64", ctx2), ("mixed", ctx2.with_precision("mixed"))):
+            with NBodyState.create(c, pos, vel, mass, device=dev) as s2:
+                for _ in range(W):
+                    s2.check("nbStepSystem", s2.step(c))
+                ms = []
+                for _ in range(K):
+                    s2.check("nbStepSystem", s2.step(c))
+                    ms.append(s2.step_time_ms())
+            v2, t2 = replica_throughput(dist, n, K, sum(ms) / 1e3)
+            theta2[name] = {"value": v2, "unit": UNIT, "ms_per_step": 1e3 * t2 / K}
+        theta2["speedup_mixed_vs_fp64"] = theta2["mixed"]["value"] / theta2["fp64"]["value"]
+        theta2["accuracy"] = form_accuracy(cfg2)
 
     # ---- roofline of the walk kernel (FP64 pipe) ----
     peak64 = peak_fma_tflops(True, dev)
@@ -469,7 +511,8 @@ def run_ours(args, dist):
                        "parallelism": "replicas: one independent dwarf per GPU",
                        "l2": "inputs larger than L2: %d tree nodes (~%.0f MB) + bodies (~%.0f MB) per step"
                              % (info.nNodes, info.nNodes * 176 / 1e6, n * 120 / 1e6)},
-            "roofline": roofline, "mixed": mixed, "accuracy": accuracy, "e2e": e2e,
+            "roofline": roofline, "mixed": mixed, "accuracy": accuracy, "energy": energy,
+            "theta2": theta2, "e2e": e2e,
             "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk, "adjoint": adj,
             "tree": {"nodes": info.nNodes, "cells": info.cellUsed, "max_depth": info.maxDepth,
                      "rsize": info.rsize},

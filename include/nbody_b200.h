@@ -203,6 +203,12 @@ NBodyCudaStatus nbStepAdjointCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, c
                                   double* dXbar, double* dVbar, double* dMbar, double* dAbarNext,
                                   double* dDtbar);
 
+/* Total energy of the current state by FP64 direct summation, O(N^2) (no reference
+ * counterpart; the energy-drift check of the walk forms): energy[0] = kinetic sum m v^2 / 2,
+ * energy[1] = self-gravity -sum_{i<j} m_i m_j / sqrt(r^2 + eps2), energy[2] = sum m Phi_ext
+ * for the context's potential (0 with EXTERNAL_POTENTIAL_NONE).  Host array of 3 doubles. */
+NBodyCudaStatus nbEnergyCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, double* energy);
+
 /* ---- tree introspection (parity checks of nbMakeTree) ---- */
 NBodyCudaStatus nbMakeTreeCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st);
 NBodyCudaStatus nbTreeInfoCUDA(NBodyCudaState* st, NBodyCudaTreeInfo* info);

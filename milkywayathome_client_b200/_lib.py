@@ -114,6 +114,7 @@ SIGNATURES = [
     ("nbRunStepsCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, ctypes.c_int]),
     ("nbMakeTreeCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp]),
     ("nbGravVJPCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, _vp, _vp, _vp]),
+    ("nbEnergyCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, _dp]),
     ("nbSaveStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbRestoreStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbReleaseStatesCUDA", ctypes.c_int, [_vp]),

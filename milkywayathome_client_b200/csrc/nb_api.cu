@@ -22,6 +22,9 @@ void nb_launch_direct_sample(const double* px, const double* py, const double* p
                              const double* mass, int n, const int* targets, int count,
                              double eps2, double* out, cudaStream_t s);
 double nb_fma_probe(int fp64, int numSMs, cudaStream_t s);
+void nb_launch_energy(const double* px, const double* py, const double* pz, const double* vx,
+                      const double* vy, const double* vz, const double* mass, int n, double eps2,
+                      const NbPot& pot, double* out, cudaStream_t s);
 void nb_launch_vjp(NbTreeBuffers& b, double* nodeBar, int capNodes, int maxDepth, int criterion,
                    const NbWalkParams& wp, const NbPot& pot, const double* abar, double* xbar,
                    double* mbar, int numSMs, cudaEvent_t walkStart, cudaEvent_t walkEnd,
@@ -223,7 +226,7 @@ static NBodyCudaStatus nb_alloc_bodies(NBodyCudaState* st, int n)
     NB_CHECK(nb_alloc(&b.delta, N)); NB_CHECK(nb_alloc(&b.cum, N));
     NB_CHECK(nb_alloc(&b.scanTmp, (size_t) nb_scan_tmp_ints((int) N)));
     NB_CHECK(nb_alloc(&b.bodyNode, N));
-    NB_CHECK(nb_alloc(&st->stage, 3 * N));
+    NB_CHECK(nb_alloc(&st->stage, 3 * N + 3));
     st->capBodies = (int) N;
     return nb_alloc_nodes(st, 2 * (int) N + 64);
 }
@@ -979,6 +982,23 @@ NBodyCudaStatus nbStepAdjointCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, c
     ms = 0.0f;
     cudaEventElapsedTime(&ms, st->evS, st->evE);
     st->stepMs = ms;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbEnergyCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, double* energy)
+{
+    if (!st || !energy) return NBODY_USER_ERROR;
+    std::string why;
+    NBodyCudaStatus rc = nb_check_ctx(ctx, why);
+    if (rc) { g_lastError = why; return rc; }
+    NB_CHECK(cudaSetDevice(st->device));
+    NbTreeBuffers& b = st->b;
+    double* dOut = st->stage;           // >= 3 doubles of device staging
+    nb_launch_energy(b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.mass, st->nbody, ctx->eps2,
+                     nb_pot_from(ctx), dOut, st->stream);
+    NB_CHECK(cudaGetLastError());
+    NB_CHECK(cudaMemcpyAsync(energy, dOut, 3 * sizeof(double), cudaMemcpyDeviceToHost, st->stream));
+    NB_CHECK(cudaStreamSynchronize(st->stream));
     return NBODY_SUCCESS;
 }
 

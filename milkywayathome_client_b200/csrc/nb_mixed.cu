@@ -1,18 +1,22 @@
 // Mixed-precision force walk (no counterpart in the reference).
 //
-// Same tree, same walk order and the same per-body opening test as the FP64 walk
-// (nbGravity, nbody/src/nbody_grav.c:42-124), but the interaction arithmetic is FP32.
-// After the FP64 moment pass, k_pack_f32 stores every node as FP32 data relative to the
-// root's centre of mass c: position as an unevaluated sum hi + lo (hi = f32(x - c),
-// lo = f32((x - c) - hi)), mass, rcrit2 and the quadrupole.  A lane forms
-// dr = (hi_node - hi_body) + (lo_node - lo_body) in FP32: the hi difference is exact for
-// nearby nodes (Sterbenz), so dr keeps FP32 relative precision however far the dwarf sits
-// from the origin -- the walk runs in coordinates relative to the walking body's own
-// neighbourhood.  Then |dr|^2, the softened inverse distance (rsqrtf), the monopole and
-// quadrupole terms are FP32; partial sums are flushed into FP64 accumulators every
-// NB_MIXED_FLUSH interactions.  Centres of mass, moments, the external potential and the
-// leapfrog stay FP64 (shared with the FP64 code).  Compiled with -fmad=false like the FP64 code (so the shared FP64 epilogue keeps the
-// reference's rounding); the FP32 interaction uses explicit fmaf.
+// Same tree and moments as the FP64 walk (nbGravity, nbody/src/nbody_grav.c:42-124); the
+// walk and the interaction arithmetic are FP32, the accumulation FP64.  After the FP64 moment
+// pass, k_pack_f32 stores every node as FP32 data relative to the root's centre of mass c:
+// position as an unevaluated sum hi + lo (hi = f32(x - c), lo = f32((x - c) - hi)), mass,
+// rcrit2, the quadrupole and the list of its children.  k_groups cuts the sorted bodies into
+// walk groups of <= 32 bodies that share a compact cell.  k_walk_mixed gives each group to one
+// warp (persistent warps take groups from an atomic counter): the warp walks the tree
+// depth-first, 32 nodes per step, with the group test |CoM - box|^2 >= rcrit2 (box = the
+// group's bounding box), which implies the per-body test for every body of the group, so a
+// group opens a superset of the cells its bodies would open.  Accepted cells and visited bodies
+// go to per-warp interaction lists in shared memory, positions taken relative to the group's
+// centre ((hi - centre) + lo, formed once by the appending lane): the walk runs in coordinates
+// relative to the walking leaf group, so FP32 keeps its relative precision however far the
+// dwarf sits from the origin.  All 32 lanes then evaluate the list, each for its own body
+// (rsqrtf, explicit fmaf), and add the partial sums into FP64 after every cell list.  Centres
+// of mass, moments, the external potential and the leapfrog stay FP64 (shared with the FP64
+// code, compiled with -fmad=false so the shared epilogue keeps the reference's rounding).
 #include "nb_common.cuh"
 #include "nb_potential.cuh"
 
@@ -86,20 +90,20 @@ constexpr int NB_GROUP_STACK = 16384;     // >= 256 x 63 + 32
 
 // Interaction lists in shared memory, one float4 array per field so that the 32 lanes'
 // appends hit consecutive 16-byte slots (no bank conflicts) while the evaluation reads each
-// entry as broadcasts.  Cell entry: {hi, mass} {lo, qxx} {qxy, qxz, qyy, qyz} {qzz, -, -, -};
-// body entry: {hi, mass} {lo, -}.
-struct CellList { float4 a[LIST_CAP], b[LIST_CAP], c[LIST_CAP], d[LIST_CAP]; };
-struct BodyList { float4 a[LIST_CAP], b[LIST_CAP]; };
+// entry as broadcasts.  Positions are stored relative to the walking group's centre (FP32):
+// the lane that appends an entry forms (hi - centre) + lo once, so an interaction costs each
+// body one subtraction per coordinate.  Cell entry: {rel, mass} {qxx, qxy, qxz, qyy}
+// {qyz, qzz, -, -}; body entry: {rel, mass}.
+struct CellList { float4 a[LIST_CAP], b[LIST_CAP], c[LIST_CAP]; };
+struct BodyList { float4 a[LIST_CAP]; };
 
-__device__ __forceinline__ void nb_eval_bodies(const BodyList& list, int n, float bhx, float bhy,
-                                               float bhz, float blx, float bly, float blz,
-                                               float eps2, float& fx, float& fy, float& fz)
+__device__ __forceinline__ void nb_eval_bodies(const BodyList& list, int n, float rbx, float rby,
+                                               float rbz, float eps2, float& fx, float& fy,
+                                               float& fz)
 {
     for (int e = 0; e < n; ++e) {
-        const float4 a = list.a[e], b = list.b[e];
-        const float dx = (a.x - bhx) + (b.x - blx);
-        const float dy = (a.y - bhy) + (b.y - bly);
-        const float dz = (a.z - bhz) + (b.z - blz);
+        const float4 a = list.a[e];
+        const float dx = a.x - rbx, dy = a.y - rby, dz = a.z - rbz;
         const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
         const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
         const float mor3 = a.w * rinv * rinv * rinv;
@@ -109,16 +113,13 @@ __device__ __forceinline__ void nb_eval_bodies(const BodyList& list, int n, floa
     }
 }
 
-__device__ __forceinline__ void nb_eval_cells(const CellList& list, int n, float bhx, float bhy,
-                                              float bhz, float blx, float bly, float blz,
-                                              float eps2, bool useQuad, float& fx, float& fy,
-                                              float& fz)
+__device__ __forceinline__ void nb_eval_cells(const CellList& list, int n, float rbx, float rby,
+                                              float rbz, float eps2, bool useQuad, float& fx,
+                                              float& fy, float& fz)
 {
     for (int e = 0; e < n; ++e) {
-        const float4 a = list.a[e], b = list.b[e];
-        const float dx = (a.x - bhx) + (b.x - blx);
-        const float dy = (a.y - bhy) + (b.y - bly);
-        const float dz = (a.z - bhz) + (b.z - blz);
+        const float4 a = list.a[e];
+        const float dx = a.x - rbx, dy = a.y - rby, dz = a.z - rbz;
         const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
         const float rinv = rsqrtf(r2);
         const float rinv2 = rinv * rinv;
@@ -127,8 +128,8 @@ __device__ __forceinline__ void nb_eval_cells(const CellList& list, int n, float
         fy = fmaf(mor3, dy, fy);
         fz = fmaf(mor3, dz, fz);
         if (useQuad) {
-            const float4 c = list.c[e], d = list.d[e];
-            const float qxx = b.w, qxy = c.x, qxz = c.y, qyy = c.z, qyz = c.w, qzz = d.x;
+            const float4 b = list.b[e], c = list.c[e];
+            const float qxx = b.x, qxy = b.y, qxz = b.z, qyy = b.w, qyz = c.x, qzz = c.y;
             const float qdx = fmaf(qxz, dz, fmaf(qxy, dy, qxx * dx));
             const float qdy = fmaf(qyz, dz, fmaf(qyy, dy, qxy * dx));
             const float qdz = fmaf(qzz, dz, fmaf(qyz, dy, qxz * dx));
@@ -238,6 +239,8 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
         }
         const float cx = 0.5f * (mnx + mxx), cy = 0.5f * (mny + mxy), cz = 0.5f * (mnz + mxz);
         const float hx = 0.5f * (mxx - mnx), hy = 0.5f * (mxy - mny), hz = 0.5f * (mxz - mnz);
+        // the body relative to the group centre
+        const float rbx = (bhx - cx) + blx, rby = (bhy - cy) + bly, rbz = (bhz - cz) + blz;
         double accx = 0.0, accy = 0.0, accz = 0.0;
         float fx = 0.f, fy = 0.f, fz = 0.f;
         int nC = 0, nB = 0;
@@ -275,29 +278,26 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
                 cBC += 32ull * __popc(cellMask);
             }
             if (nB + __popc(bodyMask) > LIST_CAP) {
-                nb_eval_bodies(bodies, nB, bhx, bhy, bhz, blx, bly, blz, eps2, fx, fy, fz);
+                nb_eval_bodies(bodies, nB, rbx, rby, rbz, eps2, fx, fy, fz);
                 nB = 0;
                 __syncwarp();
             }
             if (nC + __popc(cellMask) > LIST_CAP) {
-                nb_eval_cells(cells, nC, bhx, bhy, bhz, blx, bly, blz, eps2, useQuad, fx, fy, fz);
+                nb_eval_cells(cells, nC, rbx, rby, rbz, eps2, useQuad, fx, fy, fz);
                 nC = 0;
                 __syncwarp();
                 accx += (double) fx; accy += (double) fy; accz += (double) fz;
                 fx = fy = fz = 0.f;
             }
-            if (isBody) {
-                const int e = nB + __popc(bodyMask & ltMask);
-                bodies.a[e] = make_float4(hi.x, hi.y, hi.z, lo.w);
-                bodies.b[e] = make_float4(lo.x, lo.y, lo.z, 0.f);
-            }
+            const float4 rel = make_float4((hi.x - cx) + lo.x, (hi.y - cy) + lo.y,
+                                           (hi.z - cz) + lo.z, lo.w);
+            if (isBody) bodies.a[nB + __popc(bodyMask & ltMask)] = rel;
             if (accCell) {
                 const int e = nC + __popc(cellMask & ltMask);
                 const float4 qa = nodeQ32[2 * (size_t) k], qb = nodeQ32[2 * (size_t) k + 1];
-                cells.a[e] = make_float4(hi.x, hi.y, hi.z, lo.w);
-                cells.b[e] = make_float4(lo.x, lo.y, lo.z, qa.x);
-                cells.c[e] = make_float4(qa.y, qa.z, qa.w, qb.x);
-                cells.d[e] = make_float4(qb.y, 0.f, 0.f, 0.f);
+                cells.a[e] = rel;
+                cells.b[e] = qa;
+                cells.c[e] = qb;
             }
             nB += __popc(bodyMask);
             nC += __popc(cellMask);
@@ -324,8 +324,8 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
             __syncwarp();
         }
         __syncwarp();
-        nb_eval_bodies(bodies, nB, bhx, bhy, bhz, blx, bly, blz, eps2, fx, fy, fz);
-        nb_eval_cells(cells, nC, bhx, bhy, bhz, blx, bly, blz, eps2, useQuad, fx, fy, fz);
+        nb_eval_bodies(bodies, nB, rbx, rby, rbz, eps2, fx, fy, fz);
+        nb_eval_cells(cells, nC, rbx, rby, rbz, eps2, useQuad, fx, fy, fz);
         __syncwarp();
         accx += (double) fx; accy += (double) fy; accz += (double) fz;
         if (valid) {

@@ -69,6 +69,38 @@ __device__ __forceinline__ void nb_ext_accel(const NbPot& p, double x, double y,
     ox = axx; oy = ayy; oz = azz;
 }
 
+// The potential Phi whose gradient nb_ext_accel returns (a = -grad Phi), for energy checks
+// (not on the bit-exact path): Miyamoto-Nagai -M / sqrt(R^2 + (a + sqrt(z^2 + b^2))^2),
+// logarithmic v0^2 ln(d^2 + x^2 + y^2 + z^2/q^2), NFW -M ln(1 + r/a) / r, Hernquist
+// -M / (r + a), Plummer -M / sqrt(r^2 + a^2), with the same r floor of 2^-8 as the forces.
+__device__ __forceinline__ double nb_ext_potential(const NbPot& p, double x, double y, double z)
+{
+    const double absv = sqrt(z * z + (y * y + x * x));
+    const double r = absv > 0.00390625 ? absv : 0.00390625;
+    double phi = 0.0;
+    for (int d = 0; d < 2; ++d) {
+        const int type = d == 0 ? p.diskType : p.disk2Type;
+        if (type != NBCUDA_MIYAMOTO_NAGAI_DISK) continue;
+        const double M = d == 0 ? p.diskMass : p.disk2Mass;
+        const double a = d == 0 ? p.diskA : p.disk2A, b = d == 0 ? p.diskB : p.disk2B;
+        const double azp = a + sqrt(z * z + b * b);
+        phi -= M / sqrt(x * x + y * y + azp * azp);
+    }
+    if (p.haloType == NBCUDA_LOGARITHMIC_HALO) {
+        const double zq = z / p.haloQz;
+        phi += p.haloV * p.haloV * log(p.haloA * p.haloA + x * x + y * y + zq * zq);
+    } else if (p.haloType == NBCUDA_NFW_HALO) {
+        const double a = p.haloA;
+        const double M = p.haloV * p.haloV * a / 0.2162165954;
+        phi -= M * log((a + r) / a) / r;
+    }
+    if (p.sphType == NBCUDA_HERNQUIST_SPHERICAL)
+        phi -= p.sphMass / (r + p.sphScale);
+    else if (p.sphType == NBCUDA_PLUMMER_SPHERICAL)
+        phi -= p.sphMass / sqrt(r * r + p.sphScale * p.sphScale);
+    return phi;
+}
+
 // nbMapForceBody's epilogue (nbody/src/nbody_grav.c:167-176): a += nbExtAcceleration(pos)
 // + plummerAccel(pos, LMC at the origin, mass 0, scale 1), whose value is (0 - pos) * 0.
 __device__ __forceinline__ void nb_finish_body(const NbPot& pot, const NbWalkParams& wp, unsigned j,

@@ -172,6 +172,65 @@ k_direct_sample(const double* __restrict__ px, const double* __restrict__ py,
     if (valid) { out[3 * t] = accx; out[3 * t + 1] = accy; out[3 * t + 2] = accz; }
 }
 
+// Total energy of the current state, FP64 direct summation (the energy-drift oracle of the
+// walk forms; O(N^2)): out[0] += sum m v^2 / 2, out[1] += -sum_{i<j} m_i m_j / sqrt(r^2 + eps^2)
+// (the softened pair potential whose gradient the walk's forces are), out[2] += sum m Phi_ext.
+__global__ void __launch_bounds__(EXACT_TILE)
+k_energy(const double* __restrict__ px, const double* __restrict__ py,
+         const double* __restrict__ pz, const double* __restrict__ vx,
+         const double* __restrict__ vy, const double* __restrict__ vz,
+         const double* __restrict__ mass, int n, double eps2, NbPot pot, double* __restrict__ out)
+{
+    __shared__ double4 tile[EXACT_TILE];
+    __shared__ double red[3][EXACT_TILE / 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const double x0 = valid ? px[i] : 0.0, y0 = valid ? py[i] : 0.0, z0 = valid ? pz[i] : 0.0;
+    double phi = 0.0;
+    for (int base = 0; base < n; base += EXACT_TILE) {
+        const int k = base + threadIdx.x;
+        __syncthreads();
+        tile[threadIdx.x] = k < n ? make_double4(px[k], py[k], pz[k], mass[k]) : make_double4(0, 0, 0, 0);
+        __syncthreads();
+        const int lim = min(EXACT_TILE, n - base);
+        for (int s = 0; s < lim; ++s) {
+            const double4 b = tile[s];
+            const double dx = b.x - x0, dy = b.y - y0, dz = b.z - z0;
+            const double drSq = (dz * dz + (dy * dy + dx * dx)) + eps2;
+            phi += base + s == i ? 0.0 : b.w / sqrt(drSq);
+        }
+    }
+    double e[3] = {0.0, 0.0, 0.0};
+    if (valid) {
+        const double m = mass[i];
+        e[0] = 0.5 * m * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]);
+        e[1] = -0.5 * m * phi;
+        e[2] = pot.enabled ? m * nb_ext_potential(pot, x0, y0, z0) : 0.0;
+    }
+    for (int c = 0; c < 3; ++c) {
+        double v = e[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(NB_FULL_MASK, v, o);
+        if ((threadIdx.x & 31) == 0) red[c][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double v = 0.0;
+        for (int w = 0; w < EXACT_TILE / 32; ++w) v += red[threadIdx.x][w];
+        atomicAdd(out + threadIdx.x, v);
+    }
+}
+
+void nb_launch_energy(const double* px, const double* py, const double* pz, const double* vx,
+                      const double* vy, const double* vz, const double* mass, int n, double eps2,
+                      const NbPot& pot, double* out, cudaStream_t s)
+{
+    cudaMemsetAsync(out, 0, 3 * sizeof(double), s);
+    if (n <= 0) return;
+    k_energy<<<(n + EXACT_TILE - 1) / EXACT_TILE, EXACT_TILE, 0, s>>>(px, py, pz, vx, vy, vz, mass,
+                                                                     n, eps2, pot, out);
+    nb_count_launch();
+}
+
 // FMA throughput probe: independent FMA chains per thread (the denominator of the walk's
 // pipe roofline).  fp64 selects DFMA or FFMA.
 template <typename T>

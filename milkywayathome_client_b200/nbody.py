@@ -272,6 +272,12 @@ class NBodyState:
         self.lib.nbLastStepTimeCUDA(self._h, ctypes.byref(ms))
         return ms.value
 
+    def energy(self, ctx):
+        """(kinetic, self-gravity, external) energy of the current state, FP64 direct sum."""
+        out = (ctypes.c_double * 3)()
+        self.check("nbEnergy", self.lib.nbEnergyCUDA(ctypes.byref(ctx.struct), self._h, out))
+        return tuple(out)
+
     def direct_sample(self, eps2, targets):
         """FP64 direct-sum self-gravity at the given body indices (accuracy oracle)."""
         targets = np.ascontiguousarray(targets, dtype=np.int32)

@@ -11,7 +11,10 @@ OpenCL/BOINC/GL/curses off).
 Templates read (paths inside the reference tree):
   milkyway/include/milkyway_config.h.in, milkyway/include/milkyway_git_version.h.in,
   nbody/include/nbody_config.h.in, lua/include/luaconf.h.in,
-  popt/include/popt_config.h.in, openpa/include/opa_config.h.in
+  popt/include/popt_config.h.in, openpa/include/opa_config.h.in,
+  crlibm/crlibm_config.h.in (written twice: into the output directory for
+  ``#include "crlibm_config.h"`` and into its parent, where crlibm's
+  ``scs_lib/scs.h`` finds ``#include "../crlibm_config.h"`` through ``-I<output>``)
 
 Usage: configure_ref.py <reference-root> <output-include-dir>
 """
@@ -57,6 +60,8 @@ VALUES = {
     "OPA_HAVE_LIBPTHREAD": "1", "OPA_HAVE_PTHREAD_H": "1", "OPA_HAVE_PTHREAD_YIELD": "1",
     "OPA_HAVE_SCHED_YIELD": "1", "OPA_HAVE_STDDEF_H": "1",
     "MAX_NTHREADS": "100", "SIZEOF_INT": "4", "SIZEOF_VOID_P": "8",
+    # crlibm_config.h.in
+    "HAVE_FENV_H": "1",
 }
 
 TEMPLATES = [
@@ -66,6 +71,8 @@ TEMPLATES = [
     ("lua/include/luaconf.h.in", "luaconf.h"),
     ("popt/include/popt_config.h.in", "popt_config.h"),
     ("openpa/include/opa_config.h.in", "opa_config.h"),
+    ("crlibm/crlibm_config.h.in", "crlibm_config.h"),
+    ("crlibm/crlibm_config.h.in", os.path.join(os.pardir, "crlibm_config.h")),
 ]
 
 
