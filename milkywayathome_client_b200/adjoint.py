@@ -110,13 +110,39 @@ class DeviceState:
         return xbar, mbar
 
 
+# Device states kept between runs, one per (bodies, device): a state keeps its buffers and the
+# saved trees of its last backward pass allocated, so repeated runs (an optimisation loop)
+# allocate nothing after the first.  release_states() frees them.
+_POOL = {}
+
+
+def _acquire(n, device):
+    ds = _POOL.pop((n, device.index or 0), None)
+    return ds if ds is not None else DeviceState(n, device)
+
+
+def _release(ds):
+    key = (ds.n, ds.device.index or 0)
+    old = _POOL.pop(key, None)
+    if old is not None:
+        old.close()
+    _POOL[key] = ds
+
+
+def release_states():
+    """Free the device states (and their saved trees) kept between runs."""
+    for ds in _POOL.values():
+        ds.close()
+    _POOL.clear()
+
+
 class _Run(torch.autograd.Function):
     """(x0, v0, m, dt) -> (xN, vN) through nsteps GPU steps; see the module docstring."""
 
     @staticmethod
     def forward(fctx, x0, v0, m, dt, nbctx, nsteps, every, stats):
         n = x0.shape[0]
-        ds = DeviceState(n, x0.device)
+        ds = _acquire(n, x0.device)
         ctx = NBodyCtx.from_struct(nbctx.struct)
         ctx.struct.timestep = float(dt)
         x0c, v0c, mc = x0.detach().contiguous(), v0.detach().contiguous(), m.detach().contiguous()
@@ -146,6 +172,9 @@ class _Run(torch.autograd.Function):
             stats["forward_step_ms"] = ev0.elapsed_time(ev1) / max(nsteps, 1)
             stats["forward_step_device_ms"] = fwd_ms / max(nsteps, 1)
         fctx.save_for_backward(mc)
+        if not any(fctx.needs_input_grad[:4]):
+            fctx.ds = None                # no backward pass will come
+            _release(ds)
         return xN, vN
 
     @staticmethod
@@ -198,7 +227,7 @@ class _Run(torch.autograd.Function):
             fctx.stats["recompute_step_device_ms"] = rec_ms / max(nsteps, 1)
             fctx.stats["reverse_step_device_ms"] = rev_ms / max(rev_calls, 1)
             fctx.stats["vjp_walk_device_ms"] = rev_walk_ms / max(rev_calls, 1)
-        ds.close()
+        _release(ds)
         return xbar, vbar, mbar, dtbar, None, None, None, None
 
 

@@ -844,16 +844,20 @@ NBodyCudaStatus nbSaveStateCUDA(NBodyCudaState* st, int slot)
     NbSlot& sl = st->slots[slot];
     const size_t n = (size_t) st->nbody;
     const size_t nodes = st->haveTree ? (size_t) st->scHost->nNodes : 0;
-    const size_t need = nb_align256(10 * n * sizeof(double)) + 2 * nb_align256(n * sizeof(int)) +
-                        nb_align256(nodes * sizeof(double4)) + nb_align256(nodes * sizeof(double)) +
-                        nb_align256(nodes * sizeof(int2)) + nb_align256(6 * nodes * sizeof(double)) +
-                        nb_align256(nodes * sizeof(int)) + 256;
-    if (sl.bytes < need) {
+    auto bytesFor = [n](size_t nn) {
+        return nb_align256(10 * n * sizeof(double)) + 2 * nb_align256(n * sizeof(int)) +
+               nb_align256(nn * sizeof(double4)) + nb_align256(nn * sizeof(double)) +
+               nb_align256(nn * sizeof(int2)) + nb_align256(6 * nn * sizeof(double)) +
+               nb_align256(nn * sizeof(int)) + 256;
+    };
+    if (sl.bytes < bytesFor(nodes)) {
+        // room for a quarter more nodes: the node count changes a little from step to step
+        const size_t want = bytesFor(nodes + nodes / 4 + 1024);
         cudaFree(sl.mem);
         sl.mem = nullptr;
         sl.bytes = 0;
-        NB_CHECK(cudaMalloc((void**) &sl.mem, need));
-        sl.bytes = need;
+        NB_CHECK(cudaMalloc((void**) &sl.mem, want));
+        sl.bytes = want;
     }
     char* p = sl.mem;
     auto carve = [&p](size_t bytes) { char* q = p; p += nb_align256(bytes); return q; };
