@@ -209,6 +209,54 @@ NBodyCudaStatus nbStepAdjointCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, c
  * for the context's potential (0 with EXTERNAL_POTENTIAL_NONE).  Host array of 3 doubles. */
 NBodyCudaStatus nbEnergyCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, double* energy);
 
+/* ---- batched dwarfs (no reference counterpart: the reference runs one dwarf per process) ----
+ * Many independent dwarfs stepped together.  Each dwarf is the reference's simulation (its own
+ * root at the origin, root size, octree, softening and time step) and gets the same
+ * accelerations, bit for bit, as a single-dwarf state (FP64 precision); every phase of the step
+ * (bounding boxes, keys, sort, tree, moments, walk with the kick) is one launch over all
+ * dwarfs, and nbBatchRunStepsCUDA can replay the whole step as one captured CUDA graph.
+ * Bodies are concatenated dwarf after dwarf (dwarf 0's nbody bodies first) in every array;
+ * all of them must be massive.  The context supplies the criterion (a tree criterion), theta,
+ * quadrupoles, incest policy, potential and precision; eps2, timestep and treeRSize come from
+ * each dwarf's NBodyCudaDwarf. */
+typedef struct NBodyCudaBatch NBodyCudaBatch;
+typedef struct {
+    int nbody;           /* bodies of this dwarf, >= 2 */
+    double eps2;         /* softening length squared */
+    double timestep;     /* leapfrog step */
+    double treeRSize;    /* initial root size, a power of two */
+} NBodyCudaDwarf;
+NBodyCudaStatus nbBatchCreateCUDA(NBodyCudaBatch** batch, int device, const NBodyCudaDwarf* dwarfs,
+                                  int ndwarfs);
+NBodyCudaStatus nbBatchDestroyCUDA(NBodyCudaBatch* batch);
+/* host arrays: pos, vel 3 doubles per body, mass 1 (resets root sizes and statuses) */
+NBodyCudaStatus nbBatchSetBodiesCUDA(NBodyCudaBatch* batch, const double* pos, const double* vel,
+                                     const double* mass);
+NBodyCudaStatus nbBatchSetBodiesDeviceCUDA(NBodyCudaBatch* batch, const double* dpos,
+                                           const double* dvel, const double* dmass);
+/* host arrays; any may be NULL */
+NBodyCudaStatus nbBatchGetBodiesCUDA(NBodyCudaBatch* batch, double* pos, double* vel, double* acc);
+NBodyCudaStatus nbBatchGetBodiesDeviceCUDA(NBodyCudaBatch* batch, double* dpos, double* dvel,
+                                           double* dacc);
+/* nbGravMap of every dwarf */
+NBodyCudaStatus nbBatchGravMapCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* batch);
+/* nsteps kick-drift-kick steps of every dwarf (an initial nbGravMap if none was made);
+ * useGraph != 0 replays one captured graph per step.  Stops at the first fatal status. */
+NBodyCudaStatus nbBatchRunStepsCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* batch, int nsteps,
+                                    int useGraph);
+/* per dwarf (arrays of ndwarfs, any may be NULL): sticky status bits of its tree builds, its
+ * current root size, its root's node index and node count */
+NBodyCudaStatus nbBatchDwarfInfoCUDA(NBodyCudaBatch* batch, int* status, double* rsize,
+                                     int* rootNode, int* nodes);
+/* mixed-precision walk tuning: bodies per walk group (1..32), interaction-list entries per
+ * warp (32, 64 or 128), resident walk blocks per SM (0: as many as fit) */
+NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* batch, int groupMax, int listCap,
+                                     int blocksPerSM);
+NBodyCudaStatus nbBatchGetTuningCUDA(NBodyCudaBatch* batch, int* groupMax, int* listCap,
+                                     int* blocksPerSM);
+/* mean device time of the steps of the last nbBatchRunStepsCUDA call */
+NBodyCudaStatus nbBatchLastStepTimeCUDA(NBodyCudaBatch* batch, double* stepMs);
+
 /* ---- tree introspection (parity checks of nbMakeTree) ---- */
 NBodyCudaStatus nbMakeTreeCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st);
 NBodyCudaStatus nbTreeInfoCUDA(NBodyCudaState* st, NBodyCudaTreeInfo* info);

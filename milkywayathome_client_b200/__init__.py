@@ -6,10 +6,11 @@ sm_100a, C ABI in include/nbody_b200.h).  `nbody` mirrors the reference's step i
 (NBodyCtx, Potential, NBodyState.create / step) on top of it; `models` holds the set-up
 formulas and a synthetic dwarf sampler.
 """
-from .nbody import (Disk, Halo, NBodyCtx, NBodyError, NBodyState, Potential, Spherical,
-                    ext_acceleration, kernel_launches, milky_way_potential)
+from .nbody import (Disk, Halo, NBodyBatch, NBodyCtx, NBodyError, NBodyState, Potential,
+                    Spherical, ext_acceleration, kernel_launches, milky_way_potential)
 from ._lib import status_is_fatal, status_names
 
-__all__ = ["Disk", "Halo", "NBodyCtx", "NBodyError", "NBodyState", "Potential", "Spherical",
+__all__ = ["Disk", "Halo", "NBodyBatch", "NBodyCtx", "NBodyError", "NBodyState", "Potential",
+           "Spherical",
            "ext_acceleration", "kernel_launches", "milky_way_potential", "status_is_fatal",
            "status_names"]

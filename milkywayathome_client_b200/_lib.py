@@ -77,6 +77,11 @@ class Potential(ctypes.Structure):
     _fields_ = [("sphere", Spherical), ("disk", Disk), ("disk2", Disk), ("halo", Halo)]
 
 
+class Dwarf(ctypes.Structure):
+    _fields_ = [("nbody", ctypes.c_int), ("eps2", ctypes.c_double),
+                ("timestep", ctypes.c_double), ("treeRSize", ctypes.c_double)]
+
+
 class Ctx(ctypes.Structure):
     """NBodyCudaCtx: the NBodyCtx fields the step reads."""
     _fields_ = [("eps2", ctypes.c_double), ("theta", ctypes.c_double),
@@ -115,6 +120,19 @@ SIGNATURES = [
     ("nbMakeTreeCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp]),
     ("nbGravVJPCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, _vp, _vp, _vp]),
     ("nbEnergyCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, _dp]),
+    ("nbBatchCreateCUDA", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                         ctypes.POINTER(Dwarf), ctypes.c_int]),
+    ("nbBatchDestroyCUDA", ctypes.c_int, [_vp]),
+    ("nbBatchSetBodiesCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("nbBatchSetBodiesDeviceCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("nbBatchGetBodiesCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("nbBatchGetBodiesDeviceCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("nbBatchGravMapCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp]),
+    ("nbBatchRunStepsCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, ctypes.c_int, ctypes.c_int]),
+    ("nbBatchDwarfInfoCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    ("nbBatchSetTuningCUDA", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("nbBatchGetTuningCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("nbBatchLastStepTimeCUDA", ctypes.c_int, [_vp, _dp]),
     ("nbSaveStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbRestoreStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbReleaseStatesCUDA", ctypes.c_int, [_vp]),

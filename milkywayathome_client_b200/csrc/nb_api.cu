@@ -7,17 +7,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 // ---- kernels defined in the other translation units ----
-void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
-                         const double* nodeQuad, const unsigned* order, const double* px,
-                         const double* py, const double* pz, double* ax, double* ay, double* az,
-                         double* vx, double* vy, double* vz, const NbWalkParams& wp,
-                         const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s);
-void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int capNodes,
-                          const NbWalkParams& wp, const NbPot& pot, bool count, int numSMs,
-                          cudaStream_t s);
 void nb_launch_direct_sample(const double* px, const double* py, const double* pz,
                              const double* mass, int n, const int* targets, int count,
                              double eps2, double* out, cudaStream_t s);
@@ -1037,5 +1030,392 @@ NBodyCudaStatus nbSetCountingCUDA(NBodyCudaState* st, int enable)
 }
 
 const char* nbLastErrorCUDA(void) { return g_lastError.c_str(); }
+
+}  // extern "C"
+
+// =============================================================================================
+// Batched dwarfs (nb_batch.cu builds the forest; the walks take the forest description)
+// =============================================================================================
+int nb_build_forest(NbTreeBuffers& b, const NbForest& f, int n, int capNodes, int criterion,
+                    double theta, int useQuad, int drift, int numSMs, cudaStream_t s);
+
+struct NbBatchTuning {
+    int groupMax = 32;      // bodies per walk group of the mixed walk
+    int listCap = 64;       // interaction-list entries per warp
+    int blocksPerSM = 0;    // resident walk blocks per SM (0: as many as fit)
+};
+
+struct NBodyCudaBatch {
+    NBodyCudaState* st = nullptr;       // the bodies of all dwarfs, concatenated
+    int nDwarfs = 0;
+    std::vector<NBodyCudaDwarf> dwarfs;  // host parameters
+    NbDwarfDev* dDwarfs = nullptr;      // device table
+    NbDwarfDev* hDwarfs = nullptr;      // pinned mirror
+    int* bodyDwarf = nullptr;
+    NbBatchTuning tune;
+    int maxWalkBlocks = 0;              // walk stacks are sized for this many blocks
+    // captured step
+    cudaGraphExec_t graph = nullptr;
+    NBodyCudaCtx graphCtx{};
+    int graphDrift = -1, graphKick = -1, graphCap = -1, graphLaunches = 0;
+    NbBatchTuning graphTune;
+    double lastStepMs = 0.0;
+    int lastSteps = 0;
+};
+
+static NbForest nb_forest_of(NBodyCudaBatch* bt)
+{
+    return NbForest{bt->bodyDwarf, bt->dDwarfs, bt->nDwarfs};
+}
+
+static void nb_batch_drop_graph(NBodyCudaBatch* bt)
+{
+    if (bt->graph) cudaGraphExecDestroy(bt->graph);
+    bt->graph = nullptr;
+    bt->graphCap = -1;
+}
+
+// Walk stacks for the largest persistent grid any tuning can ask for.
+static NBodyCudaStatus nb_batch_mixed_buffers(NBodyCudaBatch* bt)
+{
+    NBodyCudaState* st = bt->st;
+    if (!bt->maxWalkBlocks) {
+        int mx = 0;
+        for (int cap : {32, 64, 128}) mx = std::max(mx, nb_mixed_walk_blocks(st->numSMs, cap));
+        bt->maxWalkBlocks = mx;
+    }
+    if (!st->mx.stacks) NB_CHECK(nb_alloc(&st->mx.stacks, nb_mixed_stack_ints(bt->maxWalkBlocks)));
+    const int fit = nb_mixed_walk_blocks(st->numSMs, bt->tune.listCap) / st->numSMs;
+    const int per = bt->tune.blocksPerSM > 0 ? std::min(bt->tune.blocksPerSM, fit) : fit;
+    st->mx.walkBlocks = std::max(1, per) * st->numSMs;
+    st->mx.groupMax = bt->tune.groupMax;
+    st->mx.listCap = bt->tune.listCap;
+    return NBODY_SUCCESS;
+}
+
+// The device work of one evaluation, enqueued on the batch's stream without any host
+// synchronisation (so that it can be captured in a graph).  Returns the launches issued.
+static int nb_batch_enqueue(NBodyCudaBatch* bt, const NBodyCudaCtx* ctx, int drift, int kick)
+{
+    NBodyCudaState* st = bt->st;
+    NbTreeBuffers& b = st->b;
+    const cudaStream_t s = st->stream;
+    const NbForest f = nb_forest_of(bt);
+    NbWalkParams wp{};
+    wp.useQuad = ctx->useQuad;
+    wp.kick = kick;
+    wp.n = st->nbody;
+    const NbPot pot = nb_pot_from(ctx);
+    int launches = nb_build_forest(b, f, st->nbody, st->capNodes, ctx->criterion, ctx->theta,
+                                   ctx->useQuad, drift, st->numSMs, s);
+    cudaEventRecord(st->ev0, s);
+    if (ctx->precision == NBCUDA_PRECISION_MIXED) {
+        nb_launch_walk_mixed(b, st->mx, st->capNodes, wp, pot, false, st->numSMs, s, &f);
+        launches += 3;
+    } else {
+        nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px, b.py,
+                            b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc, false, s, &f);
+        launches += 1;
+    }
+    cudaEventRecord(st->ev1, s);
+    cudaMemcpyAsync(st->scHost, b.sc, sizeof(NbScalars), cudaMemcpyDeviceToHost, s);
+    return launches;
+}
+
+static bool nb_same_tuning(const NbBatchTuning& a, const NbBatchTuning& b)
+{
+    return a.groupMax == b.groupMax && a.listCap == b.listCap && a.blocksPerSM == b.blocksPerSM;
+}
+
+// One evaluation of every dwarf (drift/kick: the fused halves of the leapfrog), optionally
+// through a captured graph of the whole sequence.
+static NBodyCudaStatus nb_batch_eval(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt, int drift,
+                                     int kick, bool useGraph)
+{
+    NBodyCudaState* st = bt->st;
+    const cudaStream_t s = st->stream;
+    NbTreeBuffers& b = st->b;
+    const bool mixed = ctx->precision == NBCUDA_PRECISION_MIXED;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        if (mixed) {
+            NBodyCudaStatus rc = nb_batch_mixed_buffers(bt);
+            if (rc) return rc;
+        }
+        // the capacity the build checks against (the reset kernel keeps it)
+        NB_CHECK(cudaMemcpyAsync(&b.sc->capNodes, &st->capNodes, sizeof(int),
+                                 cudaMemcpyHostToDevice, s));
+        NB_CHECK(cudaStreamSynchronize(s));
+        if (useGraph) {
+            const bool same = bt->graph && bt->graphDrift == drift && bt->graphKick == kick &&
+                              bt->graphCap == st->capNodes && nb_same_tuning(bt->graphTune, bt->tune) &&
+                              std::memcmp(&bt->graphCtx, ctx, sizeof *ctx) == 0;
+            if (!same) {
+                nb_batch_drop_graph(bt);
+                cudaGraph_t g = nullptr;
+                NB_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                const int launches = nb_batch_enqueue(bt, ctx, drift, kick);
+                NB_CHECK(cudaStreamEndCapture(s, &g));
+                cudaError_t e = cudaGraphInstantiate(&bt->graph, g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) { bt->graph = nullptr; return nb_cuda_fail(e, "cudaGraphInstantiate"); }
+                bt->graphCtx = *ctx;
+                bt->graphDrift = drift;
+                bt->graphKick = kick;
+                bt->graphCap = st->capNodes;
+                bt->graphTune = bt->tune;
+                bt->graphLaunches = launches;
+            } else {
+                nb_count_launch(bt->graphLaunches);
+            }
+            NB_CHECK(cudaEventRecord(st->evS, s));
+            NB_CHECK(cudaGraphLaunch(bt->graph, s));
+            NB_CHECK(cudaEventRecord(st->evE, s));
+        } else {
+            NB_CHECK(cudaEventRecord(st->evS, s));
+            nb_batch_enqueue(bt, ctx, drift, kick);
+            NB_CHECK(cudaEventRecord(st->evE, s));
+        }
+        NB_CHECK(cudaGetLastError());
+        NB_CHECK(cudaStreamSynchronize(s));
+        const NbScalars& h = *st->scHost;
+        if (h.status & NBODY_CELL_OVERFLOW_ERROR) {
+            // grow the node arrays and redo this evaluation (positions already drifted)
+            nb_batch_drop_graph(bt);
+            NBodyCudaStatus rc = nb_alloc_nodes(st, h.neededNodes + h.neededNodes / 4 + 64);
+            if (rc) return rc;
+            drift = 0;
+            continue;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, st->evS, st->evE);
+        st->stepMs = ms;
+        if (!useGraph) {
+            ms = 0.0f;
+            cudaEventElapsedTime(&ms, st->ev0, st->ev1);
+            st->walkMs = ms;
+        }
+        NBodyCudaStatus out = h.status;
+        if (h.incest) st->treeIncest = 1;
+        if (st->treeIncest)
+            out |= ctx->allowIncest ? NBODY_TREE_INCEST_NONFATAL : NBODY_TREE_INCEST_FATAL;
+        st->haveTree = 1;
+        st->lastCriterion = ctx->criterion;
+        return out;
+    }
+    g_lastError = "node capacity could not be grown";
+    return NBODY_CELL_OVERFLOW_ERROR;
+}
+
+static NBodyCudaStatus nb_batch_check(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt)
+{
+    if (!bt) return NBODY_USER_ERROR;
+    std::string why;
+    NBodyCudaStatus rc = nb_check_ctx(ctx, why);
+    if (rc) { g_lastError = why; return rc; }
+    if (ctx->criterion == NBCUDA_EXACT) {
+        g_lastError = "batched dwarfs use a tree criterion";
+        return NBODY_UNSUPPORTED;
+    }
+    NB_CHECK(cudaSetDevice(bt->st->device));
+    return NBODY_SUCCESS;
+}
+
+// Table of the dwarfs' parameters, root sizes back at treeRSize, statuses cleared.
+static NBodyCudaStatus nb_batch_reset_table(NBodyCudaBatch* bt)
+{
+    int first = 0;
+    for (int d = 0; d < bt->nDwarfs; ++d) {
+        NbDwarfDev& h = bt->hDwarfs[d];
+        h = NbDwarfDev{};
+        h.rsize = bt->dwarfs[d].treeRSize;
+        h.eps2 = bt->dwarfs[d].eps2;
+        h.dt = bt->dwarfs[d].timestep;
+        h.first = first;
+        h.count = bt->dwarfs[d].nbody;
+        first += h.count;
+    }
+    NB_CHECK(cudaMemcpyAsync(bt->dDwarfs, bt->hDwarfs, sizeof(NbDwarfDev) * bt->nDwarfs,
+                             cudaMemcpyHostToDevice, bt->st->stream));
+    NB_CHECK(cudaStreamSynchronize(bt->st->stream));
+    bt->st->treeIncest = 0;
+    bt->st->haveTree = 0;
+    return NBODY_SUCCESS;
+}
+
+extern "C" {
+
+NBodyCudaStatus nbBatchCreateCUDA(NBodyCudaBatch** out, int device, const NBodyCudaDwarf* dwarfs,
+                                  int ndwarfs)
+{
+    if (!out || !dwarfs || ndwarfs < 1 || ndwarfs > 65535) return NBODY_USER_ERROR;
+    *out = nullptr;
+    long long total = 0;
+    for (int d = 0; d < ndwarfs; ++d) {
+        const NBodyCudaDwarf& w = dwarfs[d];
+        if (w.nbody < 2 || !(w.eps2 >= 0.0) || !(w.timestep > 0.0)) {
+            g_lastError = "every dwarf needs >= 2 bodies, eps2 >= 0 and a positive time step";
+            return NBODY_USER_ERROR;
+        }
+        if (!nb_pow2(w.treeRSize)) {
+            g_lastError = "treeRSize must be a positive power of two";
+            return NBODY_UNSUPPORTED;
+        }
+        total += w.nbody;
+    }
+    if (total > (1ll << 30)) { g_lastError = "too many bodies"; return NBODY_USER_ERROR; }
+    NBodyCudaState* st = nullptr;
+    NBodyCudaStatus rc = nbInitCUDA(&st, device, (int) total);
+    if (rc) return rc;
+    NBodyCudaBatch* bt = new NBodyCudaBatch();
+    bt->st = st;
+    bt->nDwarfs = ndwarfs;
+    bt->dwarfs.assign(dwarfs, dwarfs + ndwarfs);
+    cudaError_t e = cudaMalloc((void**) &bt->dDwarfs, sizeof(NbDwarfDev) * ndwarfs);
+    if (e == cudaSuccess) e = cudaMallocHost((void**) &bt->hDwarfs, sizeof(NbDwarfDev) * ndwarfs);
+    if (e == cudaSuccess) e = cudaMalloc((void**) &bt->bodyDwarf, sizeof(int) * (size_t) total);
+    if (e == cudaSuccess) {
+        std::vector<int> owner((size_t) total);
+        size_t k = 0;
+        for (int d = 0; d < ndwarfs; ++d)
+            for (int i = 0; i < dwarfs[d].nbody; ++i) owner[k++] = d;
+        e = cudaMemcpy(bt->bodyDwarf, owner.data(), sizeof(int) * (size_t) total,
+                       cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) rc = nb_cuda_fail(e, "nbBatchCreateCUDA");
+    if (!rc) rc = nb_batch_reset_table(bt);
+    if (rc) { nbBatchDestroyCUDA(bt); return rc; }
+    *out = bt;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbBatchDestroyCUDA(NBodyCudaBatch* bt)
+{
+    if (!bt) return NBODY_SUCCESS;
+    if (bt->st) cudaSetDevice(bt->st->device);
+    nb_batch_drop_graph(bt);
+    cudaFree(bt->dDwarfs);
+    cudaFree(bt->bodyDwarf);
+    if (bt->hDwarfs) cudaFreeHost(bt->hDwarfs);
+    if (bt->st) nbDestroyCUDA(bt->st);
+    delete bt;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbBatchSetBodiesCUDA(NBodyCudaBatch* bt, const double* pos, const double* vel,
+                                     const double* mass)
+{
+    if (!bt) return NBODY_USER_ERROR;
+    for (int i = 0; mass && i < bt->st->nbody; ++i)
+        if (!(mass[i] != 0.0)) {
+            g_lastError = "batched dwarfs hold massive bodies only";
+            return NBODY_UNSUPPORTED;
+        }
+    NBodyCudaStatus rc = nbSetBodiesCUDA(bt->st, pos, vel, mass, bt->st->nbody, 4.0);
+    if (rc) return rc;
+    return nb_batch_reset_table(bt);
+}
+
+NBodyCudaStatus nbBatchSetBodiesDeviceCUDA(NBodyCudaBatch* bt, const double* dpos,
+                                           const double* dvel, const double* dmass)
+{
+    if (!bt) return NBODY_USER_ERROR;
+    NBodyCudaStatus rc = nbSetBodiesDeviceCUDA(bt->st, dpos, dvel, dmass, bt->st->nbody, 4.0);
+    if (rc) return rc;
+    return nb_batch_reset_table(bt);
+}
+
+NBodyCudaStatus nbBatchGetBodiesCUDA(NBodyCudaBatch* bt, double* pos, double* vel, double* acc)
+{
+    if (!bt) return NBODY_USER_ERROR;
+    NBodyCudaStatus rc = nbGetBodiesCUDA(bt->st, pos, vel);
+    if (!rc && acc) rc = nbGetAccelsCUDA(bt->st, acc);
+    return rc;
+}
+
+NBodyCudaStatus nbBatchGetBodiesDeviceCUDA(NBodyCudaBatch* bt, double* dpos, double* dvel,
+                                           double* dacc)
+{
+    if (!bt) return NBODY_USER_ERROR;
+    return nbGetBodiesDeviceCUDA(bt->st, dpos, dvel, dacc);
+}
+
+NBodyCudaStatus nbBatchGravMapCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt)
+{
+    NBodyCudaStatus rc = nb_batch_check(ctx, bt);
+    if (rc) return rc;
+    return nb_batch_eval(ctx, bt, 0, 0, false);
+}
+
+NBodyCudaStatus nbBatchRunStepsCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt, int nsteps,
+                                    int useGraph)
+{
+    NBodyCudaStatus rc = nb_batch_check(ctx, bt);
+    if (rc) return rc;
+    if (nsteps < 0) return NBODY_USER_ERROR;
+    if (!bt->st->haveTree) {
+        // the first kick needs the accelerations of the initial positions
+        rc = nb_batch_eval(ctx, bt, 0, 0, false);
+        if (rc & ~(int) NBODY_STATUS_WARNINGS_MASK) return rc;
+    }
+    double total = 0.0;
+    NBodyCudaStatus out = NBODY_SUCCESS;
+    for (int k = 0; k < nsteps; ++k) {
+        const NBodyCudaStatus rcStep = nb_batch_eval(ctx, bt, 1, 1, useGraph != 0);
+        out |= rcStep;
+        total += bt->st->stepMs;
+        bt->st->step++;
+        if (rcStep & ~(int) NBODY_STATUS_WARNINGS_MASK) break;
+    }
+    bt->lastStepMs = nsteps ? total / nsteps : 0.0;
+    bt->lastSteps = nsteps;
+    return out;
+}
+
+NBodyCudaStatus nbBatchDwarfInfoCUDA(NBodyCudaBatch* bt, int* status, double* rsize,
+                                     int* rootNode, int* nodes)
+{
+    if (!bt) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(bt->st->device));
+    NB_CHECK(cudaMemcpyAsync(bt->hDwarfs, bt->dDwarfs, sizeof(NbDwarfDev) * bt->nDwarfs,
+                             cudaMemcpyDeviceToHost, bt->st->stream));
+    NB_CHECK(cudaStreamSynchronize(bt->st->stream));
+    for (int d = 0; d < bt->nDwarfs; ++d) {
+        const NbDwarfDev& h = bt->hDwarfs[d];
+        if (status) status[d] = h.status;
+        if (rsize) rsize[d] = h.rsize;
+        if (rootNode) rootNode[d] = h.rootNode;
+        if (nodes) nodes[d] = h.rootEnd - h.rootNode;
+    }
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* bt, int groupMax, int listCap,
+                                     int blocksPerSM)
+{
+    if (!bt || groupMax < 1 || groupMax > 32 || (listCap != 32 && listCap != 64 && listCap != 128) ||
+        blocksPerSM < 0)
+        return NBODY_USER_ERROR;
+    bt->tune.groupMax = groupMax;
+    bt->tune.listCap = listCap;
+    bt->tune.blocksPerSM = blocksPerSM;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbBatchGetTuningCUDA(NBodyCudaBatch* bt, int* groupMax, int* listCap,
+                                     int* blocksPerSM)
+{
+    if (!bt) return NBODY_USER_ERROR;
+    if (groupMax) *groupMax = bt->tune.groupMax;
+    if (listCap) *listCap = bt->tune.listCap;
+    if (blocksPerSM) *blocksPerSM = bt->tune.blocksPerSM;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbBatchLastStepTimeCUDA(NBodyCudaBatch* bt, double* stepMs)
+{
+    if (!bt || !stepMs) return NBODY_USER_ERROR;
+    *stepMs = bt->lastSteps ? bt->lastStepMs : bt->st->stepMs;
+    return NBODY_SUCCESS;
+}
 
 }  // extern "C"

@@ -105,6 +105,26 @@ __device__ __forceinline__ bool nb_failed(const NbScalars* sc)
     return (*(volatile const int*) &sc->status & ~(int) NBODY_STATUS_WARNINGS_MASK) != 0;
 }
 
+// ---- batched dwarfs: a forest of independent trees in one set of arrays ----
+// Dwarf d owns bodies [first, first + count) (input order and sorted order alike: the sort
+// orders by dwarf first) and the nodes [rootNode, rootEnd) in walk order.
+struct NbDwarfDev {
+    unsigned long long xyzmaxBits;  // max |coordinate| over the dwarf's bodies (bit pattern)
+    double rsize;                   // the dwarf's root size, kept between steps
+    double gridScale;               // 2^62 / rsize
+    double eps2;                    // softening^2 of this dwarf
+    double dt;                      // time step of this dwarf
+    int first, count;               // body range
+    int rootNode, rootEnd;          // root node and Next(root)
+    int depthEps;                   // first depth whose cell size is <= DBL_EPSILON
+    int status;                     // status bits raised while building this dwarf's tree
+};
+struct NbForest {
+    const int* bodyDwarf;           // dwarf of every body (input = sorted position)
+    NbDwarfDev* dwarfs;
+    int nDwarfs;
+};
+
 // Launch accounting (all launches of this library go through nb_count_launch).
 void nb_count_launch(int n = 1);
 
@@ -118,6 +138,9 @@ struct NbSortBuffers {
 };
 // Sorts (keyA, idxA) by key in place (result in keyA/idxA); n items.
 void nb_radix_sort(NbSortBuffers& b, int n, cudaStream_t s);
+// Sorts (keyA, idxA) by (group[idx], key): the key passes, then two stable passes over the
+// 16-bit group of each item's index (result in keyA/idxA).
+void nb_radix_sort_grouped(NbSortBuffers& b, int n, const int* group, cudaStream_t s);
 // Device buffers of one simulation.
 struct NbTreeBuffers {
     double *px, *py, *pz, *vx, *vy, *vz, *ax, *ay, *az, *mass;
@@ -139,9 +162,22 @@ struct NbMixedBuffers {
     int* stacks;   // per resident warp: the group walk's depth-first stack
     int2* groups;  // walk groups: first sorted body, body count (<= 32)
     int walkBlocks;
+    int groupMax;  // bodies per walk group, 1..32 (0: 32)
+    int listCap;   // interaction-list entries per warp: 32, 64 or 128 (0: 64)
 };
-int nb_mixed_walk_blocks(int numSMs);
+int nb_mixed_walk_blocks(int numSMs, int listCap = 0);
 size_t nb_mixed_stack_ints(int blocks);
+
+// The walks (forest != nullptr: one tree per dwarf, see NbForest).
+void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
+                         const double* nodeQuad, const unsigned* order, const double* px,
+                         const double* py, const double* pz, double* ax, double* ay, double* az,
+                         double* vx, double* vy, double* vz, const NbWalkParams& wp,
+                         const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s,
+                         const NbForest* forest = nullptr);
+void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int capNodes,
+                          const NbWalkParams& wp, const NbPot& pot, bool count, int numSMs,
+                          cudaStream_t s, const NbForest* forest = nullptr);
 
 void nb_build_tree(NbTreeBuffers& b, int n, int criterion, double theta, int useQuad, int drift,
                    double dt, int numSMs, cudaStream_t s);

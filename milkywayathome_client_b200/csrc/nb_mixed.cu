@@ -28,16 +28,20 @@ __device__ __forceinline__ void nb_split(double v, float& hi, float& lo)
 }
 
 // FP32 node records for the mixed walk (one pass over the nodes after the moments).
+// FOREST: positions relative to the centre of mass of the node's own dwarf's root.
+template <bool FOREST>
 __global__ void k_pack_f32(const double4* __restrict__ nodePM, const double* __restrict__ nodeCrit,
                            const int2* __restrict__ nodeLink, const double* __restrict__ nodeQuad,
                            float4* __restrict__ nodeHi, float4* __restrict__ nodeLo,
                            float4* __restrict__ nodeQ32, int4* __restrict__ child8,
-                           const NbScalars* __restrict__ sc)
+                           const int2* __restrict__ nodeRange, const NbScalars* __restrict__ sc,
+                           NbForest forest)
 {
     if (nb_failed(sc)) return;
     const int nNodes = sc->nNodes;
-    const double4 root = nodePM[0];
+    double4 root = nodePM[0];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nNodes; k += gridDim.x * blockDim.x) {
+        if (FOREST) root = nodePM[forest.dwarfs[forest.bodyDwarf[nodeRange[k].x]].rootNode];
         const double4 p = nodePM[k];
         float hx, hy, hz, lx, ly, lz;
         nb_split(p.x - root.x, hx, lx);
@@ -85,7 +89,6 @@ __global__ void k_pack_f32(const double4* __restrict__ nodePM, const double* __r
 // into FP64 accumulators after every list.  Persistent warps take groups from a counter.
 constexpr int GROUP_WARPS = 4;
 constexpr int GROUP_THREADS = 32 * GROUP_WARPS;
-constexpr int LIST_CAP = 64;
 constexpr int NB_GROUP_STACK = 16384;     // >= 256 x 63 + 32
 
 // Interaction lists in shared memory, one float4 array per field so that the 32 lanes'
@@ -94,10 +97,11 @@ constexpr int NB_GROUP_STACK = 16384;     // >= 256 x 63 + 32
 // the lane that appends an entry forms (hi - centre) + lo once, so an interaction costs each
 // body one subtraction per coordinate.  Cell entry: {rel, mass} {qxx, qxy, qxz, qyy}
 // {qyz, qzz, -, -}; body entry: {rel, mass}.
-struct CellList { float4 a[LIST_CAP], b[LIST_CAP], c[LIST_CAP]; };
-struct BodyList { float4 a[LIST_CAP]; };
+template <int LIST_CAP> struct CellList { float4 a[LIST_CAP], b[LIST_CAP], c[LIST_CAP]; };
+template <int LIST_CAP> struct BodyList { float4 a[LIST_CAP]; };
 
-__device__ __forceinline__ void nb_eval_bodies(const BodyList& list, int n, float rbx, float rby,
+template <int LIST_CAP>
+__device__ __forceinline__ void nb_eval_bodies(const BodyList<LIST_CAP>& list, int n, float rbx, float rby,
                                                float rbz, float eps2, float& fx, float& fy,
                                                float& fz)
 {
@@ -113,7 +117,8 @@ __device__ __forceinline__ void nb_eval_bodies(const BodyList& list, int n, floa
     }
 }
 
-__device__ __forceinline__ void nb_eval_cells(const CellList& list, int n, float rbx, float rby,
+template <int LIST_CAP>
+__device__ __forceinline__ void nb_eval_cells(const CellList<LIST_CAP>& list, int n, float rbx, float rby,
                                               float rbz, float eps2, bool useQuad, float& fx,
                                               float& fy, float& fz)
 {
@@ -143,13 +148,15 @@ __device__ __forceinline__ void nb_eval_cells(const CellList& list, int n, float
     }
 }
 
-// Walk groups: contiguous runs of <= 32 sorted bodies that share a compact cell.  Every cell
-// with more than 32 bodies lays out its direct children in octant order and packs the
-// consecutive ones holding <= 32 bodies (cells or single bodies) into groups of <= 32; a
-// root with <= 32 bodies is one group; test particles (not in the tree, sorted last) form
-// groups of 32 consecutive bodies.  The groups partition the sorted bodies.
+// Walk groups: contiguous runs of <= G sorted bodies (G <= 32, the tuned group size) that
+// share a compact cell.  Every cell with more than G bodies lays out its direct children in
+// octant order and packs the consecutive ones holding <= G bodies (cells or single bodies)
+// into groups of <= G; a root with <= G bodies is one group; test particles (not in the tree,
+// sorted last) form groups of G consecutive bodies.  The groups partition the sorted bodies.
+// With a forest every dwarf's root counts as a root.
 __global__ void k_groups(const int2* __restrict__ nodeLink, const int2* __restrict__ nodeRange,
-                         int2* __restrict__ groups, int n, NbScalars* __restrict__ sc)
+                         int2* __restrict__ groups, int n, NbScalars* __restrict__ sc, int G,
+                         NbForest forest)
 {
     if (nb_failed(sc)) return;
     const int nNodes = sc->nNodes, m = sc->nTree;
@@ -160,20 +167,22 @@ __global__ void k_groups(const int2* __restrict__ nodeLink, const int2* __restri
         if (l.y >= 0) continue;                              // bodies are handled by parents
         const int2 r = nodeRange[c];
         const int cnt = r.y - r.x + 1;
-        if (cnt <= 32) {
-            if (c == 0 && cnt > 0) groups[atomicAdd(&sc->nGroups, 1)] = make_int2(r.x, cnt);
+        if (cnt <= G) {
+            const bool root = forest.dwarfs ? c == forest.dwarfs[forest.bodyDwarf[r.x]].rootNode
+                                            : c == 0;
+            if (root && cnt > 0) groups[atomicAdd(&sc->nGroups, 1)] = make_int2(r.x, cnt);
             continue;
         }
         int gFirst = -1, gCount = 0;
         for (int k = c + 1; k < l.x; k = nodeLink[k].x) {
             const int2 rk = nodeRange[k];
             const int ck = rk.y - rk.x + 1;
-            if (ck > 32) {                                   // descended by its own thread
+            if (ck > G) {                                    // descended by its own thread
                 if (gCount) groups[atomicAdd(&sc->nGroups, 1)] = make_int2(gFirst, gCount);
                 gCount = 0;
                 continue;
             }
-            if (gCount && gCount + ck > 32) {
+            if (gCount && gCount + ck > G) {
                 groups[atomicAdd(&sc->nGroups, 1)] = make_int2(gFirst, gCount);
                 gCount = 0;
             }
@@ -182,11 +191,13 @@ __global__ void k_groups(const int2* __restrict__ nodeLink, const int2* __restri
         }
         if (gCount) groups[atomicAdd(&sc->nGroups, 1)] = make_int2(gFirst, gCount);
     }
-    for (int t = tid; m + 32 * t < n; t += stride)
-        groups[atomicAdd(&sc->nGroups, 1)] = make_int2(m + 32 * t, min(32, n - m - 32 * t));
+    for (int t = tid; m + G * t < n; t += stride)
+        groups[atomicAdd(&sc->nGroups, 1)] = make_int2(m + G * t, min(G, n - m - G * t));
 }
 
-template <bool COUNT>
+// FOREST: a group belongs to one dwarf; its warp walks that dwarf's tree from its root,
+// with the dwarf's softening and time step.
+template <bool COUNT, bool FOREST, int LIST_CAP>
 __global__ void __launch_bounds__(GROUP_THREADS)
 k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeLo,
              const float4* __restrict__ nodeQ32, const int4* __restrict__ child8,
@@ -196,19 +207,20 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
              double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
              double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
              int* __restrict__ stacks, const int2* __restrict__ groups, NbWalkParams wp,
-             NbPot pot, NbScalars* __restrict__ sc)
+             NbPot pot, NbScalars* __restrict__ sc, NbForest forest)
 {
-    __shared__ CellList sCells[GROUP_WARPS];
-    __shared__ BodyList sBodies[GROUP_WARPS];
+    __shared__ CellList<LIST_CAP> sCells[GROUP_WARPS];
+    __shared__ BodyList<LIST_CAP> sBodies[GROUP_WARPS];
     if (nb_failed(sc)) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    CellList& cells = sCells[warp];
-    BodyList& bodies = sBodies[warp];
+    CellList<LIST_CAP>& cells = sCells[warp];
+    BodyList<LIST_CAP>& bodies = sBodies[warp];
     int* stack = stacks + (size_t) (blockIdx.x * GROUP_WARPS + warp) * NB_GROUP_STACK;
     const unsigned ltMask = (1u << lane) - 1u;
     const int nGroups = sc->nGroups;
-    const double4 root = nodePM[0];
-    const float eps2 = (float) wp.eps2;
+    double4 root = nodePM[0];
+    float eps2 = (float) wp.eps2;
+    int rootNode = 0;
     const bool useQuad = wp.useQuad != 0;
     const float inf = __int_as_float(0x7f800000);
     unsigned long long cVisit = 0, cBB = 0, cBC = 0, cSteps = 0;
@@ -219,6 +231,13 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
         g = __shfl_sync(NB_FULL_MASK, g, 0);
         if (g >= nGroups) break;
         const int2 grp = groups[g];
+        if (FOREST) {
+            const NbDwarfDev& dw = forest.dwarfs[forest.bodyDwarf[grp.x]];
+            rootNode = dw.rootNode;
+            root = nodePM[rootNode];
+            eps2 = (float) dw.eps2;
+            wp.dtHalf = 0.5 * dw.dt;
+        }
         const int i = grp.x + lane;
         const bool valid = lane < grp.y;
         const unsigned j = valid ? order[i] : 0u;
@@ -244,7 +263,7 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
         double accx = 0.0, accy = 0.0, accz = 0.0;
         float fx = 0.f, fy = 0.f, fz = 0.f;
         int nC = 0, nB = 0;
-        if (lane == 0) stack[0] = 0;      // the root
+        if (lane == 0) stack[0] = rootNode;      // the (dwarf's) root
         int top = 1;
         __syncwarp();
         while (top > 0) {
@@ -342,37 +361,74 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
     }
 }
 
+template <bool COUNT, bool FOREST, int LC>
+static void nb_walk_mixed_launch(const NbTreeBuffers& b, const NbMixedBuffers& m,
+                                 const NbWalkParams& wp, const NbPot& pot, int blocks,
+                                 const NbForest& f, cudaStream_t s)
+{
+    k_walk_mixed<COUNT, FOREST, LC><<<blocks, GROUP_THREADS, 0, s>>>(
+        m.hi, m.lo, m.q32, m.child8, b.nodePM, b.sort.idxA, b.px, b.py, b.pz, b.mass, b.ax, b.ay,
+        b.az, b.vx, b.vy, b.vz, m.stacks, m.groups, wp, pot, b.sc, f);
+}
+
+template <bool COUNT, bool FOREST>
+static void nb_walk_mixed_cap(const NbTreeBuffers& b, const NbMixedBuffers& m,
+                              const NbWalkParams& wp, const NbPot& pot, int blocks,
+                              const NbForest& f, cudaStream_t s)
+{
+    switch (m.listCap) {
+    case 32: nb_walk_mixed_launch<COUNT, FOREST, 32>(b, m, wp, pot, blocks, f, s); break;
+    case 128: nb_walk_mixed_launch<COUNT, FOREST, 128>(b, m, wp, pot, blocks, f, s); break;
+    default: nb_walk_mixed_launch<COUNT, FOREST, 64>(b, m, wp, pot, blocks, f, s); break;
+    }
+}
+
 void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int capNodes,
                           const NbWalkParams& wp, const NbPot& pot, bool count, int numSMs,
-                          cudaStream_t s)
+                          cudaStream_t s, const NbForest* forest)
 {
-    k_pack_f32<<<min((capNodes + 255) / 256, numSMs * 16), 256, 0, s>>>(
-        b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, m.hi, m.lo, m.q32, m.child8, b.sc);
-    k_groups<<<min((capNodes + 255) / 256, numSMs * 16), 256, 0, s>>>(b.nodeLink, b.nodeRange,
-                                                                       m.groups, wp.n, b.sc);
+    const NbForest f = forest ? *forest : NbForest{nullptr, nullptr, 0};
+    const int g = min((capNodes + 255) / 256, numSMs * 16);
+    if (forest)
+        k_pack_f32<true><<<g, 256, 0, s>>>(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, m.hi, m.lo,
+                                           m.q32, m.child8, b.nodeRange, b.sc, f);
+    else
+        k_pack_f32<false><<<g, 256, 0, s>>>(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, m.hi, m.lo,
+                                            m.q32, m.child8, b.nodeRange, b.sc, f);
+    const int G = m.groupMax >= 1 && m.groupMax <= 32 ? m.groupMax : 32;
+    k_groups<<<g, 256, 0, s>>>(b.nodeLink, b.nodeRange, m.groups, wp.n, b.sc, G, f);
     nb_count_launch(2);
     if (wp.n <= 0) return;
     const int blocks = m.walkBlocks;
-    if (count)
-        k_walk_mixed<true><<<blocks, GROUP_THREADS, 0, s>>>(m.hi, m.lo, m.q32, m.child8, b.nodePM,
-                                                            b.sort.idxA, b.px, b.py, b.pz, b.mass,
-                                                            b.ax, b.ay, b.az, b.vx, b.vy, b.vz,
-                                                            m.stacks, m.groups, wp, pot, b.sc);
-    else
-        k_walk_mixed<false><<<blocks, GROUP_THREADS, 0, s>>>(m.hi, m.lo, m.q32, m.child8, b.nodePM,
-                                                             b.sort.idxA, b.px, b.py, b.pz, b.mass,
-                                                             b.ax, b.ay, b.az, b.vx, b.vy, b.vz,
-                                                             m.stacks, m.groups, wp, pot, b.sc);
+    if (forest) {
+        if (count) nb_walk_mixed_cap<true, true>(b, m, wp, pot, blocks, f, s);
+        else nb_walk_mixed_cap<false, true>(b, m, wp, pot, blocks, f, s);
+    } else {
+        if (count) nb_walk_mixed_cap<true, false>(b, m, wp, pot, blocks, f, s);
+        else nb_walk_mixed_cap<false, false>(b, m, wp, pot, blocks, f, s);
+    }
     nb_count_launch();
 }
 
-// Persistent grid of the group walk: as many blocks as fit on the device at once.
-int nb_mixed_walk_blocks(int numSMs)
+// Persistent grid of the group walk: as many blocks as fit on the device at once (for the
+// given interaction-list capacity; 0 = the default of 64).
+int nb_mixed_walk_blocks(int numSMs, int listCap)
 {
     int perSM = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_walk_mixed<false>, GROUP_THREADS, 0)
-            != cudaSuccess || perSM < 1)
+    cudaError_t e;
+    if (listCap == 32)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_walk_mixed<false, false, 32>,
+                                                          GROUP_THREADS, 0);
+    else if (listCap == 128)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_walk_mixed<false, false, 128>,
+                                                          GROUP_THREADS, 0);
+    else
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_walk_mixed<false, false, 64>,
+                                                          GROUP_THREADS, 0);
+    if (e != cudaSuccess || perSM < 1) {
+        cudaGetLastError();
         perSM = 1;
+    }
     return perSM * numSMs;
 }
 

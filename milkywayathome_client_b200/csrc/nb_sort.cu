@@ -17,9 +17,20 @@ constexpr int RS_ROUNDS = 8;                         // keys per thread per tile
 constexpr int RS_TILE = RS_THREADS * RS_ROUNDS;      // 2048 keys per tile
 constexpr int RS_WARPS = RS_THREADS / 32;
 
+// digit of item i: 8 bits of its key, or (GROUPED) 8 bits of the group of its index
+template <bool GROUPED>
+__device__ __forceinline__ unsigned int rs_digit(unsigned long long key, unsigned int idx,
+                                                 const int* group, int shift)
+{
+    if (GROUPED) return ((unsigned) group[idx] >> shift) & 255u;
+    return (unsigned) (key >> shift) & 255u;
+}
+
+template <bool GROUPED>
 __global__ void __launch_bounds__(RS_THREADS)
-k_rs_hist(const unsigned long long* __restrict__ keys, int n, int shift,
-          unsigned int* __restrict__ hist, int nTiles)
+k_rs_hist(const unsigned long long* __restrict__ keys, const unsigned int* __restrict__ idx,
+          const int* __restrict__ group, int n, int shift, unsigned int* __restrict__ hist,
+          int nTiles)
 {
     __shared__ unsigned int cnt[256];
     cnt[threadIdx.x] = 0;
@@ -28,16 +39,20 @@ k_rs_hist(const unsigned long long* __restrict__ keys, int n, int shift,
 #pragma unroll
     for (int r = 0; r < RS_ROUNDS; ++r) {
         int i = base + r * RS_THREADS + threadIdx.x;
-        if (i < n) atomicAdd(&cnt[(unsigned) (keys[i] >> shift) & 255u], 1u);
+        if (i < n)
+            atomicAdd(&cnt[rs_digit<GROUPED>(GROUPED ? 0ull : keys[i], GROUPED ? idx[i] : 0u,
+                                             group, shift)], 1u);
     }
     __syncthreads();
     hist[threadIdx.x * nTiles + blockIdx.x] = cnt[threadIdx.x];
 }
 
+template <bool GROUPED>
 __global__ void __launch_bounds__(RS_THREADS)
 k_rs_scatter(const unsigned long long* __restrict__ keyIn, const unsigned int* __restrict__ idxIn,
              unsigned long long* __restrict__ keyOut, unsigned int* __restrict__ idxOut,
-             int n, int shift, const unsigned int* __restrict__ hist, int nTiles)
+             const int* __restrict__ group, int n, int shift,
+             const unsigned int* __restrict__ hist, int nTiles)
 {
     __shared__ unsigned int gOff[256];             // global start of each digit for this tile
     __shared__ unsigned int dRun[256];             // keys of each digit already placed
@@ -55,7 +70,7 @@ k_rs_scatter(const unsigned long long* __restrict__ keyIn, const unsigned int* _
         const bool valid = i < n;
         unsigned long long key = valid ? keyIn[i] : 0ull;
         unsigned int idx = valid ? idxIn[i] : 0u;
-        const unsigned int d = valid ? (unsigned) (key >> shift) & 255u : 256u;
+        const unsigned int d = valid ? rs_digit<GROUPED>(key, idx, group, shift) : 256u;
         const unsigned int peers = __match_any_sync(NB_FULL_MASK, d);
         const unsigned int rankInWarp = __popc(peers & ltMask);
         if (valid && rankInWarp == 0) wHist[warp][d] = __popc(peers);
@@ -164,27 +179,44 @@ k_ps_apply(int* __restrict__ data, int n, const int* __restrict__ tileSums)
 
 }  // namespace
 
-void nb_radix_sort(NbSortBuffers& b, int n, cudaStream_t s)
+static void rs_passes(NbSortBuffers& b, int n, const int* group, cudaStream_t s)
 {
     if (n <= 0) return;
     const int nTiles = (n + RS_TILE - 1) / RS_TILE;
     unsigned long long* kin = b.keyA; unsigned long long* kout = b.keyB;
     unsigned int* iin = b.idxA; unsigned int* iout = b.idxB;
-    for (int pass = 0; pass < 8; ++pass) {
-        const int shift = pass * 8;
-        k_rs_hist<<<nTiles, RS_THREADS, 0, s>>>(kin, n, shift, b.hist, nTiles);
+    const int passes = group ? 10 : 8;
+    for (int pass = 0; pass < passes; ++pass) {
+        const bool grouped = pass >= 8;
+        const int shift = grouped ? (pass - 8) * 8 : pass * 8;
+        if (grouped)
+            k_rs_hist<true><<<nTiles, RS_THREADS, 0, s>>>(kin, iin, group, n, shift, b.hist, nTiles);
+        else
+            k_rs_hist<false><<<nTiles, RS_THREADS, 0, s>>>(kin, iin, nullptr, n, shift, b.hist, nTiles);
         // exclusive scan of the (digit, tile) table, three coalesced phases
         const int len = 256 * nTiles;
         const int scanTiles = (len + PS_TILE - 1) / PS_TILE;
         k_ps_tile<true><<<scanTiles, PS_THREADS, 0, s>>>((int*) b.hist, len, b.histTmp);
         k_ps_top<<<1, PS_THREADS, 0, s>>>(b.histTmp, scanTiles);
         k_ps_apply<<<scanTiles, PS_THREADS, 0, s>>>((int*) b.hist, len, b.histTmp);
-        k_rs_scatter<<<nTiles, RS_THREADS, 0, s>>>(kin, iin, kout, iout, n, shift, b.hist, nTiles);
+        if (grouped)
+            k_rs_scatter<true><<<nTiles, RS_THREADS, 0, s>>>(kin, iin, kout, iout, group, n, shift,
+                                                             b.hist, nTiles);
+        else
+            k_rs_scatter<false><<<nTiles, RS_THREADS, 0, s>>>(kin, iin, kout, iout, nullptr, n,
+                                                              shift, b.hist, nTiles);
         nb_count_launch(5);
         unsigned long long* tk = kin; kin = kout; kout = tk;
         unsigned int* ti = iin; iin = iout; iout = ti;
     }
-    // 8 passes: the result is back in keyA / idxA.
+    // an even number of passes: the result is back in keyA / idxA.
+}
+
+void nb_radix_sort(NbSortBuffers& b, int n, cudaStream_t s) { rs_passes(b, n, nullptr, s); }
+
+void nb_radix_sort_grouped(NbSortBuffers& b, int n, const int* group, cudaStream_t s)
+{
+    rs_passes(b, n, group, s);
 }
 
 int nb_scan_tmp_ints(int n) { return (n + PS_TILE - 1) / PS_TILE + 1; }

@@ -15,7 +15,10 @@
 
 constexpr int WALK_THREADS = 128;
 
-template <bool COUNT>
+// FOREST: the nodes hold one tree per dwarf (batched dwarfs); each lane walks its own
+// dwarf's tree, [rootNode, rootEnd), with that dwarf's softening and time step.  A warp whose
+// 32 bodies straddle two dwarfs visits the union of both walks, each lane its own.
+template <bool COUNT, bool FOREST>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeCrit,
             const int2* __restrict__ nodeLink, const double* __restrict__ nodeQuad,
@@ -23,7 +26,7 @@ k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeC
             const double* __restrict__ py, const double* __restrict__ pz,
             double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
             double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
-            NbWalkParams wp, NbPot pot, NbScalars* __restrict__ sc)
+            NbWalkParams wp, NbPot pot, NbScalars* __restrict__ sc, NbForest forest)
 {
     if (nb_failed(sc)) return;
     const int end = sc->nNodes;
@@ -32,13 +35,23 @@ k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeC
     const bool valid = i < wp.n;
     const unsigned j = valid ? order[i] : 0u;
     const double x0 = valid ? px[j] : 0.0, y0 = valid ? py[j] : 0.0, z0 = valid ? pz[j] : 0.0;
-    const double eps2 = wp.eps2;
+    double eps2 = wp.eps2;
     const bool useQuad = wp.useQuad != 0;
-    int ptr = valid ? 0 : end;
+    int start = 0, myEnd = end;
+    NbDwarfDev* dw = nullptr;
+    if (FOREST && valid) {
+        dw = &forest.dwarfs[forest.bodyDwarf[i]];
+        eps2 = dw->eps2;
+        wp.dtHalf = 0.5 * dw->dt;
+        start = dw->rootNode;
+        myEnd = dw->rootEnd;
+    }
+    int ptr = valid ? start : end;
     double accx = 0.0, accy = 0.0, accz = 0.0;
     bool metSelf = false;
     unsigned long long cVisit = 0, cBB = 0, cBC = 0, cSteps = 0;
     for (;;) {
+        if (FOREST && ptr >= myEnd) ptr = end;          // this lane's tree is done
         const int q = __reduce_min_sync(NB_FULL_MASK, ptr);
         if (q >= end) break;
         if (COUNT) ++cSteps;
@@ -96,7 +109,10 @@ k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeC
     }
     if (!valid) return;
     // a body that never meets itself is tree incest (nbody/src/nbody_grav.c:111-118)
-    if (!metSelf) atomicOr(&sc->incest, 1);
+    if (!metSelf) {
+        atomicOr(&sc->incest, 1);
+        if (FOREST) atomicOr(&dw->status, NBODY_TREE_INCEST_NONFATAL);
+    }
     nb_finish_body(pot, wp, j, x0, y0, z0, accx, accy, accz, ax, ay, az, vx, vy, vz);
 }
 
@@ -261,17 +277,23 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
                          const double* nodeQuad, const unsigned* order, const double* px,
                          const double* py, const double* pz, double* ax, double* ay, double* az,
                          double* vx, double* vy, double* vz, const NbWalkParams& wp,
-                         const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s)
+                         const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s,
+                         const NbForest* forest)
 {
     const int warps = (wp.n + 31) / 32;
     const int blocks = (warps * 32 + WALK_THREADS - 1) / WALK_THREADS;
     if (blocks <= 0) return;
-    if (count)
-        k_walk_fp64<true><<<blocks, WALK_THREADS, 0, s>>>(nodePM, nodeCrit, nodeLink, nodeQuad, order,
-                                                          px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc);
-    else
-        k_walk_fp64<false><<<blocks, WALK_THREADS, 0, s>>>(nodePM, nodeCrit, nodeLink, nodeQuad, order,
-                                                           px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc);
+    const NbForest f = forest ? *forest : NbForest{nullptr, nullptr, 0};
+#define NB_WALK_ARGS nodePM, nodeCrit, nodeLink, nodeQuad, order, px, py, pz, ax, ay, az, vx, vy, \
+                     vz, wp, pot, sc, f
+    if (forest) {
+        if (count) k_walk_fp64<true, true><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
+        else k_walk_fp64<false, true><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
+    } else {
+        if (count) k_walk_fp64<true, false><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
+        else k_walk_fp64<false, false><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
+    }
+#undef NB_WALK_ARGS
     nb_count_launch();
 }
 

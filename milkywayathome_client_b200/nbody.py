@@ -301,6 +301,103 @@ class NBodyState:
         return tuple(x.value for x in v)
 
 
+class NBodyBatch:
+    """Many independent dwarfs stepped together on one GPU (nbBatch*CUDA): every phase of the
+    step is one launch over all dwarfs, and run_steps can replay each step as one captured CUDA
+    graph.  No counterpart in the reference, which runs one dwarf per process; each dwarf here
+    gets the same accelerations as an NBodyState holding it alone.
+
+    dwarfs: a list of (nbody, eps2, timestep, treeRSize).  Bodies are concatenated arrays,
+    dwarf 0's bodies first: pos (N,3), vel (N,3), mass (N,)."""
+
+    def __init__(self, dwarfs, device=0):
+        self.lib = _lib.load()
+        arr = (_lib.Dwarf * len(dwarfs))()
+        for k, (nb, eps2, dt, rsize) in enumerate(dwarfs):
+            arr[k].nbody, arr[k].eps2, arr[k].timestep, arr[k].treeRSize = int(nb), eps2, dt, rsize
+        self.counts = np.array([int(d[0]) for d in dwarfs], dtype=np.int64)
+        self.offsets = np.concatenate([[0], np.cumsum(self.counts)])
+        self.nbody = int(self.offsets[-1])
+        self.ndwarfs = len(dwarfs)
+        self.device = device
+        h = ctypes.c_void_p()
+        rc = self.lib.nbBatchCreateCUDA(ctypes.byref(h), device, arr, len(dwarfs))
+        if rc:
+            raise NBodyError("nbBatchCreateCUDA", rc)
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.nbBatchDestroyCUDA(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    check = staticmethod(NBodyState.check)
+
+    def set_bodies(self, pos, vel, mass):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        vel = np.ascontiguousarray(vel, dtype=np.float64)
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        assert len(mass) == self.nbody
+        self.check("nbBatchSetBodiesCUDA", self.lib.nbBatchSetBodiesCUDA(
+            self._h, _lib.ptr(pos), _lib.ptr(vel), _lib.ptr(mass)))
+
+    def bodies(self):
+        pos = np.empty((self.nbody, 3))
+        vel = np.empty((self.nbody, 3))
+        self.check("nbBatchGetBodiesCUDA", self.lib.nbBatchGetBodiesCUDA(
+            self._h, _lib.ptr(pos), _lib.ptr(vel), None))
+        return pos, vel
+
+    def accels(self):
+        acc = np.empty((self.nbody, 3))
+        self.check("nbBatchGetBodiesCUDA", self.lib.nbBatchGetBodiesCUDA(
+            self._h, None, None, _lib.ptr(acc)))
+        return acc
+
+    def gravMap(self, ctx):
+        return self.lib.nbBatchGravMapCUDA(ctypes.byref(ctx.struct), self._h)
+
+    def run_steps(self, ctx, nsteps, graph=True):
+        return self.lib.nbBatchRunStepsCUDA(ctypes.byref(ctx.struct), self._h, int(nsteps),
+                                            int(bool(graph)))
+
+    def dwarf_info(self):
+        """Per dwarf: status bits, root size, root node index, node count."""
+        st = np.zeros(self.ndwarfs, dtype=np.int32)
+        rs = np.zeros(self.ndwarfs)
+        root = np.zeros(self.ndwarfs, dtype=np.int32)
+        nodes = np.zeros(self.ndwarfs, dtype=np.int32)
+        self.check("nbBatchDwarfInfoCUDA", self.lib.nbBatchDwarfInfoCUDA(
+            self._h, _lib.ptr(st), _lib.ptr(rs), _lib.ptr(root), _lib.ptr(nodes)))
+        return st, rs, root, nodes
+
+    def set_tuning(self, group_max=32, list_cap=64, blocks_per_sm=0):
+        self.check("nbBatchSetTuningCUDA", self.lib.nbBatchSetTuningCUDA(
+            self._h, int(group_max), int(list_cap), int(blocks_per_sm)))
+
+    def tuning(self):
+        g, l, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self.lib.nbBatchGetTuningCUDA(self._h, ctypes.byref(g), ctypes.byref(l), ctypes.byref(b))
+        return g.value, l.value, b.value
+
+    def step_time_ms(self):
+        ms = ctypes.c_double()
+        self.lib.nbBatchLastStepTimeCUDA(self._h, ctypes.byref(ms))
+        return ms.value
+
+
 def ext_acceleration(potential, pos, device=0):
     """nbExtAcceleration (nbody/src/nbody_potential.c:627) at many positions, on the GPU."""
     lib = _lib.load()
