@@ -209,6 +209,41 @@ NBodyCudaStatus nbStepAdjointCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, c
  * for the context's potential (0 with EXTERNAL_POTENTIAL_NONE).  Host array of 3 doubles. */
 NBodyCudaStatus nbEnergyCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, double* energy);
 
+/* ---- Lambda-Beta histogram and EMD/cost likelihood on the GPU ----
+ * The normalised-counts histogram of nbCreateHistogram (nbody/src/nbody_histogram.c:671-1139)
+ * and the EMD + cost components of nbSystemLikelihood (nbody/src/nbody_likelihood.c:155-324,
+ * nbMatchEMD nbody/src/nbody_emd.c:1278-1427, nbCostComponent nbody/src/nbody_mass.c:318-391)
+ * computed from the device-resident bodies, without copying them to the host.  Bodies of type
+ * +1 are light (they count towards totalSimulated and set massPerParticle), bodies of type < 0
+ * are ignored.  The likelihood supports one beta bin and the default EMD range (the whole
+ * histogram), as the reference's two-component runs use. */
+typedef struct {
+    double phi, theta, psi;            /* Euler angles of the stream frame, degrees */
+    double lambdaStart, lambdaEnd;
+    double betaStart, betaEnd;
+    int lambdaBins, betaBins;
+    double sunGCDist;
+} NBodyCudaHistogramParams;
+typedef struct {                       /* a data histogram as nbReadHistogram reads it */
+    int nBins;                         /* lambdaBins * betaBins */
+    unsigned int totalNum;             /* "n" */
+    double massPerParticle;
+    const int* useBin;                 /* host arrays of nBins entries */
+    const double* lambda;              /* bin centres */
+    const double* variable;            /* normalised counts */
+    const double* err;                 /* count errors */
+} NBodyCudaDataHistogram;
+/* host array of nbody types (+1 light, -1 dark) */
+NBodyCudaStatus nbSetTypesCUDA(NBodyCudaState* st, const int* types);
+/* host outputs, any may be NULL: counts[nBins], totals[2] = {in range, light bodies},
+ * massPerParticle[1] */
+NBodyCudaStatus nbHistogramCUDA(NBodyCudaState* st, const NBodyCudaHistogramParams* hp,
+                                unsigned int* counts, unsigned int* totals,
+                                double* massPerParticle);
+/* out[4] = {EMD component + cost component, EMD, EMD component, cost component} */
+NBodyCudaStatus nbLikelihoodCUDA(NBodyCudaState* st, const NBodyCudaHistogramParams* hp,
+                                 const NBodyCudaDataHistogram* data, double* out);
+
 /* ---- batched dwarfs (no reference counterpart: the reference runs one dwarf per process) ----
  * Many independent dwarfs stepped together.  Each dwarf is the reference's simulation (its own
  * root at the origin, root size, octree, softening and time step) and gets the same
@@ -254,6 +289,14 @@ NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* batch, int groupMax, int li
                                      int blocksPerSM);
 NBodyCudaStatus nbBatchGetTuningCUDA(NBodyCudaBatch* batch, int* groupMax, int* listCap,
                                      int* blocksPerSM);
+/* histograms and likelihoods of every dwarf: types as nbSetTypesCUDA (all dwarfs' bodies),
+ * counts[ndwarfs * nBins], totals[2 * ndwarfs], massPerParticle[ndwarfs], out[4 * ndwarfs] */
+NBodyCudaStatus nbBatchSetTypesCUDA(NBodyCudaBatch* batch, const int* types);
+NBodyCudaStatus nbBatchHistogramCUDA(NBodyCudaBatch* batch, const NBodyCudaHistogramParams* hp,
+                                     unsigned int* counts, unsigned int* totals,
+                                     double* massPerParticle);
+NBodyCudaStatus nbBatchLikelihoodCUDA(NBodyCudaBatch* batch, const NBodyCudaHistogramParams* hp,
+                                      const NBodyCudaDataHistogram* data, double* out);
 /* mean device time of the steps of the last nbBatchRunStepsCUDA call */
 NBodyCudaStatus nbBatchLastStepTimeCUDA(NBodyCudaBatch* batch, double* stepMs);
 

@@ -9,8 +9,10 @@ formulas and a synthetic dwarf sampler.
 from .nbody import (Disk, Halo, NBodyBatch, NBodyCtx, NBodyError, NBodyState, Potential,
                     Spherical, ext_acceleration, kernel_launches, milky_way_potential)
 from ._lib import status_is_fatal, status_names
+from .histogram import DataHistogram, HistogramParams, data_from_counts, read_histogram
 
 __all__ = ["Disk", "Halo", "NBodyBatch", "NBodyCtx", "NBodyError", "NBodyState", "Potential",
            "Spherical",
            "ext_acceleration", "kernel_launches", "milky_way_potential", "status_is_fatal",
-           "status_names"]
+           "status_names", "DataHistogram", "HistogramParams", "data_from_counts",
+           "read_histogram"]

@@ -82,6 +82,23 @@ class Dwarf(ctypes.Structure):
                 ("timestep", ctypes.c_double), ("treeRSize", ctypes.c_double)]
 
 
+class HistParams(ctypes.Structure):
+    _fields_ = [("phi", ctypes.c_double), ("theta", ctypes.c_double), ("psi", ctypes.c_double),
+                ("lambdaStart", ctypes.c_double), ("lambdaEnd", ctypes.c_double),
+                ("betaStart", ctypes.c_double), ("betaEnd", ctypes.c_double),
+                ("lambdaBins", ctypes.c_int), ("betaBins", ctypes.c_int),
+                ("sunGCDist", ctypes.c_double)]
+
+
+class DataHist(ctypes.Structure):
+    _fields_ = [("nBins", ctypes.c_int), ("totalNum", ctypes.c_uint),
+                ("massPerParticle", ctypes.c_double),
+                ("useBin", ctypes.POINTER(ctypes.c_int)),
+                ("lambda_", ctypes.POINTER(ctypes.c_double)),
+                ("variable", ctypes.POINTER(ctypes.c_double)),
+                ("err", ctypes.POINTER(ctypes.c_double))]
+
+
 class Ctx(ctypes.Structure):
     """NBodyCudaCtx: the NBodyCtx fields the step reads."""
     _fields_ = [("eps2", ctypes.c_double), ("theta", ctypes.c_double),
@@ -133,6 +150,14 @@ SIGNATURES = [
     ("nbBatchSetTuningCUDA", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("nbBatchGetTuningCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("nbBatchLastStepTimeCUDA", ctypes.c_int, [_vp, _dp]),
+    ("nbSetTypesCUDA", ctypes.c_int, [_vp, _vp]),
+    ("nbHistogramCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), _vp, _vp, _vp]),
+    ("nbLikelihoodCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), ctypes.POINTER(DataHist),
+                                        _vp]),
+    ("nbBatchSetTypesCUDA", ctypes.c_int, [_vp, _vp]),
+    ("nbBatchHistogramCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), _vp, _vp, _vp]),
+    ("nbBatchLikelihoodCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams),
+                                             ctypes.POINTER(DataHist), _vp]),
     ("nbSaveStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbRestoreStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbReleaseStatesCUDA", ctypes.c_int, [_vp]),

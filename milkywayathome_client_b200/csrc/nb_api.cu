@@ -148,6 +148,9 @@ struct NBodyCudaState {
     int lastCriterion = -1;             // criterion of the last force evaluation
     std::vector<NbSlot> slots;          // saved evaluations (nbSaveStateCUDA)
     double* adjScratch = nullptr;       // reverse step: 7 doubles per body
+    int* types = nullptr;               // body types (+1 light, -1 dark), for histograms
+    char* histScratch = nullptr;        // histogram / likelihood buffers
+    size_t histScratchBytes = 0;
 };
 
 template <typename T>
@@ -244,6 +247,10 @@ static void nb_free_all(NBodyCudaState* st)
     st->slots.clear();
     cudaFree(st->adjScratch);
     st->adjScratch = nullptr;
+    cudaFree(st->types);
+    st->types = nullptr;
+    cudaFree(st->histScratch);
+    st->histScratch = nullptr;
     if (st->scHost) cudaFreeHost(st->scHost);
     if (st->ev0) cudaEventDestroy(st->ev0);
     if (st->ev1) cudaEventDestroy(st->ev1);
@@ -1034,6 +1041,157 @@ const char* nbLastErrorCUDA(void) { return g_lastError.c_str(); }
 }  // extern "C"
 
 // =============================================================================================
+// Histograms and likelihoods (kernels in nb_batch.cu)
+// =============================================================================================
+static NbHistDev nb_hist_dev(const NBodyCudaHistogramParams* hp)
+{
+    // nbGetHistTrig (nbody/src/nbody_coordinates.c:73-85) and the rotation of nbXYZToLambdaBeta
+    const double rphi = hp->phi * M_PI / 180.0, rpsi = hp->psi * M_PI / 180.0;
+    const double rth = hp->theta * M_PI / 180.0;
+    const double cosphi = cos(rphi), sinphi = sin(rphi), sinpsi = sin(rpsi), cospsi = cos(rpsi);
+    const double costh = cos(rth), sinth = sin(rth);
+    NbHistDev h{};
+    h.rot[0] = cospsi * cosphi - costh * sinphi * sinpsi;
+    h.rot[1] = cospsi * sinphi + costh * cosphi * sinpsi;
+    h.rot[2] = sinpsi * sinth;
+    h.rot[3] = -sinpsi * cosphi - costh * sinphi * cospsi;
+    h.rot[4] = -sinpsi * sinphi + costh * cosphi * cospsi;
+    h.rot[5] = cospsi * sinth;
+    h.rot[6] = sinth * sinphi;
+    h.rot[7] = -sinth * cosphi;
+    h.rot[8] = costh;
+    h.sunGCDist = hp->sunGCDist;
+    h.lambdaStart = hp->lambdaStart;
+    h.lambdaSize = (hp->lambdaEnd - hp->lambdaStart) / (double) hp->lambdaBins;
+    h.betaStart = hp->betaStart;
+    h.betaSize = (hp->betaEnd - hp->betaStart) / (double) hp->betaBins;
+    h.lambdaBins = hp->lambdaBins;
+    h.betaBins = hp->betaBins;
+    return h;
+}
+
+static size_t nb_al(size_t x) { return (x + 255) & ~(size_t) 255; }
+
+// Histograms of nDwarfs dwarfs (bodyDwarf NULL: the whole state is one dwarf) and, with a
+// data histogram, their likelihoods.  Host outputs, any may be NULL: counts (nDwarfs x nBins),
+// totals (2 per dwarf: bodies in range, light bodies), massPer (per dwarf), out (4 per dwarf).
+static NBodyCudaStatus nb_hist_run(NBodyCudaState* st, const int* bodyDwarf, int nDwarfs,
+                                   const int* nbodyOfHost, const NBodyCudaHistogramParams* hp,
+                                   const NBodyCudaDataHistogram* data, unsigned* counts,
+                                   unsigned* totals, double* massPer, double* out)
+{
+    if (!hp || hp->lambdaBins < 1 || hp->betaBins < 1 || !(hp->lambdaEnd > hp->lambdaStart) ||
+        !(hp->betaEnd > hp->betaStart)) {
+        g_lastError = "invalid histogram parameters";
+        return NBODY_USER_ERROR;
+    }
+    if (!st->types) { g_lastError = "body types not set"; return NBODY_USER_ERROR; }
+    const int nBins = hp->lambdaBins * hp->betaBins;
+    if (data) {
+        if (data->nBins != nBins || !data->useBin || !data->lambda || !data->variable || !data->err) {
+            g_lastError = "data histogram does not match the histogram parameters";
+            return NBODY_USER_ERROR;
+        }
+        if (hp->betaBins != 1) {
+            g_lastError = "the likelihood is implemented for one beta bin";
+            return NBODY_UNSUPPORTED;
+        }
+    }
+    NB_CHECK(cudaSetDevice(st->device));
+    const size_t D = (size_t) nDwarfs, B = (size_t) nBins;
+    const size_t need = nb_al(4 * D * B) + 4 * nb_al(4 * D) + nb_al(32 * D) + nb_al(4 * B) +
+                        3 * nb_al(8 * B) + 256;
+    if (st->histScratchBytes < need) {
+        cudaFree(st->histScratch);
+        st->histScratch = nullptr;
+        st->histScratchBytes = 0;
+        NB_CHECK(cudaMalloc((void**) &st->histScratch, need));
+        st->histScratchBytes = need;
+    }
+    char* p = st->histScratch;
+    auto carve = [&p](size_t bytes) { char* q = p; p += nb_al(bytes); return q; };
+    unsigned* dCounts = (unsigned*) carve(4 * D * B);
+    unsigned* dInRange = (unsigned*) carve(4 * D);
+    unsigned* dLight = (unsigned*) carve(4 * D);
+    int* dLast = (int*) carve(4 * D);
+    int* dNbody = (int*) carve(4 * D);
+    double* dOut = (double*) carve(32 * D);
+    int* dUse = (int*) carve(4 * B);
+    double* dLam = (double*) carve(8 * B);
+    double* dVar = (double*) carve(8 * B);
+    double* dErr = (double*) carve(8 * B);
+    const cudaStream_t s = st->stream;
+    NbTreeBuffers& b = st->b;
+    const NbHistDev h = nb_hist_dev(hp);
+    nb_launch_histogram(b.px, b.py, b.pz, st->types, bodyDwarf, st->nbody, nDwarfs, h, dCounts,
+                        dInRange, dLight, dLast, st->numSMs, s);
+    if (data && out) {
+        NB_CHECK(cudaMemcpyAsync(dNbody, nbodyOfHost, 4 * D, cudaMemcpyHostToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(dUse, data->useBin, 4 * B, cudaMemcpyHostToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(dLam, data->lambda, 8 * B, cudaMemcpyHostToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(dVar, data->variable, 8 * B, cudaMemcpyHostToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(dErr, data->err, 8 * B, cudaMemcpyHostToDevice, s));
+        NbDataHistDev dh{dUse, dLam, dVar, dErr, data->massPerParticle, data->totalNum, nBins};
+        nb_launch_likelihood(dCounts, dInRange, dLight, dLast, b.mass, dNbody, nDwarfs, dh, dOut, s);
+        NB_CHECK(cudaMemcpyAsync(out, dOut, 32 * D, cudaMemcpyDeviceToHost, s));
+    }
+    NB_CHECK(cudaGetLastError());
+    if (counts) NB_CHECK(cudaMemcpyAsync(counts, dCounts, 4 * D * B, cudaMemcpyDeviceToHost, s));
+    std::vector<unsigned> inR(D), light(D);
+    std::vector<int> last(D);
+    NB_CHECK(cudaMemcpyAsync(inR.data(), dInRange, 4 * D, cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaMemcpyAsync(light.data(), dLight, 4 * D, cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaMemcpyAsync(last.data(), dLast, 4 * D, cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaStreamSynchronize(s));
+    for (size_t d = 0; d < D; ++d) {
+        if (totals) { totals[2 * d] = inR[d]; totals[2 * d + 1] = light[d]; }
+        if (massPer) {
+            double m = 0.0;
+            if (last[d] >= 0)
+                NB_CHECK(cudaMemcpy(&m, b.mass + last[d], sizeof(double), cudaMemcpyDeviceToHost));
+            massPer[d] = m;
+        }
+    }
+    return NBODY_SUCCESS;
+}
+
+static NBodyCudaStatus nb_set_types(NBodyCudaState* st, const int* types)
+{
+    if (!types) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    if (!st->types) NB_CHECK(nb_alloc(&st->types, (size_t) st->capBodies));
+    if (st->nbody)
+        NB_CHECK(cudaMemcpy(st->types, types, sizeof(int) * (size_t) st->nbody, cudaMemcpyHostToDevice));
+    return NBODY_SUCCESS;
+}
+
+extern "C" {
+
+NBodyCudaStatus nbSetTypesCUDA(NBodyCudaState* st, const int* types)
+{
+    if (!st) return NBODY_USER_ERROR;
+    return nb_set_types(st, types);
+}
+
+NBodyCudaStatus nbHistogramCUDA(NBodyCudaState* st, const NBodyCudaHistogramParams* hp,
+                                unsigned int* counts, unsigned int* totals,
+                                double* massPerParticle)
+{
+    if (!st) return NBODY_USER_ERROR;
+    return nb_hist_run(st, nullptr, 1, nullptr, hp, nullptr, counts, totals, massPerParticle, nullptr);
+}
+
+NBodyCudaStatus nbLikelihoodCUDA(NBodyCudaState* st, const NBodyCudaHistogramParams* hp,
+                                 const NBodyCudaDataHistogram* data, double* out)
+{
+    if (!st || !data || !out) return NBODY_USER_ERROR;
+    const int nb = st->nbody;
+    return nb_hist_run(st, nullptr, 1, &nb, hp, data, nullptr, nullptr, nullptr, out);
+}
+
+}  // extern "C"
+
+// =============================================================================================
 // Batched dwarfs (nb_batch.cu builds the forest; the walks take the forest description)
 // =============================================================================================
 int nb_build_forest(NbTreeBuffers& b, const NbForest& f, int n, int capNodes, int criterion,
@@ -1409,6 +1567,31 @@ NBodyCudaStatus nbBatchGetTuningCUDA(NBodyCudaBatch* bt, int* groupMax, int* lis
     if (listCap) *listCap = bt->tune.listCap;
     if (blocksPerSM) *blocksPerSM = bt->tune.blocksPerSM;
     return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbBatchSetTypesCUDA(NBodyCudaBatch* bt, const int* types)
+{
+    if (!bt) return NBODY_USER_ERROR;
+    return nb_set_types(bt->st, types);
+}
+
+NBodyCudaStatus nbBatchHistogramCUDA(NBodyCudaBatch* bt, const NBodyCudaHistogramParams* hp,
+                                     unsigned int* counts, unsigned int* totals,
+                                     double* massPerParticle)
+{
+    if (!bt) return NBODY_USER_ERROR;
+    return nb_hist_run(bt->st, bt->bodyDwarf, bt->nDwarfs, nullptr, hp, nullptr, counts, totals,
+                       massPerParticle, nullptr);
+}
+
+NBodyCudaStatus nbBatchLikelihoodCUDA(NBodyCudaBatch* bt, const NBodyCudaHistogramParams* hp,
+                                      const NBodyCudaDataHistogram* data, double* out)
+{
+    if (!bt || !data || !out) return NBODY_USER_ERROR;
+    std::vector<int> nb(bt->nDwarfs);
+    for (int d = 0; d < bt->nDwarfs; ++d) nb[d] = bt->dwarfs[d].nbody;
+    return nb_hist_run(bt->st, bt->bodyDwarf, bt->nDwarfs, nb.data(), hp, data, nullptr, nullptr,
+                       nullptr, out);
 }
 
 NBodyCudaStatus nbBatchLastStepTimeCUDA(NBodyCudaBatch* bt, double* stepMs)

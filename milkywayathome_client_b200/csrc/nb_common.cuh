@@ -125,6 +125,31 @@ struct NbForest {
     int nDwarfs;
 };
 
+// Lambda-Beta histogram geometry (device copy of the histogram parameters).
+struct NbHistDev {
+    double rot[9];                  // rot11 .. rot33 of nbXYZToLambdaBeta
+    double sunGCDist, lambdaStart, lambdaSize, betaStart, betaSize;
+    int lambdaBins, betaBins;
+};
+// A data histogram to compare against (device pointers to nBins entries).
+struct NbDataHistDev {
+    const int* useBin;
+    const double* lambda;           // bin centres
+    const double* variable;         // normalised counts
+    const double* err;
+    double massPerParticle;
+    unsigned int totalNum;
+    int nBins;
+};
+void nb_launch_histogram(const double* px, const double* py, const double* pz, const int* types,
+                         const int* bodyDwarf, int n, int nDwarfs, const NbHistDev& h,
+                         unsigned int* counts, unsigned int* inRange, unsigned int* nLight,
+                         int* lastLight, int numSMs, cudaStream_t s);
+void nb_launch_likelihood(const unsigned int* counts, const unsigned int* inRange,
+                          const unsigned int* nLight, const int* lastLight, const double* mass,
+                          const int* nbodyOf, int nDwarfs, const NbDataHistDev& dh, double* out,
+                          cudaStream_t s);
+
 // Launch accounting (all launches of this library go through nb_count_launch).
 void nb_count_launch(int n = 1);
 

@@ -278,6 +278,41 @@ class NBodyState:
         self.check("nbEnergy", self.lib.nbEnergyCUDA(ctypes.byref(ctx.struct), self._h, out))
         return tuple(out)
 
+    # -- Lambda-Beta histogram and likelihood (nbCreateHistogram / nbSystemLikelihood) --
+    def set_types(self, types):
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        assert len(t) == self.nbody
+        rc = getattr(self.lib, self._fn("SetTypes"))(self._h, _lib.ptr(t))
+        self.check("%s(types)" % self._kind, rc)
+
+    def histogram(self, params):
+        """counts (ndwarfs, nBins), totals (ndwarfs, 2) = (in range, light), massPerParticle."""
+        nd = getattr(self, "ndwarfs", 1)
+        counts = np.zeros((nd, params.nbins), dtype=np.uint32)
+        totals = np.zeros((nd, 2), dtype=np.uint32)
+        mpp = np.zeros(nd)
+        hp = params.struct()
+        self.check("histogram", getattr(self.lib, self._fn("Histogram"))(
+            self._h, ctypes.byref(hp), _lib.ptr(counts), _lib.ptr(totals), _lib.ptr(mpp)))
+        return counts, totals, mpp
+
+    def likelihood(self, params, data):
+        """(ndwarfs, 4): EMD component + cost component, EMD, EMD component, cost component,
+        as nbSystemLikelihood returns them (positive; lower is better)."""
+        nd = getattr(self, "ndwarfs", 1)
+        out = np.zeros((nd, 4))
+        hp = params.struct()
+        dh = data.struct()
+        self.check("likelihood", getattr(self.lib, self._fn("Likelihood"))(
+            self._h, ctypes.byref(hp), ctypes.byref(dh), _lib.ptr(out)))
+        return out
+
+    _kind = "nbState"
+
+    @staticmethod
+    def _fn(name):
+        return "nb%sCUDA" % name
+
     def direct_sample(self, eps2, targets):
         """FP64 direct-sum self-gravity at the given body indices (accuracy oracle)."""
         targets = np.ascontiguousarray(targets, dtype=np.int32)
@@ -396,6 +431,15 @@ class NBodyBatch:
         ms = ctypes.c_double()
         self.lib.nbBatchLastStepTimeCUDA(self._h, ctypes.byref(ms))
         return ms.value
+
+    _kind = "nbBatch"
+    set_types = NBodyState.set_types
+    histogram = NBodyState.histogram
+    likelihood = NBodyState.likelihood
+
+    @staticmethod
+    def _fn(name):
+        return "nbBatch%sCUDA" % name
 
 
 def ext_acceleration(potential, pos, device=0):
