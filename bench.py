@@ -59,6 +59,11 @@ def parse_args():
     ap.add_argument("--adjoint-n", type=int, default=131072,
                     help="bodies of the adjoint-cost measurement (0 skips it)")
     ap.add_argument("--adjoint-steps", type=int, default=64)
+    ap.add_argument("--batch-dwarfs", type=int, default=256,
+                    help="dwarfs of the batched workload (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=500)
+    ap.add_argument("--batch-theta", type=float, default=1.0)
+    ap.add_argument("--batch-seed", type=int, default=2024)
     ap.add_argument("--energy-steps", type=int, default=100,
                     help="steps of the energy-drift run of both forms (0: skip)")
     ap.add_argument("--theta2", type=float, default=1.0,
@@ -274,6 +279,79 @@ def adjoint_ratio(n, steps, dev):
                    "bodies and tree in HBM) + reverse step (nbStepAdjointCUDA: force VJP on the "
                    "saved tree and reverse leapfrog) per step; both passes timed with CUDA "
                    "events around the pass"}
+
+
+def batched_run(args, dist, dev):
+    """The batched-dwarfs workload (mixed form): seeded uneven dwarfs, N log-uniform in
+    [4096, 65536], their parameters drawn as the workload states, started on the shared orbit
+    t_forward back; plus one dwarf of a seeded reference parameter set whose final histogram is
+    the likelihood target.  Dwarfs are dealt to ranks round-robin (independent units, no
+    collective on the data path).  Steps run through one captured CUDA graph each, after the
+    autotuner picked the walk tuning; the device time of the timed steps is the measure."""
+    from milkywayathome_client_b200 import (NBodyBatch, NBodyCtx, HistogramParams,
+                                            data_from_counts, milky_way_potential, models)
+    pot = milky_way_potential()
+    draws = models.dwarf_parameter_draws(args.batch_dwarfs, seed=args.batch_seed)
+    mine = draws[dist.rank::dist.world]
+    ref_draw = models.dwarf_parameter_draws(1, seed=args.batch_seed + 1)[0]
+    t0 = time.perf_counter()
+    # the workload's 500 steps span each dwarf's 3.5-4.5 Gyr forward time: dt = t_forward / 500
+    dwarfs = models.batched_dwarfs([ref_draw] + mine, pot, seed=args.batch_seed * 1000,
+                                   device=dev, nsteps=args.batch_steps)
+    t_ic = time.perf_counter() - t0
+    spec = [(len(d["mass"]), d["eps2"], d["timestep"], 4.0) for d in dwarfs]
+    n_total = int(sum(s[0] for s in spec))
+    # the config-0 tree settings: TreeCode, theta = 1.0, quadrupoles; mixed precision
+    ctx = NBodyCtx(potential=pot, precision="mixed", timestep=dwarfs[0]["timestep"],
+                   eps2=dwarfs[0]["eps2"], theta=args.batch_theta, criterion="TreeCode",
+                   useQuad=True)
+    hp = HistogramParams(lambdaStart=-150.0, lambdaEnd=150.0, lambdaBins=50, betaStart=-15.0,
+                         betaEnd=15.0, betaBins=1)
+    cat = lambda k: np.concatenate([d[k] for d in dwarfs])
+    with NBodyBatch(spec, device=dev) as bt:
+        bt.set_bodies(cat("pos"), cat("vel"), cat("mass"))
+        bt.set_types(cat("types"))
+        bt.check("nbBatchGravMap", bt.gravMap(ctx))
+        tune = bt.autotune(ctx)
+        bt.check("nbBatchRunSteps", bt.run_steps(ctx, 6, graph=True))
+        timed = max(args.batch_steps - 6, 1)         # the 6 warm-up steps count towards the run
+        dist.barrier()
+        w0 = time.perf_counter()
+        rc = bt.run_steps(ctx, timed, graph=True)
+        wall = time.perf_counter() - w0
+        bt.check("nbBatchRunSteps", rc)
+        step_ms = bt.step_time_ms()
+        status, rsize, _, nodes = bt.dwarf_info()
+        counts, totals, mpp = bt.histogram(hp)
+        data = data_from_counts(hp, counts[0], totals[0, 1], mpp[0])
+        lik = bt.likelihood(hp, data)
+        # after the run: the same state stepped with and without the captured graph
+        cmp_ms = {}
+        for name, g in (("graph", True), ("plain", False), ("graph_again", True)):
+            bt.check("nbBatchRunSteps", bt.run_steps(ctx, 4, graph=g))
+            cmp_ms[name] = bt.step_time_ms()
+    dev_s = step_ms * timed / 1e3
+    t = dist.max(dev_s)
+    updates = dist.sum(float(n_total - spec[0][0]) * timed)   # the reference dwarf excluded
+    lk = lik[1:, 0]
+    return {
+        "workload": "%d seeded dwarfs, N log-uniform in [4096, 65536] (%d bodies on this rank), "
+                    "mixed form, TreeCode theta=%g, quadrupoles, %d steps spanning each dwarf's "
+                    "forward time, one captured CUDA graph per step" % (
+                        args.batch_dwarfs, n_total, args.batch_theta, args.batch_steps),
+        "value": updates / t, "unit": UNIT, "ms_per_step": step_ms,
+        "graph_vs_plain_ms_per_step": cmp_ms, "timed_steps": timed, "wall_s": wall,
+        "ic_seconds": t_ic,
+        "dwarfs_per_rank": len(mine), "bodies_per_rank": n_total - spec[0][0],
+        "tuning": {"group_max": tune[0], "list_cap": tune[1], "blocks_per_sm": tune[2],
+                   "walk_ms": tune[3]},
+        "statuses_nonzero": int(np.count_nonzero(status)),
+        "likelihood": {"target": "final histogram of a seeded reference parameter set (50 x 1 "
+                                 "Lambda bins over [-150, 150] deg)",
+                       "min": float(np.nanmin(lk)), "median": float(np.nanmedian(lk)),
+                       "finite": int(np.isfinite(lk).sum()),
+                       "reference_self": float(lik[0, 0])},
+    }
 
 
 def run_reference(args, dist):
@@ -495,6 +573,14 @@ def run_ours(args, dist):
         except Exception as e:
             notes.append("adjoint measurement failed: %r" % (e,))
 
+    # ---- batched uneven dwarfs (mixed form, graph-captured steps, autotuned walk) ----
+    batched = None
+    if args.batch_dwarfs > 0:
+        try:
+            batched = batched_run(args, dist, dev)
+        except Exception as e:
+            notes.append("batched measurement failed: %r" % (e,))
+
     # ---- CPU baseline (rank 0, single GPU only) ----
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
@@ -518,6 +604,7 @@ def run_ours(args, dist):
             "roofline": roofline, "mixed": mixed, "accuracy": accuracy, "energy": energy,
             "theta2": theta2, "e2e": e2e,
             "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk, "adjoint": adj,
+            "batched": batched,
             "tree": {"nodes": info.nNodes, "cells": info.cellUsed, "max_depth": info.maxDepth,
                      "rsize": info.rsize},
         }

@@ -289,6 +289,12 @@ NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* batch, int groupMax, int li
                                      int blocksPerSM);
 NBodyCudaStatus nbBatchGetTuningCUDA(NBodyCudaBatch* batch, int* groupMax, int* listCap,
                                      int* blocksPerSM);
+/* autotuner of the mixed walk on the batch's current state: times every candidate tuning
+ * (groupMax 16/24/32 x listCap 32/64/128 x blocksPerSM 0/3) with force evaluations that do not
+ * move the bodies, keeps the fastest, re-evaluates the accelerations with it and returns it
+ * (and its walk time in ms).  With FP64 precision nothing is tuned. */
+NBodyCudaStatus nbBatchAutotuneCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* batch, int* groupMax,
+                                    int* listCap, int* blocksPerSM, double* walkMs);
 /* histograms and likelihoods of every dwarf: types as nbSetTypesCUDA (all dwarfs' bodies),
  * counts[ndwarfs * nBins], totals[2 * ndwarfs], massPerParticle[ndwarfs], out[4 * ndwarfs] */
 NBodyCudaStatus nbBatchSetTypesCUDA(NBodyCudaBatch* batch, const int* types);

@@ -149,6 +149,7 @@ SIGNATURES = [
     ("nbBatchDwarfInfoCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     ("nbBatchSetTuningCUDA", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("nbBatchGetTuningCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("nbBatchAutotuneCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, _vp, _vp, _vp, _dp]),
     ("nbBatchLastStepTimeCUDA", ctypes.c_int, [_vp, _dp]),
     ("nbSetTypesCUDA", ctypes.c_int, [_vp, _vp]),
     ("nbHistogramCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), _vp, _vp, _vp]),

@@ -1569,6 +1569,42 @@ NBodyCudaStatus nbBatchGetTuningCUDA(NBodyCudaBatch* bt, int* groupMax, int* lis
     return NBODY_SUCCESS;
 }
 
+// The autotuner: times the mixed walk of the batch's current state (force evaluations without
+// drift or kick, so the bodies do not move) for every candidate tuning -- bodies per walk group,
+// interaction-list capacity, resident blocks per SM -- keeps the fastest, and re-evaluates the
+// accelerations with it.  Each candidate is evaluated twice and timed on the second run.
+NBodyCudaStatus nbBatchAutotuneCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt, int* groupMax,
+                                    int* listCap, int* blocksPerSM, double* walkMs)
+{
+    NBodyCudaStatus rc = nb_batch_check(ctx, bt);
+    if (rc) return rc;
+    NbBatchTuning best = bt->tune;
+    double bestMs = -1.0;
+    if (ctx->precision == NBCUDA_PRECISION_MIXED) {
+        for (int g : {16, 24, 32})
+            for (int l : {32, 64, 128})
+                for (int b : {0, 3}) {
+                    bt->tune.groupMax = g;
+                    bt->tune.listCap = l;
+                    bt->tune.blocksPerSM = b;
+                    for (int rep = 0; rep < 2; ++rep) {
+                        rc = nb_batch_eval(ctx, bt, 0, 0, false);
+                        if (rc & ~(int) NBODY_STATUS_WARNINGS_MASK) { bt->tune = best; return rc; }
+                    }
+                    const double ms = bt->st->walkMs;
+                    if (bestMs < 0.0 || ms < bestMs) { bestMs = ms; best = bt->tune; }
+                }
+    }
+    bt->tune = best;
+    rc = nb_batch_eval(ctx, bt, 0, 0, false);
+    if (bestMs < 0.0) bestMs = bt->st->walkMs;
+    if (groupMax) *groupMax = best.groupMax;
+    if (listCap) *listCap = best.listCap;
+    if (blocksPerSM) *blocksPerSM = best.blocksPerSM;
+    if (walkMs) *walkMs = bestMs;
+    return rc;
+}
+
 NBodyCudaStatus nbBatchSetTypesCUDA(NBodyCudaBatch* bt, const int* types)
 {
     if (!bt) return NBODY_USER_ERROR;

@@ -141,3 +141,68 @@ def dwarf_config(nbody, theta=1.0, criterion="TreeCode", useQuad=True, mass_l=12
     eps2 = calculate_eps2(nbody, rscale_l, rscale_d, mass_l, mass_d)
     return dict(timestep=dt, eps2=eps2, theta=theta, criterion=criterion, useQuad=useQuad,
                 treeRSize=4.0)
+
+
+# ---- batched uneven dwarfs ----
+def dwarf_parameter_draws(ndwarfs, seed, nmin=4096, nmax=65536):
+    """Seeded parameter sets of the batched-dwarfs workload: N log-uniform in [nmin, nmax];
+    forward time U[3.5, 4.5] Gyr, baryon scale radius U[0.1, 0.5] kpc, radius ratio U[0.1, 0.5],
+    baryon mass U[1, 100] SMU, mass ratio U[0.01, 0.95]."""
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(math.log(nmin), math.log(nmax), ndwarfs)).astype(np.int64)
+    return [dict(nbody=int(n[k]), t_forward=float(rng.uniform(3.5, 4.5)),
+                 rscale_l=float(rng.uniform(0.1, 0.5)), light_r_ratio=float(rng.uniform(0.1, 0.5)),
+                 mass_l=float(rng.uniform(1.0, 100.0)), light_mass_ratio=float(rng.uniform(0.01, 0.95)))
+            for k in range(ndwarfs)]
+
+
+def reverse_orbits(potential, pos, vel, tstops, dt, device=0):
+    """nbReverseOrbit (nbody/src/nbody_orbit_integrator.c:44-86) of many orbit centres at once:
+    leapfrog backwards for each tstop with nsteps = floor(tstop / dt) + 1 steps of
+    tstop / nsteps, the potential evaluated on the GPU (nbExtAccelerationNoAllocCUDA: one small
+    call per step, no allocation)."""
+    from .nbody import ext_acceleration
+    pos = np.array(pos, dtype=np.float64).reshape(-1, 3)
+    vel = -np.array(vel, dtype=np.float64).reshape(-1, 3)
+    tstops = np.asarray(tstops, dtype=np.float64)
+    nsteps = np.floor(tstops / dt).astype(np.int64) + 1
+    dtr = (tstops / nsteps)[:, None]
+    acc = ext_acceleration(potential, pos, device, no_alloc=True)
+    for k in range(int(nsteps.max())):
+        live = (k < nsteps)[:, None]
+        v = vel + 0.5 * dtr * acc
+        x = pos + dtr * v
+        a = ext_acceleration(potential, x, device, no_alloc=True)
+        v = v + 0.5 * dtr * a
+        pos = np.where(live, x, pos)
+        vel = np.where(live, v, vel)
+        acc = np.where(live, a, acc)
+    return pos, -vel
+
+
+def batched_dwarfs(draws, potential, seed=0, orbit_dt=1e-3, device=0, nsteps=None,
+                   orbit=((218.0, 53.5, 28.6), (-156.0, 79.0, 107.0))):
+    """Initial conditions of a batch: every draw of dwarf_parameter_draws becomes a
+    two-component Plummer dwarf started on the shared orbit t_forward back from the present-day
+    position, with its own softening (calculateEps2) and time step: the two-component formula,
+    or, with nsteps, t_forward / nsteps (as nbCorrectTimestep sets it for a run of nsteps
+    steps over the evolution time).  Returns a list of dicts: pos, vel, mass, types, eps2,
+    timestep, params."""
+    (l, b, r), v0 = orbit
+    p0 = lbr_to_cartesian(l, b, r)
+    tf = [d["t_forward"] for d in draws]
+    starts, vstarts = reverse_orbits(potential, np.tile(p0, (len(draws), 1)),
+                                     np.tile(np.asarray(v0, dtype=np.float64), (len(draws), 1)),
+                                     tf, orbit_dt, device)
+    out = []
+    for k, d in enumerate(draws):
+        pos, vel, mass, typ = plummer_plummer_dwarf(
+            d["nbody"], seed=seed + k, mass_l=d["mass_l"], rscale_l=d["rscale_l"],
+            light_r_ratio=d["light_r_ratio"], light_mass_ratio=d["light_mass_ratio"],
+            position=starts[k], velocity=vstarts[k])
+        cfg = dwarf_config(d["nbody"], mass_l=d["mass_l"], rscale_l=d["rscale_l"],
+                           light_r_ratio=d["light_r_ratio"], light_mass_ratio=d["light_mass_ratio"])
+        dt = d["t_forward"] / nsteps if nsteps else cfg["timestep"]
+        out.append(dict(pos=pos, vel=vel, mass=mass, types=typ, eps2=cfg["eps2"],
+                        timestep=dt, params=d))
+    return out

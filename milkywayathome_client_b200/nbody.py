@@ -422,6 +422,15 @@ class NBodyBatch:
         self.check("nbBatchSetTuningCUDA", self.lib.nbBatchSetTuningCUDA(
             self._h, int(group_max), int(list_cap), int(blocks_per_sm)))
 
+    def autotune(self, ctx):
+        """nbBatchAutotuneCUDA: (groupMax, listCap, blocksPerSM, walk ms) of the fastest."""
+        g, l, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ms = ctypes.c_double()
+        self.check("nbBatchAutotune", self.lib.nbBatchAutotuneCUDA(
+            ctypes.byref(ctx.struct), self._h, ctypes.byref(g), ctypes.byref(l), ctypes.byref(b),
+            ctypes.byref(ms)))
+        return g.value, l.value, b.value, ms.value
+
     def tuning(self):
         g, l, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         self.lib.nbBatchGetTuningCUDA(self._h, ctypes.byref(g), ctypes.byref(l), ctypes.byref(b))
@@ -442,14 +451,16 @@ class NBodyBatch:
         return "nbBatch%sCUDA" % name
 
 
-def ext_acceleration(potential, pos, device=0):
-    """nbExtAcceleration (nbody/src/nbody_potential.c:627) at many positions, on the GPU."""
+def ext_acceleration(potential, pos, device=0, no_alloc=False):
+    """nbExtAcceleration (nbody/src/nbody_potential.c:627) at many positions, on the GPU.
+    no_alloc: through nbExtAccelerationNoAllocCUDA (at most 65,536 positions, no device
+    allocation per call: the form for loops of small calls such as orbit integration)."""
     lib = _lib.load()
     pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
     acc = np.empty_like(pos)
-    rc = lib.nbExtAccelerationCUDA(ctypes.byref(potential), _lib.ptr(pos), _lib.ptr(acc),
-                                   len(pos), device)
-    NBodyState.check("nbExtAccelerationCUDA", rc)
+    fn = lib.nbExtAccelerationNoAllocCUDA if no_alloc else lib.nbExtAccelerationCUDA
+    rc = fn(ctypes.byref(potential), _lib.ptr(pos), _lib.ptr(acc), len(pos), device)
+    NBodyState.check("nbExtAcceleration", rc)
     return acc
 
 

@@ -109,3 +109,25 @@ def test_batch_rejects_bad_input():
     with NBodyBatch([(4, 1e-3, 1e-3, 4.0)]) as bt:
         with pytest.raises(NBodyError):                    # massless bodies
             bt.set_bodies(np.zeros((4, 3)), np.zeros((4, 3)), np.array([1.0, 0.0, 1.0, 1.0]))
+
+
+def test_autotune_picks_a_candidate_and_leaves_its_accelerations():
+    from milkywayathome_client_b200 import NBodyBatch, NBodyCtx, milky_way_potential
+    dwarfs = _batch_dwarfs()
+    ctx = NBodyCtx(potential=milky_way_potential(), precision="mixed", **dwarfs[0][3])
+    spec = [(len(m), cfg["eps2"], cfg["timestep"], 4.0) for _, _, m, cfg in dwarfs]
+    cat = lambda k: np.concatenate([d[k] for d in dwarfs])
+    with NBodyBatch(spec) as bt:
+        bt.set_bodies(cat(0), cat(1), cat(2))
+        bt.check("nbBatchGravMap", bt.gravMap(ctx))
+        g, l, b, ms = bt.autotune(ctx)
+        assert g in (16, 24, 32) and l in (32, 64, 128) and b in (0, 3) and ms > 0
+        assert bt.tuning() == (g, l, b)
+        tuned = bt.accels()
+        pos0, _ = bt.bodies()
+    assert _same(pos0, cat(0))                      # the autotuner does not move the bodies
+    with NBodyBatch(spec) as bt2:
+        bt2.set_bodies(cat(0), cat(1), cat(2))
+        bt2.set_tuning(g, l, b)
+        bt2.check("nbBatchGravMap", bt2.gravMap(ctx))
+        assert _same(bt2.accels(), tuned)
