@@ -53,7 +53,10 @@ POTENTIAL_DEFAULT, POTENTIAL_NONE, POTENTIAL_CUSTOM_LUA = 0, 1, 2
 # spherical_t / disk_t / halo_t (nbody/include/nbody_potential_types.h)
 NO_SPHERICAL, HERNQUIST_SPHERICAL, PLUMMER_SPHERICAL = 0, 1, 2
 NO_DISK, MIYAMOTO_NAGAI_DISK = 0, 1
-NO_HALO, LOGARITHMIC_HALO, NFW_HALO = 0, 1, 2
+NO_HALO, LOGARITHMIC_HALO, NFW_HALO, TRIAXIAL_HALO, CAUSTIC_HALO = 0, 1, 2, 3, 4
+ALLEN_SANTILLAN_HALO, WILKINSON_EVANS_HALO, NFW_MASS_HALO = 5, 6, 7
+PLUMMER_HALO, HERNQUIST_HALO, NINKOVIC_HALO = 8, 9, 10
+ORBITING_BAR = 5
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 
 

@@ -270,6 +270,11 @@ NbPot nb_pot_from(const NBodyCudaCtx* c)
     p.disk2A = c->pot.disk2.scaleLength; p.disk2B = c->pot.disk2.scaleHeight;
     p.haloType = c->pot.halo.type; p.haloV = c->pot.halo.vhalo;
     p.haloA = c->pot.halo.scaleLength; p.haloQz = c->pot.halo.flattenZ;
+    p.haloMass = c->pot.halo.mass; p.haloGamma = c->pot.halo.gamma;
+    p.haloLambda = c->pot.halo.lambda; p.haloRho0 = c->pot.halo.rho0;
+    p.haloC1 = c->pot.halo.c1; p.haloC2 = c->pot.halo.c2; p.haloC3 = c->pot.halo.c3;
+    p.disk2Pattern = c->pot.disk2.patternSpeed; p.disk2StartAngle = c->pot.disk2.startAngle;
+    p.time = 0.0;
     return p;
 }
 
@@ -292,11 +297,26 @@ NBodyCudaStatus nb_check_ctx(const NBodyCudaCtx* c, std::string& why)
         if (p.sphere.type != NBCUDA_NO_SPHERICAL && p.sphere.type != NBCUDA_HERNQUIST_SPHERICAL &&
             p.sphere.type != NBCUDA_PLUMMER_SPHERICAL) { why = "bulge type"; return NBODY_UNSUPPORTED; }
         if (p.disk.type != NBCUDA_NO_DISK && p.disk.type != NBCUDA_MIYAMOTO_NAGAI_DISK) { why = "disk type"; return NBODY_UNSUPPORTED; }
-        if (p.disk2.type != NBCUDA_NO_DISK && p.disk2.type != NBCUDA_MIYAMOTO_NAGAI_DISK) { why = "disk2 type"; return NBODY_UNSUPPORTED; }
-        if (p.halo.type != NBCUDA_NO_HALO && p.halo.type != NBCUDA_LOGARITHMIC_HALO &&
-            p.halo.type != NBCUDA_NFW_HALO) { why = "halo type"; return NBODY_UNSUPPORTED; }
+        if (p.disk2.type != NBCUDA_NO_DISK && p.disk2.type != NBCUDA_MIYAMOTO_NAGAI_DISK &&
+            p.disk2.type != NBCUDA_ORBITING_BAR) { why = "disk2 type"; return NBODY_UNSUPPORTED; }
+        // the caustic halo is not evaluated on the GPU; every other halo of the reference is
+        if (p.halo.type < NBCUDA_NO_HALO || p.halo.type > NBCUDA_NINKOVIC_HALO ||
+            p.halo.type == NBCUDA_CAUSTIC_HALO) { why = "halo type"; return NBODY_UNSUPPORTED; }
     }
     return NBODY_SUCCESS;
+}
+
+// Potentials whose Jacobian (the adjoint's dual numbers) and potential energy are implemented:
+// Miyamoto-Nagai disks, logarithmic and NFW halos, Hernquist and Plummer bulges.
+static bool nb_pot_basic(const NBodyCudaCtx* c, std::string& why)
+{
+    if (c->potentialType != NBCUDA_POTENTIAL_DEFAULT) return true;
+    const int d2 = c->pot.disk2.type, h = c->pot.halo.type;
+    if ((d2 == NBCUDA_NO_DISK || d2 == NBCUDA_MIYAMOTO_NAGAI_DISK) &&
+        (h == NBCUDA_NO_HALO || h == NBCUDA_LOGARITHMIC_HALO || h == NBCUDA_NFW_HALO))
+        return true;
+    why = "implemented for Miyamoto-Nagai disks, logarithmic/NFW halos and Hernquist/Plummer bulges";
+    return false;
 }
 
 static int nb_blocks(NBodyCudaState* st, int n)
@@ -321,7 +341,8 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
     const int n = st->nbody;
     const cudaStream_t s = st->stream;
     NbTreeBuffers& b = st->b;
-    const NbPot pot = nb_pot_from(ctx);
+    NbPot pot = nb_pot_from(ctx);
+    pot.time = st->step * ctx->timestep;   // barTime (nbody/src/nbody_grav.c:141)
     NbWalkParams wp{};
     wp.eps2 = ctx->eps2;
     wp.dtHalf = 0.5 * ctx->timestep;
@@ -803,6 +824,7 @@ NBodyCudaStatus nbGravVJPCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, const
         g_lastError = "the adjoint follows the FP64 walk";
         return NBODY_UNSUPPORTED;
     }
+    if (!nb_pot_basic(ctx, why)) { g_lastError = "the adjoint is " + why; return NBODY_UNSUPPORTED; }
     if (ctx->criterion != st->lastCriterion || (ctx->criterion != NBCUDA_EXACT && !st->haveTree)) {
         g_lastError = "nbGravVJPCUDA needs a force evaluation with the same context first";
         return NBODY_USER_ERROR;
@@ -955,6 +977,7 @@ NBodyCudaStatus nbStepAdjointCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, c
         g_lastError = "the adjoint follows the FP64 walk";
         return NBODY_UNSUPPORTED;
     }
+    if (!nb_pot_basic(ctx, why)) { g_lastError = "the adjoint is " + why; return NBODY_UNSUPPORTED; }
     if (ctx->criterion != st->lastCriterion || (ctx->criterion != NBCUDA_EXACT && !st->haveTree)) {
         g_lastError = "nbStepAdjointCUDA needs the force evaluation of the step's end state first";
         return NBODY_USER_ERROR;
@@ -995,6 +1018,7 @@ NBodyCudaStatus nbEnergyCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, double
     std::string why;
     NBodyCudaStatus rc = nb_check_ctx(ctx, why);
     if (rc) { g_lastError = why; return rc; }
+    if (!nb_pot_basic(ctx, why)) { g_lastError = "the potential energy is " + why; return NBODY_UNSUPPORTED; }
     NB_CHECK(cudaSetDevice(st->device));
     NbTreeBuffers& b = st->b;
     double* dOut = st->stage;           // >= 3 doubles of device staging
@@ -1299,9 +1323,11 @@ static NBodyCudaStatus nb_batch_eval(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt
             NBodyCudaStatus rc = nb_batch_mixed_buffers(bt);
             if (rc) return rc;
         }
-        // the capacity the build checks against (the reset kernel keeps it)
+        // the capacity the build checks against and the step count (the bar's time); the
+        // reset kernel keeps both
         NB_CHECK(cudaMemcpyAsync(&b.sc->capNodes, &st->capNodes, sizeof(int),
                                  cudaMemcpyHostToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(&b.sc->step, &st->step, sizeof(int), cudaMemcpyHostToDevice, s));
         NB_CHECK(cudaStreamSynchronize(s));
         if (useGraph) {
             const bool same = bt->graph && bt->graphDrift == drift && bt->graphKick == kick &&

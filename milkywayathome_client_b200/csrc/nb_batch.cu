@@ -42,7 +42,10 @@ __global__ void k_b_reset(NbScalars* __restrict__ sc, NbDwarfDev* __restrict__ d
         sc->nGroups = 0;
         sc->maxDepth = 0;
     }
-    for (int d = t; d < nDwarfs; d += gridDim.x * blockDim.x) dw[d].xyzmaxBits = 0;
+    for (int d = t; d < nDwarfs; d += gridDim.x * blockDim.x) {
+        dw[d].xyzmaxBits = 0;
+        dw[d].time = sc->step * dw[d].dt;              // barTime of this evaluation
+    }
 }
 
 // advancePosVel (nbody/src/nbody_plain.c:268-284) with each dwarf's time step, fused with

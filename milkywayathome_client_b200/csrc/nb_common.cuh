@@ -45,6 +45,7 @@ struct NbScalars {
     unsigned long long nWarpSteps;  // walk iterations summed over warps (SIMT utilisation)
     int groupNext;                  // next group for the persistent group walk
     int nGroups;                    // walk groups formed for the mixed walk
+    int step;                       // batched dwarfs: steps taken (the bar's time)
 };
 
 // Potential parameters in constant-friendly POD form.
@@ -52,7 +53,11 @@ struct NbPot {
     int sphType; double sphMass, sphScale;
     int diskType; double diskMass, diskA, diskB;
     int disk2Type; double disk2Mass, disk2A, disk2B;
+    double disk2Pattern, disk2StartAngle;            // orbiting bar (disk2)
     int haloType; double haloV, haloA, haloQz;
+    double haloMass, haloGamma, haloLambda, haloRho0;  // mass-parameterised halos
+    double haloC1, haloC2, haloC3;                     // triaxial halo constants
+    double time;   // the bar's time: step * timestep (nbody/src/nbody_grav.c:141)
     int enabled;   // potentialType == DEFAULT
 };
 
@@ -118,6 +123,7 @@ struct NbDwarfDev {
     int rootNode, rootEnd;          // root node and Next(root)
     int depthEps;                   // first depth whose cell size is <= DBL_EPSILON
     int status;                     // status bits raised while building this dwarf's tree
+    double time;                    // the bar's time of this evaluation: step * dt
 };
 struct NbForest {
     const int* bodyDwarf;           // dwarf of every body (input = sorted position)

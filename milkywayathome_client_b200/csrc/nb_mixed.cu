@@ -237,6 +237,7 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
             root = nodePM[rootNode];
             eps2 = (float) dw.eps2;
             wp.dtHalf = 0.5 * dw.dt;
+            pot.time = dw.time;
         }
         const int i = grp.x + lane;
         const bool valid = lane < grp.y;

@@ -4,6 +4,116 @@
 #pragma once
 #include "nb_common.cuh"
 
+// The halos of nbody/src/nbody_potential.c:518-625 beyond the logarithmic and NFW ones
+// (the caustic halo is not supported): triaxial logarithmic (:518-541, constants c1..c3 as
+// nbody/src/nbody_check_params.c:182-194 sets them), Allen-Santillan (:543-561),
+// Wilkinson-Evans (:563-573), NFW by mass (:575-585), Plummer (:587-592), Hernquist
+// (:594-599) and the Ninkovic special case (:601-625), in the reference's operation order.
+// Their general powers and logarithms are CUDA's (<= 2 ulp), so runs with these halos agree
+// with the reference to rounding, not bit for bit.
+__device__ __forceinline__ void nb_halo_accel_more(const NbPot& p, double x, double y, double z,
+                                                   double r, double& tx, double& ty, double& tz)
+{
+    const double a = p.haloA, M = p.haloMass;
+    double c = 0.0;                    // acceleration = pos * c for the spherical halos
+    switch (p.haloType) {
+    case NBCUDA_TRIAXIAL_HALO: {
+        const double qzs = p.haloQz * p.haloQz;
+        const double rhalosqr = a * a;
+        const double mvsqr = -(p.haloV * p.haloV);
+        const double xsqr = x * x, ysqr = y * y, zsqr = z * z;
+        const double arst = rhalosqr + (p.haloC1 * xsqr) + (p.haloC3 * x * y) + (p.haloC2 * ysqr);
+        const double arst2 = (zsqr / qzs) + arst;
+        tx = mvsqr * (((2.0 * p.haloC1) * x) + (p.haloC3 * y)) / arst2;
+        ty = mvsqr * (((2.0 * p.haloC2) * y) + (p.haloC3 * x)) / arst2;
+        tz = (2.0 * mvsqr * z) / ((qzs * arst) + zsqr);
+        return;
+    }
+    case NBCUDA_ALLEN_SANTILLAN_HALO: {
+        const double gam = p.haloGamma, lam = p.haloLambda;
+        const double scaleR = r / a, scaleL = lam / a;
+        double cc;
+        if (r < lam) {
+            const double pw = pow(scaleR, gam - 1.0);
+            cc = -(M / (a * r)) * pw / (1.0 + pw);
+        } else {
+            cc = -(M / (r * r)) * pow(scaleL, gam) / (1.0 + pow(scaleL, gam - 1.0));
+        }
+        c = cc / r;
+        break;
+    }
+    case NBCUDA_WILKINSON_EVANS_HALO: {
+        const double sum2 = a * a + r * r;
+        const double cc = (-M / r) * (a + sqrt(sum2)) / (sum2 + a * sqrt(sum2));
+        c = cc / r;
+        break;
+    }
+    case NBCUDA_NFW_MASS_HALO: {
+        const double ar = a + r;
+        c = (-M / (r * r)) * (log(ar / a) / r - 1 / ar);
+        break;
+    }
+    case NBCUDA_PLUMMER_HALO: {
+        const double tmp = sqrt(a * a + r * r);
+        c = -M / (tmp * tmp * tmp);
+        break;
+    }
+    case NBCUDA_HERNQUIST_HALO: {
+        const double tmp = a + r;
+        c = -M / (r * (tmp * tmp));
+        break;
+    }
+    case NBCUDA_NINKOVIC_HALO: {
+        const double pi = 3.1415926535;                 // the reference's constant (:35)
+        const double lambda = p.haloLambda;
+        const double zr = r / a, zl = lambda / a;
+        const double f = 4.0 * pi / 3.0 * p.haloRho0 * (a * a * a);
+        const double zl3 = zl * zl * zl;
+        double menc;
+        if (r > lambda) menc = f * (log(1.0 + zl3) - zl3 / (1 + zl3));
+        else {
+            const double z3 = zr * zr * zr;
+            menc = f * (log(1.0 + z3) - z3 / (1 + zl3));
+        }
+        c = -menc / (r * r * r);
+        break;
+    }
+    default:
+        break;
+    }
+    tx = x * c; ty = y * c; tz = z * c;
+}
+
+// orbitingBarAccel (nbody/src/nbody_potential.c:410-457): the softened needle bar rotating at
+// patternSpeed, at the time p.time; atan, sin and cos are CUDA's.
+__device__ __forceinline__ void nb_bar_accel(const NbPot& p, double x, double y, double z,
+                                             double& ox, double& oy, double& oz)
+{
+    const double amp = p.disk2Mass, a = p.disk2A;
+    const double b = 1.4, c = 1;
+    const double curAngle = (p.disk2Pattern * p.time * -1) + p.disk2StartAngle;
+    double Radi = sqrt(x * x + y * y);
+    double Phi = atan(y / x);
+    Phi -= curAngle;
+    if (x < 0) Radi = Radi * -1;
+    const double xr = Radi * cos(Phi);
+    const double yr = Radi * sin(Phi);
+    const double zr = z;
+    const double sq = sqrt(c * c + zr * zr);
+    const double secondpart = yr * yr + (b + sq) * (b + sq);
+    const double Tp = sqrt((a + xr) * (a + xr) + secondpart);
+    const double Tm = sqrt((a - xr) * (a - xr) + secondpart);
+    const double fx = -2. * xr / Tp / Tm / (Tp + Tm);
+    const double sq2 = sqrt(zr * zr + c * c);
+    const double fy = -yr / 2. / Tp / Tm * (Tp + Tm - 4. * (xr * xr) / (Tp + Tm)) /
+                      (yr * yr + (b + sq2) * (b + sq2));
+    const double fz = fy * zr / yr * (b + sq2) / sq2;
+    const double cp = cos(curAngle), sp = sin(curAngle);
+    ox = (cp * fx - sp * fy) * amp;
+    oy = (sp * fx + cp * fy) * amp;
+    oz = fz * amp;
+}
+
 // nbExtAcceleration (nbody/src/nbody_potential.c:627-762) for the supported components:
 // Miyamoto-Nagai disks (:173-194), logarithmic (:488-504) and NFW (:506-515) halos,
 // Hernquist (:157-162) and Plummer (:164-169) bulges.
@@ -33,6 +143,8 @@ __device__ __forceinline__ void nb_ext_accel(const NbPot& p, double x, double y,
             tx = -p.disk2Mass * x / rth;
             ty = -p.disk2Mass * y / rth;
             tz = -p.disk2Mass * z * azp / (zp * rth);
+        } else if (p.disk2Type == NBCUDA_ORBITING_BAR) {
+            nb_bar_accel(p, x, y, z, tx, ty, tz);
         }
         axx = axx + tx; ayy = ayy + ty; azz = azz + tz;
     }
@@ -50,6 +162,8 @@ __device__ __forceinline__ void nb_ext_accel(const NbPot& p, double x, double y,
             const double ar = a + r;
             const double c = (-M / (r * r)) * (log(ar / a) / r - 1 / ar);
             tx = c * x; ty = c * y; tz = c * z;
+        } else if (p.haloType != NBCUDA_NO_HALO) {
+            nb_halo_accel_more(p, x, y, z, r, tx, ty, tz);
         }
         axx = axx + tx; ayy = ayy + ty; azz = azz + tz;
     }

@@ -43,6 +43,7 @@ k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeC
         dw = &forest.dwarfs[forest.bodyDwarf[i]];
         eps2 = dw->eps2;
         wp.dtHalf = 0.5 * dw->dt;
+        pot.time = dw->time;
         start = dw->rootNode;
         myEnd = dw->rootEnd;
     }

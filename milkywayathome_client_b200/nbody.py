@@ -49,6 +49,11 @@ class Disk:
         return _lib.Disk(_lib.MIYAMOTO_NAGAI_DISK, mass, scaleLength, scaleHeight, 0.0, 0.0)
 
     @staticmethod
+    def orbitingBar(mass, scaleLength, patternSpeed, startAngle):
+        """The softened needle bar (disk2 only), rotating at patternSpeed (rad/Gyr)."""
+        return _lib.Disk(_lib.ORBITING_BAR, mass, scaleLength, 0.0, patternSpeed, startAngle)
+
+    @staticmethod
     def none(mass=0.0):
         return _lib.Disk(_lib.NO_DISK, mass, 0.0, 0.0, 0.0, 0.0)
 
@@ -65,6 +70,55 @@ class Halo:
         h = _lib.Halo()
         h.type, h.vhalo, h.scaleLength = _lib.NFW_HALO, vhalo, scaleLength
         return h
+
+    @staticmethod
+    def triaxial(vhalo, scaleLength, flattenX, flattenY, flattenZ, triaxAngle):
+        """Triaxial logarithmic halo; c1..c3 as nbCheckParams derives them
+        (nbody/src/nbody_check_params.c:182-194)."""
+        h = _lib.Halo()
+        h.type, h.vhalo, h.scaleLength = _lib.TRIAXIAL_HALO, vhalo, scaleLength
+        h.flattenX, h.flattenY, h.flattenZ, h.triaxAngle = flattenX, flattenY, flattenZ, triaxAngle
+        phi = triaxAngle * math.pi / 180.0
+        cp, sp = math.cos(phi), math.sin(phi)
+        cps, sps = cp * cp, sp * sp
+        qxs, qys = flattenX * flattenX, flattenY * flattenY
+        h.c1 = (cps / qxs) + (sps / qys)
+        h.c2 = (cps / qys) + (sps / qxs)
+        h.c3 = math.sin(2.0 * phi) * ((qys - qxs) / (qxs * qys))
+        return h
+
+    @staticmethod
+    def _mass_halo(kind, mass, scaleLength, **extra):
+        h = _lib.Halo()
+        h.type, h.mass, h.scaleLength = kind, mass, scaleLength
+        for k, v in extra.items():
+            setattr(h, k, v)
+        return h
+
+    @staticmethod
+    def allenSantillan(mass, scaleLength, gamma, lambda_):
+        return Halo._mass_halo(_lib.ALLEN_SANTILLAN_HALO, mass, scaleLength, gamma=gamma,
+                               lambda_=lambda_)
+
+    @staticmethod
+    def wilkinsonEvans(mass, scaleLength):
+        return Halo._mass_halo(_lib.WILKINSON_EVANS_HALO, mass, scaleLength)
+
+    @staticmethod
+    def nfwMass(mass, scaleLength):
+        return Halo._mass_halo(_lib.NFW_MASS_HALO, mass, scaleLength)
+
+    @staticmethod
+    def plummer(mass, scaleLength):
+        return Halo._mass_halo(_lib.PLUMMER_HALO, mass, scaleLength)
+
+    @staticmethod
+    def hernquist(mass, scaleLength):
+        return Halo._mass_halo(_lib.HERNQUIST_HALO, mass, scaleLength)
+
+    @staticmethod
+    def ninkovic(rho0, scaleLength, lambda_):
+        return Halo._mass_halo(_lib.NINKOVIC_HALO, 0.0, scaleLength, rho0=rho0, lambda_=lambda_)
 
     @staticmethod
     def none(mass=0.0):

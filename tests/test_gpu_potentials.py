@@ -1,0 +1,75 @@
+"""The halo components beyond the logarithmic and NFW ones and the orbiting bar, against the
+reference itself (oracle/_ref: nbGravMap and nbStepSystem of the reference build).
+
+These components use general powers, logarithms and trigonometric functions (crlibm / libm in
+the reference, CUDA's on the GPU), so the accelerations agree to rounding (1e-12 relative),
+and a few steps stay within 1e-10; the bar's rotation is followed through the step count
+(barTime = step * timestep, nbody/src/nbody_grav.c:141).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _potentials():
+    from milkywayathome_client_b200 import nbody
+    bulge = nbody.Spherical.hernquist(mass=1.52954402e5, scale=0.7)
+    disk = nbody.Disk.miyamotoNagai(mass=4.45865888e5, scaleLength=6.5, scaleHeight=0.26)
+    log_halo = nbody.Halo.logarithmic(vhalo=73, scaleLength=12, flattenZ=1)
+    halos = {
+        "triaxial": nbody.Halo.triaxial(vhalo=116.0, scaleLength=16.0, flattenX=1.38,
+                                        flattenY=1.0, flattenZ=1.36, triaxAngle=97.0),
+        "allen-santillan": nbody.Halo.allenSantillan(mass=5e5, scaleLength=12.0, gamma=2.0,
+                                                     lambda_=200.0),
+        "wilkinson-evans": nbody.Halo.wilkinsonEvans(mass=5e5, scaleLength=12.0),
+        "nfw-mass": nbody.Halo.nfwMass(mass=5e5, scaleLength=12.0),
+        "plummer-halo": nbody.Halo.plummer(mass=5e5, scaleLength=12.0),
+        "hernquist-halo": nbody.Halo.hernquist(mass=5e5, scaleLength=12.0),
+        "ninkovic": nbody.Halo.ninkovic(rho0=100.0, scaleLength=12.0, lambda_=200.0),
+    }
+    pots = {k: nbody.Potential.create(spherical=bulge, disk=disk, halo=h) for k, h in halos.items()}
+    pots["bar"] = nbody.Potential.create(
+        spherical=bulge, disk=disk, halo=log_halo,
+        disk2=nbody.Disk.orbitingBar(mass=2e4, scaleLength=5.0, patternSpeed=40.0,
+                                     startAngle=0.5))
+    return pots
+
+
+POTS = ["triaxial", "allen-santillan", "wilkinson-evans", "nfw-mass", "plummer-halo",
+        "hernquist-halo", "ninkovic", "bar"]
+
+
+@pytest.mark.parametrize("name", POTS)
+def test_potential_against_reference_steps(dwarf_small, name):
+    from oracle import bindings as ob
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    from conftest import make_ctx
+    from milkywayathome_client_b200 import NBodyState
+    pos, vel, mass, _ = dwarf_small
+    ctx = make_ctx(len(mass), potential=_potentials()[name])
+    ref = ob.RefState.create(ctx.struct, pos, vel, mass)
+    assert ref.gravmap() == 0
+    want0 = ref.get()
+    with NBodyState.create(ctx, pos, vel, mass) as st:
+        got0 = st.accels()
+        np.testing.assert_allclose(got0, want0["acc"], rtol=1e-12,
+                                   atol=1e-12 * np.abs(want0["acc"]).max())
+        assert st.run_steps(ctx, 5) == 0
+        p, v = st.bodies()
+        a = st.accels()
+    assert ref.step(5) == 0
+    want = ref.get()
+    for g, w in ((p, want["pos"]), (v, want["vel"]), (a, want["acc"])):
+        np.testing.assert_allclose(g, w, rtol=1e-10, atol=1e-10 * np.abs(w).max())
+
+
+def test_adjoint_and_energy_reject_potentials_without_jacobian(dwarf_small):
+    from conftest import make_ctx
+    from milkywayathome_client_b200 import NBodyError, NBodyState
+    pos, vel, mass, _ = dwarf_small
+    ctx = make_ctx(len(mass), potential=_potentials()["triaxial"])
+    with NBodyState.create(ctx, pos, vel, mass) as st:
+        with pytest.raises(NBodyError):
+            st.energy(ctx)
