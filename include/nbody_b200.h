@@ -233,6 +233,11 @@ typedef struct {                       /* a data histogram as nbReadHistogram re
     const double* variable;            /* normalised counts */
     const double* err;                 /* count errors */
 } NBodyCudaDataHistogram;
+/* The bar's time origin, the reference's st->previousForwardTime (nbody/src/nbody.c:440-442):
+ * the orbiting bar is evaluated at step * timestep - previousForwardTime (0 by default).
+ * For a batch, set it on the batch's state through nbBatchSetTimeOriginCUDA. */
+NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTime);
+
 /* host array of nbody types (+1 light, -1 dark) */
 NBodyCudaStatus nbSetTypesCUDA(NBodyCudaState* st, const int* types);
 /* host outputs, any may be NULL: counts[nBins], totals[2] = {in range, light bodies},
@@ -243,6 +248,26 @@ NBodyCudaStatus nbHistogramCUDA(NBodyCudaState* st, const NBodyCudaHistogramPara
 /* out[4] = {EMD component + cost component, EMD, EMD component, cost component} */
 NBodyCudaStatus nbLikelihoodCUDA(NBodyCudaState* st, const NBodyCudaHistogramParams* hp,
                                  const NBodyCudaDataHistogram* data, double* out);
+
+/* ---- two-component Plummer dwarf initial conditions on the GPU ----
+ * The sampler of nbGenerateMixedDwarfCore (nbody/src/nbody_mixeddwarf.c:765-1026) for
+ * Dwarf.plummer components: rejection sampling of radii from r^2 rho(r) and of speeds from the
+ * Eddington distribution function (evaluated numerically as the reference does), isotropic
+ * directions, each component recentred on its centre of mass and velocity and shifted to
+ * position/velocity.  One thread per body with its own counter-based random stream: the
+ * samples follow the reference's distributions, not its dSFMT stream.  Baryons (type +1) are
+ * the first nbodyBaryon bodies, dark matter (type -1) the rest. */
+typedef struct {
+    int nbody, nbodyBaryon;
+    double massLight, scaleLight;      /* comp1 */
+    double massDark, scaleDark;        /* comp2 */
+    double position[3], velocity[3];   /* the dwarf's centre on its orbit */
+    unsigned long long seed;
+} NBodyCudaPlummerDwarf;
+/* fills the state's bodies and types (nbody must match the state) and resets the run like
+ * nbSetBodiesCUDA with treeRSize */
+NBodyCudaStatus nbGenerateDwarfCUDA(NBodyCudaState* st, const NBodyCudaPlummerDwarf* dwarf,
+                                    double treeRSize);
 
 /* ---- batched dwarfs (no reference counterpart: the reference runs one dwarf per process) ----
  * Many independent dwarfs stepped together.  Each dwarf is the reference's simulation (its own
@@ -298,11 +323,15 @@ NBodyCudaStatus nbBatchAutotuneCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bat
 /* histograms and likelihoods of every dwarf: types as nbSetTypesCUDA (all dwarfs' bodies),
  * counts[ndwarfs * nBins], totals[2 * ndwarfs], massPerParticle[ndwarfs], out[4 * ndwarfs] */
 NBodyCudaStatus nbBatchSetTypesCUDA(NBodyCudaBatch* batch, const int* types);
+NBodyCudaStatus nbBatchSetTimeOriginCUDA(NBodyCudaBatch* batch, double previousForwardTime);
 NBodyCudaStatus nbBatchHistogramCUDA(NBodyCudaBatch* batch, const NBodyCudaHistogramParams* hp,
                                      unsigned int* counts, unsigned int* totals,
                                      double* massPerParticle);
 NBodyCudaStatus nbBatchLikelihoodCUDA(NBodyCudaBatch* batch, const NBodyCudaHistogramParams* hp,
                                       const NBodyCudaDataHistogram* data, double* out);
+/* initial conditions of every dwarf of the batch in one launch per phase (one
+ * NBodyCudaPlummerDwarf per dwarf, nbody matching the batch); resets root sizes and statuses */
+NBodyCudaStatus nbBatchGenerateDwarfsCUDA(NBodyCudaBatch* batch, const NBodyCudaPlummerDwarf* dwarfs);
 /* mean device time of the steps of the last nbBatchRunStepsCUDA call */
 NBodyCudaStatus nbBatchLastStepTimeCUDA(NBodyCudaBatch* batch, double* stepMs);
 

@@ -85,6 +85,14 @@ class Dwarf(ctypes.Structure):
                 ("timestep", ctypes.c_double), ("treeRSize", ctypes.c_double)]
 
 
+class PlummerDwarf(ctypes.Structure):
+    _fields_ = [("nbody", ctypes.c_int), ("nbodyBaryon", ctypes.c_int),
+                ("massLight", ctypes.c_double), ("scaleLight", ctypes.c_double),
+                ("massDark", ctypes.c_double), ("scaleDark", ctypes.c_double),
+                ("position", ctypes.c_double * 3), ("velocity", ctypes.c_double * 3),
+                ("seed", ctypes.c_uint64)]
+
+
 class HistParams(ctypes.Structure):
     _fields_ = [("phi", ctypes.c_double), ("theta", ctypes.c_double), ("psi", ctypes.c_double),
                 ("lambdaStart", ctypes.c_double), ("lambdaEnd", ctypes.c_double),
@@ -155,6 +163,10 @@ SIGNATURES = [
     ("nbBatchAutotuneCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, _vp, _vp, _vp, _dp]),
     ("nbBatchLastStepTimeCUDA", ctypes.c_int, [_vp, _dp]),
     ("nbSetTypesCUDA", ctypes.c_int, [_vp, _vp]),
+    ("nbSetTimeOriginCUDA", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("nbBatchSetTimeOriginCUDA", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("nbGenerateDwarfCUDA", ctypes.c_int, [_vp, ctypes.POINTER(PlummerDwarf), ctypes.c_double]),
+    ("nbBatchGenerateDwarfsCUDA", ctypes.c_int, [_vp, ctypes.POINTER(PlummerDwarf)]),
     ("nbHistogramCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), _vp, _vp, _vp]),
     ("nbLikelihoodCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), ctypes.POINTER(DataHist),
                                         _vp]),

@@ -32,6 +32,10 @@ void nb_launch_direct_fp64(const double* px, const double* py, const double* pz,
                            double* vy, double* vz, const NbWalkParams& wp, const NbPot& pot,
                            NbScalars* sc, cudaStream_t s);
 void nb_launch_ext_only(const double* dpos, double* dacc, int n, const NbPot& pot, cudaStream_t s);
+int nb_launch_ic(const NBodyCudaPlummerDwarf* host, int nD, const int* firsts, void* dTable,
+                 double* scratch, NbTreeBuffers& b, int* types, int n, int numSMs, NbScalars* sc,
+                 cudaStream_t s);
+size_t nb_ic_table_bytes(int nD);
 
 static std::atomic<unsigned long long> g_launches{0};
 void nb_count_launch(int n) { g_launches.fetch_add((unsigned long long) n); }
@@ -149,6 +153,7 @@ struct NBodyCudaState {
     std::vector<NbSlot> slots;          // saved evaluations (nbSaveStateCUDA)
     double* adjScratch = nullptr;       // reverse step: 7 doubles per body
     int* types = nullptr;               // body types (+1 light, -1 dark), for histograms
+    double timeOrigin = 0.0;            // st->previousForwardTime: barTime = step * dt - this
     char* histScratch = nullptr;        // histogram / likelihood buffers
     size_t histScratchBytes = 0;
 };
@@ -342,7 +347,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
     const cudaStream_t s = st->stream;
     NbTreeBuffers& b = st->b;
     NbPot pot = nb_pot_from(ctx);
-    pot.time = st->step * ctx->timestep;   // barTime (nbody/src/nbody_grav.c:141)
+    pot.time = st->step * ctx->timestep - st->timeOrigin;   // barTime (nbody/src/nbody_grav.c:141)
     NbWalkParams wp{};
     wp.eps2 = ctx->eps2;
     wp.dtHalf = 0.5 * ctx->timestep;
@@ -1189,7 +1194,67 @@ static NBodyCudaStatus nb_set_types(NBodyCudaState* st, const int* types)
     return NBODY_SUCCESS;
 }
 
+// Samples nD dwarfs into the state's bodies (dwarf k from body firsts[k]) and types.
+static NBodyCudaStatus nb_generate(NBodyCudaState* st, const NBodyCudaPlummerDwarf* d, int nD,
+                                   const int* firsts)
+{
+    for (int k = 0; k < nD; ++k) {
+        const NBodyCudaPlummerDwarf& w = d[k];
+        if (w.nbody < 1 || w.nbodyBaryon < 0 || w.nbodyBaryon > w.nbody ||
+            !(w.scaleLight > 0.0) || !(w.scaleDark > 0.0) || !(w.massLight >= 0.0) ||
+            !(w.massDark >= 0.0)) {
+            g_lastError = "invalid dwarf parameters";
+            return NBODY_USER_ERROR;
+        }
+    }
+    NB_CHECK(cudaSetDevice(st->device));
+    if (!st->types) NB_CHECK(nb_alloc(&st->types, (size_t) st->capBodies));
+    void* table = nullptr;
+    double* scratch = nullptr;
+    NB_CHECK(cudaMalloc(&table, nb_ic_table_bytes(nD)));
+    cudaError_t e = cudaMalloc((void**) &scratch, sizeof(double) * 12 * (size_t) nD);
+    if (e != cudaSuccess) { cudaFree(table); return nb_cuda_fail(e, "cudaMalloc"); }
+    const cudaStream_t s = st->stream;
+    NbScalars init{};
+    init.rsize = st->rsize;
+    init.capNodes = st->capNodes;
+    e = cudaMemcpyAsync(st->b.sc, &init, sizeof init, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        nb_launch_ic(d, nD, firsts, table, scratch, st->b, st->types, st->nbody, st->numSMs,
+                     st->b.sc, s);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(st->scHost, st->b.sc, sizeof(NbScalars),
+                                              cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(table);
+    cudaFree(scratch);
+    if (e != cudaSuccess) return nb_cuda_fail(e, "nbGenerateDwarf");
+    if (st->scHost->status & ~(int) NBODY_STATUS_WARNINGS_MASK) {
+        g_lastError = "the sampler found no radius or speed for some body";
+        return st->scHost->status;
+    }
+    return NBODY_SUCCESS;
+}
+
 extern "C" {
+
+NBodyCudaStatus nbGenerateDwarfCUDA(NBodyCudaState* st, const NBodyCudaPlummerDwarf* dwarf,
+                                    double treeRSize)
+{
+    if (!st || !dwarf || dwarf->nbody != st->nbody) return NBODY_USER_ERROR;
+    NBodyCudaStatus rc = nb_reset_run(st, treeRSize);
+    if (rc) return rc;
+    const int first = 0;
+    return nb_generate(st, dwarf, 1, &first);
+}
+
+NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTime)
+{
+    if (!st) return NBODY_USER_ERROR;
+    st->timeOrigin = previousForwardTime;
+    return NBODY_SUCCESS;
+}
 
 NBodyCudaStatus nbSetTypesCUDA(NBodyCudaState* st, const int* types)
 {
@@ -1328,6 +1393,8 @@ static NBodyCudaStatus nb_batch_eval(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt
         NB_CHECK(cudaMemcpyAsync(&b.sc->capNodes, &st->capNodes, sizeof(int),
                                  cudaMemcpyHostToDevice, s));
         NB_CHECK(cudaMemcpyAsync(&b.sc->step, &st->step, sizeof(int), cudaMemcpyHostToDevice, s));
+        NB_CHECK(cudaMemcpyAsync(&b.sc->timeOrigin, &st->timeOrigin, sizeof(double),
+                                 cudaMemcpyHostToDevice, s));
         NB_CHECK(cudaStreamSynchronize(s));
         if (useGraph) {
             const bool same = bt->graph && bt->graphDrift == drift && bt->graphKick == kick &&
@@ -1631,6 +1698,13 @@ NBodyCudaStatus nbBatchAutotuneCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt,
     return rc;
 }
 
+NBodyCudaStatus nbBatchSetTimeOriginCUDA(NBodyCudaBatch* bt, double previousForwardTime)
+{
+    if (!bt) return NBODY_USER_ERROR;
+    bt->st->timeOrigin = previousForwardTime;
+    return NBODY_SUCCESS;
+}
+
 NBodyCudaStatus nbBatchSetTypesCUDA(NBodyCudaBatch* bt, const int* types)
 {
     if (!bt) return NBODY_USER_ERROR;
@@ -1654,6 +1728,24 @@ NBodyCudaStatus nbBatchLikelihoodCUDA(NBodyCudaBatch* bt, const NBodyCudaHistogr
     for (int d = 0; d < bt->nDwarfs; ++d) nb[d] = bt->dwarfs[d].nbody;
     return nb_hist_run(bt->st, bt->bodyDwarf, bt->nDwarfs, nb.data(), hp, data, nullptr, nullptr,
                        nullptr, out);
+}
+
+NBodyCudaStatus nbBatchGenerateDwarfsCUDA(NBodyCudaBatch* bt, const NBodyCudaPlummerDwarf* dwarfs)
+{
+    if (!bt || !dwarfs) return NBODY_USER_ERROR;
+    std::vector<int> firsts(bt->nDwarfs);
+    int first = 0;
+    for (int d = 0; d < bt->nDwarfs; ++d) {
+        if (dwarfs[d].nbody != bt->dwarfs[d].nbody) {
+            g_lastError = "dwarf body counts do not match the batch";
+            return NBODY_USER_ERROR;
+        }
+        firsts[d] = first;
+        first += dwarfs[d].nbody;
+    }
+    NBodyCudaStatus rc = nb_generate(bt->st, dwarfs, bt->nDwarfs, firsts.data());
+    if (rc) return rc;
+    return nb_batch_reset_table(bt);
 }
 
 NBodyCudaStatus nbBatchLastStepTimeCUDA(NBodyCudaBatch* bt, double* stepMs)

@@ -44,7 +44,7 @@ __global__ void k_b_reset(NbScalars* __restrict__ sc, NbDwarfDev* __restrict__ d
     }
     for (int d = t; d < nDwarfs; d += gridDim.x * blockDim.x) {
         dw[d].xyzmaxBits = 0;
-        dw[d].time = sc->step * dw[d].dt;              // barTime of this evaluation
+        dw[d].time = sc->step * dw[d].dt - sc->timeOrigin;   // barTime of this evaluation
     }
 }
 

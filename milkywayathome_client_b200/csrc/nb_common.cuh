@@ -46,6 +46,7 @@ struct NbScalars {
     int groupNext;                  // next group for the persistent group walk
     int nGroups;                    // walk groups formed for the mixed walk
     int step;                       // batched dwarfs: steps taken (the bar's time)
+    double timeOrigin;              // batched dwarfs: the bar's time origin
 };
 
 // Potential parameters in constant-friendly POD form.

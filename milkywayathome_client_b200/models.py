@@ -206,3 +206,26 @@ def batched_dwarfs(draws, potential, seed=0, orbit_dt=1e-3, device=0, nsteps=Non
         out.append(dict(pos=pos, vel=vel, mass=mass, types=typ, eps2=cfg["eps2"],
                         timestep=dt, params=d))
     return out
+
+
+def batched_dwarf_structs(draws, potential, seed=0, orbit_dt=1e-3, device=0, nsteps=None,
+                          orbit=((218.0, 53.5, 28.6), (-156.0, 79.0, 107.0))):
+    """As batched_dwarfs, for the GPU sampler: returns the batch spec [(nbody, eps2, timestep,
+    treeRSize)] and one NBodyCudaPlummerDwarf per draw (nbBatchGenerateDwarfsCUDA samples the
+    bodies on the device with the reference's two-component algorithm)."""
+    from .nbody import plummer_dwarf_struct
+    (l, b, r), v0 = orbit
+    p0 = lbr_to_cartesian(l, b, r)
+    starts, vstarts = reverse_orbits(potential, np.tile(p0, (len(draws), 1)),
+                                     np.tile(np.asarray(v0, dtype=np.float64), (len(draws), 1)),
+                                     [d["t_forward"] for d in draws], orbit_dt, device)
+    spec, structs = [], []
+    for k, d in enumerate(draws):
+        cfg = dwarf_config(d["nbody"], mass_l=d["mass_l"], rscale_l=d["rscale_l"],
+                           light_r_ratio=d["light_r_ratio"], light_mass_ratio=d["light_mass_ratio"])
+        dt = d["t_forward"] / nsteps if nsteps else cfg["timestep"]
+        spec.append((d["nbody"], cfg["eps2"], dt, 4.0))
+        structs.append(plummer_dwarf_struct(d["nbody"], seed + k, None, d["mass_l"], d["rscale_l"],
+                                            d["light_r_ratio"], d["light_mass_ratio"], starts[k],
+                                            vstarts[k]))
+    return spec, structs

@@ -200,6 +200,25 @@ class NBodyCtx:
         return self._c
 
 
+def plummer_dwarf_struct(nbody, seed, nbody_baryon=None, mass_l=12.0, rscale_l=0.2,
+                         light_r_ratio=0.2, light_mass_ratio=0.2, position=None, velocity=None):
+    """NBodyCudaPlummerDwarf with the parameterisation of the sample workunits
+    (for_developers.lua: dark radius rscale_l / light_r_ratio * (1 - light_r_ratio), dark mass
+    mass_l / light_mass_ratio * (1 - light_mass_ratio))."""
+    d = _lib.PlummerDwarf()
+    d.nbody = int(nbody)
+    d.nbodyBaryon = int(nbody // 2 if nbody_baryon is None else nbody_baryon)
+    d.massLight, d.scaleLight = mass_l, rscale_l
+    d.massDark = mass_l / light_mass_ratio * (1.0 - light_mass_ratio)
+    d.scaleDark = rscale_l / light_r_ratio * (1.0 - light_r_ratio)
+    pos = np.zeros(3) if position is None else np.asarray(position, dtype=np.float64)
+    vel = np.zeros(3) if velocity is None else np.asarray(velocity, dtype=np.float64)
+    for c in range(3):
+        d.position[c], d.velocity[c] = float(pos[c]), float(vel[c])
+    d.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    return d
+
+
 class NBodyState:
     """Device-resident N-body state: NBodyState.create(ctx, bodies) and state:step(ctx)
     (nbody/src/nbody_lua_types/nbody_lua_nbodystate.c:60-147) over the CUDA library.
@@ -252,6 +271,26 @@ class NBodyState:
         if status_is_fatal(rc):
             raise NBodyError(what, rc)
         return rc
+
+    @classmethod
+    def generate(cls, ctx, nbody, seed, nbody_baryon=None, mass_l=12.0, rscale_l=0.2,
+                 light_r_ratio=0.2, light_mass_ratio=0.2, position=None, velocity=None,
+                 device=0, gravmap=True):
+        """A two-component Plummer dwarf sampled on the GPU (nbGenerateDwarfCUDA) with the
+        parameters of plummer_plummer_dwarf, then nbGravMap."""
+        st = cls(nbody, device)
+        d = plummer_dwarf_struct(nbody, seed, nbody_baryon, mass_l, rscale_l, light_r_ratio,
+                                 light_mass_ratio, position, velocity)
+        st.check("nbGenerateDwarf", st.lib.nbGenerateDwarfCUDA(st._h, ctypes.byref(d),
+                                                                float(ctx.treeRSize)))
+        if gravmap:
+            st.check("nbGravMap", st.gravMap(ctx))
+        return st
+
+    def set_time_origin(self, previous_forward_time):
+        """The orbiting bar's time origin (the reference's st->previousForwardTime)."""
+        self.check("nbSetTimeOrigin", self.lib.nbSetTimeOriginCUDA(self._h,
+                                                                  float(previous_forward_time)))
 
     # -- marshalling (nbMarshalBodies) --
     def set_bodies(self, pos, vel, mass, treeRSize=4.0):
@@ -494,6 +533,16 @@ class NBodyBatch:
         ms = ctypes.c_double()
         self.lib.nbBatchLastStepTimeCUDA(self._h, ctypes.byref(ms))
         return ms.value
+
+    def generate(self, dwarfs):
+        """Sample every dwarf on the GPU in one launch per phase (nbBatchGenerateDwarfsCUDA):
+        dwarfs is a list of plummer_dwarf_struct()s matching the batch's sizes."""
+        arr = (_lib.PlummerDwarf * len(dwarfs))(*dwarfs)
+        self.check("nbBatchGenerateDwarfs", self.lib.nbBatchGenerateDwarfsCUDA(self._h, arr))
+
+    def set_time_origin(self, previous_forward_time):
+        self.check("nbBatchSetTimeOrigin", self.lib.nbBatchSetTimeOriginCUDA(
+            self._h, float(previous_forward_time)))
 
     _kind = "nbBatch"
     set_types = NBodyState.set_types

@@ -245,6 +245,10 @@ class RefState:
                                  ctypes.byref(stp), ctypes.byref(inc))
         return dict(pos=pos, vel=vel, acc=acc, rsize=rs.value, step=stp.value, incest=inc.value)
 
+    def set_time_origin(self, t):
+        self.lib.nbref_state_set_time_origin.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        self.lib.nbref_state_set_time_origin(self.h, float(t))
+
     def set(self, pos=None, vel=None):
         self.lib.nbref_state_set(self.h, _p(None if pos is None else np.ascontiguousarray(pos, dtype=np.float64)),
                                  _p(None if vel is None else np.ascontiguousarray(vel, dtype=np.float64)))

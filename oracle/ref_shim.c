@@ -222,6 +222,12 @@ void nbref_state_masses(void* hv, double* mass, int* type)
     }
 }
 
+/* st->previousForwardTime: the bar's time origin (barTime = step * timestep - this) */
+void nbref_state_set_time_origin(void* hv, double t)
+{
+    ((RefHandle*) hv)->st.previousForwardTime = t;
+}
+
 void nbref_state_set(void* hv, const double* pos, const double* vel)
 {
     RefHandle* h = (RefHandle*) hv;
