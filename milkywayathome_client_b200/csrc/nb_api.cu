@@ -550,8 +550,7 @@ static NBodyCudaStatus nb_download3(NBodyCudaState* st, double* host, const doub
     nb_count_launch();
     NB_CHECK(cudaMemcpyAsync(host, st->stage, 3 * (size_t) n * sizeof(double),
                              cudaMemcpyDeviceToHost, st->stream));
-    NB_CHECK(cudaStreamSynchronize(st->stream));
-    return NBODY_SUCCESS;
+    return NBODY_SUCCESS;          // the caller synchronises (stream order protects the stage)
 }
 
 NBodyCudaStatus nbSetBodiesCUDA(NBodyCudaState* st, const double* pos, const double* vel,
@@ -580,6 +579,7 @@ NBodyCudaStatus nbGetBodiesCUDA(NBodyCudaState* st, double* pos, double* vel)
     NBodyCudaStatus rc = NBODY_SUCCESS;
     if (pos) rc = nb_download3(st, pos, b.px, b.py, b.pz, st->nbody);
     if (!rc && vel) rc = nb_download3(st, vel, b.vx, b.vy, b.vz, st->nbody);
+    if (!rc) NB_CHECK(cudaStreamSynchronize(st->stream));
     return rc;
 }
 
@@ -587,7 +587,9 @@ NBodyCudaStatus nbGetAccelsCUDA(NBodyCudaState* st, double* acc)
 {
     if (!st || !acc) return NBODY_USER_ERROR;
     NB_CHECK(cudaSetDevice(st->device));
-    return nb_download3(st, acc, st->b.ax, st->b.ay, st->b.az, st->nbody);
+    NBodyCudaStatus rc = nb_download3(st, acc, st->b.ax, st->b.ay, st->b.az, st->nbody);
+    if (!rc) NB_CHECK(cudaStreamSynchronize(st->stream));
+    return rc;
 }
 
 NBodyCudaStatus nbSetBodiesDeviceCUDA(NBodyCudaState* st, const double* dpos, const double* dvel,

@@ -308,9 +308,15 @@ class NBodyState:
                                           int(bool(to_device)), float(treeRSize))
         self.check("nbMarshalBodiesCUDA", rc)
 
-    def bodies(self):
-        pos = np.empty((self.nbody, 3))
-        vel = np.empty((self.nbody, 3))
+    def bodies(self, out=None):
+        """(pos, vel) of every body; out: two C-contiguous float64 (n,3) arrays to fill (page-
+        locked ones make the copy a direct DMA)."""
+        if out is None:
+            pos, vel = np.empty((self.nbody, 3)), np.empty((self.nbody, 3))
+        else:
+            pos, vel = out
+            for a in out:
+                assert a.dtype == np.float64 and a.flags.c_contiguous and a.shape == (self.nbody, 3)
         self.check("nbGetBodiesCUDA", self.lib.nbGetBodiesCUDA(self._h, _lib.ptr(pos), _lib.ptr(vel)))
         return pos, vel
 
