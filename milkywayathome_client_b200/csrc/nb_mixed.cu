@@ -237,7 +237,6 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
             root = nodePM[rootNode];
             eps2 = (float) dw.eps2;
             wp.dtHalf = 0.5 * dw.dt;
-            pot.time = dw.time;
         }
         const int i = grp.x + lane;
         const bool valid = lane < grp.y;
@@ -351,7 +350,7 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
         if (valid) {
             // test particles are not in the tree and never meet themselves (nbody_grav.c:111-118)
             if (mass[j] == 0.0) atomicOr(&sc->incest, 1);
-            nb_finish_body(pot, wp, j, x0, y0, z0, accx, accy, accz, ax, ay, az, vx, vy, vz);
+            ax[j] = accx; ay[j] = accy; az[j] = accz;   // k_body_epilogue adds the rest
         }
     }
     if (COUNT && lane == 0) {
@@ -384,6 +383,11 @@ static void nb_walk_mixed_cap(const NbTreeBuffers& b, const NbMixedBuffers& m,
     }
 }
 
+void nb_launch_body_epilogue(const double* px, const double* py, const double* pz, double* ax,
+                             double* ay, double* az, double* vx, double* vy, double* vz,
+                             const NbWalkParams& wp, const NbPot& pot, const NbScalars* sc,
+                             int numSMs, cudaStream_t s, const NbForest* forest);
+
 void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int capNodes,
                           const NbWalkParams& wp, const NbPot& pot, bool count, int numSMs,
                           cudaStream_t s, const NbForest* forest)
@@ -409,6 +413,8 @@ void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int c
         else nb_walk_mixed_cap<false, false>(b, m, wp, pot, blocks, f, s);
     }
     nb_count_launch();
+    nb_launch_body_epilogue(b.px, b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
+                            numSMs, s, forest);
 }
 
 // Persistent grid of the group walk: as many blocks as fit on the device at once (for the

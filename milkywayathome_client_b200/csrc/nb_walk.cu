@@ -43,7 +43,6 @@ k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeC
         dw = &forest.dwarfs[forest.bodyDwarf[i]];
         eps2 = dw->eps2;
         wp.dtHalf = 0.5 * dw->dt;
-        pot.time = dw->time;
         start = dw->rootNode;
         myEnd = dw->rootEnd;
     }
@@ -114,7 +113,50 @@ k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeC
         atomicOr(&sc->incest, 1);
         if (FOREST) atomicOr(&dw->status, NBODY_TREE_INCEST_NONFATAL);
     }
-    nb_finish_body(pot, wp, j, x0, y0, z0, accx, accy, accz, ax, ay, az, vx, vy, vz);
+    // self-gravity only; k_body_epilogue adds the external potential and kicks (kept out of
+    // this kernel so that its registers serve the walk)
+    ax[j] = accx; ay[j] = accy; az[j] = accz;
+}
+
+// nbMapForceBody's epilogue for every body after a tree walk: a = self-gravity (as the walk
+// stored it) + nbExtAcceleration + the zero LMC term, then the optional kick (nb_finish_body).
+// FOREST: each body with its dwarf's time step and the bar's time of its dwarf.
+template <bool FOREST>
+__global__ void k_body_epilogue(const double* __restrict__ px, const double* __restrict__ py,
+                                const double* __restrict__ pz, double* __restrict__ ax,
+                                double* __restrict__ ay, double* __restrict__ az,
+                                double* __restrict__ vx, double* __restrict__ vy,
+                                double* __restrict__ vz, NbWalkParams wp, NbPot pot,
+                                const NbScalars* __restrict__ sc, NbForest forest)
+{
+    if (nb_failed(sc)) return;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < wp.n; j += gridDim.x * blockDim.x) {
+        NbWalkParams w = wp;
+        NbPot p = pot;
+        if (FOREST) {
+            const NbDwarfDev& d = forest.dwarfs[forest.bodyDwarf[j]];
+            w.dtHalf = 0.5 * d.dt;
+            p.time = d.time;
+        }
+        nb_finish_body(p, w, (unsigned) j, px[j], py[j], pz[j], ax[j], ay[j], az[j], ax, ay, az,
+                       vx, vy, vz);
+    }
+}
+
+void nb_launch_body_epilogue(const double* px, const double* py, const double* pz, double* ax,
+                             double* ay, double* az, double* vx, double* vy, double* vz,
+                             const NbWalkParams& wp, const NbPot& pot, const NbScalars* sc,
+                             int numSMs, cudaStream_t s, const NbForest* forest)
+{
+    if (wp.n <= 0) return;
+    const int g = numSMs > 0 ? min((wp.n + 255) / 256, numSMs * 8) : (wp.n + 255) / 256;
+    if (forest)
+        k_body_epilogue<true><<<g, 256, 0, s>>>(px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc,
+                                                *forest);
+    else
+        k_body_epilogue<false><<<g, 256, 0, s>>>(px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc,
+                                                 NbForest{nullptr, nullptr, 0});
+    nb_count_launch();
 }
 
 // nbGravity_Exact (nbody/src/nbody_grav.c:205-227): direct sum over all bodies in input
@@ -274,6 +316,11 @@ __global__ void k_ext_only(const double* __restrict__ pos, double* __restrict__ 
 }
 
 // ---- host launchers ----
+void nb_launch_body_epilogue(const double* px, const double* py, const double* pz, double* ax,
+                             double* ay, double* az, double* vx, double* vy, double* vz,
+                             const NbWalkParams& wp, const NbPot& pot, const NbScalars* sc,
+                             int numSMs, cudaStream_t s, const NbForest* forest);
+
 void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
                          const double* nodeQuad, const unsigned* order, const double* px,
                          const double* py, const double* pz, double* ax, double* ay, double* az,
@@ -296,6 +343,7 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
     }
 #undef NB_WALK_ARGS
     nb_count_launch();
+    nb_launch_body_epilogue(px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc, 0, s, forest);
 }
 
 void nb_launch_direct_fp64(const double* px, const double* py, const double* pz,
