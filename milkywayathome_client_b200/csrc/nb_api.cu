@@ -172,6 +172,7 @@ static void nb_free_nodes(NBodyCudaState* st)
     cudaFree(b.nodePM); cudaFree(b.nodeCrit); cudaFree(b.nodeLink); cudaFree(b.nodeQuad);
     cudaFree(b.nodeDepth); cudaFree(b.parent); cudaFree(b.nchild); cudaFree(b.arrive);
     cudaFree(b.nodeRange); b.nodeRange = nullptr;
+    cudaFree(b.walkRec); b.walkRec = nullptr;
     cudaFree(st->mx.groups);
     cudaFree(st->mx.hi); cudaFree(st->mx.lo); cudaFree(st->mx.q32); cudaFree(st->mx.child8);
     b.nodePM = nullptr; b.nodeCrit = nullptr; b.nodeLink = nullptr; b.nodeQuad = nullptr;
@@ -197,6 +198,7 @@ static NBodyCudaStatus nb_alloc_nodes(NBodyCudaState* st, int cap)
     NB_CHECK(nb_alloc(&b.nchild, cap));
     NB_CHECK(nb_alloc(&b.arrive, cap));
     NB_CHECK(nb_alloc(&b.nodeRange, cap));
+    NB_CHECK(nb_alloc(&b.walkRec, 3 * (size_t) cap));
     NB_CHECK(nb_alloc(&st->mx.groups, cap));
     NB_CHECK(nb_alloc(&st->mx.hi, cap));
     NB_CHECK(nb_alloc(&st->mx.lo, cap));
@@ -391,7 +393,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
             else
                 nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px,
                                     b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
-                                    st->counting != 0, s);
+                                    st->counting != 0, s, b.walkRec, st->capNodes);
             NB_CHECK(cudaEventRecord(st->ev1, s));
             st->walkLaunches = 1;
             st->haveTree = 1;
@@ -1363,7 +1365,8 @@ static int nb_batch_enqueue(NBodyCudaBatch* bt, const NBodyCudaCtx* ctx, int dri
         launches += 3;
     } else {
         nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px, b.py,
-                            b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc, false, s, &f);
+                            b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc, false, s,
+                            b.walkRec, st->capNodes, &f);
         launches += 1;
     }
     cudaEventRecord(st->ev1, s);

@@ -182,6 +182,7 @@ struct NbTreeBuffers {
     double4* nodePM; double* nodeCrit; int2* nodeLink; double* nodeQuad;
     int *nodeDepth, *parent, *nchild, *arrive;
     int2* nodeRange;   // first and last sorted body of every node's subtree
+    double4* walkRec;  // 3 per node: the FP64 walk's packed node records
     NbScalars* sc;
 };
 
@@ -206,7 +207,7 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
                          const double* py, const double* pz, double* ax, double* ay, double* az,
                          double* vx, double* vy, double* vz, const NbWalkParams& wp,
                          const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s,
-                         const NbForest* forest = nullptr);
+                         double4* walkRec, int capNodes, const NbForest* forest = nullptr);
 void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int capNodes,
                           const NbWalkParams& wp, const NbPot& pot, bool count, int numSMs,
                           cudaStream_t s, const NbForest* forest = nullptr);

@@ -18,10 +18,31 @@ constexpr int WALK_THREADS = 128;
 // FOREST: the nodes hold one tree per dwarf (batched dwarfs); each lane walks its own
 // dwarf's tree, [rootNode, rootEnd), with that dwarf's softening and time step.  A warp whose
 // 32 bodies straddle two dwarfs visits the union of both walks, each lane its own.
+// The walk reads one packed record per node (k_pack_walk): 96 bytes, three double4 --
+// {CoM, mass}, {rcrit2, Next and body index as one 64-bit word, Qxx, Qxy},
+// {Qxz, Qyy, Qyz, Qzz} -- so a visit touches one record instead of four arrays.
+__global__ void k_pack_walk(const double4* __restrict__ nodePM, const double* __restrict__ nodeCrit,
+                            const int2* __restrict__ nodeLink, const double* __restrict__ nodeQuad,
+                            double4* __restrict__ rec, const NbScalars* __restrict__ sc)
+{
+    if (nb_failed(sc)) return;
+    const int nNodes = sc->nNodes;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nNodes; k += gridDim.x * blockDim.x) {
+        const int2 l = nodeLink[k];
+        const long long word = (long long) (unsigned) l.x | ((long long) l.y << 32);
+        const double* Q = nodeQuad + 6 * (size_t) k;
+        const bool body = l.y >= 0;
+        rec[3 * (size_t) k] = nodePM[k];
+        rec[3 * (size_t) k + 1] = make_double4(nodeCrit[k], __longlong_as_double(word),
+                                               body ? 0.0 : Q[0], body ? 0.0 : Q[1]);
+        rec[3 * (size_t) k + 2] = body ? make_double4(0.0, 0.0, 0.0, 0.0)
+                                       : make_double4(Q[2], Q[3], Q[4], Q[5]);
+    }
+}
+
 template <bool COUNT, bool FOREST>
 __global__ void __launch_bounds__(WALK_THREADS)
-k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeCrit,
-            const int2* __restrict__ nodeLink, const double* __restrict__ nodeQuad,
+k_walk_fp64(const double4* __restrict__ rec,
             const unsigned int* __restrict__ order, const double* __restrict__ px,
             const double* __restrict__ py, const double* __restrict__ pz,
             double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
@@ -56,13 +77,15 @@ k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeC
         if (q >= end) break;
         if (COUNT) ++cSteps;
         if (ptr != q) continue;
-        const double4 nd = nodePM[q];
-        const int2 link = nodeLink[q];
+        const double4 nd = rec[3 * (size_t) q];
+        const double4 r1 = rec[3 * (size_t) q + 1];
+        const long long word = __double_as_longlong(r1.y);
+        const int2 link = make_int2((int) (unsigned) (word & 0xffffffffll), (int) (word >> 32));
         const double dx = nd.x - x0, dy = nd.y - y0, dz = nd.z - z0;
         double drSq = dz * dz + (dy * dy + dx * dx);
         const bool isBody = link.y >= 0;
         if (COUNT) ++cVisit;
-        if (isBody || drSq >= nodeCrit[q]) {
+        if (isBody || drSq >= r1.x) {
             ptr = link.x;
             if (isBody && (unsigned) link.y == j) { metSelf = true; continue; }
             if (COUNT) { if (isBody) ++cBB; else ++cBC; }
@@ -74,9 +97,8 @@ k_walk_fp64(const double4* __restrict__ nodePM, const double* __restrict__ nodeC
             accy = accy + mor3 * dy;
             accz = accz + mor3 * dz;
             if (useQuad && !isBody) {
-                const double2* Q2 = reinterpret_cast<const double2*>(nodeQuad + 6 * (size_t) q);
-                const double2 q01 = Q2[0], q23 = Q2[1], q45 = Q2[2];
-                const double qxx = q01.x, qxy = q01.y, qxz = q23.x, qyy = q23.y, qyz = q45.x, qzz = q45.y;
+                const double4 r2 = rec[3 * (size_t) q + 2];
+                const double qxx = r1.z, qxy = r1.w, qxz = r2.x, qyy = r2.y, qyz = r2.z, qzz = r2.w;
                 const double qdx = qxx * dx + qxy * dy + qxz * dz;
                 const double qdy = qxy * dx + qyy * dy + qyz * dz;
                 const double qdz = qxz * dx + qyz * dy + qzz * dz;
@@ -326,14 +348,16 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
                          const double* py, const double* pz, double* ax, double* ay, double* az,
                          double* vx, double* vy, double* vz, const NbWalkParams& wp,
                          const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s,
-                         const NbForest* forest)
+                         double4* walkRec, int capNodes, const NbForest* forest)
 {
     const int warps = (wp.n + 31) / 32;
     const int blocks = (warps * 32 + WALK_THREADS - 1) / WALK_THREADS;
     if (blocks <= 0) return;
+    k_pack_walk<<<min((capNodes + 255) / 256, 4096), 256, 0, s>>>(nodePM, nodeCrit, nodeLink,
+                                                                  nodeQuad, walkRec, sc);
+    nb_count_launch();
     const NbForest f = forest ? *forest : NbForest{nullptr, nullptr, 0};
-#define NB_WALK_ARGS nodePM, nodeCrit, nodeLink, nodeQuad, order, px, py, pz, ax, ay, az, vx, vy, \
-                     vz, wp, pot, sc, f
+#define NB_WALK_ARGS walkRec, order, px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc, f
     if (forest) {
         if (count) k_walk_fp64<true, true><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
         else k_walk_fp64<false, true><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
