@@ -238,6 +238,10 @@ typedef struct {                       /* a data histogram as nbReadHistogram re
  * For a batch, set it on the batch's state through nbBatchSetTimeOriginCUDA. */
 NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTime);
 
+/* Mixed-precision walk tuning of a single state (as nbBatchSetTuningCUDA): bodies per walk
+ * group (1..64), interaction-list entries per warp (32, 64, 128), walk blocks per SM (0: max). */
+NBodyCudaStatus nbSetMixedTuningCUDA(NBodyCudaState* st, int groupMax, int listCap, int blocksPerSM);
+
 /* host array of nbody types (+1 light, -1 dark) */
 NBodyCudaStatus nbSetTypesCUDA(NBodyCudaState* st, const int* types);
 /* host outputs, any may be NULL: counts[nBins], totals[2] = {in range, light bodies},
@@ -308,14 +312,15 @@ NBodyCudaStatus nbBatchRunStepsCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bat
  * current root size, its root's node index and node count */
 NBodyCudaStatus nbBatchDwarfInfoCUDA(NBodyCudaBatch* batch, int* status, double* rsize,
                                      int* rootNode, int* nodes);
-/* mixed-precision walk tuning: bodies per walk group (1..32), interaction-list entries per
- * warp (32, 64 or 128), resident walk blocks per SM (0: as many as fit) */
+/* mixed-precision walk tuning: bodies per walk group (1..64; above 32 each lane walks for two
+ * bodies), interaction-list entries per warp (32, 64 or 128), resident walk blocks per SM
+ * (0: as many as fit) */
 NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* batch, int groupMax, int listCap,
                                      int blocksPerSM);
 NBodyCudaStatus nbBatchGetTuningCUDA(NBodyCudaBatch* batch, int* groupMax, int* listCap,
                                      int* blocksPerSM);
 /* autotuner of the mixed walk on the batch's current state: times every candidate tuning
- * (groupMax 16/24/32 x listCap 32/64/128 x blocksPerSM 0/3) with force evaluations that do not
+ * (groupMax 24/32/48/64 x listCap 32/64/128 x blocksPerSM 0/3) with force evaluations that do not
  * move the bodies, keeps the fastest, re-evaluates the accelerations with it and returns it
  * (and its walk time in ms).  With FP64 precision nothing is tuned. */
 NBodyCudaStatus nbBatchAutotuneCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* batch, int* groupMax,

@@ -154,6 +154,7 @@ struct NBodyCudaState {
     double* adjScratch = nullptr;       // reverse step: 7 doubles per body
     int* types = nullptr;               // body types (+1 light, -1 dark), for histograms
     double timeOrigin = 0.0;            // st->previousForwardTime: barTime = step * dt - this
+    int mixGroupMax = 32, mixListCap = 64, mixBlocksPerSM = 0;   // mixed-walk tuning
     char* histScratch = nullptr;        // histogram / likelihood buffers
     size_t histScratchBytes = 0;
 };
@@ -384,8 +385,20 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
             NB_CHECK(cudaEventRecord(st->ev0, s));
             if (mixed) {
                 if (!st->mx.stacks) {
-                    st->mx.walkBlocks = nb_mixed_walk_blocks(st->numSMs);
-                    NB_CHECK(nb_alloc(&st->mx.stacks, nb_mixed_stack_ints(st->mx.walkBlocks)));
+                    // stacks for the largest persistent grid any list capacity allows
+                    int mxb = 0;
+                    for (int cap : {32, 64, 128})
+                        for (int gm : {32, 64})
+                            mxb = std::max(mxb, nb_mixed_walk_blocks(st->numSMs, cap, gm));
+                    NB_CHECK(nb_alloc(&st->mx.stacks, nb_mixed_stack_ints(mxb)));
+                }
+                {
+                    const int fit = nb_mixed_walk_blocks(st->numSMs, st->mixListCap,
+                                                         st->mixGroupMax) / st->numSMs;
+                    const int per = st->mixBlocksPerSM > 0 ? std::min(st->mixBlocksPerSM, fit) : fit;
+                    st->mx.walkBlocks = std::max(1, per) * st->numSMs;
+                    st->mx.groupMax = st->mixGroupMax;
+                    st->mx.listCap = st->mixListCap;
                 }
                 nb_launch_walk_mixed(b, st->mx, st->capNodes, wp, pot, st->counting != 0,
                                      st->numSMs, s);
@@ -1253,6 +1266,17 @@ NBodyCudaStatus nbGenerateDwarfCUDA(NBodyCudaState* st, const NBodyCudaPlummerDw
     return nb_generate(st, dwarf, 1, &first);
 }
 
+NBodyCudaStatus nbSetMixedTuningCUDA(NBodyCudaState* st, int groupMax, int listCap, int blocksPerSM)
+{
+    if (!st || groupMax < 1 || groupMax > 64 || (listCap != 32 && listCap != 64 && listCap != 128) ||
+        blocksPerSM < 0)
+        return NBODY_USER_ERROR;
+    st->mixGroupMax = groupMax;
+    st->mixListCap = listCap;
+    st->mixBlocksPerSM = blocksPerSM;
+    return NBODY_SUCCESS;
+}
+
 NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTime)
 {
     if (!st) return NBODY_USER_ERROR;
@@ -1332,11 +1356,12 @@ static NBodyCudaStatus nb_batch_mixed_buffers(NBodyCudaBatch* bt)
     NBodyCudaState* st = bt->st;
     if (!bt->maxWalkBlocks) {
         int mx = 0;
-        for (int cap : {32, 64, 128}) mx = std::max(mx, nb_mixed_walk_blocks(st->numSMs, cap));
+        for (int cap : {32, 64, 128})
+            for (int gm : {32, 64}) mx = std::max(mx, nb_mixed_walk_blocks(st->numSMs, cap, gm));
         bt->maxWalkBlocks = mx;
     }
     if (!st->mx.stacks) NB_CHECK(nb_alloc(&st->mx.stacks, nb_mixed_stack_ints(bt->maxWalkBlocks)));
-    const int fit = nb_mixed_walk_blocks(st->numSMs, bt->tune.listCap) / st->numSMs;
+    const int fit = nb_mixed_walk_blocks(st->numSMs, bt->tune.listCap, bt->tune.groupMax) / st->numSMs;
     const int per = bt->tune.blocksPerSM > 0 ? std::min(bt->tune.blocksPerSM, fit) : fit;
     st->mx.walkBlocks = std::max(1, per) * st->numSMs;
     st->mx.groupMax = bt->tune.groupMax;
@@ -1648,7 +1673,7 @@ NBodyCudaStatus nbBatchDwarfInfoCUDA(NBodyCudaBatch* bt, int* status, double* rs
 NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* bt, int groupMax, int listCap,
                                      int blocksPerSM)
 {
-    if (!bt || groupMax < 1 || groupMax > 32 || (listCap != 32 && listCap != 64 && listCap != 128) ||
+    if (!bt || groupMax < 1 || groupMax > 64 || (listCap != 32 && listCap != 64 && listCap != 128) ||
         blocksPerSM < 0)
         return NBODY_USER_ERROR;
     bt->tune.groupMax = groupMax;
@@ -1679,7 +1704,7 @@ NBodyCudaStatus nbBatchAutotuneCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt,
     NbBatchTuning best = bt->tune;
     double bestMs = -1.0;
     if (ctx->precision == NBCUDA_PRECISION_MIXED) {
-        for (int g : {16, 24, 32})
+        for (int g : {24, 32, 48, 64})
             for (int l : {32, 64, 128})
                 for (int b : {0, 3}) {
                     bt->tune.groupMax = g;

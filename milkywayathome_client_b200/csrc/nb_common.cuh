@@ -195,10 +195,10 @@ struct NbMixedBuffers {
     int* stacks;   // per resident warp: the group walk's depth-first stack
     int2* groups;  // walk groups: first sorted body, body count (<= 32)
     int walkBlocks;
-    int groupMax;  // bodies per walk group, 1..32 (0: 32)
+    int groupMax;  // bodies per walk group, 1..64 (0: 32; above 32, two bodies per lane)
     int listCap;   // interaction-list entries per warp: 32, 64 or 128 (0: 64)
 };
-int nb_mixed_walk_blocks(int numSMs, int listCap = 0);
+int nb_mixed_walk_blocks(int numSMs, int listCap = 0, int groupMax = 32);
 size_t nb_mixed_stack_ints(int blocks);
 
 // The walks (forest != nullptr: one tree per dwarf, see NbForest).

@@ -100,50 +100,59 @@ constexpr int NB_GROUP_STACK = 16384;     // >= 256 x 63 + 32
 template <int LIST_CAP> struct CellList { float4 a[LIST_CAP], b[LIST_CAP], c[LIST_CAP]; };
 template <int LIST_CAP> struct BodyList { float4 a[LIST_CAP]; };
 
-template <int LIST_CAP>
-__device__ __forceinline__ void nb_eval_bodies(const BodyList<LIST_CAP>& list, int n, float rbx, float rby,
-                                               float rbz, float eps2, float& fx, float& fy,
-                                               float& fz)
+// Evaluation of a full list by the 32 lanes, each for its BPL bodies (entries read once as
+// shared-memory broadcasts and used for every body of the lane).
+template <int LIST_CAP, int BPL>
+__device__ __forceinline__ void nb_eval_bodies(const BodyList<LIST_CAP>& list, int n,
+                                               const float (&rb)[BPL][3], float eps2,
+                                               float (&f)[BPL][3])
 {
     for (int e = 0; e < n; ++e) {
         const float4 a = list.a[e];
-        const float dx = a.x - rbx, dy = a.y - rby, dz = a.z - rbz;
-        const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-        const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
-        const float mor3 = a.w * rinv * rinv * rinv;
-        fx = fmaf(mor3, dx, fx);
-        fy = fmaf(mor3, dy, fy);
-        fz = fmaf(mor3, dz, fz);
+#pragma unroll
+        for (int q = 0; q < BPL; ++q) {
+            const float dx = a.x - rb[q][0], dy = a.y - rb[q][1], dz = a.z - rb[q][2];
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+            const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
+            const float mor3 = a.w * rinv * rinv * rinv;
+            f[q][0] = fmaf(mor3, dx, f[q][0]);
+            f[q][1] = fmaf(mor3, dy, f[q][1]);
+            f[q][2] = fmaf(mor3, dz, f[q][2]);
+        }
     }
 }
 
-template <int LIST_CAP>
-__device__ __forceinline__ void nb_eval_cells(const CellList<LIST_CAP>& list, int n, float rbx, float rby,
-                                              float rbz, float eps2, bool useQuad, float& fx,
-                                              float& fy, float& fz)
+template <int LIST_CAP, int BPL>
+__device__ __forceinline__ void nb_eval_cells(const CellList<LIST_CAP>& list, int n,
+                                              const float (&rb)[BPL][3], float eps2, bool useQuad,
+                                              float (&f)[BPL][3])
 {
     for (int e = 0; e < n; ++e) {
         const float4 a = list.a[e];
-        const float dx = a.x - rbx, dy = a.y - rby, dz = a.z - rbz;
-        const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-        const float rinv = rsqrtf(r2);
-        const float rinv2 = rinv * rinv;
-        const float mor3 = a.w * rinv * rinv2;
-        fx = fmaf(mor3, dx, fx);
-        fy = fmaf(mor3, dy, fy);
-        fz = fmaf(mor3, dz, fz);
-        if (useQuad) {
-            const float4 b = list.b[e], c = list.c[e];
-            const float qxx = b.x, qxy = b.y, qxz = b.z, qyy = b.w, qyz = c.x, qzz = c.y;
-            const float qdx = fmaf(qxz, dz, fmaf(qxy, dy, qxx * dx));
-            const float qdy = fmaf(qyz, dz, fmaf(qyy, dy, qxy * dx));
-            const float qdz = fmaf(qzz, dz, fmaf(qyz, dy, qxz * dx));
-            const float drQdr = fmaf(qdz, dz, fmaf(qdy, dy, qdx * dx));
-            const float dr5inv = rinv2 * rinv2 * rinv;
-            const float phiQ = 2.5f * dr5inv * drQdr * rinv2;
-            fx = fmaf(phiQ, dx, fmaf(-dr5inv, qdx, fx));
-            fy = fmaf(phiQ, dy, fmaf(-dr5inv, qdy, fy));
-            fz = fmaf(phiQ, dz, fmaf(-dr5inv, qdz, fz));
+        float4 b = make_float4(0.f, 0.f, 0.f, 0.f), c = b;
+        if (useQuad) { b = list.b[e]; c = list.c[e]; }
+#pragma unroll
+        for (int q = 0; q < BPL; ++q) {
+            const float dx = a.x - rb[q][0], dy = a.y - rb[q][1], dz = a.z - rb[q][2];
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+            const float rinv = rsqrtf(r2);
+            const float rinv2 = rinv * rinv;
+            const float mor3 = a.w * rinv * rinv2;
+            f[q][0] = fmaf(mor3, dx, f[q][0]);
+            f[q][1] = fmaf(mor3, dy, f[q][1]);
+            f[q][2] = fmaf(mor3, dz, f[q][2]);
+            if (useQuad) {
+                const float qxx = b.x, qxy = b.y, qxz = b.z, qyy = b.w, qyz = c.x, qzz = c.y;
+                const float qdx = fmaf(qxz, dz, fmaf(qxy, dy, qxx * dx));
+                const float qdy = fmaf(qyz, dz, fmaf(qyy, dy, qxy * dx));
+                const float qdz = fmaf(qzz, dz, fmaf(qyz, dy, qxz * dx));
+                const float drQdr = fmaf(qdz, dz, fmaf(qdy, dy, qdx * dx));
+                const float dr5inv = rinv2 * rinv2 * rinv;
+                const float phiQ = 2.5f * dr5inv * drQdr * rinv2;
+                f[q][0] = fmaf(phiQ, dx, fmaf(-dr5inv, qdx, f[q][0]));
+                f[q][1] = fmaf(phiQ, dy, fmaf(-dr5inv, qdy, f[q][1]));
+                f[q][2] = fmaf(phiQ, dz, fmaf(-dr5inv, qdz, f[q][2]));
+            }
         }
     }
 }
@@ -196,8 +205,9 @@ __global__ void k_groups(const int2* __restrict__ nodeLink, const int2* __restri
 }
 
 // FOREST: a group belongs to one dwarf; its warp walks that dwarf's tree from its root,
-// with the dwarf's softening and time step.
-template <bool COUNT, bool FOREST, int LIST_CAP>
+// with the dwarf's softening and time step.  BPL: bodies per lane (groups of up to 32 BPL
+// bodies; each lane walks for bodies lane and lane + 32).
+template <bool COUNT, bool FOREST, int LIST_CAP, int BPL>
 __global__ void __launch_bounds__(GROUP_THREADS)
 k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeLo,
              const float4* __restrict__ nodeQ32, const int4* __restrict__ child8,
@@ -205,9 +215,8 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
              const double* __restrict__ px, const double* __restrict__ py,
              const double* __restrict__ pz, const double* __restrict__ mass,
              double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
-             double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
              int* __restrict__ stacks, const int2* __restrict__ groups, NbWalkParams wp,
-             NbPot pot, NbScalars* __restrict__ sc, NbForest forest)
+             NbScalars* __restrict__ sc, NbForest forest)
 {
     __shared__ CellList<LIST_CAP> sCells[GROUP_WARPS];
     __shared__ BodyList<LIST_CAP> sBodies[GROUP_WARPS];
@@ -236,18 +245,27 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
             rootNode = dw.rootNode;
             root = nodePM[rootNode];
             eps2 = (float) dw.eps2;
-            wp.dtHalf = 0.5 * dw.dt;
         }
-        const int i = grp.x + lane;
-        const bool valid = lane < grp.y;
-        const unsigned j = valid ? order[i] : 0u;
-        const double x0 = valid ? px[j] : 0.0, y0 = valid ? py[j] : 0.0, z0 = valid ? pz[j] : 0.0;
-        float bhx, bhy, bhz, blx, bly, blz;
-        nb_split(x0 - root.x, bhx, blx);
-        nb_split(y0 - root.y, bhy, bly);
-        nb_split(z0 - root.z, bhz, blz);
-        float mnx = valid ? bhx + blx : inf, mny = valid ? bhy + bly : inf, mnz = valid ? bhz + blz : inf;
-        float mxx = valid ? bhx + blx : -inf, mxy = valid ? bhy + bly : -inf, mxz = valid ? bhz + blz : -inf;
+        bool valid[BPL];
+        unsigned jb[BPL];
+        float bh[BPL][3], bl[BPL][3];
+        float mnx = inf, mny = inf, mnz = inf, mxx = -inf, mxy = -inf, mxz = -inf;
+#pragma unroll
+        for (int q = 0; q < BPL; ++q) {
+            const int slot = lane + 32 * q;
+            valid[q] = slot < grp.y;
+            jb[q] = valid[q] ? order[grp.x + slot] : 0u;
+            const double x0 = valid[q] ? px[jb[q]] : 0.0, y0 = valid[q] ? py[jb[q]] : 0.0;
+            const double z0 = valid[q] ? pz[jb[q]] : 0.0;
+            nb_split(x0 - root.x, bh[q][0], bl[q][0]);
+            nb_split(y0 - root.y, bh[q][1], bl[q][1]);
+            nb_split(z0 - root.z, bh[q][2], bl[q][2]);
+            if (valid[q]) {
+                const float X = bh[q][0] + bl[q][0], Y = bh[q][1] + bl[q][1], Z = bh[q][2] + bl[q][2];
+                mnx = fminf(mnx, X); mny = fminf(mny, Y); mnz = fminf(mnz, Z);
+                mxx = fmaxf(mxx, X); mxy = fmaxf(mxy, Y); mxz = fmaxf(mxz, Z);
+            }
+        }
         for (int o = 16; o > 0; o >>= 1) {
             mnx = fminf(mnx, __shfl_xor_sync(NB_FULL_MASK, mnx, o));
             mny = fminf(mny, __shfl_xor_sync(NB_FULL_MASK, mny, o));
@@ -258,10 +276,17 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
         }
         const float cx = 0.5f * (mnx + mxx), cy = 0.5f * (mny + mxy), cz = 0.5f * (mnz + mxz);
         const float hx = 0.5f * (mxx - mnx), hy = 0.5f * (mxy - mny), hz = 0.5f * (mxz - mnz);
-        // the body relative to the group centre
-        const float rbx = (bhx - cx) + blx, rby = (bhy - cy) + bly, rbz = (bhz - cz) + blz;
-        double accx = 0.0, accy = 0.0, accz = 0.0;
-        float fx = 0.f, fy = 0.f, fz = 0.f;
+        // the bodies relative to the group centre
+        float rb[BPL][3], f[BPL][3];
+        double acc[BPL][3];
+#pragma unroll
+        for (int q = 0; q < BPL; ++q) {
+            rb[q][0] = (bh[q][0] - cx) + bl[q][0];
+            rb[q][1] = (bh[q][1] - cy) + bl[q][1];
+            rb[q][2] = (bh[q][2] - cz) + bl[q][2];
+            f[q][0] = f[q][1] = f[q][2] = 0.f;
+            acc[q][0] = acc[q][1] = acc[q][2] = 0.0;
+        }
         int nC = 0, nB = 0;
         if (lane == 0) stack[0] = rootNode;      // the (dwarf's) root
         int top = 1;
@@ -297,16 +322,20 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
                 cBC += 32ull * __popc(cellMask);
             }
             if (nB + __popc(bodyMask) > LIST_CAP) {
-                nb_eval_bodies(bodies, nB, rbx, rby, rbz, eps2, fx, fy, fz);
+                nb_eval_bodies<LIST_CAP, BPL>(bodies, nB, rb, eps2, f);
                 nB = 0;
                 __syncwarp();
             }
             if (nC + __popc(cellMask) > LIST_CAP) {
-                nb_eval_cells(cells, nC, rbx, rby, rbz, eps2, useQuad, fx, fy, fz);
+                nb_eval_cells<LIST_CAP, BPL>(cells, nC, rb, eps2, useQuad, f);
                 nC = 0;
                 __syncwarp();
-                accx += (double) fx; accy += (double) fy; accz += (double) fz;
-                fx = fy = fz = 0.f;
+#pragma unroll
+                for (int q = 0; q < BPL; ++q) {
+                    acc[q][0] += (double) f[q][0]; acc[q][1] += (double) f[q][1];
+                    acc[q][2] += (double) f[q][2];
+                    f[q][0] = f[q][1] = f[q][2] = 0.f;
+                }
             }
             const float4 rel = make_float4((hi.x - cx) + lo.x, (hi.y - cy) + lo.y,
                                            (hi.z - cz) + lo.z, lo.w);
@@ -343,14 +372,19 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
             __syncwarp();
         }
         __syncwarp();
-        nb_eval_bodies(bodies, nB, rbx, rby, rbz, eps2, fx, fy, fz);
-        nb_eval_cells(cells, nC, rbx, rby, rbz, eps2, useQuad, fx, fy, fz);
+        nb_eval_bodies<LIST_CAP, BPL>(bodies, nB, rb, eps2, f);
+        nb_eval_cells<LIST_CAP, BPL>(cells, nC, rb, eps2, useQuad, f);
         __syncwarp();
-        accx += (double) fx; accy += (double) fy; accz += (double) fz;
-        if (valid) {
+#pragma unroll
+        for (int q = 0; q < BPL; ++q) {
+            if (!valid[q]) continue;
+            const unsigned j = jb[q];
             // test particles are not in the tree and never meet themselves (nbody_grav.c:111-118)
             if (mass[j] == 0.0) atomicOr(&sc->incest, 1);
-            ax[j] = accx; ay[j] = accy; az[j] = accz;   // k_body_epilogue adds the rest
+            // self-gravity only; k_body_epilogue adds the rest
+            ax[j] = acc[q][0] + (double) f[q][0];
+            ay[j] = acc[q][1] + (double) f[q][1];
+            az[j] = acc[q][2] + (double) f[q][2];
         }
     }
     if (COUNT && lane == 0) {
@@ -361,25 +395,33 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
     }
 }
 
-template <bool COUNT, bool FOREST, int LC>
+template <bool COUNT, bool FOREST, int LC, int BPL>
 static void nb_walk_mixed_launch(const NbTreeBuffers& b, const NbMixedBuffers& m,
-                                 const NbWalkParams& wp, const NbPot& pot, int blocks,
-                                 const NbForest& f, cudaStream_t s)
+                                 const NbWalkParams& wp, int blocks, const NbForest& f,
+                                 cudaStream_t s)
 {
-    k_walk_mixed<COUNT, FOREST, LC><<<blocks, GROUP_THREADS, 0, s>>>(
+    k_walk_mixed<COUNT, FOREST, LC, BPL><<<blocks, GROUP_THREADS, 0, s>>>(
         m.hi, m.lo, m.q32, m.child8, b.nodePM, b.sort.idxA, b.px, b.py, b.pz, b.mass, b.ax, b.ay,
-        b.az, b.vx, b.vy, b.vz, m.stacks, m.groups, wp, pot, b.sc, f);
+        b.az, m.stacks, m.groups, wp, b.sc, f);
 }
 
 template <bool COUNT, bool FOREST>
 static void nb_walk_mixed_cap(const NbTreeBuffers& b, const NbMixedBuffers& m,
-                              const NbWalkParams& wp, const NbPot& pot, int blocks,
-                              const NbForest& f, cudaStream_t s)
+                              const NbWalkParams& wp, int blocks, const NbForest& f,
+                              cudaStream_t s)
 {
+    if (m.groupMax > 32) {                    // two bodies per lane
+        switch (m.listCap) {
+        case 32: nb_walk_mixed_launch<COUNT, FOREST, 32, 2>(b, m, wp, blocks, f, s); break;
+        case 128: nb_walk_mixed_launch<COUNT, FOREST, 128, 2>(b, m, wp, blocks, f, s); break;
+        default: nb_walk_mixed_launch<COUNT, FOREST, 64, 2>(b, m, wp, blocks, f, s); break;
+        }
+        return;
+    }
     switch (m.listCap) {
-    case 32: nb_walk_mixed_launch<COUNT, FOREST, 32>(b, m, wp, pot, blocks, f, s); break;
-    case 128: nb_walk_mixed_launch<COUNT, FOREST, 128>(b, m, wp, pot, blocks, f, s); break;
-    default: nb_walk_mixed_launch<COUNT, FOREST, 64>(b, m, wp, pot, blocks, f, s); break;
+    case 32: nb_walk_mixed_launch<COUNT, FOREST, 32, 1>(b, m, wp, blocks, f, s); break;
+    case 128: nb_walk_mixed_launch<COUNT, FOREST, 128, 1>(b, m, wp, blocks, f, s); break;
+    default: nb_walk_mixed_launch<COUNT, FOREST, 64, 1>(b, m, wp, blocks, f, s); break;
     }
 }
 
@@ -400,17 +442,17 @@ void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int c
     else
         k_pack_f32<false><<<g, 256, 0, s>>>(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, m.hi, m.lo,
                                             m.q32, m.child8, b.nodeRange, b.sc, f);
-    const int G = m.groupMax >= 1 && m.groupMax <= 32 ? m.groupMax : 32;
+    const int G = m.groupMax >= 1 && m.groupMax <= 64 ? m.groupMax : 32;
     k_groups<<<g, 256, 0, s>>>(b.nodeLink, b.nodeRange, m.groups, wp.n, b.sc, G, f);
     nb_count_launch(2);
     if (wp.n <= 0) return;
     const int blocks = m.walkBlocks;
     if (forest) {
-        if (count) nb_walk_mixed_cap<true, true>(b, m, wp, pot, blocks, f, s);
-        else nb_walk_mixed_cap<false, true>(b, m, wp, pot, blocks, f, s);
+        if (count) nb_walk_mixed_cap<true, true>(b, m, wp, blocks, f, s);
+        else nb_walk_mixed_cap<false, true>(b, m, wp, blocks, f, s);
     } else {
-        if (count) nb_walk_mixed_cap<true, false>(b, m, wp, pot, blocks, f, s);
-        else nb_walk_mixed_cap<false, false>(b, m, wp, pot, blocks, f, s);
+        if (count) nb_walk_mixed_cap<true, false>(b, m, wp, blocks, f, s);
+        else nb_walk_mixed_cap<false, false>(b, m, wp, blocks, f, s);
     }
     nb_count_launch();
     nb_launch_body_epilogue(b.px, b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
@@ -418,24 +460,29 @@ void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int c
 }
 
 // Persistent grid of the group walk: as many blocks as fit on the device at once (for the
-// given interaction-list capacity; 0 = the default of 64).
-int nb_mixed_walk_blocks(int numSMs, int listCap)
+// given interaction-list capacity, 0 = the default of 64, and group size).
+template <int LC, int BPL>
+static int nb_walk_per_sm()
 {
     int perSM = 0;
-    cudaError_t e;
-    if (listCap == 32)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_walk_mixed<false, false, 32>,
-                                                          GROUP_THREADS, 0);
-    else if (listCap == 128)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_walk_mixed<false, false, 128>,
-                                                          GROUP_THREADS, 0);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_walk_mixed<false, false, 64>,
-                                                          GROUP_THREADS, 0);
-    if (e != cudaSuccess || perSM < 1) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_walk_mixed<false, false, LC, BPL>,
+                                                      GROUP_THREADS, 0) != cudaSuccess ||
+        perSM < 1) {
         cudaGetLastError();
         perSM = 1;
     }
+    return perSM;
+}
+
+int nb_mixed_walk_blocks(int numSMs, int listCap, int groupMax)
+{
+    int perSM;
+    if (groupMax > 32)
+        perSM = listCap == 32 ? nb_walk_per_sm<32, 2>() : listCap == 128 ? nb_walk_per_sm<128, 2>()
+                                                                          : nb_walk_per_sm<64, 2>();
+    else
+        perSM = listCap == 32 ? nb_walk_per_sm<32, 1>() : listCap == 128 ? nb_walk_per_sm<128, 1>()
+                                                                          : nb_walk_per_sm<64, 1>();
     return perSM * numSMs;
 }
 

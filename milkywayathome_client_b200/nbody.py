@@ -287,6 +287,11 @@ class NBodyState:
             st.check("nbGravMap", st.gravMap(ctx))
         return st
 
+    def set_mixed_tuning(self, group_max=32, list_cap=64, blocks_per_sm=0):
+        """Mixed-precision walk tuning (nbSetMixedTuningCUDA)."""
+        self.check("nbSetMixedTuning", self.lib.nbSetMixedTuningCUDA(
+            self._h, int(group_max), int(list_cap), int(blocks_per_sm)))
+
     def set_time_origin(self, previous_forward_time):
         """The orbiting bar's time origin (the reference's st->previousForwardTime)."""
         self.check("nbSetTimeOrigin", self.lib.nbSetTimeOriginCUDA(self._h,

@@ -121,7 +121,7 @@ def test_autotune_picks_a_candidate_and_leaves_its_accelerations():
         bt.set_bodies(cat(0), cat(1), cat(2))
         bt.check("nbBatchGravMap", bt.gravMap(ctx))
         g, l, b, ms = bt.autotune(ctx)
-        assert g in (16, 24, 32) and l in (32, 64, 128) and b in (0, 3) and ms > 0
+        assert g in (24, 32, 48, 64) and l in (32, 64, 128) and b in (0, 3) and ms > 0
         assert bt.tuning() == (g, l, b)
         tuned = bt.accels()
         pos0, _ = bt.bodies()
