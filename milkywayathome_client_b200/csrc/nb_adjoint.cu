@@ -110,7 +110,8 @@ struct Vjp1 {
     double rx, ry, rz, m, q[6];
 };
 __device__ __forceinline__ Vjp1 nb_interaction_vjp(double dx, double dy, double dz, double m,
-                                                   const double* Q, bool quad, double eps2,
+                                                   double Q0, double Q1, double Q2, double Q3,
+                                                   double Q4, double Q5, bool quad, double eps2,
                                                    double abx, double aby, double abz)
 {
     Vjp1 o;
@@ -126,7 +127,7 @@ __device__ __forceinline__ Vjp1 nb_interaction_vjp(double dx, double dy, double 
     o.m = al * r3;
     for (int c = 0; c < 6; ++c) o.q[c] = 0.0;
     if (quad) {
-        const double qxx = Q[0], qxy = Q[1], qxz = Q[2], qyy = Q[3], qyz = Q[4], qzz = Q[5];
+        const double qxx = Q0, qxy = Q1, qxz = Q2, qyy = Q3, qyz = Q4, qzz = Q5;
         const double qdx = qxx * dx + qxy * dy + qxz * dz;
         const double qdy = qxy * dx + qyy * dy + qyz * dz;
         const double qdz = qxz * dx + qyz * dy + qzz * dz;
@@ -175,8 +176,7 @@ __device__ __forceinline__ double nb_warp_sum_transposed(double (&r)[V], int lan
 
 // Node adjoints: nodeBar[k*10 + 0..2] = CoM, [3] = mass, [4..9] = quadrupole.
 __global__ void __launch_bounds__(128, 5)
-k_walk_vjp(const double4* __restrict__ nodePM, const double* __restrict__ nodeCrit,
-           const int2* __restrict__ nodeLink, const double* __restrict__ nodeQuad,
+k_walk_vjp(const double4* __restrict__ rec,
            const unsigned int* __restrict__ order, const double* __restrict__ px,
            const double* __restrict__ py, const double* __restrict__ pz,
            const double* __restrict__ abar, double* __restrict__ xbar,
@@ -198,19 +198,24 @@ k_walk_vjp(const double4* __restrict__ nodePM, const double* __restrict__ nodeCr
         const int q = __reduce_min_sync(NB_FULL_MASK, ptr);
         if (q >= end) break;
         const bool active = ptr == q;
-        const double4 nd = nodePM[q];
-        const int2 link = nodeLink[q];
+        // the FP64 walk's packed record: {CoM, mass}, {rcrit2, links, Qxx, Qxy}, {Qxz .. Qzz}
+        const double4 nd = rec[3 * (size_t) q];
+        const double4 r1 = rec[3 * (size_t) q + 1];
+        const long long word = __double_as_longlong(r1.y);
+        const int2 link = make_int2((int) (unsigned) (word & 0xffffffffll), (int) (word >> 32));
         const bool isBody = link.y >= 0;
         bool inter = false;
         Vjp1 v;
         if (active) {
             const double dx = nd.x - x0, dy = nd.y - y0, dz = nd.z - z0;
             const double drSq = dz * dz + (dy * dy + dx * dx);
-            if (isBody || drSq >= nodeCrit[q]) {
+            if (isBody || drSq >= r1.x) {
                 ptr = link.x;
                 inter = !(isBody && (unsigned) link.y == j);
                 if (inter) {
-                    v = nb_interaction_vjp(dx, dy, dz, nd.w, nodeQuad + 6 * (size_t) q,
+                    double4 r2 = make_double4(0.0, 0.0, 0.0, 0.0);
+                    if (useQuad && !isBody) r2 = rec[3 * (size_t) q + 2];
+                    v = nb_interaction_vjp(dx, dy, dz, nd.w, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w,
                                            useQuad && !isBody, wp.eps2, abx, aby, abz);
                     gx -= v.rx; gy -= v.ry; gz -= v.rz;
                 }
@@ -346,11 +351,11 @@ k_direct_vjp(const double* __restrict__ px, const double* __restrict__ py,
             const double4 b = tp[t];
             const double4 ab = ta[t];
             // j as the walker, source b: r = x_b - x_j
-            const Vjp1 w = nb_interaction_vjp(b.x - xj, b.y - yj, b.z - zj, b.w, nullptr, false,
-                                              wp.eps2, abx, aby, abz);
+            const Vjp1 w = nb_interaction_vjp(b.x - xj, b.y - yj, b.z - zj, b.w, 0, 0, 0, 0, 0, 0,
+                                              false, wp.eps2, abx, aby, abz);
             // j as the source of walker b: r = x_j - x_b
-            const Vjp1 s = nb_interaction_vjp(xj - b.x, yj - b.y, zj - b.z, mj, nullptr, false,
-                                              wp.eps2, ab.x, ab.y, ab.z);
+            const Vjp1 s = nb_interaction_vjp(xj - b.x, yj - b.y, zj - b.z, mj, 0, 0, 0, 0, 0, 0,
+                                              false, wp.eps2, ab.x, ab.y, ab.z);
             gx += s.rx - w.rx; gy += s.ry - w.ry; gz += s.rz - w.rz;
             gm += s.m;
         }
@@ -380,9 +385,10 @@ void nb_launch_vjp(NbTreeBuffers& b, double* nodeBar, int capNodes, int maxDepth
     cudaMemsetAsync(nodeBar, 0, 10 * sizeof(double) * (size_t) capNodes, s);
     const int warps = (n + 31) / 32;
     cudaEventRecord(walkStart, s);
-    k_walk_vjp<<<(warps * 32 + 127) / 128, 128, 0, s>>>(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad,
-                                                        b.sort.idxA, b.px, b.py, b.pz, abar, xbar,
-                                                        nodeBar, wp, pot, b.sc);
+    // packed records from the (possibly restored) tree arrays
+    nb_launch_pack_walk(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.walkRec, capNodes, b.sc, s);
+    k_walk_vjp<<<(warps * 32 + 127) / 128, 128, 0, s>>>(b.walkRec, b.sort.idxA, b.px, b.py, b.pz,
+                                                        abar, xbar, nodeBar, wp, pot, b.sc);
     cudaEventRecord(walkEnd, s);
     const int g = min((capNodes + 255) / 256, numSMs * 16);
     for (int d = 0; d <= maxDepth; ++d)

@@ -201,6 +201,11 @@ struct NbMixedBuffers {
 int nb_mixed_walk_blocks(int numSMs, int listCap = 0, int groupMax = 32);
 size_t nb_mixed_stack_ints(int blocks);
 
+// The FP64 walks' packed node records (3 double4 per node) from the tree arrays.
+void nb_launch_pack_walk(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
+                         const double* nodeQuad, double4* rec, int capNodes, const NbScalars* sc,
+                         cudaStream_t s);
+
 // The walks (forest != nullptr: one tree per dwarf, see NbForest).
 void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
                          const double* nodeQuad, const unsigned* order, const double* px,

@@ -343,6 +343,15 @@ void nb_launch_body_epilogue(const double* px, const double* py, const double* p
                              const NbWalkParams& wp, const NbPot& pot, const NbScalars* sc,
                              int numSMs, cudaStream_t s, const NbForest* forest);
 
+void nb_launch_pack_walk(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
+                         const double* nodeQuad, double4* rec, int capNodes, const NbScalars* sc,
+                         cudaStream_t s)
+{
+    k_pack_walk<<<min((capNodes + 255) / 256, 4096), 256, 0, s>>>(nodePM, nodeCrit, nodeLink,
+                                                                  nodeQuad, rec, sc);
+    nb_count_launch();
+}
+
 void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
                          const double* nodeQuad, const unsigned* order, const double* px,
                          const double* py, const double* pz, double* ax, double* ay, double* az,
@@ -353,9 +362,7 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
     const int warps = (wp.n + 31) / 32;
     const int blocks = (warps * 32 + WALK_THREADS - 1) / WALK_THREADS;
     if (blocks <= 0) return;
-    k_pack_walk<<<min((capNodes + 255) / 256, 4096), 256, 0, s>>>(nodePM, nodeCrit, nodeLink,
-                                                                  nodeQuad, walkRec, sc);
-    nb_count_launch();
+    nb_launch_pack_walk(nodePM, nodeCrit, nodeLink, nodeQuad, walkRec, capNodes, sc, s);
     const NbForest f = forest ? *forest : NbForest{nullptr, nullptr, 0};
 #define NB_WALK_ARGS walkRec, order, px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc, f
     if (forest) {
