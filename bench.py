@@ -68,7 +68,7 @@ def parse_args():
                     help="steps of the energy-drift run of both forms (0: skip)")
     ap.add_argument("--theta2", type=float, default=1.0,
                     help="second opening angle measured for both forms (0: skip)")
-    ap.add_argument("--profile", choices=["fp64", "mixed", "adjoint"],
+    ap.add_argument("--profile", choices=["fp64", "mixed", "adjoint", "batch"],
                     help="profiling entry: build the dwarf, run two force evaluations, exit")
     return ap.parse_args()
 
@@ -616,6 +616,21 @@ def run_profile(args):
     """Small committed entry for ncu: the dwarf, one warm-up and one profiled gravMap (or, for
     --profile adjoint, one force evaluation followed by one force VJP at --adjoint-n bodies)."""
     from milkywayathome_client_b200 import models
+    if args.profile == "batch":
+        from milkywayathome_client_b200 import NBodyBatch, NBodyCtx, milky_way_potential
+        pot = milky_way_potential()
+        draws = models.dwarf_parameter_draws(args.batch_dwarfs, seed=args.batch_seed)
+        spec, structs = models.batched_dwarf_structs(draws, pot, seed=args.batch_seed * 1000,
+                                                     nsteps=args.batch_steps)
+        ctx = NBodyCtx(potential=pot, precision="mixed", timestep=spec[0][2], eps2=spec[0][1],
+                       theta=args.batch_theta)
+        with NBodyBatch(spec) as bt:
+            bt.generate(structs)
+            bt.check("nbBatchGravMap", bt.gravMap(ctx))
+            bt.check("nbBatchRunSteps", bt.run_steps(ctx, 2, graph=False))
+            print(json.dumps({"profile": "batch", "dwarfs": len(spec), "bodies": bt.nbody,
+                              "step_ms": bt.step_time_ms()}))
+        return 0
     if args.profile == "adjoint":
         import torch
         from milkywayathome_client_b200.adjoint import DeviceState
