@@ -325,6 +325,13 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
                 nb_eval_bodies<LIST_CAP, BPL>(bodies, nB, rb, eps2, f);
                 nB = 0;
                 __syncwarp();
+                // near-field terms are large and cancel: add every list's partial sum into FP64
+#pragma unroll
+                for (int q = 0; q < BPL; ++q) {
+                    acc[q][0] += (double) f[q][0]; acc[q][1] += (double) f[q][1];
+                    acc[q][2] += (double) f[q][2];
+                    f[q][0] = f[q][1] = f[q][2] = 0.f;
+                }
             }
             if (nC + __popc(cellMask) > LIST_CAP) {
                 nb_eval_cells<LIST_CAP, BPL>(cells, nC, rb, eps2, useQuad, f);
@@ -373,6 +380,12 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
         }
         __syncwarp();
         nb_eval_bodies<LIST_CAP, BPL>(bodies, nB, rb, eps2, f);
+#pragma unroll
+        for (int q = 0; q < BPL; ++q) {
+            acc[q][0] += (double) f[q][0]; acc[q][1] += (double) f[q][1];
+            acc[q][2] += (double) f[q][2];
+            f[q][0] = f[q][1] = f[q][2] = 0.f;
+        }
         nb_eval_cells<LIST_CAP, BPL>(cells, nC, rb, eps2, useQuad, f);
         __syncwarp();
 #pragma unroll
