@@ -2,8 +2,8 @@
 """Generate the golden fixtures of tests/golden/ from the reference tree (run once, here).
 
   * golden_likelihoods.json -- the reference's own golden end-to-end likelihoods for the
-    single-Plummer Orphan models 4 and 5 (nbody/tests/RunTestUnits.lua:105-156), which
-    tests/golden/orphan_dwarf.lua restates;
+    single-Plummer Orphan models 4 and 5 (nbody/tests/RunTestUnits.lua:105-156) and the
+    triaxial-halo model (model_triaxial, :313-338), which tests/golden/orphan_dwarf.lua restates;
   * orphan_model_histogram_3 -- the data histogram those tests match against
     (nbody/tests/orphan_models/orphan_model_histogram_3), copied verbatim (data).
 
@@ -34,7 +34,8 @@ def main():
     golden = {
         "source": "nbody/tests/RunTestUnits.lua (refResults), tolerance 1e-10",
         "tolerance": 1e-10,
-        "models": {"4": parse_results(text, "model_4"), "5": parse_results(text, "model_5")},
+        "models": {"4": parse_results(text, "model_4"), "5": parse_results(text, "model_5"),
+                   "triaxial": parse_results(text, "model_triaxial")},
     }
     with open(os.path.join(HERE, "golden_likelihoods.json"), "w") as f:
         json.dump(golden, f, indent=1, sort_keys=True)

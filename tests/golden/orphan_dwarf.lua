@@ -2,7 +2,10 @@
 -- likelihood tests (nbody/tests/orphan_models/model_4.lua and model_5.lua, driven by
 -- nbody/tests/RunTestUnits.lua), restated for this repository's golden checks.
 -- Arguments: nbody, variant ("4": Hernquist bulge, vhalo 114, r 28.9, v (-179,106,109);
---                             "5": Plummer bulge,   vhalo 73,  r 28.6, v (-156, 79,107)).
+--                             "5": Plummer bulge,   vhalo 73,  r 28.6, v (-156, 79,107);
+--                             "triaxial": Hernquist bulge, the triaxial halo of
+--                             nbody/tests/orphan_models/model_triaxial.lua, r 29.5,
+--                             v (-183,101,107)).
 -- The seed comes from the command line (argSeed), as in the reference tests.
 
 arg = {...}
@@ -20,9 +23,14 @@ dwarfMass = 16
 dwarfRadius = 0.2
 
 local bulgeIsPlummer = (variant == "5")
+local triaxial = (variant == "triaxial")
 local haloSpeed = bulgeIsPlummer and 73 or 114
 local orbitR = bulgeIsPlummer and 28.6 or 28.9
 local orbitV = bulgeIsPlummer and { -156, 79, 107 } or { -179, 106, 109 }
+if triaxial then
+   orbitR = 29.5
+   orbitV = { -183, 101, 107 }
+end
 
 function makePotential()
    local bulge
@@ -35,7 +43,10 @@ function makePotential()
       spherical = bulge,
       disk      = Disk.miyamotoNagai{ mass = 4.45865888E5, scaleLength = 6.5, scaleHeight = 0.26 },
       disk2     = Disk.none{ mass = 3.0e5 },
-      halo      = Halo.logarithmic{ vhalo = haloSpeed, scaleLength = 12, flattenZ = 1 }
+      halo      = triaxial
+                  and Halo.triaxial{ vhalo = 116, scaleLength = 16.3, flattenZ = 1.43,
+                                     flattenX = 1.26, flattenY = 1.0, triaxAngle = 96 }
+                  or Halo.logarithmic{ vhalo = haloSpeed, scaleLength = 12, flattenZ = 1 }
    }
 end
 

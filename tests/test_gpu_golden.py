@@ -4,7 +4,8 @@ The reference's own Lua set-up (oracle/_ref: nbSetup, its dSFMT Plummer sampler 
 orbit) builds the initial dwarf of tests/golden/orphan_dwarf.lua; all nStep kick-drift-kick
 steps then run in libnbody_b200.so; the final bodies go back to the reference for its
 histogram + EMD likelihood (nbCreateHistogram / nbSystemLikelihood).  The result must equal
-the reference's golden table (nbody/tests/RunTestUnits.lua) within its own tolerance, 1e-10:
+the reference's golden table (nbody/tests/RunTestUnits.lua, models 4, 5 and model_triaxial)
+within its own tolerance, 1e-10:
 thousands of chaotic N-body steps only reproduce it if every step is bit-exact.
 """
 import json
@@ -18,6 +19,10 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = [("5", "100", s) for s in ("670828913", "886885833", "715144259", "430281807", "543966758")]
 CASES += [("4", "100", s) for s in ("670828913", "886885833")]
 CASES += [("5", "1024", "886885833"), ("4", "1024", "670828913")]
+# The triaxial halo (model_triaxial): its force has no power, logarithm or trigonometric
+# function (c1..c3 come over from the reference's own set-up), so it is bit-exact too.
+CASES += [("triaxial", "100", s) for s in ("670828913", "886885833", "715144259")]
+CASES += [("triaxial", "1024", "670828913")]
 
 
 @pytest.mark.parametrize("variant,nbody,seed", CASES)
