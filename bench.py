@@ -320,8 +320,8 @@ def batched_run(args, dist, dev):
         bt.check("nbBatchRunSteps", rc)
         step_ms = bt.step_time_ms()
         status, rsize, _, nodes = bt.dwarf_info()
-        counts, totals, mpp = bt.histogram(hp)
-        data = data_from_counts(hp, counts[0], totals[0, 1], mpp[0])
+        counts, totals, mpp, comps = bt.histogram(hp, components=True)
+        data = data_from_counts(hp, counts[0], totals[0, 1], mpp[0], comps[0])
         lik = bt.likelihood(hp, data)
         # after the run: the same state stepped with and without the captured graph
         cmp_ms = {}
@@ -347,7 +347,8 @@ def batched_run(args, dist, dev):
                    "walk_ms": tune[3]},
         "statuses_nonzero": int(np.count_nonzero(status)),
         "likelihood": {"target": "final histogram of a seeded reference parameter set (50 x 1 "
-                                 "Lambda bins over [-150, 150] deg)",
+                                 "Lambda bins over [-150, 150] deg, counts and beta "
+                                 "dispersions; EMD + cost + beta-dispersion terms)",
                        "min": float(np.nanmin(lk)), "median": float(np.nanmedian(lk)),
                        "finite": int(np.isfinite(lk).sum()),
                        "reference_self": float(lik[0, 0])},

@@ -209,20 +209,36 @@ NBodyCudaStatus nbStepAdjointCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, c
  * for the context's potential (0 with EXTERNAL_POTENTIAL_NONE).  Host array of 3 doubles. */
 NBodyCudaStatus nbEnergyCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, double* energy);
 
-/* ---- Lambda-Beta histogram and EMD/cost likelihood on the GPU ----
- * The normalised-counts histogram of nbCreateHistogram (nbody/src/nbody_histogram.c:671-1139)
- * and the EMD + cost components of nbSystemLikelihood (nbody/src/nbody_likelihood.c:155-324,
- * nbMatchEMD nbody/src/nbody_emd.c:1278-1427, nbCostComponent nbody/src/nbody_mass.c:318-391)
- * computed from the device-resident bodies, without copying them to the host.  Bodies of type
- * +1 are light (they count towards totalSimulated and set massPerParticle), bodies of type < 0
- * are ignored.  The likelihood supports one beta bin and the default EMD range (the whole
- * histogram), as the reference's two-component runs use. */
+/* ---- Lambda-Beta histograms and the likelihood on the GPU ----
+ * nbCreateHistogram (nbody/src/nbody_histogram.c:671-1139) and nbSystemLikelihood
+ * (nbody/src/nbody_likelihood.c:155-324) from the device-resident bodies, without copying them
+ * to the host: the normalised counts; the beta and line-of-sight velocity dispersions and, when
+ * a comparison needs them, the averages of the line-of-sight velocity, beta, distance and the
+ * proper motions, each with IterMax passes of sigma-clipping outlier rejection (nbCalcDisp,
+ * nbRemoveOutliers, nbody/src/nbody_mass.c:190-316); the EMD and cost components and the
+ * comparisons (nbLikelihood, nbody_mass.c:395-469) the flags enable.  Bodies of type +1 are
+ * light (they count towards totalSimulated and set massPerParticle), bodies of type < 0 are
+ * ignored.  The likelihood supports one beta bin and the default EMD range (the whole
+ * histogram), as the reference's runs use.  The dispersions' sums are formed in a fixed order
+ * on the device (deterministic); they may differ from the reference's body-order sums by
+ * rounding. */
+#define NBODY_CUDA_HIST_COMPONENTS 7   /* histograms 1..7 of the reference's MainStruct */
+#define NBODY_CUDA_LIKELIHOOD_TERMS 11
 typedef struct {
     double phi, theta, psi;            /* Euler angles of the stream frame, degrees */
     double lambdaStart, lambdaEnd;
     double betaStart, betaEnd;
     int lambdaBins, betaBins;
     double sunGCDist;
+    /* the comparisons nbSystemLikelihood adds (NBodyCtx fields of the reference; its defaults:
+     * useBetaDisp 1, the others 0) */
+    int useBetaDisp, useVelDisp, useBetaComp, useVlos, useDist, usePropMot;
+    int iterMax;                       /* outlier-rejection passes (IterMax; default 6) */
+    int reserved;
+    double betaSigma, velSigma, distSigma, pmSigma;          /* cut-offs (default 2.5) */
+    double betaCorrect, velCorrect, distCorrect, pmCorrect;  /* dispersion corrections (1.111) */
+    double sunVelx, sunVely, sunVelz;  /* km/s (default 10.3, 229.2, 6.9) */
+    double NGPdec, NGPra, lNCP;        /* radians (default d2r(27.4), d2r(192), d2r(123)) */
 } NBodyCudaHistogramParams;
 typedef struct {                       /* a data histogram as nbReadHistogram reads it */
     int nBins;                         /* lambdaBins * betaBins */
@@ -232,7 +248,56 @@ typedef struct {                       /* a data histogram as nbReadHistogram re
     const double* lambda;              /* bin centres */
     const double* variable;            /* normalised counts */
     const double* err;                 /* count errors */
+    int betaDispBins;                  /* "betaDispBins =" (0 when absent) */
+    int reserved;
+    /* histograms 1..7: beta dispersion, line-of-sight velocity dispersion, line-of-sight
+     * velocity, beta, distance, dec and RA proper motion: values and errors of nBins entries
+     * each, NULL where the file holds none */
+    const double* compVariable[NBODY_CUDA_HIST_COMPONENTS];
+    const double* compErr[NBODY_CUDA_HIST_COMPONENTS];
 } NBodyCudaDataHistogram;
+/* ---- nbRunSystem: the run loop with the best-likelihood scan and the bar's calibration ----
+ * The forward evolution of nbody/src/nbody.c:420-520 around nbRunSystemPlain
+ * (nbody/src/nbody_plain.c:365-470) and get_likelihood (:100-237), on the device:
+ *   - the bar's time origin starts at timeEvolve / (2 - s') with useBestLike (s' =
+ *     2 BestLikeStart / (BestLikeStart + 1), the window start before the Lua's rescaling),
+ *     else at timeEvolve;
+ *   - each run: nbGravMap, then steps up to nStep; after a step with step / nStep >=
+ *     BestLikeStart (with useBestLike) the likelihood against data is evaluated on the device
+ *     and kept when its magnitude beats the best so far (NaN or beyond the worst case counts
+ *     as the worst case, 0 as the best case), with its time step / nStep * timeEvolve;
+ *   - with an orbiting bar, calibrationRuns more runs from the same initial state, each with
+ *     the previous run's best time as the bar's time origin;
+ *   - the result is the final state's likelihood, or the best one when the final one is worse
+ *     (nbody.c:320-345).
+ * The state must start at the run's first step (as nbody.c's initial state); it ends at
+ * nStep.  With data NULL no likelihood is evaluated (the runs are the bare loop).  One host
+ * synchronisation per step (the tree-build status), none for the scan. */
+typedef struct {
+    int nStep;                  /* ctx->nStep */
+    int useBestLike;            /* ctx->useBestLike */
+    double timeEvolve;          /* ctx->timeEvolve */
+    double bestLikeStart;       /* ctx->BestLikeStart (as the context holds it) */
+    int calibrationRuns;        /* ctx->calibrationRuns (used with an orbiting bar only) */
+    int keepBestBodies;         /* keep the bodies of the best likelihood (nbGetBestBodiesCUDA) */
+} NBodyCudaRunParams;
+typedef struct {
+    double result[NBODY_CUDA_LIKELIHOOD_TERMS];  /* the likelihood the reference reports */
+    double final[NBODY_CUDA_LIKELIHOOD_TERMS];   /* the final state's (likelihood clamped) */
+    double best[NBODY_CUDA_LIKELIHOOD_TERMS];    /* st->bestLikelihood* of the last run */
+    double bestTime;                             /* st->bestLikelihood_time (0: none) */
+    double previousForwardTime;                  /* the bar's time origin of the last run */
+    int bestStep, bestCount;                     /* step of the best, improvements counted */
+    int runs;                                    /* forward runs made */
+    int reserved;
+} NBodyCudaRunResult;
+NBodyCudaStatus nbRunSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st,
+                                const NBodyCudaRunParams* rp, const NBodyCudaHistogramParams* hp,
+                                const NBodyCudaDataHistogram* data, NBodyCudaRunResult* res);
+/* the bodies at the best likelihood of the last nbRunSystemCUDA with keepBestBodies (the
+ * reference's bestLikelihoodBodyTab, nbody/src/nbody_plain.c:226-231), host arrays of 3n */
+NBodyCudaStatus nbGetBestBodiesCUDA(NBodyCudaState* st, double* pos, double* vel);
+
 /* The bar's time origin, the reference's st->previousForwardTime (nbody/src/nbody.c:440-442):
  * the orbiting bar is evaluated at step * timestep - previousForwardTime (0 by default).
  * For a batch, set it on the batch's state through nbBatchSetTimeOriginCUDA. */
@@ -245,11 +310,17 @@ NBodyCudaStatus nbSetMixedTuningCUDA(NBodyCudaState* st, int groupMax, int listC
 /* host array of nbody types (+1 light, -1 dark) */
 NBodyCudaStatus nbSetTypesCUDA(NBodyCudaState* st, const int* types);
 /* host outputs, any may be NULL: counts[nBins], totals[2] = {in range, light bodies},
- * massPerParticle[1] */
+ * massPerParticle[1], comps[NBODY_CUDA_HIST_COMPONENTS][2][nBins] = histograms 1..7 as
+ * {values, errors} (1 and 2 always; 3..7 when useVlos, useBetaComp, useDist or usePropMot is
+ * set, as the reference builds them; zeros otherwise) */
 NBodyCudaStatus nbHistogramCUDA(NBodyCudaState* st, const NBodyCudaHistogramParams* hp,
                                 unsigned int* counts, unsigned int* totals,
-                                double* massPerParticle);
-/* out[4] = {EMD component + cost component, EMD, EMD component, cost component} */
+                                double* massPerParticle, double* comps);
+/* out[NBODY_CUDA_LIKELIHOOD_TERMS]: the reference's likelihood array (likelihood, EMD
+ * component, cost component, beta dispersion, velocity dispersion, beta average,
+ * line-of-sight velocity, distance, dec and RA proper motion; NaN where not compared; all NaN
+ * when a comparison's data histogram is missing), then the EMD itself.  Positive; lower is
+ * better. */
 NBodyCudaStatus nbLikelihoodCUDA(NBodyCudaState* st, const NBodyCudaHistogramParams* hp,
                                  const NBodyCudaDataHistogram* data, double* out);
 
@@ -329,9 +400,11 @@ NBodyCudaStatus nbBatchAutotuneCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bat
  * counts[ndwarfs * nBins], totals[2 * ndwarfs], massPerParticle[ndwarfs], out[4 * ndwarfs] */
 NBodyCudaStatus nbBatchSetTypesCUDA(NBodyCudaBatch* batch, const int* types);
 NBodyCudaStatus nbBatchSetTimeOriginCUDA(NBodyCudaBatch* batch, double previousForwardTime);
+/* as nbHistogramCUDA / nbLikelihoodCUDA, per dwarf: counts[ndwarfs][nBins], totals[ndwarfs][2],
+ * massPerParticle[ndwarfs], comps[ndwarfs][7][2][nBins], out[ndwarfs][11] */
 NBodyCudaStatus nbBatchHistogramCUDA(NBodyCudaBatch* batch, const NBodyCudaHistogramParams* hp,
                                      unsigned int* counts, unsigned int* totals,
-                                     double* massPerParticle);
+                                     double* massPerParticle, double* comps);
 NBodyCudaStatus nbBatchLikelihoodCUDA(NBodyCudaBatch* batch, const NBodyCudaHistogramParams* hp,
                                       const NBodyCudaDataHistogram* data, double* out);
 /* initial conditions of every dwarf of the batch in one launch per phase (one

@@ -9,10 +9,11 @@ formulas and a synthetic dwarf sampler.
 from .nbody import (Disk, Halo, NBodyBatch, NBodyCtx, NBodyError, NBodyState, Potential,
                     Spherical, ext_acceleration, kernel_launches, milky_way_potential)
 from ._lib import status_is_fatal, status_names
-from .histogram import DataHistogram, HistogramParams, data_from_counts, read_histogram
+from .histogram import (DataHistogram, HistogramParams, data_from_counts, read_histogram,
+                        write_histogram)
 
 __all__ = ["Disk", "Halo", "NBodyBatch", "NBodyCtx", "NBodyError", "NBodyState", "Potential",
            "Spherical",
            "ext_acceleration", "kernel_launches", "milky_way_potential", "status_is_fatal",
-           "status_names", "DataHistogram", "HistogramParams", "data_from_counts",
+           "status_names", "DataHistogram", "HistogramParams", "data_from_counts", "write_histogram",
            "read_histogram"]

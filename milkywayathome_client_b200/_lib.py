@@ -93,12 +93,27 @@ class PlummerDwarf(ctypes.Structure):
                 ("seed", ctypes.c_uint64)]
 
 
+HIST_COMPONENTS = 7       # NBODY_CUDA_HIST_COMPONENTS
+LIKELIHOOD_TERMS = 11     # NBODY_CUDA_LIKELIHOOD_TERMS
+
+
 class HistParams(ctypes.Structure):
     _fields_ = [("phi", ctypes.c_double), ("theta", ctypes.c_double), ("psi", ctypes.c_double),
                 ("lambdaStart", ctypes.c_double), ("lambdaEnd", ctypes.c_double),
                 ("betaStart", ctypes.c_double), ("betaEnd", ctypes.c_double),
                 ("lambdaBins", ctypes.c_int), ("betaBins", ctypes.c_int),
-                ("sunGCDist", ctypes.c_double)]
+                ("sunGCDist", ctypes.c_double),
+                ("useBetaDisp", ctypes.c_int), ("useVelDisp", ctypes.c_int),
+                ("useBetaComp", ctypes.c_int), ("useVlos", ctypes.c_int),
+                ("useDist", ctypes.c_int), ("usePropMot", ctypes.c_int),
+                ("iterMax", ctypes.c_int), ("reserved", ctypes.c_int),
+                ("betaSigma", ctypes.c_double), ("velSigma", ctypes.c_double),
+                ("distSigma", ctypes.c_double), ("pmSigma", ctypes.c_double),
+                ("betaCorrect", ctypes.c_double), ("velCorrect", ctypes.c_double),
+                ("distCorrect", ctypes.c_double), ("pmCorrect", ctypes.c_double),
+                ("sunVelx", ctypes.c_double), ("sunVely", ctypes.c_double),
+                ("sunVelz", ctypes.c_double), ("NGPdec", ctypes.c_double),
+                ("NGPra", ctypes.c_double), ("lNCP", ctypes.c_double)]
 
 
 class DataHist(ctypes.Structure):
@@ -107,7 +122,25 @@ class DataHist(ctypes.Structure):
                 ("useBin", ctypes.POINTER(ctypes.c_int)),
                 ("lambda_", ctypes.POINTER(ctypes.c_double)),
                 ("variable", ctypes.POINTER(ctypes.c_double)),
-                ("err", ctypes.POINTER(ctypes.c_double))]
+                ("err", ctypes.POINTER(ctypes.c_double)),
+                ("betaDispBins", ctypes.c_int), ("reserved", ctypes.c_int),
+                ("compVariable", ctypes.POINTER(ctypes.c_double) * HIST_COMPONENTS),
+                ("compErr", ctypes.POINTER(ctypes.c_double) * HIST_COMPONENTS)]
+
+
+class RunParams(ctypes.Structure):
+    _fields_ = [("nStep", ctypes.c_int), ("useBestLike", ctypes.c_int),
+                ("timeEvolve", ctypes.c_double), ("bestLikeStart", ctypes.c_double),
+                ("calibrationRuns", ctypes.c_int), ("keepBestBodies", ctypes.c_int)]
+
+
+class RunResult(ctypes.Structure):
+    _fields_ = [("result", ctypes.c_double * LIKELIHOOD_TERMS),
+                ("final", ctypes.c_double * LIKELIHOOD_TERMS),
+                ("best", ctypes.c_double * LIKELIHOOD_TERMS),
+                ("bestTime", ctypes.c_double), ("previousForwardTime", ctypes.c_double),
+                ("bestStep", ctypes.c_int), ("bestCount", ctypes.c_int),
+                ("runs", ctypes.c_int), ("reserved", ctypes.c_int)]
 
 
 class Ctx(ctypes.Structure):
@@ -168,13 +201,17 @@ SIGNATURES = [
     ("nbBatchSetTimeOriginCUDA", ctypes.c_int, [_vp, ctypes.c_double]),
     ("nbGenerateDwarfCUDA", ctypes.c_int, [_vp, ctypes.POINTER(PlummerDwarf), ctypes.c_double]),
     ("nbBatchGenerateDwarfsCUDA", ctypes.c_int, [_vp, ctypes.POINTER(PlummerDwarf)]),
-    ("nbHistogramCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), _vp, _vp, _vp]),
+    ("nbHistogramCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), _vp, _vp, _vp, _vp]),
     ("nbLikelihoodCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), ctypes.POINTER(DataHist),
                                         _vp]),
     ("nbBatchSetTypesCUDA", ctypes.c_int, [_vp, _vp]),
-    ("nbBatchHistogramCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), _vp, _vp, _vp]),
+    ("nbBatchHistogramCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), _vp, _vp, _vp, _vp]),
     ("nbBatchLikelihoodCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams),
                                              ctypes.POINTER(DataHist), _vp]),
+    ("nbRunSystemCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, ctypes.POINTER(RunParams),
+                                       ctypes.POINTER(HistParams), ctypes.POINTER(DataHist),
+                                       ctypes.POINTER(RunResult)]),
+    ("nbGetBestBodiesCUDA", ctypes.c_int, [_vp, _vp, _vp]),
     ("nbSaveStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbRestoreStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbReleaseStatesCUDA", ctypes.c_int, [_vp]),

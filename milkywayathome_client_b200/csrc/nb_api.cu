@@ -157,6 +157,11 @@ struct NBodyCudaState {
     int mixGroupMax = 32, mixListCap = 64, mixBlocksPerSM = 0;   // mixed-walk tuning
     char* histScratch = nullptr;        // histogram / likelihood buffers
     size_t histScratchBytes = 0;
+    NbSlot runStart;                    // nbRunSystemCUDA: the initial state of the runs
+    NbBestDev* best = nullptr;          // nbRunSystemCUDA: device best-likelihood record
+    double* keepPos = nullptr;          // bodies at the best likelihood (3n each)
+    double* keepVel = nullptr;
+    int haveKeep = 0;
 };
 
 template <typename T>
@@ -259,6 +264,13 @@ static void nb_free_all(NBodyCudaState* st)
     st->types = nullptr;
     cudaFree(st->histScratch);
     st->histScratch = nullptr;
+    cudaFree(st->runStart.mem);
+    st->runStart = NbSlot{};
+    cudaFree(st->best);
+    st->best = nullptr;
+    cudaFree(st->keepPos);
+    cudaFree(st->keepVel);
+    st->keepPos = st->keepVel = nullptr;
     if (st->scHost) cudaFreeHost(st->scHost);
     if (st->ev0) cudaEventDestroy(st->ev0);
     if (st->ev1) cudaEventDestroy(st->ev1);
@@ -880,12 +892,9 @@ NBodyCudaStatus nbGravVJPCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st, const
 
 static size_t nb_align256(size_t x) { return (x + 255) & ~(size_t) 255; }
 
-NBodyCudaStatus nbSaveStateCUDA(NBodyCudaState* st, int slot)
+static NBodyCudaStatus nb_save_slot(NBodyCudaState* st, NbSlot& sl)
 {
-    if (!st || slot < 0 || slot >= (1 << 16)) return NBODY_USER_ERROR;
     NB_CHECK(cudaSetDevice(st->device));
-    if ((int) st->slots.size() <= slot) st->slots.resize(slot + 1);
-    NbSlot& sl = st->slots[slot];
     const size_t n = (size_t) st->nbody;
     const size_t nodes = st->haveTree ? (size_t) st->scHost->nNodes : 0;
     auto bytesFor = [n](size_t nn) {
@@ -938,14 +947,16 @@ NBodyCudaStatus nbSaveStateCUDA(NBodyCudaState* st, int slot)
     return NBODY_SUCCESS;
 }
 
-NBodyCudaStatus nbRestoreStateCUDA(NBodyCudaState* st, int slot)
+NBodyCudaStatus nbSaveStateCUDA(NBodyCudaState* st, int slot)
 {
-    if (!st || slot < 0 || slot >= (int) st->slots.size() || !st->slots[slot].valid) {
-        g_lastError = "nbRestoreStateCUDA: no state saved in this slot";
-        return NBODY_USER_ERROR;
-    }
+    if (!st || slot < 0 || slot >= (1 << 16)) return NBODY_USER_ERROR;
+    if ((int) st->slots.size() <= slot) st->slots.resize(slot + 1);
+    return nb_save_slot(st, st->slots[slot]);
+}
+
+static NBodyCudaStatus nb_restore_slot(NBodyCudaState* st, NbSlot& sl)
+{
     NB_CHECK(cudaSetDevice(st->device));
-    NbSlot& sl = st->slots[slot];
     const size_t n = (size_t) st->nbody;
     const size_t nodes = sl.haveTree ? (size_t) sl.sc.nNodes : 0;
     if (sl.haveTree && st->capNodes < sl.sc.nNodes) {
@@ -976,6 +987,15 @@ NBodyCudaStatus nbRestoreStateCUDA(NBodyCudaState* st, int slot)
     st->step = sl.step;
     st->treeIncest = sl.treeIncest;
     return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbRestoreStateCUDA(NBodyCudaState* st, int slot)
+{
+    if (!st || slot < 0 || slot >= (int) st->slots.size() || !st->slots[slot].valid) {
+        g_lastError = "nbRestoreStateCUDA: no state saved in this slot";
+        return NBODY_USER_ERROR;
+    }
+    return nb_restore_slot(st, st->slots[slot]);
 }
 
 NBodyCudaStatus nbReleaseStatesCUDA(NBodyCudaState* st)
@@ -1087,7 +1107,7 @@ const char* nbLastErrorCUDA(void) { return g_lastError.c_str(); }
 }  // extern "C"
 
 // =============================================================================================
-// Histograms and likelihoods (kernels in nb_batch.cu)
+// Histograms and likelihoods (kernels in nb_likelihood.cu)
 // =============================================================================================
 static NbHistDev nb_hist_dev(const NBodyCudaHistogramParams* hp)
 {
@@ -1113,28 +1133,62 @@ static NbHistDev nb_hist_dev(const NBodyCudaHistogramParams* hp)
     h.betaSize = (hp->betaEnd - hp->betaStart) / (double) hp->betaBins;
     h.lambdaBins = hp->lambdaBins;
     h.betaBins = hp->betaBins;
+    // cartesianalign (nbody/src/nbody_coordinates.c:192-224)
+    const double cl = cos(M_PI - hp->lNCP), sl = sin(M_PI - hp->lNCP);
+    const double cd = cos(M_PI_2 - hp->NGPdec), sd = sin(M_PI_2 - hp->NGPdec);
+    const double ca = cos(hp->NGPra), sa = sin(hp->NGPra);
+    h.align[0] = ca * cd * cl - sa * sl;
+    h.align[1] = -ca * cd * sl - sa * cl;
+    h.align[2] = ca * sd;
+    h.align[3] = sa * cd * cl + ca * sl;
+    h.align[4] = -sa * cd * sl + ca * cl;
+    h.align[5] = sa * sd;
+    h.align[6] = -sd * cl;
+    h.align[7] = sd * sl;
+    h.align[8] = cd;
+    h.sunVel[0] = hp->sunVelx;
+    h.sunVel[1] = hp->sunVely;
+    h.sunVel[2] = hp->sunVelz;
     return h;
 }
 
 static size_t nb_al(size_t x) { return (x + 255) & ~(size_t) 255; }
 
-// Histograms of nDwarfs dwarfs (bodyDwarf NULL: the whole state is one dwarf) and, with a
-// data histogram, their likelihoods.  Host outputs, any may be NULL: counts (nDwarfs x nBins),
-// totals (2 per dwarf: bodies in range, light bodies), massPer (per dwarf), out (4 per dwarf).
-static NBodyCudaStatus nb_hist_run(NBodyCudaState* st, const int* bodyDwarf, int nDwarfs,
-                                   const int* nbodyOfHost, const NBodyCudaHistogramParams* hp,
-                                   const NBodyCudaDataHistogram* data, unsigned* counts,
-                                   unsigned* totals, double* massPer, double* out)
+static NbLikeFlags nb_like_flags(const NBodyCudaHistogramParams* hp)
+{
+    return NbLikeFlags{hp->useBetaDisp != 0, hp->useVelDisp != 0, hp->useBetaComp != 0,
+                       hp->useVlos != 0, hp->useDist != 0, hp->usePropMot != 0};
+}
+
+// Device buffers of one histogram evaluation, carved from the state's scratch block.
+struct NbHistRun {
+    NbHistPlan p{};
+    NbDataHistDev dh{};
+    NbLikeFlags f{};
+    int* nbodyOf = nullptr;     // device, per dwarf
+    double* out = nullptr;      // device, NB_LIKELIHOOD_TERMS per dwarf
+    double* comps = nullptr;    // device, 7 x 2 x B per dwarf
+};
+
+// Plans the histograms of the dwarfs with nbodyOf[d] consecutive bodies each (one dwarf: the
+// whole state) for the likelihood against data (data != NULL: the histograms its comparisons
+// use) or for export (every histogram the reference builds).  Uploads the chunk table, the
+// dwarf sizes and the data histogram on the state's stream.
+static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int>& nbodyOf,
+                                       const NBodyCudaHistogramParams* hp,
+                                       const NBodyCudaDataHistogram* data, bool exportAll,
+                                       NbHistRun& r)
 {
     if (!hp || hp->lambdaBins < 1 || hp->betaBins < 1 || !(hp->lambdaEnd > hp->lambdaStart) ||
-        !(hp->betaEnd > hp->betaStart)) {
+        !(hp->betaEnd > hp->betaStart) || hp->iterMax < 0 || hp->iterMax > 1000) {
         g_lastError = "invalid histogram parameters";
         return NBODY_USER_ERROR;
     }
     if (!st->types) { g_lastError = "body types not set"; return NBODY_USER_ERROR; }
-    const int nBins = hp->lambdaBins * hp->betaBins;
+    const int B = hp->lambdaBins * hp->betaBins;
+    const NbLikeFlags f = nb_like_flags(hp);
     if (data) {
-        if (data->nBins != nBins || !data->useBin || !data->lambda || !data->variable || !data->err) {
+        if (data->nBins != B || !data->useBin || !data->lambda || !data->variable || !data->err) {
             g_lastError = "data histogram does not match the histogram parameters";
             return NBODY_USER_ERROR;
         }
@@ -1142,11 +1196,81 @@ static NBodyCudaStatus nb_hist_run(NBodyCudaState* st, const int* bodyDwarf, int
             g_lastError = "the likelihood is implemented for one beta bin";
             return NBODY_UNSUPPORTED;
         }
+        if ((f.betaDisp && (!data->compVariable[0] || !data->compErr[0])) ||
+            (f.velDisp && (!data->compVariable[1] || !data->compErr[1]))) {
+            g_lastError = "the data histogram has no dispersion columns for an enabled comparison";
+            return NBODY_USER_ERROR;
+        }
+        for (int k = 2; k < NB_HIST_COMPONENTS; ++k)
+            if (!data->compVariable[k] != !data->compErr[k]) {
+                g_lastError = "data histogram: a component has values without errors or errors "
+                              "without values";
+                return NBODY_USER_ERROR;
+            }
     }
+    // histograms 1..7 to build and the quantity each bins
+    static const int kQuantity[NB_HIST_COMPONENTS] = {NB_Q_BETA, NB_Q_VLOS, NB_Q_VLOS, NB_Q_BETA,
+                                                      NB_Q_DIST, NB_Q_MUDEC, NB_Q_MURA};
+    bool built[NB_HIST_COMPONENTS] = {};
+    if (exportAll) {
+        const bool avgs = f.vlos || f.betaComp || f.dist || f.propMot;
+        for (int k = 0; k < NB_HIST_COMPONENTS; ++k) built[k] = k < 2 || avgs;
+    } else if (data) {
+        built[0] = f.betaDisp; built[1] = f.velDisp; built[2] = f.vlos; built[3] = f.betaComp;
+        built[4] = f.dist; built[5] = built[6] = f.propMot;
+    }
+    NbHistPlan& p = r.p;
+    p = NbHistPlan{};
+    p.h = nb_hist_dev(hp);
+    int slotOf[NB_NQ];
+    for (int q = 0; q < NB_NQ; ++q) slotOf[q] = -1;
+    for (int k = 0; k < NB_HIST_COMPONENTS; ++k) {
+        p.histSlot[k] = -1;
+        if (!built[k]) continue;
+        const int q = kQuantity[k];
+        if (slotOf[q] < 0) {
+            slotOf[q] = p.h.nq;
+            p.h.q[p.h.nq++] = q;
+        }
+        p.histSlot[k] = slotOf[q];
+    }
+    for (int k = 0; k < p.h.nq; ++k) {
+        switch (p.h.q[k]) {
+        case NB_Q_BETA: p.cut[k] = hp->betaSigma; p.corr[k] = hp->betaCorrect; break;
+        case NB_Q_VLOS: p.cut[k] = hp->velSigma; p.corr[k] = hp->velCorrect; break;
+        case NB_Q_DIST: p.cut[k] = hp->distSigma; p.corr[k] = hp->distCorrect; break;
+        default: p.cut[k] = hp->pmSigma; p.corr[k] = hp->pmCorrect; break;
+        }
+    }
+    const int n = st->nbody;
+    const int D = (int) nbodyOf.size();
+    p.n = n;
+    p.D = D;
+    p.B = B;
+    p.iterMax = hp->iterMax;
+    // chunks of at most ch bodies within one dwarf
+    const size_t ch = nb_hist_chunk_bodies(n, p.h.nq, B);
+    std::vector<int4> chunks;
+    std::vector<int> chunkFirst(D + 1);
+    int first = 0;
+    for (int d = 0; d < D; ++d) {
+        chunkFirst[d] = (int) chunks.size();
+        for (int c = first; c < first + nbodyOf[d]; c += (int) ch)
+            chunks.push_back(make_int4(c, std::min(first + nbodyOf[d], c + (int) ch), d, 0));
+        first += nbodyOf[d];
+    }
+    chunkFirst[D] = (int) chunks.size();
+    if (first != n) { g_lastError = "dwarf sizes do not add up to the body count"; return NBODY_USER_ERROR; }
+    p.nChunks = (int) chunks.size();
+    const size_t Dz = (size_t) D, Bz = (size_t) B, nz = (size_t) n, nq = (size_t) p.h.nq;
+    const size_t QDB = std::max<size_t>(nq, 1) * Dz * Bz;
+    const size_t need = nb_al(4 * Dz * Bz) + 4 * nb_al(4 * Dz) + nb_al(4 * nz) +
+                        nb_al(8 * nq * nz) + nb_al(16 * chunks.size()) + nb_al(4 * (Dz + 1)) +
+                        nb_al(8 * chunks.size() * std::max<size_t>(nq, 1) * 3 * Bz) +
+                        5 * nb_al(8 * QDB) + nb_al(4 * Dz) + nb_al(8 * NB_LIKELIHOOD_TERMS * Dz) +
+                        nb_al(8 * Dz * NB_HIST_COMPONENTS * 2 * Bz) + nb_al(4 * Bz) +
+                        (3 + 2 * NB_HIST_COMPONENTS) * nb_al(8 * Bz) + 256;
     NB_CHECK(cudaSetDevice(st->device));
-    const size_t D = (size_t) nDwarfs, B = (size_t) nBins;
-    const size_t need = nb_al(4 * D * B) + 4 * nb_al(4 * D) + nb_al(32 * D) + nb_al(4 * B) +
-                        3 * nb_al(8 * B) + 256;
     if (st->histScratchBytes < need) {
         cudaFree(st->histScratch);
         st->histScratch = nullptr;
@@ -1154,47 +1278,109 @@ static NBodyCudaStatus nb_hist_run(NBodyCudaState* st, const int* bodyDwarf, int
         NB_CHECK(cudaMalloc((void**) &st->histScratch, need));
         st->histScratchBytes = need;
     }
-    char* p = st->histScratch;
-    auto carve = [&p](size_t bytes) { char* q = p; p += nb_al(bytes); return q; };
-    unsigned* dCounts = (unsigned*) carve(4 * D * B);
-    unsigned* dInRange = (unsigned*) carve(4 * D);
-    unsigned* dLight = (unsigned*) carve(4 * D);
-    int* dLast = (int*) carve(4 * D);
-    int* dNbody = (int*) carve(4 * D);
-    double* dOut = (double*) carve(32 * D);
-    int* dUse = (int*) carve(4 * B);
-    double* dLam = (double*) carve(8 * B);
-    double* dVar = (double*) carve(8 * B);
-    double* dErr = (double*) carve(8 * B);
+    char* cur = st->histScratch;
+    auto carve = [&cur](size_t bytes) { char* q = cur; cur += nb_al(bytes); return q; };
+    p.counts = (unsigned*) carve(4 * Dz * Bz);
+    p.inRange = (unsigned*) carve(4 * Dz);
+    p.nLight = (unsigned*) carve(4 * Dz);
+    p.lastLight = (int*) carve(4 * Dz);
+    p.binOf = (int*) carve(4 * nz);
+    p.val = (double*) carve(8 * nq * nz);
+    p.chunks = (int4*) carve(16 * chunks.size());
+    p.chunkFirst = (int*) carve(4 * (Dz + 1));
+    p.part = (double*) carve(8 * chunks.size() * std::max<size_t>(nq, 1) * 3 * Bz);
+    p.sum = (double*) carve(8 * QDB);
+    p.sq = (double*) carve(8 * QDB);
+    p.rem = (double*) carve(8 * QDB);
+    p.var = (double*) carve(8 * QDB);
+    p.err = (double*) carve(8 * QDB);
+    r.nbodyOf = (int*) carve(4 * Dz);
+    r.out = (double*) carve(8 * NB_LIKELIHOOD_TERMS * Dz);
+    r.comps = (double*) carve(8 * Dz * NB_HIST_COMPONENTS * 2 * Bz);
     const cudaStream_t s = st->stream;
-    NbTreeBuffers& b = st->b;
-    const NbHistDev h = nb_hist_dev(hp);
-    nb_launch_histogram(b.px, b.py, b.pz, st->types, bodyDwarf, st->nbody, nDwarfs, h, dCounts,
-                        dInRange, dLight, dLast, st->numSMs, s);
-    if (data && out) {
-        NB_CHECK(cudaMemcpyAsync(dNbody, nbodyOfHost, 4 * D, cudaMemcpyHostToDevice, s));
-        NB_CHECK(cudaMemcpyAsync(dUse, data->useBin, 4 * B, cudaMemcpyHostToDevice, s));
-        NB_CHECK(cudaMemcpyAsync(dLam, data->lambda, 8 * B, cudaMemcpyHostToDevice, s));
-        NB_CHECK(cudaMemcpyAsync(dVar, data->variable, 8 * B, cudaMemcpyHostToDevice, s));
-        NB_CHECK(cudaMemcpyAsync(dErr, data->err, 8 * B, cudaMemcpyHostToDevice, s));
-        NbDataHistDev dh{dUse, dLam, dVar, dErr, data->massPerParticle, data->totalNum, nBins};
-        nb_launch_likelihood(dCounts, dInRange, dLight, dLast, b.mass, dNbody, nDwarfs, dh, dOut, s);
-        NB_CHECK(cudaMemcpyAsync(out, dOut, 32 * D, cudaMemcpyDeviceToHost, s));
+    if (!chunks.empty())
+        NB_CHECK(cudaMemcpyAsync(p.chunks, chunks.data(), 16 * chunks.size(),
+                                 cudaMemcpyHostToDevice, s));
+    NB_CHECK(cudaMemcpyAsync(p.chunkFirst, chunkFirst.data(), 4 * (Dz + 1), cudaMemcpyHostToDevice, s));
+    NB_CHECK(cudaMemcpyAsync(r.nbodyOf, nbodyOf.data(), 4 * Dz, cudaMemcpyHostToDevice, s));
+    r.f = f;
+    r.dh = NbDataHistDev{};
+    if (data) {
+        NbDataHistDev& dh = r.dh;
+        int* dUse = (int*) carve(4 * Bz);
+        NB_CHECK(cudaMemcpyAsync(dUse, data->useBin, 4 * Bz, cudaMemcpyHostToDevice, s));
+        auto up = [&](const double* src) -> const double* {
+            if (!src) return nullptr;
+            double* dst = (double*) carve(8 * Bz);
+            cudaMemcpyAsync(dst, src, 8 * Bz, cudaMemcpyHostToDevice, s);
+            return dst;
+        };
+        dh.useBin = dUse;
+        dh.lambda = up(data->lambda);
+        dh.variable = up(data->variable);
+        dh.err = up(data->err);
+        for (int k = 0; k < NB_HIST_COMPONENTS; ++k) {
+            dh.compVar[k] = up(data->compVariable[k]);
+            dh.compErr[k] = up(data->compErr[k]);
+        }
+        dh.massPerParticle = data->massPerParticle;
+        dh.totalNum = data->totalNum;
+        dh.nBins = B;
+        dh.betaDispBins = data->betaDispBins;
+        NB_CHECK(cudaGetLastError());
     }
+    return NBODY_SUCCESS;
+}
+
+// Launches the histogram passes of a prepared run (and, with data, the likelihood into r.out).
+static int nb_hist_launch(NBodyCudaState* st, const int* bodyDwarf, const NbHistRun& r, bool like)
+{
+    NbTreeBuffers& b = st->b;
+    int launches = nb_launch_hist_plan(r.p, b.px, b.py, b.pz, b.vx, b.vy, b.vz, st->types,
+                                       bodyDwarf, st->numSMs, st->stream);
+    if (like) {
+        nb_launch_likelihood(r.p, b.mass, r.nbodyOf, r.dh, r.f, r.out, st->stream);
+        ++launches;
+    }
+    return launches;
+}
+
+// Histograms of the dwarfs (bodyDwarf NULL: the whole state is one dwarf) and, with a data
+// histogram, their likelihoods.  Host outputs, any may be NULL: counts (D x B), totals (2 per
+// dwarf: bodies in range, light bodies), massPer (per dwarf), comps (7 x 2 x B per dwarf),
+// out (NB_LIKELIHOOD_TERMS per dwarf).
+static NBodyCudaStatus nb_hist_run(NBodyCudaState* st, const int* bodyDwarf,
+                                   const std::vector<int>& nbodyOf,
+                                   const NBodyCudaHistogramParams* hp,
+                                   const NBodyCudaDataHistogram* data, unsigned* counts,
+                                   unsigned* totals, double* massPer, double* comps, double* out)
+{
+    NbHistRun r;
+    const bool like = data && out;
+    NBodyCudaStatus rc = nb_hist_prepare(st, nbodyOf, hp, like ? data : nullptr, comps != nullptr, r);
+    if (rc != NBODY_SUCCESS) return rc;
+    const cudaStream_t s = st->stream;
+    nb_hist_launch(st, bodyDwarf, r, like);
+    const size_t D = nbodyOf.size(), B = (size_t) r.p.B;
+    if (comps) nb_launch_hist_export(r.p, r.comps, s);
     NB_CHECK(cudaGetLastError());
-    if (counts) NB_CHECK(cudaMemcpyAsync(counts, dCounts, 4 * D * B, cudaMemcpyDeviceToHost, s));
+    if (out) NB_CHECK(cudaMemcpyAsync(out, r.out, 8 * NB_LIKELIHOOD_TERMS * D, cudaMemcpyDeviceToHost, s));
+    if (comps)
+        NB_CHECK(cudaMemcpyAsync(comps, r.comps, 8 * D * NB_HIST_COMPONENTS * 2 * B,
+                                 cudaMemcpyDeviceToHost, s));
+    if (counts) NB_CHECK(cudaMemcpyAsync(counts, r.p.counts, 4 * D * B, cudaMemcpyDeviceToHost, s));
     std::vector<unsigned> inR(D), light(D);
     std::vector<int> last(D);
-    NB_CHECK(cudaMemcpyAsync(inR.data(), dInRange, 4 * D, cudaMemcpyDeviceToHost, s));
-    NB_CHECK(cudaMemcpyAsync(light.data(), dLight, 4 * D, cudaMemcpyDeviceToHost, s));
-    NB_CHECK(cudaMemcpyAsync(last.data(), dLast, 4 * D, cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaMemcpyAsync(inR.data(), r.p.inRange, 4 * D, cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaMemcpyAsync(light.data(), r.p.nLight, 4 * D, cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaMemcpyAsync(last.data(), r.p.lastLight, 4 * D, cudaMemcpyDeviceToHost, s));
     NB_CHECK(cudaStreamSynchronize(s));
     for (size_t d = 0; d < D; ++d) {
         if (totals) { totals[2 * d] = inR[d]; totals[2 * d + 1] = light[d]; }
         if (massPer) {
             double m = 0.0;
             if (last[d] >= 0)
-                NB_CHECK(cudaMemcpy(&m, b.mass + last[d], sizeof(double), cudaMemcpyDeviceToHost));
+                NB_CHECK(cudaMemcpy(&m, st->b.mass + last[d], sizeof(double), cudaMemcpyDeviceToHost));
             massPer[d] = m;
         }
     }
@@ -1292,18 +1478,146 @@ NBodyCudaStatus nbSetTypesCUDA(NBodyCudaState* st, const int* types)
 
 NBodyCudaStatus nbHistogramCUDA(NBodyCudaState* st, const NBodyCudaHistogramParams* hp,
                                 unsigned int* counts, unsigned int* totals,
-                                double* massPerParticle)
+                                double* massPerParticle, double* comps)
 {
     if (!st) return NBODY_USER_ERROR;
-    return nb_hist_run(st, nullptr, 1, nullptr, hp, nullptr, counts, totals, massPerParticle, nullptr);
+    return nb_hist_run(st, nullptr, {st->nbody}, hp, nullptr, counts, totals, massPerParticle,
+                       comps, nullptr);
 }
 
 NBodyCudaStatus nbLikelihoodCUDA(NBodyCudaState* st, const NBodyCudaHistogramParams* hp,
                                  const NBodyCudaDataHistogram* data, double* out)
 {
     if (!st || !data || !out) return NBODY_USER_ERROR;
-    const int nb = st->nbody;
-    return nb_hist_run(st, nullptr, 1, &nb, hp, data, nullptr, nullptr, nullptr, out);
+    return nb_hist_run(st, nullptr, {st->nbody}, hp, data, nullptr, nullptr, nullptr, nullptr, out);
+}
+
+// One forward run of nbRunSystemPlain (nbody/src/nbody_plain.c:365-470): nbGravMap, steps up
+// to nStep with the best-likelihood scan on the device, the final likelihood.
+static NBodyCudaStatus nb_run_once(const NBodyCudaCtx* ctx, NBodyCudaState* st,
+                                   const NBodyCudaRunParams* rp, NbHistRun* hr,
+                                   NbBestDev& bestHost, double* finalOut)
+{
+    const cudaStream_t s = st->stream;
+    NbBestDev init{};
+    init.best[0] = 9999999.9;                       // st->bestLikelihood = DEFAULT_WORST_CASE
+    init.timeEvolve = rp->timeEvolve;
+    NB_CHECK(cudaMemcpyAsync(st->best, &init, sizeof init, cudaMemcpyHostToDevice, s));
+    NBodyCudaStatus all = nbGravMapCUDA(ctx, st);
+    if (all & ~(int) NBODY_STATUS_WARNINGS_MASK) return all;
+    const bool scan = hr && rp->useBestLike;
+    while (st->step < rp->nStep) {
+        NBodyCudaStatus rc = nbStepSystemCUDA(ctx, st);
+        all |= rc;
+        if (rc & ~(int) NBODY_STATUS_WARNINGS_MASK) return all;
+        if (scan && (double) st->step / (double) rp->nStep >= rp->bestLikeStart) {
+            nb_hist_launch(st, nullptr, *hr, true);
+            nb_launch_best_update(hr->out, st->best, 1, st->step, rp->nStep, hr->f, s);
+            if (rp->keepBestBodies) {
+                NbTreeBuffers& b = st->b;
+                nb_launch_keep_best(st->best, nullptr, b.px, b.py, b.pz, b.vx, b.vy, b.vz,
+                                    st->nbody, st->keepPos, st->keepVel, st->numSMs, s);
+            }
+        }
+    }
+    if (hr) {
+        nb_hist_launch(st, nullptr, *hr, true);
+        NB_CHECK(cudaMemcpyAsync(finalOut, hr->out, 8 * NB_LIKELIHOOD_TERMS,
+                                 cudaMemcpyDeviceToHost, s));
+    }
+    NB_CHECK(cudaMemcpyAsync(&bestHost, st->best, sizeof bestHost, cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaGetLastError());
+    NB_CHECK(cudaStreamSynchronize(s));
+    return all;
+}
+
+NBodyCudaStatus nbRunSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st,
+                                const NBodyCudaRunParams* rp, const NBodyCudaHistogramParams* hp,
+                                const NBodyCudaDataHistogram* data, NBodyCudaRunResult* res)
+{
+    if (!st || !ctx || !rp || !res || rp->nStep < 0 || rp->calibrationRuns < 0) {
+        g_lastError = "nbRunSystemCUDA: invalid arguments";
+        return NBODY_USER_ERROR;
+    }
+    if ((rp->useBestLike || rp->keepBestBodies) && (!hp || !data)) {
+        g_lastError = "nbRunSystemCUDA: the best-likelihood scan needs histogram parameters and data";
+        return NBODY_USER_ERROR;
+    }
+    if (st->step > rp->nStep) {
+        g_lastError = "nbRunSystemCUDA: the state is past nStep";
+        return NBODY_USER_ERROR;
+    }
+    NB_CHECK(cudaSetDevice(st->device));
+    *res = NBodyCudaRunResult{};
+    for (int t = 0; t < NB_LIKELIHOOD_TERMS; ++t) res->result[t] = res->final[t] = NAN;
+    NbHistRun hr;
+    const bool like = hp && data;
+    if (like) {
+        NBodyCudaStatus rc = nb_hist_prepare(st, {st->nbody}, hp, data, false, hr);
+        if (rc != NBODY_SUCCESS) return rc;
+    }
+    if (!st->best) NB_CHECK(cudaMalloc((void**) &st->best, sizeof(NbBestDev)));
+    if (rp->keepBestBodies && !st->keepPos) {
+        NB_CHECK(nb_alloc(&st->keepPos, 3 * (size_t) st->nbody));
+        NB_CHECK(nb_alloc(&st->keepVel, 3 * (size_t) st->nbody));
+    }
+    // nbody.c:436-447: the bar's first time origin; calibration only with an orbiting bar
+    const double og = (2 * rp->bestLikeStart) / (rp->bestLikeStart + 1);
+    double pft = rp->useBestLike ? rp->timeEvolve / (2 - og) : rp->timeEvolve;
+    const bool bar = ctx->potentialType == NBCUDA_POTENTIAL_DEFAULT &&
+                     ctx->pot.disk2.type == NBCUDA_ORBITING_BAR;
+    const int runs = 1 + (bar ? rp->calibrationRuns : 0);
+    if (runs > 1) {
+        NBodyCudaStatus rc = nb_save_slot(st, st->runStart);
+        if (rc != NBODY_SUCCESS) return rc;
+    }
+    NBodyCudaStatus all = NBODY_SUCCESS;
+    NbBestDev best{};
+    double fin[NB_LIKELIHOOD_TERMS];
+    for (int i = 0; i < runs; ++i) {
+        if (i > 0) {
+            NBodyCudaStatus rc = nb_restore_slot(st, st->runStart);
+            if (rc != NBODY_SUCCESS) return rc;
+        }
+        st->timeOrigin = pft;
+        st->haveKeep = 0;
+        all |= nb_run_once(ctx, st, rp, like ? &hr : nullptr, best, fin);
+        res->runs = i + 1;
+        if (all & ~(int) NBODY_STATUS_WARNINGS_MASK) break;
+        if (i < runs - 1) pft = best.bestTime;          // nbody.c:508-516
+    }
+    res->previousForwardTime = pft;
+    res->bestTime = best.bestTime;
+    res->bestStep = best.bestStep;
+    res->bestCount = best.count;
+    st->haveKeep = rp->keepBestBodies && best.count > 0;
+    for (int t = 0; t < NB_LIKELIHOOD_TERMS; ++t) res->best[t] = best.best[t];
+    if (like && !(all & ~(int) NBODY_STATUS_WARNINGS_MASK)) {
+        // nbody.c:308-345: clamp the final likelihood, then the best one replaces it if better
+        for (int t = 0; t < NB_LIKELIHOOD_TERMS; ++t) res->final[t] = fin[t];
+        double& l = res->final[0];
+        const double worst = 9999999.9;
+        if (l > worst || l < -1 * worst) l = worst;
+        else if (l == 0.0) l = 1e-9;
+        const bool useBest = rp->useBestLike && fabs(res->final[0]) > fabs(best.best[0]);
+        for (int t = 0; t < NB_LIKELIHOOD_TERMS; ++t)
+            res->result[t] = useBest ? best.best[t] : res->final[t];
+    }
+    return all;
+}
+
+NBodyCudaStatus nbGetBestBodiesCUDA(NBodyCudaState* st, double* pos, double* vel)
+{
+    if (!st || !st->haveKeep) {
+        g_lastError = "nbGetBestBodiesCUDA: no best-likelihood bodies kept";
+        return NBODY_USER_ERROR;
+    }
+    NB_CHECK(cudaSetDevice(st->device));
+    const size_t bytes = 3 * (size_t) st->nbody * sizeof(double);
+    if (pos) NB_CHECK(cudaMemcpyAsync(pos, st->keepPos, bytes, cudaMemcpyDeviceToHost, st->stream));
+    if (vel) NB_CHECK(cudaMemcpyAsync(vel, st->keepVel, bytes, cudaMemcpyDeviceToHost, st->stream));
+    NB_CHECK(cudaStreamSynchronize(st->stream));
+    return NBODY_SUCCESS;
 }
 
 }  // extern "C"
@@ -1741,23 +2055,28 @@ NBodyCudaStatus nbBatchSetTypesCUDA(NBodyCudaBatch* bt, const int* types)
     return nb_set_types(bt->st, types);
 }
 
+static std::vector<int> nb_batch_sizes(const NBodyCudaBatch* bt)
+{
+    std::vector<int> nb(bt->nDwarfs);
+    for (int d = 0; d < bt->nDwarfs; ++d) nb[d] = bt->dwarfs[d].nbody;
+    return nb;
+}
+
 NBodyCudaStatus nbBatchHistogramCUDA(NBodyCudaBatch* bt, const NBodyCudaHistogramParams* hp,
                                      unsigned int* counts, unsigned int* totals,
-                                     double* massPerParticle)
+                                     double* massPerParticle, double* comps)
 {
     if (!bt) return NBODY_USER_ERROR;
-    return nb_hist_run(bt->st, bt->bodyDwarf, bt->nDwarfs, nullptr, hp, nullptr, counts, totals,
-                       massPerParticle, nullptr);
+    return nb_hist_run(bt->st, bt->bodyDwarf, nb_batch_sizes(bt), hp, nullptr, counts, totals,
+                       massPerParticle, comps, nullptr);
 }
 
 NBodyCudaStatus nbBatchLikelihoodCUDA(NBodyCudaBatch* bt, const NBodyCudaHistogramParams* hp,
                                       const NBodyCudaDataHistogram* data, double* out)
 {
     if (!bt || !data || !out) return NBODY_USER_ERROR;
-    std::vector<int> nb(bt->nDwarfs);
-    for (int d = 0; d < bt->nDwarfs; ++d) nb[d] = bt->dwarfs[d].nbody;
-    return nb_hist_run(bt->st, bt->bodyDwarf, bt->nDwarfs, nb.data(), hp, data, nullptr, nullptr,
-                       nullptr, out);
+    return nb_hist_run(bt->st, bt->bodyDwarf, nb_batch_sizes(bt), hp, data, nullptr, nullptr,
+                       nullptr, nullptr, out);
 }
 
 NBodyCudaStatus nbBatchGenerateDwarfsCUDA(NBodyCudaBatch* bt, const NBodyCudaPlummerDwarf* dwarfs)

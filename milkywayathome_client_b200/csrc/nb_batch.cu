@@ -455,162 +455,3 @@ int nb_build_forest(NbTreeBuffers& b, const NbForest& f, int n, int capNodes, in
     return launches;
 }
 
-// =============================================================================================
-// Lambda-Beta histograms and the EMD/cost likelihood of every dwarf
-// =============================================================================================
-// nbCreateHistogram (nbody/src/nbody_histogram.c:671-1139, the normalised-counts histogram):
-// a body of type +1 counts towards totalSimulated and sets massPerParticle (the last such body
-// in body order); a body of type >= 0 is binned: nbXYZToLambdaBeta
-// (nbody/src/nbody_coordinates.c:129-164) after x += sunGCDist, then
-// index = floor((lambda - lambdaStart) / lambdaSize), likewise for beta, counted if in range.
-
-
-__global__ void k_histogram(const double* __restrict__ px, const double* __restrict__ py,
-                            const double* __restrict__ pz, const int* __restrict__ types,
-                            const int* __restrict__ bodyDwarf, int n, NbHistDev h,
-                            unsigned int* __restrict__ counts, unsigned int* __restrict__ inRange,
-                            unsigned int* __restrict__ nLight, int* __restrict__ lastLight)
-{
-    const int nBins = h.lambdaBins * h.betaBins;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int t = types[i];
-        if (t < 0) continue;                              // ignoreBody (dark matter)
-        const int d = bodyDwarf ? bodyDwarf[i] : 0;
-        if (t == 1) {
-            atomicAdd(&nLight[d], 1u);
-            atomicMax(&lastLight[d], i);
-        }
-        const double x = px[i] + h.sunGCDist, y = py[i], z = pz[i];
-        const double tx = h.rot[0] * x + h.rot[1] * y + h.rot[2] * z;
-        const double ty = h.rot[3] * x + h.rot[4] * y + h.rot[5] * z;
-        double tz = h.rot[6] * x + h.rot[7] * y + h.rot[8] * z;
-        const double r = sqrt(tx * tx + ty * ty + tz * tz);
-        tz = -tz;
-        const double lambda = atan2(ty, tx) * 180.0 / M_PI;       // r2d
-        const double beta = asin(tz / r) * 180.0 / M_PI;
-        // (unsigned int) of the floor as the reference's x86-64 build converts it: through a
-        // 64-bit signed integer, so a negative index wraps out of range (a direct conversion to
-        // unsigned would saturate it to bin 0 here)
-        const unsigned li = (unsigned) (long long) floor((lambda - h.lambdaStart) / h.lambdaSize);
-        const unsigned bi = (unsigned) (long long) floor((beta - h.betaStart) / h.betaSize);
-        if (li < (unsigned) h.lambdaBins && bi < (unsigned) h.betaBins) {
-            atomicAdd(&counts[(size_t) d * nBins + li * h.betaBins + bi], 1u);
-            atomicAdd(&inRange[d], 1u);
-        }
-    }
-}
-
-// nbMatchEMD (nbody/src/nbody_emd.c:1278-1427) with the default EMD range (the whole
-// histogram) and nbCostComponent (nbody/src/nbody_mass.c:318-391), one thread per dwarf, for
-// one beta bin: the EMD between two weight sets on the lambda axis with the L2 ground
-// distance of the reference's emdCalc is then the 1-D transport cost
-// sum_k |F_sim(k) - F_data(k)| (lambda_{k+1} - lambda_k) over the used bins.
-// out[4 d ..]: likelihood (EMD component + cost), EMD, EMD component, cost component.
-
-
-__global__ void k_likelihood(const unsigned int* __restrict__ counts,
-                             const unsigned int* __restrict__ inRange,
-                             const unsigned int* __restrict__ nLight,
-                             const int* __restrict__ lastLight, const double* __restrict__ mass,
-                             const int* __restrict__ nbodyOf, int nDwarfs, NbDataHistDev dh,
-                             double* __restrict__ out)
-{
-    const int d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= nDwarfs) return;
-    const int nb = dh.nBins;
-    const unsigned* c = counts + (size_t) d * nb;
-    const unsigned nSimU = inRange[d];                  // histogram->totalNum
-    const double histMass = lastLight[d] >= 0 ? mass[lastLight[d]] : 0.0;
-    const double n = (double) nLight[d];                // totalSimulated
-    double* o = out + 4 * (size_t) d;
-    const double worst = 9999999.9;                     // DEFAULT_WORST_CASE
-    // nbSystemLikelihood (nbody/src/nbody_likelihood.c:186-215): too few bodies in range
-    if ((double) nSimU < 0.0001 * (double) nbodyOf[d]) {
-        o[0] = worst; o[1] = worst; o[2] = worst; o[3] = 0.0;
-        return;
-    }
-    const unsigned nData = dh.totalNum;
-    double emdComp;
-    double emd = 0.0;
-    if (nSimU == 0 || nData == 0) {
-        emdComp = INFINITY;
-    } else if (histMass <= 0.0 || dh.massPerParticle <= 0.0) {
-        emdComp = NAN;
-    } else {
-        // weights of the used bins, as nbMatchEMD forms them
-        unsigned simRange = 0, dataRange = 0;
-        for (int j = 0; j < nb; ++j) {
-            if (!dh.useBin[j]) continue;
-            const double var = (double) c[j] / (double) nSimU;
-            simRange += (unsigned) round(var * (double) nSimU);
-            dataRange += (unsigned) round(dh.variable[j] * (double) nData);
-        }
-        double Fs = 0.0, Fd = 0.0, cost = 0.0, prevL = 0.0;
-        bool first = true;
-        for (int j = 0; j < nb; ++j) {
-            if (!dh.useBin[j]) continue;
-            if (!first) cost += fabs(Fs - Fd) * (dh.lambda[j] - prevL);
-            const double var = (double) c[j] / (double) nSimU;
-            Fs += var * (double) nSimU / (1.0 * simRange);
-            Fd += dh.variable[j] * (double) nData / (1.0 * dataRange);
-            prevL = dh.lambda[j];
-            first = false;
-        }
-        emd = cost * ((double) dataRange / (1.0 * nData));
-        emd = emd * (double) (nData / dataRange);       // integer division, as the reference
-        emd = round(emd * 1.0e9) * 1.0e-9;
-        emdComp = emd > 50.0 ? NAN : -(300.0 * log(1.0 - emd / 50.0));
-    }
-    // nbCostComponent
-    double costComp;
-    if (nSimU == 0 || nData == 0) {
-        costComp = INFINITY;
-    } else if (histMass <= 0.0 || dh.massPerParticle <= 0.0) {
-        costComp = NAN;
-    } else {
-        double nSim = (double) nSimU, nDataVar = 0.0;
-        const double nDataD = (double) nData;
-        for (int j = 0; j < nb; ++j) {
-            if (!dh.useBin[j]) nSim -= round(((double) c[j] / (double) nSimU) * (double) nSimU);
-            else nDataVar += (dh.err[j] * nDataD) * (dh.err[j] * nDataD);
-        }
-        const double p = nSim / n;
-        const double dm = dh.massPerParticle * nDataD - histMass * nSim;
-        const double num = -(dm * dm);
-        const double denom = 2.0 * ((dh.massPerParticle * dh.massPerParticle) * nDataVar +
-                                    (histMass * histMass) * nSim * p * (1.0 - p));
-        costComp = -(num / denom);
-    }
-    o[0] = emdComp + costComp;
-    o[1] = emd;
-    o[2] = emdComp;
-    o[3] = costComp;
-}
-
-// Histograms (counts, in-range totals, light-body totals) of every dwarf and, when a data
-// histogram is given, their likelihoods.  scratch: 4 nDwarfs ints of device memory.
-void nb_launch_histogram(const double* px, const double* py, const double* pz, const int* types,
-                         const int* bodyDwarf, int n, int nDwarfs, const NbHistDev& h,
-                         unsigned int* counts, unsigned int* inRange, unsigned int* nLight,
-                         int* lastLight, int numSMs, cudaStream_t s)
-{
-    const int nBins = h.lambdaBins * h.betaBins;
-    cudaMemsetAsync(counts, 0, sizeof(unsigned) * (size_t) nDwarfs * nBins, s);
-    cudaMemsetAsync(inRange, 0, sizeof(unsigned) * nDwarfs, s);
-    cudaMemsetAsync(nLight, 0, sizeof(unsigned) * nDwarfs, s);
-    cudaMemsetAsync(lastLight, 0xff, sizeof(int) * nDwarfs, s);    // -1
-    if (n > 0)
-        k_histogram<<<nb_b_grid(n, 256, numSMs * 8), 256, 0, s>>>(px, py, pz, types, bodyDwarf, n, h,
-                                                                  counts, inRange, nLight, lastLight);
-    nb_count_launch();
-}
-
-void nb_launch_likelihood(const unsigned int* counts, const unsigned int* inRange,
-                          const unsigned int* nLight, const int* lastLight, const double* mass,
-                          const int* nbodyOf, int nDwarfs, const NbDataHistDev& dh, double* out,
-                          cudaStream_t s)
-{
-    k_likelihood<<<(nDwarfs + 127) / 128, 128, 0, s>>>(counts, inRange, nLight, lastLight, mass,
-                                                       nbodyOf, nDwarfs, dh, out);
-    nb_count_launch();
-}

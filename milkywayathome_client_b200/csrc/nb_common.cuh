@@ -132,11 +132,44 @@ struct NbForest {
     int nDwarfs;
 };
 
-// Lambda-Beta histogram geometry (device copy of the histogram parameters).
+// ---- Lambda-Beta histograms and the likelihood (nb_likelihood.cu) ----
+// Per-body quantities that the comparison histograms bin (a slot of the plan holds one):
+enum { NB_Q_BETA = 0, NB_Q_VLOS = 1, NB_Q_DIST = 2, NB_Q_MUDEC = 3, NB_Q_MURA = 4, NB_NQ = 5 };
+constexpr int NB_HIST_COMPONENTS = 7;     // histograms 1..7 of the reference's MainStruct
+constexpr int NB_LIKELIHOOD_TERMS = 11;   // nbSystemLikelihood's 10 terms + the EMD itself
+
+// Histogram geometry and the per-body quantities to evaluate (device copy).
 struct NbHistDev {
     double rot[9];                  // rot11 .. rot33 of nbXYZToLambdaBeta
     double sunGCDist, lambdaStart, lambdaSize, betaStart, betaSize;
     int lambdaBins, betaBins;
+    double align[9];                // cartesianalign's rotation (proper motions)
+    double sunVel[3];
+    int nq;                         // active quantity slots
+    int q[NB_NQ];                   // quantity of each slot
+};
+// One histogram evaluation of nDwarfs dwarfs: device arrays (carved from one scratch block)
+// and the outlier-rejection constants.  Bodies are processed in chunks that never straddle a
+// dwarf, one warp per chunk, so every per-bin sum is formed in a fixed order.
+struct NbHistPlan {
+    NbHistDev h;
+    int n, D, B, nChunks, iterMax;
+    double cut[NB_NQ], corr[NB_NQ]; // sigma cut-off and dispersion correction of each slot
+    int histSlot[NB_HIST_COMPONENTS];  // slot of histograms 1..7 (-1: not built)
+    unsigned int* counts;           // D*B raw counts
+    unsigned int* inRange;          // D
+    unsigned int* nLight;           // D
+    int* lastLight;                 // D (-1: none)
+    int* binOf;                     // n: bin of the body within its dwarf, -1 if not binned
+    double* val;                    // nq*n: the body's quantities
+    int4* chunks;                   // {first, end, dwarf, 0}
+    int* chunkFirst;                // D+1: first chunk of each dwarf
+    double* part;                   // nChunks*nq*3*B: per-chunk sum, sum of squares, removed
+    double* sum;                    // nq*D*B: the reference's HistData sum, sq_sum,
+    double* sq;                     //   outliersRemoved, variable and err of each
+    double* rem;                    //   dispersion quantity
+    double* var;
+    double* err;
 };
 // A data histogram to compare against (device pointers to nBins entries).
 struct NbDataHistDev {
@@ -144,18 +177,43 @@ struct NbDataHistDev {
     const double* lambda;           // bin centres
     const double* variable;         // normalised counts
     const double* err;
+    const double* compVar[NB_HIST_COMPONENTS];  // histograms 1..7 (nullptr: absent)
+    const double* compErr[NB_HIST_COMPONENTS];
     double massPerParticle;
     unsigned int totalNum;
     int nBins;
+    int betaDispBins;
 };
-void nb_launch_histogram(const double* px, const double* py, const double* pz, const int* types,
-                         const int* bodyDwarf, int n, int nDwarfs, const NbHistDev& h,
-                         unsigned int* counts, unsigned int* inRange, unsigned int* nLight,
-                         int* lastLight, int numSMs, cudaStream_t s);
-void nb_launch_likelihood(const unsigned int* counts, const unsigned int* inRange,
-                          const unsigned int* nLight, const int* lastLight, const double* mass,
-                          const int* nbodyOf, int nDwarfs, const NbDataHistDev& dh, double* out,
-                          cudaStream_t s);
+// Which comparison terms nbSystemLikelihood adds (the reference's st->use* flags).
+struct NbLikeFlags {
+    int betaDisp, velDisp, betaComp, vlos, dist, propMot;
+};
+// Counts, per-body quantities and the dispersions with their outlier passes.
+int nb_launch_hist_plan(const NbHistPlan& p, const double* px, const double* py, const double* pz,
+                        const double* vx, const double* vy, const double* vz, const int* types,
+                        const int* bodyDwarf, int numSMs, cudaStream_t s);
+// out: NB_LIKELIHOOD_TERMS doubles per dwarf.
+void nb_launch_likelihood(const NbHistPlan& p, const double* mass, const int* nbodyOf,
+                          const NbDataHistDev& dh, NbLikeFlags f, double* out, cudaStream_t s);
+// comps: per dwarf, histograms 1..7 x {variable[B], err[B]} (zeros where not built).
+void nb_launch_hist_export(const NbHistPlan& p, double* comps, cudaStream_t s);
+size_t nb_hist_chunk_bodies(int n, int nq, int B);
+// The best likelihood of a run so far (st->bestLikelihood* of the reference), per dwarf.
+struct NbBestDev {
+    double best[NB_LIKELIHOOD_TERMS];
+    double timeEvolve;              // in: the dwarf's timeEvolve
+    double bestTime;
+    int bestStep, count, improved, pad;
+};
+// get_likelihood's update (nbody/src/nbody_plain.c:155-232) after step `step` of nStep, from
+// the likelihoods in out; with keep, the improved dwarfs' bodies are copied to keepPos/keepVel
+// (3n each, xyz interleaved).
+void nb_launch_best_update(const double* out, NbBestDev* best, int D, int step, int nStep,
+                           NbLikeFlags f, cudaStream_t s);
+void nb_launch_keep_best(const NbBestDev* best, const int* bodyDwarf, const double* px,
+                         const double* py, const double* pz, const double* vx, const double* vy,
+                         const double* vz, int n, double* keepPos, double* keepVel, int numSMs,
+                         cudaStream_t s);
 
 // Launch accounting (all launches of this library go through nb_count_launch).
 void nb_count_launch(int n = 1);

@@ -340,6 +340,38 @@ class NBodyState:
     def run_steps(self, ctx, nsteps):
         return self.lib.nbRunStepsCUDA(ctypes.byref(ctx.struct), self._h, int(nsteps))
 
+    def run_system(self, ctx, nstep, time_evolve, params=None, data=None, use_best_like=False,
+                   best_like_start=0.95, calibration_runs=0, keep_best_bodies=False):
+        """The reference's forward evolution (nbRunSystemCUDA: nbody.c's calibration runs
+        around nbRunSystemPlain with its best-likelihood scan): steps to nstep from the current
+        step; with params and data, the likelihood of the result.  Returns (status, dict) with
+        result / final / best (histogram.TERMS arrays), best_time, best_step, best_count,
+        previous_forward_time and runs."""
+        rp = _lib.RunParams(int(nstep), int(bool(use_best_like)), float(time_evolve),
+                            float(best_like_start), int(calibration_runs),
+                            int(bool(keep_best_bodies)))
+        res = _lib.RunResult()
+        hp = params.struct() if params is not None else None
+        dh = data.struct() if data is not None else None
+        rc = self.lib.nbRunSystemCUDA(ctypes.byref(ctx.struct), self._h, ctypes.byref(rp),
+                                      ctypes.byref(hp) if hp is not None else None,
+                                      ctypes.byref(dh) if dh is not None else None,
+                                      ctypes.byref(res))
+        out = {"result": np.array(res.result[:]), "final": np.array(res.final[:]),
+               "best": np.array(res.best[:]), "best_time": res.bestTime,
+               "best_step": res.bestStep, "best_count": res.bestCount,
+               "previous_forward_time": res.previousForwardTime, "runs": res.runs}
+        return rc, out
+
+    def best_bodies(self):
+        """Positions and velocities (n, 3) at the best likelihood of the last run_system with
+        keep_best_bodies (the reference's bestLikelihoodBodyTab)."""
+        pos = np.empty((self.nbody, 3))
+        vel = np.empty((self.nbody, 3))
+        self.check("nbGetBestBodiesCUDA",
+                   self.lib.nbGetBestBodiesCUDA(self._h, _lib.ptr(pos), _lib.ptr(vel)))
+        return pos, vel
+
     def makeTree(self, ctx):
         return self.lib.nbMakeTreeCUDA(ctypes.byref(ctx.struct), self._h)
 
@@ -389,22 +421,31 @@ class NBodyState:
         rc = getattr(self.lib, self._fn("SetTypes"))(self._h, _lib.ptr(t))
         self.check("%s(types)" % self._kind, rc)
 
-    def histogram(self, params):
-        """counts (ndwarfs, nBins), totals (ndwarfs, 2) = (in range, light), massPerParticle."""
+    def histogram(self, params, components=False):
+        """counts (ndwarfs, nBins), totals (ndwarfs, 2) = (in range, light), massPerParticle;
+        with components=True also histograms 1..7 (ndwarfs, 7, 2, nBins) as (values, errors):
+        the beta and line-of-sight velocity dispersions and, when params compare averages, the
+        averages (zeros where not built)."""
         nd = getattr(self, "ndwarfs", 1)
         counts = np.zeros((nd, params.nbins), dtype=np.uint32)
         totals = np.zeros((nd, 2), dtype=np.uint32)
         mpp = np.zeros(nd)
+        comps = np.zeros((nd, _lib.HIST_COMPONENTS, 2, params.nbins)) if components else None
         hp = params.struct()
         self.check("histogram", getattr(self.lib, self._fn("Histogram"))(
-            self._h, ctypes.byref(hp), _lib.ptr(counts), _lib.ptr(totals), _lib.ptr(mpp)))
+            self._h, ctypes.byref(hp), _lib.ptr(counts), _lib.ptr(totals), _lib.ptr(mpp),
+            _lib.ptr(comps) if components else None))
+        if components:
+            return counts, totals, mpp, comps
         return counts, totals, mpp
 
     def likelihood(self, params, data):
-        """(ndwarfs, 4): EMD component + cost component, EMD, EMD component, cost component,
-        as nbSystemLikelihood returns them (positive; lower is better)."""
+        """(ndwarfs, 11): the reference's likelihood array -- likelihood, EMD component, cost
+        component, beta dispersion, velocity dispersion, beta average, line-of-sight velocity,
+        distance, dec and RA proper motion (NaN where not compared) -- then the EMD itself
+        (histogram.TERMS).  Positive; lower is better."""
         nd = getattr(self, "ndwarfs", 1)
-        out = np.zeros((nd, 4))
+        out = np.zeros((nd, _lib.LIKELIHOOD_TERMS))
         hp = params.struct()
         dh = data.struct()
         self.check("likelihood", getattr(self.lib, self._fn("Likelihood"))(

@@ -90,6 +90,7 @@ def ref():
                                      ctypes.POINTER(ctypes.c_char_p), ctypes.c_int]),
             "nbref_handle_ctx": (None, [_vp, _vp, _ip, _dp]),
             "nbref_run": (ctypes.c_int, [_vp]),
+            "nbref_handle_run_params": (None, [_vp, _ip, _dp, _ip]),
             "nbref_likelihood": (ctypes.c_int, [_vp, _vp]),
             "nbref_pow_rn": (ctypes.c_double, [ctypes.c_double, ctypes.c_double]),
             "nbref_log_rn": (ctypes.c_double, [ctypes.c_double]),
@@ -289,6 +290,13 @@ class RefState:
         ns, te = ctypes.c_int(), ctypes.c_double()
         self.lib.nbref_handle_ctx(self.h, ctypes.byref(c), ctypes.byref(ns), ctypes.byref(te))
         return c, ns.value, te.value
+
+    def run_params(self):
+        """(useBestLike, BestLikeStart, calibrationRuns) of the context."""
+        u, c = ctypes.c_int(), ctypes.c_int()
+        b = ctypes.c_double()
+        self.lib.nbref_handle_run_params(self.h, ctypes.byref(u), ctypes.byref(b), ctypes.byref(c))
+        return bool(u.value), b.value, c.value
 
     def likelihood(self):
         out = np.zeros(10)

@@ -408,6 +408,17 @@ void nbref_handle_ctx(void* hv, NBodyCudaCtx* out, int* nStep, double* timeEvolv
     if (timeEvolve) *timeEvolve = h->ctx.timeEvolve;
 }
 
+/* The run-loop settings of the handle's context: useBestLike, BestLikeStart and
+ * calibrationRuns (nbody/include/nbody_types.h:477-512). */
+void nbref_handle_run_params(void* hv, int* useBestLike, double* bestLikeStart,
+                             int* calibrationRuns)
+{
+    RefHandle* h = (RefHandle*) hv;
+    *useBestLike = (int) h->ctx.useBestLike;
+    *bestLikeStart = h->ctx.BestLikeStart;
+    *calibrationRuns = (int) h->ctx.calibrationRuns;
+}
+
 /* The reference's run loop without checkpoints / best-likelihood tracking:
  * nbGravMap once, then nStep x nbStepSystem (nbody/src/nbody_plain.c:366-446). */
 int nbref_run(void* hv)

@@ -3,7 +3,8 @@
 
   * golden_likelihoods.json -- the reference's own golden end-to-end likelihoods for the
     single-Plummer Orphan models 4 and 5 (nbody/tests/RunTestUnits.lua:105-156) and the
-    triaxial-halo model (model_triaxial, :313-338), which tests/golden/orphan_dwarf.lua restates;
+    triaxial-halo (model_triaxial, :313-338) and orbiting-bar (model_bar, :443-468) models, which
+    tests/golden/orphan_dwarf.lua restates;
   * orphan_model_histogram_3 -- the data histogram those tests match against
     (nbody/tests/orphan_models/orphan_model_histogram_3), copied verbatim (data).
 
@@ -35,7 +36,8 @@ def main():
         "source": "nbody/tests/RunTestUnits.lua (refResults), tolerance 1e-10",
         "tolerance": 1e-10,
         "models": {"4": parse_results(text, "model_4"), "5": parse_results(text, "model_5"),
-                   "triaxial": parse_results(text, "model_triaxial")},
+                   "triaxial": parse_results(text, "model_triaxial"),
+                   "bar": parse_results(text, "model_bar")},
     }
     with open(os.path.join(HERE, "golden_likelihoods.json"), "w") as f:
         json.dump(golden, f, indent=1, sort_keys=True)

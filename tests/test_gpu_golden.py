@@ -7,10 +7,15 @@ histogram + EMD likelihood (nbCreateHistogram / nbSystemLikelihood).  The result
 the reference's golden table (nbody/tests/RunTestUnits.lua, models 4, 5 and model_triaxial)
 within its own tolerance, 1e-10:
 thousands of chaotic N-body steps only reproduce it if every step is bit-exact.
+
+nbRunSystemCUDA (the reference's run loop with its best-likelihood scan and, for the orbiting
+bar, its calibration runs) is checked the same way: against the reference's own executable on
+model 5 with the scan enabled, and against the golden table of model_bar.
 """
 import json
 import os
 
+import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -48,3 +53,75 @@ def test_golden_likelihood_through_gpu_steps(variant, nbody, seed):
     r.set(pos, vel)
     got = r.likelihood()[0]
     assert abs(got - want) < 1e-10, (got, want)
+
+
+def _reference_exe_likelihood(tmp_path, nbody, seed, args):
+    """<search_likelihood> of the reference's own executable (negated: positive, lower better)."""
+    import subprocess
+    from oracle import bindings as ob
+    out = subprocess.run(
+        [ob.REF_EXE, "--checkpoint-interval=-1", "-g", "-f", os.path.join(GOLDEN, "orphan_dwarf.lua"),
+         "-h", os.path.join(GOLDEN, "orphan_model_histogram_3"), "--seed", seed,
+         "--ignore-checkpoint", nbody] + list(args), capture_output=True, text=True, timeout=600,
+        cwd=str(tmp_path))
+    line = [l for l in out.stderr.splitlines() + out.stdout.splitlines()
+            if l.startswith("<search_likelihood>")][0]
+    return -float(line.split(">")[1].split("<")[0])
+
+
+def _gpu_run_system(variant, nbody, seed, options=()):
+    from oracle import bindings as ob
+    from milkywayathome_client_b200 import HistogramParams, NBodyCtx, NBodyState, _lib, read_histogram
+    r = ob.RefState.open_lua(os.path.join(GOLDEN, "orphan_dwarf.lua"),
+                             os.path.join(GOLDEN, "orphan_model_histogram_3"), int(seed),
+                             [nbody, variant] + list(options))
+    c, nstep, time_evolve = r.ctx(_lib.Ctx)
+    use_best, start, calib = r.run_params()
+    ctx = NBodyCtx.from_struct(c, nstep)
+    init = r.get()
+    mass, types = r.masses()
+    params = HistogramParams()              # makeHistogram of orphan_dwarf.lua; ctx defaults
+    data = read_histogram(os.path.join(GOLDEN, "orphan_model_histogram_3"))
+    with NBodyState.create(ctx, init["pos"], init["vel"], mass) as st:
+        st.set_types(types)
+        rc, res = st.run_system(ctx, nstep, time_evolve, params, data, use_best_like=use_best,
+                                best_like_start=start, calibration_runs=calib,
+                                keep_best_bodies=use_best)
+        assert rc == 0
+        assert st.step_count == nstep
+        if use_best and res["best_count"] > 0:
+            bpos, _ = st.best_bodies()
+            assert np.all(np.isfinite(bpos))
+    return res, (use_best, start, calib, nstep)
+
+
+@pytest.mark.parametrize("nbody,seed", [("100", "670828913"), ("100", "715144259"),
+                                        ("1024", "886885833")])
+def test_best_likelihood_scan_matches_reference_executable(tmp_path, nbody, seed):
+    """Model 5 (bit-exact steps) with the best-likelihood scan over the last 5% of the steps:
+    nbRunSystemCUDA's result equals the reference executable's."""
+    from oracle import bindings as ob
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    want = _reference_exe_likelihood(tmp_path, nbody, seed, ["5", "bestlike"])
+    res, (use_best, start, calib, nstep) = _gpu_run_system("5", nbody, seed, ["bestlike"])
+    assert use_best and calib == 0 and res["runs"] == 1
+    assert res["best_count"] >= 1 and res["best_step"] >= 0.95 * nstep
+    assert abs(res["result"][0] - want) < 1e-10, (res, want)
+
+
+BAR_CASES = [("100", s) for s in ("670828913", "886885833", "715144259")] + [("1024", "670828913")]
+
+
+@pytest.mark.parametrize("nbody,seed", BAR_CASES)
+def test_bar_golden_through_gpu_run_system(nbody, seed):
+    """model_bar: the orbiting bar, the best-likelihood window and two calibration runs, all on
+    the GPU, against the reference's golden table."""
+    from oracle import bindings as ob
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    with open(os.path.join(GOLDEN, "golden_likelihoods.json")) as f:
+        want = json.load(f)["models"]["bar"][nbody][seed]
+    res, (use_best, start, calib, nstep) = _gpu_run_system("bar", nbody, seed)
+    assert use_best and calib == 2 and res["runs"] == 3
+    assert abs(res["result"][0] - want) < 1e-10, (res, want)

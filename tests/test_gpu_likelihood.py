@@ -1,10 +1,14 @@
-"""The Lambda-Beta histogram and EMD/cost likelihood computed on the GPU against the reference.
+"""The Lambda-Beta histograms and the likelihood computed on the GPU against the reference.
 
 The reference's own Lua set-up (oracle/_ref) builds the Orphan-model dwarfs of
 tests/golden/orphan_dwarf.lua, the steps run on the GPU, and the final bodies are evaluated
 twice: by the reference's nbCreateHistogram + nbSystemLikelihood (through oracle/_ref) and by
-nbLikelihoodCUDA from the device-resident bodies.  The EMD and cost components must agree
-(the reference rounds the EMD to 1e-9); a batch of dwarfs must give each dwarf the
+nbLikelihoodCUDA from the device-resident bodies.  Every term of the reference's likelihood
+array must agree (the EMD is rounded to 1e-9 by both; the dispersions' sums are formed in
+another order, so they agree to rounding): the default comparisons (EMD, cost, beta
+dispersion), and every comparison (velocity dispersion, line-of-sight velocity, beta average,
+distance, proper motions, beta-dispersion averaging over neighbouring bins) against a data
+file in the reference's extended format.  A batch of dwarfs must give each dwarf the
 single-state likelihood.
 """
 import os
@@ -16,22 +20,41 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 HIST = os.path.join(GOLDEN, "orphan_model_histogram_3")
+LUA = os.path.join(GOLDEN, "orphan_dwarf.lua")
 CASES = [("5", "1024", "886885833"), ("4", "1024", "670828913"), ("5", "100", "670828913")]
+WORST, BEST = 9999999.9, 1e-9
+ALL = dict(useVelDisp=True, useBetaComp=True, useVlos=True, useDist=True, usePropMot=True)
 
 
-def _orphan_params():
+def _orphan_params(**flags):
     from milkywayathome_client_b200 import HistogramParams
     # makeHistogram of tests/golden/orphan_dwarf.lua; the reference's default sunGCDist
     return HistogramParams(phi=128.79, theta=54.39, psi=90.70, lambdaStart=-50.0, lambdaEnd=50.0,
                            lambdaBins=34, betaStart=-15.0, betaEnd=15.0, betaBins=1,
-                           sunGCDist=8.0)
+                           sunGCDist=8.0, **flags)
 
 
-def _run_case(variant, nbody, seed):
+def _clamped(x):
+    """The worst/best-case clamps the reference applies to the likelihood itself."""
+    if np.isnan(x) or x > WORST or x < -WORST:
+        return WORST
+    return BEST if x == 0.0 else x
+
+
+def _assert_terms(got, ref):
+    got = np.array(got[:10], dtype=float)
+    got[0] = _clamped(got[0])
+    for k in range(10):
+        if np.isnan(ref[k]):
+            assert np.isnan(got[k]), (k, got, ref)
+        else:
+            assert abs(got[k] - ref[k]) <= 1e-9 * max(1.0, abs(ref[k])), (k, got, ref)
+
+
+def _run_case(variant, nbody, seed, extra=()):
     from oracle import bindings as ob
     from milkywayathome_client_b200 import NBodyCtx, NBodyState, _lib
-    r = ob.RefState.open_lua(os.path.join(GOLDEN, "orphan_dwarf.lua"), HIST, int(seed),
-                             [nbody, variant])
+    r = ob.RefState.open_lua(LUA, HIST, int(seed), [nbody, variant] + list(extra))
     c, nstep, _ = r.ctx(_lib.Ctx)
     ctx = NBodyCtx.from_struct(c, nstep)
     init = r.get()
@@ -58,8 +81,44 @@ def test_likelihood_matches_reference(variant, nbody, seed):
     counts, totals, mpp = st.histogram(params)
     st.close()
     assert totals[0, 0] == counts.sum()
-    assert abs(got[2] - ref[1]) <= 1e-9 * max(1.0, abs(ref[1])), (got, ref)
-    assert abs(got[3] - ref[2]) <= 1e-9 * max(1.0, abs(ref[2])), (got, ref)
+    assert np.isfinite(ref[3])                 # the beta-dispersion term is compared
+    _assert_terms(got, ref)
+
+
+@pytest.mark.parametrize("beta_disp_bins", [0, 3, 4])
+def test_every_comparison_term_matches_reference(tmp_path, beta_disp_bins):
+    from oracle import bindings as ob
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    from milkywayathome_client_b200 import data_from_counts, read_histogram, write_histogram
+    seed = "886885833"
+    r, st, _ = _run_case("5", "1024", seed, ["allterms"])
+    params = _orphan_params(**ALL)
+    # the Orphan data file has no proper-motion columns: the reference's NaN array
+    got = st.likelihood(params, read_histogram(HIST))[0]
+    ref = r.likelihood()
+    assert np.all(np.isnan(got[:10])) and ref[0] == WORST and np.all(np.isnan(ref[1:]))
+    # a data file in the extended format from the GPU's own histograms, perturbed so that
+    # every comparison contributes
+    counts, totals, mpp, comps = st.histogram(params, components=True)
+    assert np.any(comps[0, 4, 1] > 0) and np.any(comps[0, 5, 1] > 0)   # averages were built
+    data = data_from_counts(params, counts[0], totals[0, 1], mpp[0], comps[0])
+    rng = np.random.default_rng(5)
+    data.components = [(c[0] * (1.0 + 0.05 * rng.standard_normal(len(c[0]))) + 0.01,
+                        np.abs(c[1]) + 0.02) for c in data.components]
+    data.betaDispBins = beta_disp_bins
+    path = str(tmp_path / "hist_all")
+    write_histogram(path, params, data)
+    data2 = read_histogram(path)
+    assert data2.betaDispBins == beta_disp_bins and all(c is not None for c in data2.components)
+    pos, vel = st.bodies()
+    r2 = ob.RefState.open_lua(LUA, path, int(seed), ["1024", "5", "allterms"])
+    r2.set(pos, vel)
+    ref2 = r2.likelihood()
+    got2 = st.likelihood(params, data2)[0]
+    st.close()
+    assert np.all(np.isfinite(ref2))
+    _assert_terms(got2, ref2)
 
 
 def test_batch_likelihood_matches_single_states():
@@ -87,4 +146,4 @@ def test_batch_likelihood_matches_single_states():
         assert np.array_equal(counts[k], c1[0])
         assert np.array_equal(totals[k], t1[0])
         assert mpp[k] == m1[0]
-        assert np.array_equal(out[k], lk)
+        assert np.array_equal(out[k], lk, equal_nan=True)
