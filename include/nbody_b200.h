@@ -306,6 +306,13 @@ NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTi
 /* Mixed-precision walk tuning of a single state (as nbBatchSetTuningCUDA): bodies per walk
  * group (1..64), interaction-list entries per warp (32, 64, 128), walk blocks per SM (0: max). */
 NBodyCudaStatus nbSetMixedTuningCUDA(NBodyCudaState* st, int groupMax, int listCap, int blocksPerSM);
+/* Interaction sets of the mixed walk.  exactSet = 1 (the default): a group of bodies walks the
+ * tree together, but every body takes exactly the cells and bodies its own opening test takes
+ * (the FP64 walk's set), so the mixed form's error is the FP64 walk's up to FP32 rounding.
+ * exactSet = 0: every body of a group takes the group's set (cells accepted for the whole group
+ * box) -- faster, never coarser per cell, but the shell of accepted cells is no longer
+ * symmetric about each body and the truncation errors cancel less: a heavier error tail. */
+NBodyCudaStatus nbSetMixedModeCUDA(NBodyCudaState* st, int exactSet);
 
 /* host array of nbody types (+1 light, -1 dark) */
 NBodyCudaStatus nbSetTypesCUDA(NBodyCudaState* st, const int* types);
@@ -388,6 +395,8 @@ NBodyCudaStatus nbBatchDwarfInfoCUDA(NBodyCudaBatch* batch, int* status, double*
  * (0: as many as fit) */
 NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* batch, int groupMax, int listCap,
                                      int blocksPerSM);
+/* as nbSetMixedModeCUDA, for every dwarf of the batch */
+NBodyCudaStatus nbBatchSetMixedModeCUDA(NBodyCudaBatch* batch, int exactSet);
 NBodyCudaStatus nbBatchGetTuningCUDA(NBodyCudaBatch* batch, int* groupMax, int* listCap,
                                      int* blocksPerSM);
 /* autotuner of the mixed walk on the batch's current state: times every candidate tuning

@@ -212,6 +212,8 @@ SIGNATURES = [
                                        ctypes.POINTER(HistParams), ctypes.POINTER(DataHist),
                                        ctypes.POINTER(RunResult)]),
     ("nbGetBestBodiesCUDA", ctypes.c_int, [_vp, _vp, _vp]),
+    ("nbSetMixedModeCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nbBatchSetMixedModeCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbSaveStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbRestoreStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbReleaseStatesCUDA", ctypes.c_int, [_vp]),

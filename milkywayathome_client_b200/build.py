@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libnbody_b200.so")
 SOURCES = ["nb_sort.cu", "nb_tree.cu", "nb_walk.cu", "nb_mixed.cu", "nb_api.cu", "nb_noalloc.cu", "nb_adjoint.cu", "nb_batch.cu", "nb_ic.cu", "nb_likelihood.cu"]
-HEADERS = ["nb_common.cuh", "nb_potential.cuh", "nb_tree_util.cuh"]
+HEADERS = ["nb_common.cuh", "nb_potential.cuh", "nb_tree_util.cuh", "nb_crmath.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",

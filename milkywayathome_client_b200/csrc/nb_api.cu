@@ -155,6 +155,7 @@ struct NBodyCudaState {
     int* types = nullptr;               // body types (+1 light, -1 dark), for histograms
     double timeOrigin = 0.0;            // st->previousForwardTime: barTime = step * dt - this
     int mixGroupMax = 32, mixListCap = 64, mixBlocksPerSM = 0;   // mixed-walk tuning
+    int mixExact = 1;                   // 1: each body's own interaction set (nbSetMixedModeCUDA)
     char* histScratch = nullptr;        // histogram / likelihood buffers
     size_t histScratchBytes = 0;
     NbSlot runStart;                    // nbRunSystemCUDA: the initial state of the runs
@@ -411,6 +412,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
                     st->mx.walkBlocks = std::max(1, per) * st->numSMs;
                     st->mx.groupMax = st->mixGroupMax;
                     st->mx.listCap = st->mixListCap;
+                    st->mx.exact = st->mixExact;
                 }
                 nb_launch_walk_mixed(b, st->mx, st->capNodes, wp, pot, st->counting != 0,
                                      st->numSMs, s);
@@ -1266,7 +1268,7 @@ static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int
     const size_t QDB = std::max<size_t>(nq, 1) * Dz * Bz;
     const size_t need = nb_al(4 * Dz * Bz) + 4 * nb_al(4 * Dz) + nb_al(4 * nz) +
                         nb_al(8 * nq * nz) + nb_al(16 * chunks.size()) + nb_al(4 * (Dz + 1)) +
-                        nb_al(8 * chunks.size() * std::max<size_t>(nq, 1) * 3 * Bz) +
+                        nb_al(4 * chunks.size() * Bz) + nb_al(4 * Dz * Bz) + nb_al(4 * nz) +
                         5 * nb_al(8 * QDB) + nb_al(4 * Dz) + nb_al(8 * NB_LIKELIHOOD_TERMS * Dz) +
                         nb_al(8 * Dz * NB_HIST_COMPONENTS * 2 * Bz) + nb_al(4 * Bz) +
                         (3 + 2 * NB_HIST_COMPONENTS) * nb_al(8 * Bz) + 256;
@@ -1288,7 +1290,9 @@ static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int
     p.val = (double*) carve(8 * nq * nz);
     p.chunks = (int4*) carve(16 * chunks.size());
     p.chunkFirst = (int*) carve(4 * (Dz + 1));
-    p.part = (double*) carve(8 * chunks.size() * std::max<size_t>(nq, 1) * 3 * Bz);
+    p.rows = (int*) carve(4 * chunks.size() * Bz);
+    p.segStart = (int*) carve(4 * Dz * Bz);
+    p.list = (int*) carve(4 * nz);
     p.sum = (double*) carve(8 * QDB);
     p.sq = (double*) carve(8 * QDB);
     p.rem = (double*) carve(8 * QDB);
@@ -1463,6 +1467,13 @@ NBodyCudaStatus nbSetMixedTuningCUDA(NBodyCudaState* st, int groupMax, int listC
     return NBODY_SUCCESS;
 }
 
+NBodyCudaStatus nbSetMixedModeCUDA(NBodyCudaState* st, int exactSet)
+{
+    if (!st || (exactSet != 0 && exactSet != 1)) return NBODY_USER_ERROR;
+    st->mixExact = exactSet;
+    return NBODY_SUCCESS;
+}
+
 NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTime)
 {
     if (!st) return NBODY_USER_ERROR;
@@ -1632,6 +1643,7 @@ struct NbBatchTuning {
     int groupMax = 32;      // bodies per walk group of the mixed walk
     int listCap = 64;       // interaction-list entries per warp
     int blocksPerSM = 0;    // resident walk blocks per SM (0: as many as fit)
+    int exact = 1;          // each body's own interaction set (nbBatchSetMixedModeCUDA)
 };
 
 struct NBodyCudaBatch {
@@ -1680,6 +1692,7 @@ static NBodyCudaStatus nb_batch_mixed_buffers(NBodyCudaBatch* bt)
     st->mx.walkBlocks = std::max(1, per) * st->numSMs;
     st->mx.groupMax = bt->tune.groupMax;
     st->mx.listCap = bt->tune.listCap;
+    st->mx.exact = bt->tune.exact;
     return NBODY_SUCCESS;
 }
 
@@ -1715,7 +1728,8 @@ static int nb_batch_enqueue(NBodyCudaBatch* bt, const NBodyCudaCtx* ctx, int dri
 
 static bool nb_same_tuning(const NbBatchTuning& a, const NbBatchTuning& b)
 {
-    return a.groupMax == b.groupMax && a.listCap == b.listCap && a.blocksPerSM == b.blocksPerSM;
+    return a.groupMax == b.groupMax && a.listCap == b.listCap && a.blocksPerSM == b.blocksPerSM &&
+           a.exact == b.exact;
 }
 
 // One evaluation of every dwarf (drift/kick: the fused halves of the leapfrog), optionally
@@ -1993,6 +2007,13 @@ NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* bt, int groupMax, int listC
     bt->tune.groupMax = groupMax;
     bt->tune.listCap = listCap;
     bt->tune.blocksPerSM = blocksPerSM;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbBatchSetMixedModeCUDA(NBodyCudaBatch* bt, int exactSet)
+{
+    if (!bt || (exactSet != 0 && exactSet != 1)) return NBODY_USER_ERROR;
+    bt->tune.exact = exactSet;
     return NBODY_SUCCESS;
 }
 

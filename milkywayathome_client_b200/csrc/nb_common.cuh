@@ -149,8 +149,9 @@ struct NbHistDev {
     int q[NB_NQ];                   // quantity of each slot
 };
 // One histogram evaluation of nDwarfs dwarfs: device arrays (carved from one scratch block)
-// and the outlier-rejection constants.  Bodies are processed in chunks that never straddle a
-// dwarf, one warp per chunk, so every per-bin sum is formed in a fixed order.
+// and the outlier-rejection constants.  A stable counting sort (chunks of bodies that never
+// straddle a dwarf, one warp per chunk) lists every bin's bodies in body order, so each bin's
+// sums are formed in the reference's order.
 struct NbHistPlan {
     NbHistDev h;
     int n, D, B, nChunks, iterMax;
@@ -164,7 +165,9 @@ struct NbHistPlan {
     double* val;                    // nq*n: the body's quantities
     int4* chunks;                   // {first, end, dwarf, 0}
     int* chunkFirst;                // D+1: first chunk of each dwarf
-    double* part;                   // nChunks*nq*3*B: per-chunk sum, sum of squares, removed
+    int* rows;                      // nChunks*B: bodies of each bin in a chunk, then offsets
+    int* segStart;                  // D*B: first list entry of each (dwarf, bin)
+    int* list;                      // n: the binned bodies, bin after bin, in body order
     double* sum;                    // nq*D*B: the reference's HistData sum, sq_sum,
     double* sq;                     //   outliersRemoved, variable and err of each
     double* rem;                    //   dispersion quantity
@@ -255,6 +258,7 @@ struct NbMixedBuffers {
     int walkBlocks;
     int groupMax;  // bodies per walk group, 1..64 (0: 32; above 32, two bodies per lane)
     int listCap;   // interaction-list entries per warp: 32, 64 or 128 (0: 64)
+    int exact;     // 1: every lane takes exactly its own body's interaction set (groups <= 32)
 };
 int nb_mixed_walk_blocks(int numSMs, int listCap = 0, int groupMax = 32);
 size_t nb_mixed_stack_ints(int blocks);

@@ -9,14 +9,16 @@
 // nbSystemLikelihood (nbody/src/nbody_likelihood.c:155-324) adds the EMD and cost components
 // and one nbLikelihood comparison (nbody_mass.c:395-469) per enabled histogram.
 //
-// Layout: one thread per body computes its bin and quantities (k_hist_bodies); every
-// outlier pass then runs one warp per chunk of bodies (chunks never straddle a dwarf), which
-// sums the kept values of each bin in lane order into the chunk's own row (k_hist_pass), and
-// one thread per (quantity, dwarf, bin) adds the rows of its dwarf in chunk order and
-// applies nbCalcDisp (k_hist_finalize).  The sums are therefore formed in a fixed order,
-// the same on every run; the reference adds in body order, so a sum may differ from its by
-// rounding.  Counts are integers and exact.
+// Layout: one thread per body computes its bin and quantities (k_hist_bodies).  A stable
+// counting sort then lists the bodies of every bin in body order: one warp per chunk of bodies
+// (chunks never straddle a dwarf) counts its bins (k_bin_rows), one block turns the counts into
+// list offsets (k_bin_offsets), and the chunk warps place their bodies (k_bin_scatter, lanes
+// of one bin ranked in lane order).  Finally one thread per (quantity, dwarf, bin) walks its
+// bin's list once per pass -- the initial sums and IterMax outlier passes, each followed by
+// nbCalcDisp -- adding in body order, as the reference does (k_disp_bins): the dispersions
+// and averages equal the reference's bit for bit.  Counts are integers and exact.
 #include "nb_common.cuh"
+#include "nb_crmath.cuh"
 
 #include <math.h>
 
@@ -146,98 +148,147 @@ __global__ void k_hist_bodies(const double* __restrict__ px, const double* __res
     }
 }
 
-// One pass over the bodies of every chunk: the kept values of each bin are summed in lane
-// order by the lowest lane of the bin's group and added to the chunk's row in batch order.
-// pass 0 keeps every binned body (the initial sums of nbCreateHistogram); a later pass is
-// nbRemoveOutliers: a body is kept if |bin average - value| < cut-off * bin dispersion, with
-// the average and dispersion of the previous pass (the removed bodies are counted).
-__global__ void __launch_bounds__(HW * 32) k_hist_pass(NbHistPlan p, int pass)
+// Bodies of each bin in every chunk: rows[c * B + b].  Lanes holding the same bin form a group
+// (__match_any_sync); its lowest lane adds the group's size.
+__global__ void __launch_bounds__(HW * 32) k_bin_rows(NbHistPlan p)
 {
-    __shared__ double stage[HW][3][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int c = blockIdx.x * HW + w;
     if (c >= p.nChunks) return;                           // the whole warp leaves together
     const int4 ch = p.chunks[c];
-    const int B = p.B, nq = p.h.nq, d = ch.z;
-    double* row = p.part + (size_t) c * nq * 3 * B;
-    for (int j = lane; j < nq * 3 * B; j += 32) row[j] = 0.0;
+    int* row = p.rows + (size_t) c * p.B;
+    for (int j = lane; j < p.B; j += 32) row[j] = 0;
     __syncwarp();
     for (int base = ch.x; base < ch.y; base += 32) {
         const int i = base + lane;
         const int b = i < ch.y ? p.binOf[i] : -1;
         const unsigned grp = __match_any_sync(0xffffffffu, b);
-        const bool lead = b >= 0 && __ffs(grp) - 1 == lane;
-        for (int k = 0; k < nq; ++k) {
-            double s1 = 0.0, s2 = 0.0, r = 0.0;
-            if (b >= 0) {
-                const double v = p.val[(size_t) k * p.n + i];
-                bool keep = true;
-                if (pass > 0) {
-                    const size_t g = ((size_t) k * p.D + d) * B + b;
-                    const double newCount = (double) p.counts[(size_t) d * B + b] - p.rem[g];
-                    const double ave = p.sum[g] / newCount;
-                    keep = fabs(ave - v) < p.cut[k] * p.var[g];
-                }
-                if (keep) {
-                    s1 = v;
-                    s2 = v * v;
-                } else {
-                    r = 1.0;
-                }
-            }
-            stage[w][0][lane] = s1;
-            stage[w][1][lane] = s2;
-            stage[w][2][lane] = r;
-            __syncwarp();
-            if (lead) {
-                double a1 = 0.0, a2 = 0.0, a3 = 0.0;
-                for (unsigned m = grp; m; m &= m - 1) {
-                    const int j = __ffs(m) - 1;
-                    a1 += stage[w][0][j];
-                    a2 += stage[w][1][j];
-                    a3 += stage[w][2][j];
-                }
-                double* rk = row + (size_t) k * 3 * B;
-                rk[b] += a1;
-                rk[B + b] += a2;
-                rk[2 * B + b] += a3;
-            }
-            __syncwarp();
+        if (b >= 0 && __ffs(grp) - 1 == lane) row[b] += __popc(grp);
+        __syncwarp();
+    }
+}
+
+// One block: segStart = exclusive prefix of the counts over (dwarf, bin); then, per (dwarf,
+// bin), the chunk rows become the first list entry of each chunk's bodies of that bin.
+__global__ void k_bin_offsets(NbHistPlan p)
+{
+    __shared__ int carry;
+    const int DB = p.D * p.B;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < DB; base += blockDim.x) {
+        const int t = base + threadIdx.x;
+        const int v = t < DB ? (int) p.counts[t] : 0;
+        // block-wide inclusive scan of v (Hillis-Steele in shared memory)
+        __shared__ int sc[1024];
+        sc[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < blockDim.x; o <<= 1) {
+            const int u = threadIdx.x >= o ? sc[threadIdx.x - o] : 0;
+            __syncthreads();
+            sc[threadIdx.x] += u;
+            __syncthreads();
+        }
+        if (t < DB) p.segStart[t] = carry + sc[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += sc[threadIdx.x];
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < DB; t += blockDim.x) {
+        const int d = t / p.B, b = t - d * p.B;
+        int acc = p.segStart[t];
+        for (int c = p.chunkFirst[d]; c < p.chunkFirst[d + 1]; ++c) {
+            int* r = p.rows + (size_t) c * p.B + b;
+            const int k = *r;
+            *r = acc;
+            acc += k;
         }
     }
 }
 
-// The rows of a dwarf's chunks added in chunk order, then nbCalcDisp
-// (nbody/src/nbody_mass.c:190-244): a bin with more than 10 kept bodies gets its dispersion
-// (corrected after an outlier pass) and its error; other bins keep their previous values.
-__global__ void k_hist_finalize(NbHistPlan p, int initial)
+// Every chunk places its binned bodies: a body goes to its bin's next list entry, lanes of one
+// bin in lane order, batches in order -- so each bin's list is in body order.
+__global__ void __launch_bounds__(HW * 32) k_bin_scatter(NbHistPlan p)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int c = blockIdx.x * HW + w;
+    if (c >= p.nChunks) return;
+    const int4 ch = p.chunks[c];
+    int* row = p.rows + (size_t) c * p.B;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int base = ch.x; base < ch.y; base += 32) {
+        const int i = base + lane;
+        const int b = i < ch.y ? p.binOf[i] : -1;
+        const unsigned grp = __match_any_sync(0xffffffffu, b);
+        int at = 0;
+        if (b >= 0) at = row[b];
+        __syncwarp();
+        if (b >= 0) {
+            p.list[at + __popc(grp & lt)] = i;
+            if (__ffs(grp) - 1 == lane) row[b] = at + __popc(grp);
+        }
+        __syncwarp();
+    }
+}
+
+// The dispersions of one (quantity, dwarf, bin) per thread: the initial sums over the bin's
+// bodies, then IterMax passes of nbRemoveOutliers (nbody/src/nbody_mass.c:246-316: a body is
+// kept if |bin mean - value| < cut-off x bin dispersion, mean and dispersion of the previous
+// pass), each followed by nbCalcDisp (:190-244: a bin with more than 10 kept bodies gets its
+// dispersion, corrected after an outlier pass, and its error; other bins keep their previous
+// values).  Values are added in body order, as the reference adds them.
+__global__ void k_disp_bins(NbHistPlan p)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int B = p.B, nq = p.h.nq;
     if (t >= nq * p.D * B) return;
-    const int k = t / (p.D * B), r = t - k * p.D * B, d = r / B, b = r - d * B;
-    double s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    for (int c = p.chunkFirst[d]; c < p.chunkFirst[d + 1]; ++c) {
-        const double* rk = p.part + ((size_t) c * nq + k) * 3 * B;
-        s1 += rk[b];
-        s2 += rk[B + b];
-        s3 += rk[2 * B + b];
+    const int k = t / (p.D * B), r = t - k * p.D * B;
+    const int first = p.segStart[r];
+    const unsigned raw = p.counts[r];
+    const double* val = p.val + (size_t) k * p.n;
+    const double cut = p.cut[k], corr = p.corr[k];
+    double sum = 0.0, sq = 0.0, rem = 0.0, var = 0.0, err = 0.0;
+    for (int pass = 0; pass <= p.iterMax; ++pass) {
+        double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        if (pass == 0) {
+            for (unsigned j = 0; j < raw; ++j) {
+                const double v = val[p.list[first + j]];
+                s1 += v;
+                s2 += v * v;
+            }
+        } else {
+            const double newCount = (double) raw - rem;
+            const double ave = sum / newCount;
+            for (unsigned j = 0; j < raw; ++j) {
+                const double v = val[p.list[first + j]];
+                if (fabs(ave - v) < cut * var) {
+                    s1 += v;
+                    s2 += v * v;
+                } else {
+                    s3 += 1.0;
+                }
+            }
+        }
+        sum = s1;
+        sq = s2;
+        rem = s3;
+        double count = (double) raw;
+        count -= rem;
+        if (count > 10.0) {
+            const double n_new = count - 1.0;
+            const double n_ratio = count / n_new;
+            const double mean = sum / count;
+            double dispsq = (sq / n_new) - n_ratio * (mean * mean);
+            if (pass > 0) dispsq *= corr;
+            var = sqrt(dispsq);
+            err = sqrt((count + 1) / (count * n_new)) * var;
+        }
     }
-    p.sum[t] = s1;
-    p.sq[t] = s2;
-    p.rem[t] = s3;
-    double count = (double) p.counts[(size_t) d * B + b];
-    count -= s3;
-    if (count > 10.0) {
-        const double n_new = count - 1.0;
-        const double n_ratio = count / n_new;
-        const double mean = s1 / count;
-        double dispsq = (s2 / n_new) - n_ratio * (mean * mean);
-        if (!initial) dispsq *= p.corr[k];
-        const double v = sqrt(dispsq);
-        p.var[t] = v;
-        p.err[t] = sqrt((count + 1) / (count * n_new)) * v;
-    }
+    p.sum[t] = sum;
+    p.sq[t] = sq;
+    p.rem[t] = rem;
+    p.var[t] = var;
+    p.err[t] = err;
 }
 
 // Bin b of the simulated histogram comp + 1 (1..7) of dwarf d: the dispersions (1, 2) as
@@ -384,7 +435,7 @@ __global__ void k_likelihood(NbHistPlan p, const double* __restrict__ mass,
         emd = cost * ((double) dataRange / (1.0 * nData));
         emd = emd * (double) (nData / dataRange);       // integer division, as the reference
         emd = round(emd * 1.0e9) * 1.0e-9;
-        emdComp = emd > 50.0 ? NAN : -(300.0 * log(1.0 - emd / 50.0));
+        emdComp = emd > 50.0 ? NAN : -(300.0 * nb_log_rn(1.0 - emd / 50.0));   // mw_log
     }
     double costComp;
     if (nSimU == 0 || nData == 0) {
@@ -541,18 +592,19 @@ static inline int nb_l_grid(int n, int threads, int cap)
     return g < cap ? g : cap;
 }
 
-// Bodies per chunk: 1024, more when the chunk rows would exceed 64 MB.
+// Bodies per chunk: 1024, more when the chunk rows (B ints each) would exceed 64 MB.
 size_t nb_hist_chunk_bodies(int n, int nq, int B)
 {
-    const double rowBytes = 8.0 * 3.0 * (double) (nq > 0 ? nq : 1) * (double) B;
+    (void) nq;
+    const double rowBytes = 4.0 * (double) B;
     size_t ch = 1024;
     const double limit = 64.0 * 1024.0 * 1024.0;
     while ((double) n / (double) ch * rowBytes > limit) ch *= 2;
     return ch;
 }
 
-// Counts, totals and per-body quantities, then the initial dispersions and iterMax outlier
-// passes.  Returns the number of kernel launches.
+// Counts, totals and per-body quantities, then (with quantities to bin) the per-bin lists and
+// the dispersions with their iterMax outlier passes.  Returns the number of kernel launches.
 int nb_launch_hist_plan(const NbHistPlan& p, const double* px, const double* py, const double* pz,
                         const double* vx, const double* vy, const double* vz, const int* types,
                         const int* bodyDwarf, int numSMs, cudaStream_t s)
@@ -570,16 +622,13 @@ int nb_launch_hist_plan(const NbHistPlan& p, const double* px, const double* py,
         ++launches;
     }
     if (p.h.nq > 0 && p.n > 0) {
+        const int chunkBlocks = (p.nChunks + HW - 1) / HW;
         const size_t Q = (size_t) p.h.nq * DB;
-        cudaMemsetAsync(p.var, 0, sizeof(double) * Q, s);
-        cudaMemsetAsync(p.err, 0, sizeof(double) * Q, s);
-        const int passBlocks = (p.nChunks + HW - 1) / HW;
-        const int finBlocks = (int) ((Q + 127) / 128);
-        for (int pass = 0; pass <= p.iterMax; ++pass) {
-            k_hist_pass<<<passBlocks, HW * 32, 0, s>>>(p, pass);
-            k_hist_finalize<<<finBlocks, 128, 0, s>>>(p, pass == 0);
-            launches += 2;
-        }
+        k_bin_rows<<<chunkBlocks, HW * 32, 0, s>>>(p);
+        k_bin_offsets<<<1, 1024, 0, s>>>(p);
+        k_bin_scatter<<<chunkBlocks, HW * 32, 0, s>>>(p);
+        k_disp_bins<<<(int) ((Q + 127) / 128), 128, 0, s>>>(p);
+        launches += 4;
     }
     nb_count_launch(launches);
     return launches;

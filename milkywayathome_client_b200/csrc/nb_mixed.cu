@@ -98,13 +98,18 @@ constexpr int NB_GROUP_STACK = 16384;     // >= 256 x 63 + 32
 // the lane that appends an entry forms (hi - centre) + lo once, so an interaction costs each
 // body one subtraction per coordinate.  Cell entry: {rel, mass} {qxx, qxy, qxz, qyy}
 // {qyz, qzz, -, -}; body entry: {rel, mass}.
-template <int LIST_CAP> struct CellList { float4 a[LIST_CAP], b[LIST_CAP], c[LIST_CAP]; };
-template <int LIST_CAP> struct BodyList { float4 a[LIST_CAP]; };
+// use[q][e]: the lanes whose body q takes entry e (all lanes, except in the exact-set walk).
+template <int LIST_CAP> struct CellList {
+    float4 a[LIST_CAP], b[LIST_CAP], c[LIST_CAP];
+    unsigned use[2][LIST_CAP];
+};
+template <int LIST_CAP> struct BodyList { float4 a[LIST_CAP]; unsigned use[2][LIST_CAP]; };
 
 // Evaluation of a full list by the 32 lanes, each for its BPL bodies (entries read once as
 // shared-memory broadcasts and used for every body of the lane).
-template <int LIST_CAP, int BPL>
-__device__ __forceinline__ void nb_eval_bodies(const BodyList<LIST_CAP>& list, int n,
+// MASKED (the exact-set walk): lanes outside an entry's use mask take it with mass 0.
+template <int LIST_CAP, int BPL, bool MASKED>
+__device__ __forceinline__ void nb_eval_bodies(const BodyList<LIST_CAP>& list, int n, int lane,
                                                const float (&rb)[BPL][3], float eps2,
                                                float (&f)[BPL][3])
 {
@@ -112,10 +117,11 @@ __device__ __forceinline__ void nb_eval_bodies(const BodyList<LIST_CAP>& list, i
         const float4 a = list.a[e];
 #pragma unroll
         for (int q = 0; q < BPL; ++q) {
+            const float m = MASKED ? ((list.use[q][e] >> lane) & 1u ? a.w : 0.f) : a.w;
             const float dx = a.x - rb[q][0], dy = a.y - rb[q][1], dz = a.z - rb[q][2];
             const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
             const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
-            const float mor3 = a.w * rinv * rinv * rinv;
+            const float mor3 = m * rinv * rinv * rinv;
             f[q][0] = fmaf(mor3, dx, f[q][0]);
             f[q][1] = fmaf(mor3, dy, f[q][1]);
             f[q][2] = fmaf(mor3, dz, f[q][2]);
@@ -123,8 +129,8 @@ __device__ __forceinline__ void nb_eval_bodies(const BodyList<LIST_CAP>& list, i
     }
 }
 
-template <int LIST_CAP, int BPL>
-__device__ __forceinline__ void nb_eval_cells(const CellList<LIST_CAP>& list, int n,
+template <int LIST_CAP, int BPL, bool MASKED>
+__device__ __forceinline__ void nb_eval_cells(const CellList<LIST_CAP>& list, int n, int lane,
                                               const float (&rb)[BPL][3], float eps2, bool useQuad,
                                               float (&f)[BPL][3])
 {
@@ -134,11 +140,13 @@ __device__ __forceinline__ void nb_eval_cells(const CellList<LIST_CAP>& list, in
         if (useQuad) { b = list.b[e]; c = list.c[e]; }
 #pragma unroll
         for (int q = 0; q < BPL; ++q) {
+            const float take = MASKED ? ((list.use[q][e] >> lane) & 1u ? 1.f : 0.f) : 1.f;
+            const float m = a.w * take;
             const float dx = a.x - rb[q][0], dy = a.y - rb[q][1], dz = a.z - rb[q][2];
             const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
             const float rinv = rsqrtf(r2);
             const float rinv2 = rinv * rinv;
-            const float mor3 = a.w * rinv * rinv2;
+            const float mor3 = m * rinv * rinv2;
             f[q][0] = fmaf(mor3, dx, f[q][0]);
             f[q][1] = fmaf(mor3, dy, f[q][1]);
             f[q][2] = fmaf(mor3, dz, f[q][2]);
@@ -148,7 +156,7 @@ __device__ __forceinline__ void nb_eval_cells(const CellList<LIST_CAP>& list, in
                 const float qdy = fmaf(qyz, dz, fmaf(qyy, dy, qxy * dx));
                 const float qdz = fmaf(qzz, dz, fmaf(qyz, dy, qxz * dx));
                 const float drQdr = fmaf(qdz, dz, fmaf(qdy, dy, qdx * dx));
-                const float dr5inv = rinv2 * rinv2 * rinv;
+                const float dr5inv = rinv2 * rinv2 * rinv * take;
                 const float phiQ = 2.5f * dr5inv * drQdr * rinv2;
                 f[q][0] = fmaf(phiQ, dx, fmaf(-dr5inv, qdx, f[q][0]));
                 f[q][1] = fmaf(phiQ, dy, fmaf(-dr5inv, qdy, f[q][1]));
@@ -224,7 +232,7 @@ __global__ void k_groups(const int2* __restrict__ nodeLink, const int2* __restri
 // FOREST: a group belongs to one dwarf; its warp walks that dwarf's tree from its root,
 // with the dwarf's softening and time step.  BPL: bodies per lane (groups of up to 32 BPL
 // bodies; each lane walks for bodies lane and lane + 32).
-template <bool COUNT, bool FOREST, int LIST_CAP, int BPL>
+template <bool COUNT, bool FOREST, int LIST_CAP, int BPL, bool EXACT>
 __global__ void __launch_bounds__(GROUP_THREADS)
 k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeLo,
              const float4* __restrict__ nodeQ32, const int4* __restrict__ child8,
@@ -241,7 +249,9 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     CellList<LIST_CAP>& cells = sCells[warp];
     BodyList<LIST_CAP>& bodies = sBodies[warp];
-    int* stack = stacks + (size_t) (blockIdx.x * GROUP_WARPS + warp) * NB_GROUP_STACK;
+    int* stack = stacks + (size_t) (blockIdx.x * GROUP_WARPS + warp) * (3 * NB_GROUP_STACK);
+    // covered-lanes masks of every stack entry, one array per body slot
+    unsigned* stackCover = reinterpret_cast<unsigned*>(stack + NB_GROUP_STACK);
     const unsigned ltMask = (1u << lane) - 1u;
     const int nGroups = sc->nGroups;
     double4 root = nodePM[0];
@@ -305,33 +315,89 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
             acc[q][0] = acc[q][1] = acc[q][2] = 0.0;
         }
         int nC = 0, nB = 0;
-        if (lane == 0) stack[0] = rootNode;      // the (dwarf's) root
+        // exact-set walk: lanes without a body count as covered from the start
+        unsigned cover0[BPL];
+#pragma unroll
+        for (int q = 0; q < BPL; ++q) cover0[q] = ~__ballot_sync(NB_FULL_MASK, valid[q]);
+        if (lane == 0) {
+            stack[0] = rootNode;                 // the (dwarf's) root
+            if (EXACT)
+                for (int q = 0; q < BPL; ++q) stackCover[q * NB_GROUP_STACK] = cover0[q];
+        }
         int top = 1;
         __syncwarp();
         while (top > 0) {
             const int take = min(32, top);
             const int base = top - take;
             const int k = lane < take ? stack[base + lane] : -1;
+            // lanes that already took an ancestor of this node (exact-set walk)
+            unsigned cover[BPL];
+#pragma unroll
+            for (int q = 0; q < BPL; ++q)
+                cover[q] = EXACT && k >= 0 ? stackCover[q * NB_GROUP_STACK + base + lane] : 0u;
             top = base;
             float4 hi = make_float4(0.f, 0.f, 0.f, 0.f), lo = hi;
-            bool isBody = false, accCell = false, openCell = false;
+            bool isBody = false, accCell = false, openCell = false, boundary = false;
             if (k >= 0) {
                 hi = nodeHi[k];
                 lo = nodeLo[k];
                 isBody = hi.w == -inf;          // bodies carry rcrit2 = -inf
                 if (!isBody) {
-                    const float ddx = fmaxf(fabsf((hi.x + lo.x) - cx) - hx, 0.f);
-                    const float ddy = fmaxf(fabsf((hi.y + lo.y) - cy) - hy, 0.f);
-                    const float ddz = fmaxf(fabsf((hi.z + lo.z) - cz) - hz, 0.f);
+                    const float ox = fabsf((hi.x + lo.x) - cx), oy = fabsf((hi.y + lo.y) - cy);
+                    const float oz = fabsf((hi.z + lo.z) - cz);
+                    const float ddx = fmaxf(ox - hx, 0.f);
+                    const float ddy = fmaxf(oy - hy, 0.f);
+                    const float ddz = fmaxf(oz - hz, 0.f);
                     const float d2 = fmaf(ddz, ddz, fmaf(ddy, ddy, ddx * ddx));
                     accCell = d2 >= hi.w;
                     openCell = !accCell;
+                    if (EXACT && openCell) {
+                        // some body of the group may still accept it: its farthest corner does
+                        const float fx = ox + hx, fy = oy + hy, fz = oz + hz;
+                        boundary = fmaf(fz, fz, fmaf(fy, fy, fx * fx)) >= hi.w;
+                    }
                 }
             }
+            const float4 rel = make_float4((hi.x - cx) + lo.x, (hi.y - cy) + lo.y,
+                                           (hi.z - cz) + lo.z, lo.w);
+            // exact-set walk: use = the lanes that take this node.  An accepted cell or a body
+            // is taken by every lane not yet covered; a cell the group opens is taken by the
+            // lanes whose own body test (|CoM - x|^2 >= rcrit2, nbody/src/nbody_grav.c:58)
+            // passes, and its subtree is then skipped for them -- each lane gets exactly its
+            // body's interaction set.
+            unsigned use[BPL];
+            bool anyUse = false, allCovered = true;
+#pragma unroll
+            for (int q = 0; q < BPL; ++q) use[q] = EXACT && openCell ? 0u : ~cover[q];
+            if (EXACT) {
+                unsigned bm = __ballot_sync(NB_FULL_MASK, boundary);
+                while (bm) {
+                    const int j = __ffs(bm) - 1;
+                    bm &= bm - 1;
+                    const float qx = __shfl_sync(NB_FULL_MASK, rel.x, j);
+                    const float qy = __shfl_sync(NB_FULL_MASK, rel.y, j);
+                    const float qz = __shfl_sync(NB_FULL_MASK, rel.z, j);
+                    const float rc2 = __shfl_sync(NB_FULL_MASK, hi.w, j);
+#pragma unroll
+                    for (int q = 0; q < BPL; ++q) {
+                        const float ex = qx - rb[q][0], ey = qy - rb[q][1], ez = qz - rb[q][2];
+                        const unsigned pass = __ballot_sync(
+                            NB_FULL_MASK, fmaf(ez, ez, fmaf(ey, ey, ex * ex)) >= rc2);
+                        if (lane == j) use[q] = pass & ~cover[q];
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < BPL; ++q) {
+                    anyUse |= use[q] != 0u;
+                    allCovered &= (cover[q] | use[q]) == 0xffffffffu;
+                }
+                if (openCell && allCovered) openCell = false;      // every body is covered
+            }
+            const bool addCell = accCell || (EXACT && boundary && anyUse);
             int4 c0 = make_int4(-1, -1, -1, -1), c1 = c0;
             if (openCell) { c0 = child8[2 * (size_t) k]; c1 = child8[2 * (size_t) k + 1]; }
             const unsigned bodyMask = __ballot_sync(NB_FULL_MASK, isBody);
-            const unsigned cellMask = __ballot_sync(NB_FULL_MASK, accCell);
+            const unsigned cellMask = __ballot_sync(NB_FULL_MASK, addCell);
             if (COUNT) {
                 ++cSteps;
                 cVisit += 32ull * (unsigned) __popc(__ballot_sync(NB_FULL_MASK, k >= 0));
@@ -339,7 +405,7 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
                 cBC += 32ull * __popc(cellMask);
             }
             if (nB + __popc(bodyMask) > LIST_CAP) {
-                nb_eval_bodies<LIST_CAP, BPL>(bodies, nB, rb, eps2, f);
+                nb_eval_bodies<LIST_CAP, BPL, EXACT>(bodies, nB, lane, rb, eps2, f);
                 nB = 0;
                 __syncwarp();
                 // near-field terms are large and cancel: add every list's partial sum into FP64
@@ -351,7 +417,7 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
                 }
             }
             if (nC + __popc(cellMask) > LIST_CAP) {
-                nb_eval_cells<LIST_CAP, BPL>(cells, nC, rb, eps2, useQuad, f);
+                nb_eval_cells<LIST_CAP, BPL, EXACT>(cells, nC, lane, rb, eps2, useQuad, f);
                 nC = 0;
                 __syncwarp();
 #pragma unroll
@@ -361,15 +427,20 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
                     f[q][0] = f[q][1] = f[q][2] = 0.f;
                 }
             }
-            const float4 rel = make_float4((hi.x - cx) + lo.x, (hi.y - cy) + lo.y,
-                                           (hi.z - cz) + lo.z, lo.w);
-            if (isBody) bodies.a[nB + __popc(bodyMask & ltMask)] = rel;
-            if (accCell) {
+            if (isBody) {
+                const int e = nB + __popc(bodyMask & ltMask);
+                bodies.a[e] = rel;
+                if (EXACT)
+                    for (int q = 0; q < BPL; ++q) bodies.use[q][e] = use[q];
+            }
+            if (addCell) {
                 const int e = nC + __popc(cellMask & ltMask);
                 const float4 qa = nodeQ32[2 * (size_t) k], qb = nodeQ32[2 * (size_t) k + 1];
                 cells.a[e] = rel;
                 cells.b[e] = qa;
                 cells.c[e] = qb;
+                if (EXACT)
+                    for (int q = 0; q < BPL; ++q) cells.use[q][e] = use[q];
             }
             nB += __popc(bodyMask);
             nC += __popc(cellMask);
@@ -391,19 +462,24 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
             const int cl[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
 #pragma unroll
             for (int m = 0; m < 8; ++m)
-                if (cl[m] >= 0) stack[w++] = cl[m];
+                if (cl[m] >= 0) {
+                    if (EXACT)
+                        for (int q = 0; q < BPL; ++q)
+                            stackCover[q * NB_GROUP_STACK + w] = cover[q] | use[q];
+                    stack[w++] = cl[m];
+                }
             top += total;
             __syncwarp();
         }
         __syncwarp();
-        nb_eval_bodies<LIST_CAP, BPL>(bodies, nB, rb, eps2, f);
+        nb_eval_bodies<LIST_CAP, BPL, EXACT>(bodies, nB, lane, rb, eps2, f);
 #pragma unroll
         for (int q = 0; q < BPL; ++q) {
             acc[q][0] += (double) f[q][0]; acc[q][1] += (double) f[q][1];
             acc[q][2] += (double) f[q][2];
             f[q][0] = f[q][1] = f[q][2] = 0.f;
         }
-        nb_eval_cells<LIST_CAP, BPL>(cells, nC, rb, eps2, useQuad, f);
+        nb_eval_cells<LIST_CAP, BPL, EXACT>(cells, nC, lane, rb, eps2, useQuad, f);
         __syncwarp();
 #pragma unroll
         for (int q = 0; q < BPL; ++q) {
@@ -430,9 +506,14 @@ static void nb_walk_mixed_launch(const NbTreeBuffers& b, const NbMixedBuffers& m
                                  const NbWalkParams& wp, int blocks, const NbForest& f,
                                  cudaStream_t s)
 {
-    k_walk_mixed<COUNT, FOREST, LC, BPL><<<blocks, GROUP_THREADS, 0, s>>>(
-        m.hi, m.lo, m.q32, m.child8, b.nodePM, b.sort.idxA, b.px, b.py, b.pz, b.mass, b.ax, b.ay,
-        b.az, m.stacks, m.groups, wp, b.sc, f);
+    if (m.exact)
+        k_walk_mixed<COUNT, FOREST, LC, BPL, true><<<blocks, GROUP_THREADS, 0, s>>>(
+            m.hi, m.lo, m.q32, m.child8, b.nodePM, b.sort.idxA, b.px, b.py, b.pz, b.mass, b.ax,
+            b.ay, b.az, m.stacks, m.groups, wp, b.sc, f);
+    else
+        k_walk_mixed<COUNT, FOREST, LC, BPL, false><<<blocks, GROUP_THREADS, 0, s>>>(
+            m.hi, m.lo, m.q32, m.child8, b.nodePM, b.sort.idxA, b.px, b.py, b.pz, b.mass, b.ax,
+            b.ay, b.az, m.stacks, m.groups, wp, b.sc, f);
 }
 
 template <bool COUNT, bool FOREST>
@@ -494,13 +575,22 @@ void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int c
 template <int LC, int BPL>
 static int nb_walk_per_sm()
 {
-    int perSM = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_walk_mixed<false, false, LC, BPL>,
+    // the fewer of the two variants' resident blocks, so one grid (and stack allocation)
+    // serves both
+    int perSM = 0, perSM2 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_walk_mixed<false, false, LC, BPL, false>,
                                                       GROUP_THREADS, 0) != cudaSuccess ||
         perSM < 1) {
         cudaGetLastError();
         perSM = 1;
     }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &perSM2, k_walk_mixed<false, false, LC, BPL, true>, GROUP_THREADS, 0) != cudaSuccess ||
+        perSM2 < 1) {
+        cudaGetLastError();
+        perSM2 = 1;
+    }
+    perSM = perSM2 < perSM ? perSM2 : perSM;
     return perSM;
 }
 
@@ -516,4 +606,5 @@ int nb_mixed_walk_blocks(int numSMs, int listCap, int groupMax)
     return perSM * numSMs;
 }
 
-size_t nb_mixed_stack_ints(int blocks) { return (size_t) blocks * GROUP_WARPS * NB_GROUP_STACK; }
+// per warp: the node stack and, beside it, the covered-lanes mask of every entry
+size_t nb_mixed_stack_ints(int blocks) { return (size_t) blocks * GROUP_WARPS * 3 * NB_GROUP_STACK; }

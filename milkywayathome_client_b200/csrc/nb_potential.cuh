@@ -3,14 +3,15 @@
 // reference's rounding.
 #pragma once
 #include "nb_common.cuh"
+#include "nb_crmath.cuh"
 
 // The halos of nbody/src/nbody_potential.c:518-625 beyond the logarithmic and NFW ones
 // (the caustic halo is not supported): triaxial logarithmic (:518-541, constants c1..c3 as
 // nbody/src/nbody_check_params.c:182-194 sets them), Allen-Santillan (:543-561),
 // Wilkinson-Evans (:563-573), NFW by mass (:575-585), Plummer (:587-592), Hernquist
 // (:594-599) and the Ninkovic special case (:601-625), in the reference's operation order.
-// Their general powers and logarithms are CUDA's (<= 2 ulp), so runs with these halos agree
-// with the reference to rounding, not bit for bit.
+// Their powers and logarithms are correctly rounded (nb_crmath.cuh), as crlibm's pow_rn and
+// log_rn in the reference, so these halos reproduce the reference bit for bit.
 __device__ __forceinline__ void nb_halo_accel_more(const NbPot& p, double x, double y, double z,
                                                    double r, double& tx, double& ty, double& tz)
 {
@@ -34,10 +35,10 @@ __device__ __forceinline__ void nb_halo_accel_more(const NbPot& p, double x, dou
         const double scaleR = r / a, scaleL = lam / a;
         double cc;
         if (r < lam) {
-            const double pw = pow(scaleR, gam - 1.0);
+            const double pw = nb_pow_rn(scaleR, gam - 1.0);
             cc = -(M / (a * r)) * pw / (1.0 + pw);
         } else {
-            cc = -(M / (r * r)) * pow(scaleL, gam) / (1.0 + pow(scaleL, gam - 1.0));
+            cc = -(M / (r * r)) * nb_pow_rn(scaleL, gam) / (1.0 + nb_pow_rn(scaleL, gam - 1.0));
         }
         c = cc / r;
         break;
@@ -50,7 +51,7 @@ __device__ __forceinline__ void nb_halo_accel_more(const NbPot& p, double x, dou
     }
     case NBCUDA_NFW_MASS_HALO: {
         const double ar = a + r;
-        c = (-M / (r * r)) * (log(ar / a) / r - 1 / ar);
+        c = (-M / (r * r)) * (nb_log_rn(ar / a) / r - 1 / ar);
         break;
     }
     case NBCUDA_PLUMMER_HALO: {
@@ -70,10 +71,10 @@ __device__ __forceinline__ void nb_halo_accel_more(const NbPot& p, double x, dou
         const double f = 4.0 * pi / 3.0 * p.haloRho0 * (a * a * a);
         const double zl3 = zl * zl * zl;
         double menc;
-        if (r > lambda) menc = f * (log(1.0 + zl3) - zl3 / (1 + zl3));
+        if (r > lambda) menc = f * (nb_log_rn(1.0 + zl3) - zl3 / (1 + zl3));
         else {
             const double z3 = zr * zr * zr;
-            menc = f * (log(1.0 + z3) - z3 / (1 + zl3));
+            menc = f * (nb_log_rn(1.0 + z3) - z3 / (1 + zl3));
         }
         c = -menc / (r * r * r);
         break;
@@ -160,7 +161,7 @@ __device__ __forceinline__ void nb_ext_accel(const NbPot& p, double x, double y,
             const double a = p.haloA;
             const double M = p.haloV * p.haloV * a / 0.2162165954;
             const double ar = a + r;
-            const double c = (-M / (r * r)) * (log(ar / a) / r - 1 / ar);
+            const double c = (-M / (r * r)) * (nb_log_rn(ar / a) / r - 1 / ar);
             tx = c * x; ty = c * y; tz = c * z;
         } else if (p.haloType != NBCUDA_NO_HALO) {
             nb_halo_accel_more(p, x, y, z, r, tx, ty, tz);
@@ -202,11 +203,11 @@ __device__ __forceinline__ double nb_ext_potential(const NbPot& p, double x, dou
     }
     if (p.haloType == NBCUDA_LOGARITHMIC_HALO) {
         const double zq = z / p.haloQz;
-        phi += p.haloV * p.haloV * log(p.haloA * p.haloA + x * x + y * y + zq * zq);
+        phi += p.haloV * p.haloV * nb_log_rn(p.haloA * p.haloA + x * x + y * y + zq * zq);
     } else if (p.haloType == NBCUDA_NFW_HALO) {
         const double a = p.haloA;
         const double M = p.haloV * p.haloV * a / 0.2162165954;
-        phi -= M * log((a + r) / a) / r;
+        phi -= M * nb_log_rn((a + r) / a) / r;
     }
     if (p.sphType == NBCUDA_HERNQUIST_SPHERICAL)
         phi -= p.sphMass / (r + p.sphScale);

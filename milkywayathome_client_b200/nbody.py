@@ -292,6 +292,12 @@ class NBodyState:
         self.check("nbSetMixedTuning", self.lib.nbSetMixedTuningCUDA(
             self._h, int(group_max), int(list_cap), int(blocks_per_sm)))
 
+    def set_mixed_mode(self, exact=True):
+        """Mixed walk interaction sets (nbSetMixedModeCUDA): exact=True (default) gives every
+        body its own FP64 interaction set; False lets a group share its box's set (faster,
+        heavier error tail)."""
+        self.check("nbSetMixedMode", self.lib.nbSetMixedModeCUDA(self._h, int(bool(exact))))
+
     def set_time_origin(self, previous_forward_time):
         """The orbiting bar's time origin (the reference's st->previousForwardTime)."""
         self.check("nbSetTimeOrigin", self.lib.nbSetTimeOriginCUDA(self._h,
@@ -566,6 +572,11 @@ class NBodyBatch:
     def set_tuning(self, group_max=32, list_cap=64, blocks_per_sm=0):
         self.check("nbBatchSetTuningCUDA", self.lib.nbBatchSetTuningCUDA(
             self._h, int(group_max), int(list_cap), int(blocks_per_sm)))
+
+    def set_mixed_mode(self, exact=True):
+        """nbBatchSetMixedModeCUDA: as NBodyState.set_mixed_mode for every dwarf."""
+        self.check("nbBatchSetMixedModeCUDA",
+                   self.lib.nbBatchSetMixedModeCUDA(self._h, int(bool(exact))))
 
     def autotune(self, ctx):
         """nbBatchAutotuneCUDA: (groupMax, listCap, blocksPerSM, walk ms) of the fastest."""

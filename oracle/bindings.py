@@ -91,6 +91,7 @@ def ref():
             "nbref_handle_ctx": (None, [_vp, _vp, _ip, _dp]),
             "nbref_run": (ctypes.c_int, [_vp]),
             "nbref_handle_run_params": (None, [_vp, _ip, _dp, _ip]),
+            "nbref_handle_like_params": (None, [_vp, _vp, _vp, _ip, _vp]),
             "nbref_likelihood": (ctypes.c_int, [_vp, _vp]),
             "nbref_pow_rn": (ctypes.c_double, [ctypes.c_double, ctypes.c_double]),
             "nbref_log_rn": (ctypes.c_double, [ctypes.c_double]),
@@ -297,6 +298,22 @@ class RefState:
         b = ctypes.c_double()
         self.lib.nbref_handle_run_params(self.h, ctypes.byref(u), ctypes.byref(b), ctypes.byref(c))
         return bool(u.value), b.value, c.value
+
+    def like_params(self):
+        """The context's likelihood settings as HistogramParams keyword arguments."""
+        flags = np.zeros(6, np.int32)
+        sig = np.zeros(8)
+        sun = np.zeros(7)
+        it = ctypes.c_int()
+        self.lib.nbref_handle_like_params(self.h, _p(flags), _p(sig), ctypes.byref(it), _p(sun))
+        names = ("useBetaDisp", "useVelDisp", "useBetaComp", "useVlos", "useDist", "usePropMot")
+        kw = {k: bool(v) for k, v in zip(names, flags)}
+        kw.update(zip(("BetaSigma", "VelSigma", "DistSigma", "PMSigma", "BetaCorrect",
+                       "VelCorrect", "DistCorrect", "PMCorrect"), (float(x) for x in sig)))
+        kw.update(zip(("sunGCDist", "sunVelx", "sunVely", "sunVelz", "NGPdec", "NGPra", "lNCP"),
+                      (float(x) for x in sun)))
+        kw["IterMax"] = it.value
+        return kw
 
     def likelihood(self):
         out = np.zeros(10)

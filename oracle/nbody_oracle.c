@@ -60,6 +60,78 @@ double or_pow_3(double x)
     return hi + lo;
 }
 
+/* ---- correctly rounded log (crlibm log_rn, the reference's mw_log) ----
+ * x = m 2^e with m in [1/sqrt(2), sqrt(2)); log(m) = 2 atanh(u), u = (m-1)/(m+1), by the
+ * series sum u^(2k+1)/(2k+1) (|u| <= 0.1716, k = 0..21) in double-double arithmetic (values
+ * hi + lo; error-free sums and fma products), plus e ln(2); rounded once. */
+typedef struct { double hi, lo; } OrDD;
+
+static OrDD or_dd(double hi, double lo) { OrDD r; r.hi = hi; r.lo = lo; return r; }
+
+static OrDD or_sum(double a, double b)              /* exact: s + e = a + b */
+{
+    double s = a + b, bb = s - a;
+    return or_dd(s, (a - (s - bb)) + (b - bb));
+}
+
+static OrDD or_fast_sum(double a, double b)         /* exact for |a| >= |b| */
+{
+    double s = a + b;
+    return or_dd(s, b - (s - a));
+}
+
+static OrDD or_add(OrDD a, OrDD b)
+{
+    OrDD s = or_sum(a.hi, b.hi), t = or_sum(a.lo, b.lo);
+    s.lo += t.hi;
+    s = or_fast_sum(s.hi, s.lo);
+    s.lo += t.lo;
+    return or_fast_sum(s.hi, s.lo);
+}
+
+static OrDD or_mul(OrDD a, OrDD b)
+{
+    double p = a.hi * b.hi;
+    double e = fma(a.hi, b.hi, -p);
+    e += a.hi * b.lo + a.lo * b.hi;
+    return or_fast_sum(p, e);
+}
+
+static OrDD or_div(OrDD a, OrDD b)
+{
+    double q1 = a.hi / b.hi, q2, q3;
+    OrDD r = or_add(a, or_mul(b, or_dd(-q1, 0.0)));
+    q2 = r.hi / b.hi;
+    r = or_add(r, or_mul(b, or_dd(-q2, 0.0)));
+    q3 = r.hi / b.hi;
+    return or_add(or_fast_sum(q1, q2), or_dd(q3, 0.0));
+}
+
+double or_log_rn(double x)
+{
+    int e = 0, k;
+    double m, f;
+    OrDD u, u2, s, lm, el;
+    if (!(x > 0.0) || isinf(x)) return log(x);
+    if (x == 1.0) return 0.0;
+    m = frexp(x, &e);
+    if (m < 0.70710678118654752440) { m *= 2.0; e -= 1; }
+    f = m - 1.0;
+    u = or_div(or_dd(f, 0.0), or_sum(m, 1.0));
+    u2 = or_mul(u, u);
+    s = or_dd(0.0, 0.0);
+    for (k = 21; k >= 0; --k) {
+        const double n = 2.0 * k + 1.0, c = 1.0 / n;   /* 1/n = c + (1 - c n)/n */
+        s = or_add(or_mul(s, u2), or_dd(c, fma(-c, n, 1.0) / n));
+    }
+    lm = or_mul(u, s);
+    lm.hi *= 2.0; lm.lo *= 2.0;
+    /* ln 2 = 0.6931471805599453094172321214581765680755... */
+    el = or_mul(or_dd(6.93147180559945286227e-01, 2.31904681384629955842e-17), or_dd((double) e, 0.0));
+    lm = or_add(el, lm);
+    return lm.hi + lm.lo;
+}
+
 /* ---- external potential: nbExtAcceleration (nbody_potential.c:627-762) ---- */
 static void or_mn_disk(double M, double a, double b, double x, double y, double z, double* o)
 {   /* miyamotoNagaiDiskAccel, nbody_potential.c:173-194 */
@@ -96,7 +168,7 @@ void or_ext_accel_one(const NBodyCudaPotential* p, const double* pos, double* ou
         const double a = p->halo.scaleLength;
         const double M = p->halo.vhalo * p->halo.vhalo * a / 0.2162165954;
         const double ar = a + r;
-        const double c = (-M / (r * r)) * (log(ar / a) / r - 1 / ar);
+        const double c = (-M / (r * r)) * (or_log_rn(ar / a) / r - 1 / ar);
         t[0] = c * x; t[1] = c * y; t[2] = c * z;
     }
     acc[0] = acc[0] + t[0]; acc[1] = acc[1] + t[1]; acc[2] = acc[2] + t[2];

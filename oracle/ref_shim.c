@@ -419,6 +419,24 @@ void nbref_handle_run_params(void* hv, int* useBestLike, double* bestLikeStart,
     *calibrationRuns = (int) h->ctx.calibrationRuns;
 }
 
+/* The likelihood settings of the handle's context: flags[6] = useBetaDisp, useVelDisp,
+ * useBetaComp, useVlos, useDist, usePropMot; sig[8] = Beta/Vel/Dist/PM sigma cut-offs, then
+ * Beta/Vel/Dist/PM corrections; *iterMax = IterMax; sun[7] = sunGCDist, sunVelx/y/z, NGPdec,
+ * NGPra, lNCP (nbody/include/nbody_types.h:455-512). */
+void nbref_handle_like_params(void* hv, int* flags, double* sig, int* iterMax, double* sun)
+{
+    RefHandle* h = (RefHandle*) hv;
+    const NBodyCtx* c = &h->ctx;
+    flags[0] = (int) c->useBetaDisp; flags[1] = (int) c->useVelDisp;
+    flags[2] = (int) c->useBetaComp; flags[3] = (int) c->useVlos;
+    flags[4] = (int) c->useDist; flags[5] = (int) c->usePropMot;
+    sig[0] = c->BetaSigma; sig[1] = c->VelSigma; sig[2] = c->DistSigma; sig[3] = c->PMSigma;
+    sig[4] = c->BetaCorrect; sig[5] = c->VelCorrect; sig[6] = c->DistCorrect; sig[7] = c->PMCorrect;
+    *iterMax = (int) c->IterMax;
+    sun[0] = c->sunGCDist; sun[1] = c->sunVelx; sun[2] = c->sunVely; sun[3] = c->sunVelz;
+    sun[4] = c->NGPdec; sun[5] = c->NGPra; sun[6] = c->lNCP;
+}
+
 /* The reference's run loop without checkpoints / best-likelihood tracking:
  * nbGravMap once, then nStep x nbStepSystem (nbody/src/nbody_plain.c:366-446). */
 int nbref_run(void* hv)

@@ -1,116 +1,122 @@
--- Single-Plummer dwarf on the Orphan-stream orbit: the set-up of the reference's golden
--- likelihood tests (nbody/tests/orphan_models/model_4.lua and model_5.lua, driven by
--- nbody/tests/RunTestUnits.lua), restated for this repository's golden checks.
--- Arguments: nbody, variant ("4": Hernquist bulge, vhalo 114, r 28.9, v (-179,106,109);
---                             "5": Plummer bulge,   vhalo 73,  r 28.6, v (-156, 79,107);
---                             "triaxial": Hernquist bulge, the triaxial halo of
---                             nbody/tests/orphan_models/model_triaxial.lua, r 29.5,
---                             v (-183,101,107);
---                             "bar": nbody/tests/orphan_models/model_bar.lua -- Hernquist
---                             bulge, lighter disk, orbiting bar, vhalo 74.61, r 28.8,
---                             v (-170,94,108), evolved to the end of the best-likelihood
---                             window with two bar-calibration runs).
--- An optional third argument holds options: "allterms" turns on every comparison of the
--- likelihood (velocity dispersion, line-of-sight velocity, beta average, distance, proper
--- motions); "bestlike" turns on the best-likelihood scan over the last 5% of the steps.
+-- Single-Plummer dwarfs on Orphan-stream orbits: the set-ups of the reference's golden
+-- likelihood tests (nbody/tests/orphan_models/model_*.lua, driven by
+-- nbody/tests/RunTestUnits.lua), restated as one table of variants for this repository's
+-- golden checks.
+-- Arguments: nbody, variant (a key of `variants` below; default "5"), options.
+--   variant "4", "5", "5b" (model_5_bounds_test), "6", "8", "9", "ninkovic", "triaxial",
+--   "newhist1".."newhist3", "bar"; each entry records its potential, dwarf, orbit and the
+--   context fields that differ between the models.
+--   options (optional): "allterms" turns on every comparison of the likelihood (velocity
+--   dispersion, line-of-sight velocity, beta average, distance, proper motions); "bestlike"
+--   turns on the best-likelihood scan over the last 5% of the steps.
 -- The seed comes from the command line (argSeed), as in the reference tests.
 
 arg = {...}
 
 seed = argSeed
 nbody = arg[1]
-variant = arg[2] or "5"
+local variantName = arg[2] or "5"
+local options = arg[3] or ""
+local allTerms = string.find(options, "allterms") ~= nil
+local bestLike = string.find(options, "bestlike") ~= nil
 
 assert(seed ~= nil, "seed argument missing")
 assert(nbody ~= nil, "body count argument missing")
 
 prng = DSFMT.create(seed)
 
-dwarfMass = 16
-dwarfRadius = 0.2
-
-local bulgeIsPlummer = (variant == "5")
-local triaxial = (variant == "triaxial")
-local bar = (variant == "bar")
-local options = arg[3] or ""
-local allTerms = string.find(options, "allterms") ~= nil
-local bestLike = string.find(options, "bestlike") ~= nil
-local haloSpeed = bulgeIsPlummer and 73 or 114
-local orbitR = bulgeIsPlummer and 28.6 or 28.9
-local orbitV = bulgeIsPlummer and { -156, 79, 107 } or { -179, 106, 109 }
-if triaxial then
-   orbitR = 29.5
-   orbitV = { -183, 101, 107 }
-elseif bar then
-   orbitR = 28.8
-   orbitV = { -170, 94, 108 }
+-- potential components, built on demand
+local function hernquist(m, a) return function() return Spherical.hernquist{ mass = m, scale = a } end end
+local function plummer(m, a) return function() return Spherical.plummer{ mass = m, scale = a } end end
+local function mn(m, a, b)
+   return function() return Disk.miyamotoNagai{ mass = m, scaleLength = a, scaleHeight = b } end
+end
+local function logHalo(v, d, q)
+   return function() return Halo.logarithmic{ vhalo = v, scaleLength = d, flattenZ = q } end
 end
 
--- The best-likelihood window: evolve to its end, (2 - start) * 3.945 Gyr, and start the
--- likelihood scan at start / (2 - start) of that (the bar model's window starts at 0.95).
-local windowStart = 0.95
-local evolveTime = bar and (2.0 - windowStart) * 3.945 or 3.945
+local windowStart = 0.95          -- the bar model's best-likelihood window starts here
+
+local variants = {
+   ["4"] = { bulge = hernquist(1.52954402E5, 0.7), disk = mn(4.45865888E5, 6.5, 0.26),
+             halo = logHalo(114, 12, 1), eps2Kind = 1, r = 28.9, v = { -179, 106, 109 } },
+   ["5"] = { bulge = plummer(1.52954402E5, 0.7), disk = mn(4.45865888E5, 6.5, 0.26),
+             halo = logHalo(73, 12, 1), eps2Kind = 1, r = 28.6, v = { -156, 79, 107 } },
+   ["5b"] = { bulge = plummer(1.52954402E5, 0.7), disk = mn(4.45865888E5, 6.5, 0.26),
+              halo = logHalo(73, 12, 1), eps2Kind = 1, r = 28.6, v = { -156, 79, 107 },
+              dwarfMass = 1, dwarfRadius = 0.05, timeEvolve = 4.132339410448132,
+              tstop = 4.291337464901487 },
+   ["6"] = { bulge = plummer(1.52954402E5, 0.7), disk = mn(4.45865888E5, 6.5, 0.26),
+             halo = function() return Halo.nfw{ vhalo = 155, scaleLength = 22.25 } end,
+             eps2Kind = 0, r = 28.9, v = { -178, 106, 108 } },
+   ["8"] = { bulge = plummer(4.0373214139267E4, 0.249), disk = mn(3.2340408839019E5, 3.67, 0.305),
+             halo = function()
+                return Halo.allenSantillan{ mass = 4.7276406194167E4, scaleLength = 1.52,
+                                            lambda = 200.0, gamma = 2.0 }
+             end,
+             eps2Kind = 0, r = 28.9, v = { -179, 106, 109 } },
+   ["9"] = { bulge = plummer(14852.322299938, 0.25), disk = mn(285750.313545277, 5.16, 0.311),
+             halo = function()
+                return Halo.wilkinsonEvans{ mass = 2570079.320803279, scaleLength = 64.3 }
+             end,
+             eps2Kind = 1, r = 28.9, v = { -179, 106, 109 } },
+   ["ninkovic"] = { bulge = hernquist(1.52954402E5, 0.7), disk = mn(4.45865888E5, 6.5, 0.26),
+                    halo = function()
+                       return Halo.ninkovic{ rho0 = 23.6, scaleLength = 17.0, lambda = 93.6 }
+                    end,
+                    eps2Kind = 0, r = 28.9, v = { -179, 106, 109 } },
+   ["triaxial"] = { bulge = hernquist(1.52954402E5, 0.7), disk = mn(4.45865888E5, 6.5, 0.26),
+                    halo = function()
+                       return Halo.triaxial{ vhalo = 116, scaleLength = 16.3, flattenZ = 1.43,
+                                             flattenX = 1.26, flattenY = 1.0, triaxAngle = 96 }
+                    end,
+                    eps2Kind = 1, r = 29.5, v = { -183, 101, 107 } },
+   ["bar"] = { bulge = hernquist(1.52954402e5, 0.7), disk = mn(4.18972480e5, 6.5, 0.26),
+               disk2 = function()
+                  return Disk.orbitingBar{ mass = 2.689340798e4, scaleLength = 5.4,
+                                           patternSpeed = 250.61, startAngle = 0.488692 }
+               end,
+               halo = logHalo(74.61, 12.0, 1.0), eps2Kind = 0, r = 28.8, v = { -170, 94, 108 },
+               -- evolve to the end of the best-likelihood window, scan from its start, and
+               -- calibrate the bar's phase with two more runs
+               timeEvolve = (2.0 - windowStart) * 3.945, timeBack = 3.945,
+               useBestLike = true, bestLikeStart = windowStart / (2.0 - windowStart),
+               calibrationRuns = 2 },
+}
+-- newhist1..3: a 12-mass dwarf with the beta-average, line-of-sight and distance comparisons
+local newhist = { { 1, 53.4, 28.7, { -158, 76, 108 } }, { 0, 53.6, 28.5, { -154, 78, 109 } },
+                  { 1, 53.8, 28.9, { -159, 80, 105 } } }
+for k, h in ipairs(newhist) do
+   variants["newhist" .. k] = {
+      bulge = plummer(152954.402000, 0.7), disk = mn(445865.888000, 6.5, 0.26),
+      halo = logHalo(74.61, 12, 1), eps2Kind = h[1], b = h[2], r = h[3], v = h[4],
+      dwarfMass = 12, newhist = true }
+end
+
+local V = variants[variantName]
+assert(V ~= nil, "unknown variant " .. variantName)
+
+dwarfMass = V.dwarfMass or 16
+dwarfRadius = V.dwarfRadius or 0.2
 
 function makePotential()
-   if bar then
-      return Potential.create{
-         spherical = Spherical.hernquist{ mass = 1.52954402e5, scale = 0.7 },
-         disk      = Disk.miyamotoNagai{ mass = 4.18972480e5, scaleLength = 6.5, scaleHeight = 0.26 },
-         disk2     = Disk.orbitingBar{ mass = 2.689340798e4, scaleLength = 5.4,
-                                       patternSpeed = 250.61, startAngle = 0.488692 },
-         halo      = Halo.logarithmic{ vhalo = 74.61, scaleLength = 12.0, flattenZ = 1.0 }
-      }
-   end
-   local bulge
-   if bulgeIsPlummer then
-      bulge = Spherical.plummer{ mass = 1.52954402E5, scale = 0.7 }
-   else
-      bulge = Spherical.hernquist{ mass = 1.52954402E5, scale = 0.7 }
-   end
    return Potential.create{
-      spherical = bulge,
-      disk      = Disk.miyamotoNagai{ mass = 4.45865888E5, scaleLength = 6.5, scaleHeight = 0.26 },
-      disk2     = Disk.none{ mass = 3.0e5 },
-      halo      = triaxial
-                  and Halo.triaxial{ vhalo = 116, scaleLength = 16.3, flattenZ = 1.43,
-                                     flattenX = 1.26, flattenY = 1.0, triaxAngle = 96 }
-                  or Halo.logarithmic{ vhalo = haloSpeed, scaleLength = 12, flattenZ = 1 }
+      spherical = V.bulge(),
+      disk      = V.disk(),
+      disk2     = V.disk2 and V.disk2() or Disk.none{ mass = 3.0e5 },
+      halo      = V.halo()
    }
 end
 
 function makeContext()
-   if bar then
-      return NBodyCtx.create{
-         timestep        = calculateTimestep(dwarfMass, dwarfRadius),
-         timeEvolve      = evolveTime,
-         timeBack        = 3.945,
-         eps2            = calculateEps2(nbody, dwarfRadius, 0),
-         criterion       = "sw93",
-         useQuad         = true,
-         theta           = 1.0,
-         useBestLike     = true,
-         BestLikeStart   = windowStart / (2.0 - windowStart),
-         BetaSigma       = 2.5,
-         VelSigma        = 2.5,
-         DistSigma       = 2.5,
-         PMSigma         = 2.5,
-         BetaCorrect     = 1.111,
-         VelCorrect      = 1.111,
-         DistCorrect     = 1.111,
-         PMCorrect       = 1.111,
-         IterMax         = 6,
-         calibrationRuns = 2
-      }
-   end
-   return NBodyCtx.create{
+   local c = {
       timestep      = calculateTimestep(dwarfMass, dwarfRadius),
-      timeEvolve    = 3.945,
-      eps2          = calculateEps2(nbody, dwarfRadius, 1),
+      timeEvolve    = V.timeEvolve or 3.945,
+      eps2          = calculateEps2(nbody, dwarfRadius, V.eps2Kind),
       criterion     = "sw93",
       useQuad       = true,
       theta         = 1.0,
-      useBestLike   = bestLike,
-      BestLikeStart = 0.95,
+      BestLikeStart = V.bestLikeStart or 0.95,
       BetaSigma     = 2.5,
       VelSigma      = 2.5,
       DistSigma     = 2.5,
@@ -119,21 +125,37 @@ function makeContext()
       VelCorrect    = 1.111,
       DistCorrect   = 1.111,
       PMCorrect     = 1.111,
-      IterMax       = 6,
-      useVelDisp    = allTerms,
-      useBetaComp   = allTerms,
-      useVlos       = allTerms,
-      useDist       = allTerms,
-      usePropMot    = allTerms
+      IterMax       = 6
    }
+   if V.timeBack then c.timeBack = V.timeBack end
+   if V.calibrationRuns then c.calibrationRuns = V.calibrationRuns end
+   if V.useBestLike or bestLike then c.useBestLike = true end
+   if V.newhist then
+      c.b = V.b
+      c.r = V.r
+      c.vx = V.v[1]
+      c.vy = V.v[2]
+      c.vz = V.v[3]
+      c.useBetaComp = true
+      c.useVlos = true
+      c.useDist = true
+   end
+   if allTerms then
+      c.useVelDisp = true
+      c.useBetaComp = true
+      c.useVlos = true
+      c.useDist = true
+      c.usePropMot = true
+   end
+   return NBodyCtx.create(c)
 end
 
 function makeBodies(ctx, potential)
    local finalPosition, finalVelocity = reverseOrbit{
       potential = potential,
-      position  = lbrToCartesian(ctx, Vector.create(218, 53.5, orbitR)),
-      velocity  = Vector.create(orbitV[1], orbitV[2], orbitV[3]),
-      tstop     = 4.0,
+      position  = lbrToCartesian(ctx, Vector.create(218, V.b or 53.5, V.r)),
+      velocity  = Vector.create(V.v[1], V.v[2], V.v[3]),
+      tstop     = V.tstop or 4.0,
       dt        = ctx.timestep / 10.0
    }
 

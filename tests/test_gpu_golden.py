@@ -80,7 +80,7 @@ def _gpu_run_system(variant, nbody, seed, options=()):
     ctx = NBodyCtx.from_struct(c, nstep)
     init = r.get()
     mass, types = r.masses()
-    params = HistogramParams()              # makeHistogram of orphan_dwarf.lua; ctx defaults
+    params = HistogramParams(**r.like_params())   # makeHistogram of orphan_dwarf.lua + the ctx
     data = read_histogram(os.path.join(GOLDEN, "orphan_model_histogram_3"))
     with NBodyState.create(ctx, init["pos"], init["vel"], mass) as st:
         st.set_types(types)
@@ -108,6 +108,29 @@ def test_best_likelihood_scan_matches_reference_executable(tmp_path, nbody, seed
     assert use_best and calib == 0 and res["runs"] == 1
     assert res["best_count"] >= 1 and res["best_step"] >= 0.95 * nstep
     assert abs(res["result"][0] - want) < 1e-10, (res, want)
+
+
+RUN_VARIANTS = ("5b", "6", "8", "9", "ninkovic", "newhist1", "newhist2", "newhist3")
+RUN_CASES = [(v, "100", s) for v in RUN_VARIANTS for s in ("670828913", "886885833", "715144259")]
+RUN_CASES += [(v, "1024", "670828913") for v in ("4", "5", "triaxial") + RUN_VARIANTS]
+
+
+@pytest.mark.parametrize("variant,nbody,seed", RUN_CASES)
+def test_golden_likelihood_through_gpu_run_system(variant, nbody, seed):
+    """Every step and the likelihood on the GPU (nbRunSystemCUDA with the context's comparison
+    terms: the newhist models add the beta-average, line-of-sight velocity and distance
+    comparisons) against the reference's golden table.  Models 6, 8 and ninkovic evaluate
+    halos with logarithms and powers, correctly rounded on both sides, so every model here runs
+    bit for bit like the reference and the likelihood (per-bin sums in body order) equals its
+    golden value to the table's tolerance."""
+    from oracle import bindings as ob
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    with open(os.path.join(GOLDEN, "golden_likelihoods.json")) as f:
+        want = json.load(f)["models"][variant][nbody][seed]
+    res, (use_best, _, calib, _) = _gpu_run_system(variant, nbody, seed)
+    assert not use_best and res["runs"] == 1
+    assert abs(res["result"][0] - want) < 1e-10, (res["result"], want)
 
 
 BAR_CASES = [("100", s) for s in ("670828913", "886885833", "715144259")] + [("1024", "670828913")]

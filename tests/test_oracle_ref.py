@@ -146,4 +146,4 @@ def test_external_potential_equals_reference():
         assert bits_equal(ob.ext_accel(pot, pos), ob.ref_ext_accel(pot, pos))
     nfw = nbody.Potential.create(spherical=nbody.Spherical.hernquist(1.5e5, 0.7),
                                  halo=nbody.Halo.nfw(155, 22.25))
-    np.testing.assert_allclose(ob.ext_accel(nfw, pos), ob.ref_ext_accel(nfw, pos), rtol=1e-14)
+    assert bits_equal(ob.ext_accel(nfw, pos), ob.ref_ext_accel(nfw, pos))
