@@ -107,7 +107,31 @@ template <int LIST_CAP> struct BodyList { float4 a[LIST_CAP]; unsigned use[2][LI
 
 // Evaluation of a full list by the 32 lanes, each for its BPL bodies (entries read once as
 // shared-memory broadcasts and used for every body of the lane).
-// MASKED (the exact-set walk): lanes outside an entry's use mask take it with mass 0.
+// Accumulations of a masked entry: the lane adds only when its bit of the entry's use mask is
+// set (tk != 0), as predicated FMAs under one predicate.
+__device__ __forceinline__ void nb_acc_if(unsigned tk, float s, float dx, float dy, float dz,
+                                          float& fx, float& fy, float& fz)
+{
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %3, 0;\n\t"
+        "@p fma.rn.f32 %0, %4, %5, %0;\n\t@p fma.rn.f32 %1, %4, %6, %1;\n\t"
+        "@p fma.rn.f32 %2, %4, %7, %2;\n\t}"
+        : "+f"(fx), "+f"(fy), "+f"(fz)
+        : "r"(tk), "f"(s), "f"(dx), "f"(dy), "f"(dz));
+}
+// f += phiQ d - dr5inv qd under the predicate (the quadrupole term of a masked cell)
+__device__ __forceinline__ void nb_acc_quad_if(unsigned tk, float phiQ, float dx, float dy,
+                                               float dz, float ndr5, float qx, float qy, float qz,
+                                               float& fx, float& fy, float& fz)
+{
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %3, 0;\n\t"
+        "@p fma.rn.f32 %0, %8, %9, %0;\n\t@p fma.rn.f32 %0, %4, %5, %0;\n\t"
+        "@p fma.rn.f32 %1, %8, %10, %1;\n\t@p fma.rn.f32 %1, %4, %6, %1;\n\t"
+        "@p fma.rn.f32 %2, %8, %11, %2;\n\t@p fma.rn.f32 %2, %4, %7, %2;\n\t}"
+        : "+f"(fx), "+f"(fy), "+f"(fz)
+        : "r"(tk), "f"(phiQ), "f"(dx), "f"(dy), "f"(dz), "f"(ndr5), "f"(qx), "f"(qy), "f"(qz));
+}
+
+// MASKED (the exact-set walk): lanes outside an entry's use mask skip its accumulation.
 template <int LIST_CAP, int BPL, bool MASKED>
 __device__ __forceinline__ void nb_eval_bodies(const BodyList<LIST_CAP>& list, int n, int lane,
                                                const float (&rb)[BPL][3], float eps2,
@@ -117,14 +141,18 @@ __device__ __forceinline__ void nb_eval_bodies(const BodyList<LIST_CAP>& list, i
         const float4 a = list.a[e];
 #pragma unroll
         for (int q = 0; q < BPL; ++q) {
-            const float m = MASKED ? ((list.use[q][e] >> lane) & 1u ? a.w : 0.f) : a.w;
             const float dx = a.x - rb[q][0], dy = a.y - rb[q][1], dz = a.z - rb[q][2];
             const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
             const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
-            const float mor3 = m * rinv * rinv * rinv;
-            f[q][0] = fmaf(mor3, dx, f[q][0]);
-            f[q][1] = fmaf(mor3, dy, f[q][1]);
-            f[q][2] = fmaf(mor3, dz, f[q][2]);
+            const float mor3 = a.w * rinv * rinv * rinv;
+            if (MASKED) {
+                nb_acc_if(list.use[q][e] & (1u << lane), mor3, dx, dy, dz, f[q][0], f[q][1],
+                          f[q][2]);
+            } else {
+                f[q][0] = fmaf(mor3, dx, f[q][0]);
+                f[q][1] = fmaf(mor3, dy, f[q][1]);
+                f[q][2] = fmaf(mor3, dz, f[q][2]);
+            }
         }
     }
 }
@@ -140,27 +168,35 @@ __device__ __forceinline__ void nb_eval_cells(const CellList<LIST_CAP>& list, in
         if (useQuad) { b = list.b[e]; c = list.c[e]; }
 #pragma unroll
         for (int q = 0; q < BPL; ++q) {
-            const float take = MASKED ? ((list.use[q][e] >> lane) & 1u ? 1.f : 0.f) : 1.f;
-            const float m = a.w * take;
+            const unsigned tk = MASKED ? list.use[q][e] & (1u << lane) : 1u;
             const float dx = a.x - rb[q][0], dy = a.y - rb[q][1], dz = a.z - rb[q][2];
             const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
             const float rinv = rsqrtf(r2);
             const float rinv2 = rinv * rinv;
-            const float mor3 = m * rinv * rinv2;
-            f[q][0] = fmaf(mor3, dx, f[q][0]);
-            f[q][1] = fmaf(mor3, dy, f[q][1]);
-            f[q][2] = fmaf(mor3, dz, f[q][2]);
+            const float mor3 = a.w * rinv * rinv2;
+            if (MASKED) {
+                nb_acc_if(tk, mor3, dx, dy, dz, f[q][0], f[q][1], f[q][2]);
+            } else {
+                f[q][0] = fmaf(mor3, dx, f[q][0]);
+                f[q][1] = fmaf(mor3, dy, f[q][1]);
+                f[q][2] = fmaf(mor3, dz, f[q][2]);
+            }
             if (useQuad) {
                 const float qxx = b.x, qxy = b.y, qxz = b.z, qyy = b.w, qyz = c.x, qzz = c.y;
                 const float qdx = fmaf(qxz, dz, fmaf(qxy, dy, qxx * dx));
                 const float qdy = fmaf(qyz, dz, fmaf(qyy, dy, qxy * dx));
                 const float qdz = fmaf(qzz, dz, fmaf(qyz, dy, qxz * dx));
                 const float drQdr = fmaf(qdz, dz, fmaf(qdy, dy, qdx * dx));
-                const float dr5inv = rinv2 * rinv2 * rinv * take;
+                const float dr5inv = rinv2 * rinv2 * rinv;
                 const float phiQ = 2.5f * dr5inv * drQdr * rinv2;
-                f[q][0] = fmaf(phiQ, dx, fmaf(-dr5inv, qdx, f[q][0]));
-                f[q][1] = fmaf(phiQ, dy, fmaf(-dr5inv, qdy, f[q][1]));
-                f[q][2] = fmaf(phiQ, dz, fmaf(-dr5inv, qdz, f[q][2]));
+                if (MASKED) {
+                    nb_acc_quad_if(tk, phiQ, dx, dy, dz, -dr5inv, qdx, qdy, qdz, f[q][0], f[q][1],
+                                   f[q][2]);
+                } else {
+                    f[q][0] = fmaf(phiQ, dx, fmaf(-dr5inv, qdx, f[q][0]));
+                    f[q][1] = fmaf(phiQ, dy, fmaf(-dr5inv, qdy, f[q][1]));
+                    f[q][2] = fmaf(phiQ, dz, fmaf(-dr5inv, qdz, f[q][2]));
+                }
             }
         }
     }
