@@ -99,6 +99,12 @@ typedef struct {
     int precision;        /* NBCUDA_PRECISION_* (no reference counterpart) */
     int reserved;
     NBodyCudaPotential pot;
+    /* the LMC as a moving Plummer sphere (ctx->LMC, LMCDynaFric, LMCmass, LMCscale,
+     * coulomb_log); its position, velocity and the Milky Way's reflex accelerations are state
+     * (nbSetLMCCUDA) */
+    int lmc;
+    int lmcDynaFric;
+    double lmcMass, lmcScale, coulombLog;
 } NBodyCudaCtx;
 
 /* Layout of the reference's Body (nbody/include/nbody_types.h:103-125): pos is an
@@ -297,6 +303,20 @@ NBodyCudaStatus nbRunSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st,
 /* the bodies at the best likelihood of the last nbRunSystemCUDA with keepBestBodies (the
  * reference's bestLikelihoodBodyTab, nbody/src/nbody_plain.c:226-231), host arrays of 3n */
 NBodyCudaStatus nbGetBestBodiesCUDA(NBodyCudaState* st, double* pos, double* vel);
+
+/* ---- the LMC (contexts with lmc = 1) ----
+ * nbStepSystemPlain's LMC (nbody/src/nbody_plain.c:268-360): every body feels the LMC as a
+ * Plummer sphere (plummerAccel, nbody/src/nbody_potential.c:145-152) at the LMC's current
+ * position, and both half kicks of step k add the Milky Way's reflex acceleration
+ * shift[k] / shift[k + 1] to every body; the LMC itself drifts with its velocity and is kicked
+ * by the external potential plus Chandrasekhar dynamical friction (dynamicalFriction_LMC,
+ * nbody/src/nbody_friction.c:85-132, with nbExtDensity, nbody/src/nbody_density.c:250-369) and
+ * the same reflex accelerations, all on the device.  pos3/vel3 (st->LMCpos, st->LMCvel) and
+ * shift (st->shiftByLMC, nShift >= the run's nStep + 1 vectors) are what the reference's
+ * set-up (reverseOrbit_LMC, nbody/src/nbody_orbit_integrator.c:92-285) leaves. */
+NBodyCudaStatus nbSetLMCCUDA(NBodyCudaState* st, const double* pos3, const double* vel3,
+                             const double* shift, int nShift);
+NBodyCudaStatus nbGetLMCCUDA(NBodyCudaState* st, double* pos3, double* vel3);
 
 /* The bar's time origin, the reference's st->previousForwardTime (nbody/src/nbody.c:440-442):
  * the orbiting bar is evaluated at step * timestep - previousForwardTime (0 by default).

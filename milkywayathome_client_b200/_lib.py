@@ -150,7 +150,10 @@ class Ctx(ctypes.Structure):
                 ("criterion", ctypes.c_int), ("useQuad", ctypes.c_int),
                 ("allowIncest", ctypes.c_int), ("potentialType", ctypes.c_int),
                 ("precision", ctypes.c_int), ("reserved", ctypes.c_int),
-                ("pot", Potential)]
+                ("pot", Potential),
+                ("lmc", ctypes.c_int), ("lmcDynaFric", ctypes.c_int),
+                ("lmcMass", ctypes.c_double), ("lmcScale", ctypes.c_double),
+                ("coulombLog", ctypes.c_double)]
 
 
 class TreeInfo(ctypes.Structure):
@@ -213,6 +216,8 @@ SIGNATURES = [
                                        ctypes.POINTER(RunResult)]),
     ("nbGetBestBodiesCUDA", ctypes.c_int, [_vp, _vp, _vp]),
     ("nbSetMixedModeCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nbSetLMCCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int]),
+    ("nbGetLMCCUDA", ctypes.c_int, [_vp, _vp, _vp]),
     ("nbBatchSetMixedModeCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbSaveStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbRestoreStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libnbody_b200.so")
-SOURCES = ["nb_sort.cu", "nb_tree.cu", "nb_walk.cu", "nb_mixed.cu", "nb_api.cu", "nb_noalloc.cu", "nb_adjoint.cu", "nb_batch.cu", "nb_ic.cu", "nb_likelihood.cu"]
+SOURCES = ["nb_sort.cu", "nb_tree.cu", "nb_walk.cu", "nb_mixed.cu", "nb_api.cu", "nb_noalloc.cu", "nb_adjoint.cu", "nb_batch.cu", "nb_ic.cu", "nb_likelihood.cu", "nb_lmc.cu"]
 HEADERS = ["nb_common.cuh", "nb_potential.cuh", "nb_tree_util.cuh", "nb_crmath.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -96,12 +96,12 @@ __global__ void k_to_bodies(unsigned char* __restrict__ aos, const double* px, c
 // advanceVelocities alone, for a step whose force evaluation failed (the reference still
 // kicks with the previous accelerations, nbody/src/nbody_plain.c:352-353).
 __global__ void k_kick(double* vx, double* vy, double* vz, const double* ax, const double* ay,
-                       const double* az, int n, double dtHalf)
+                       const double* az, int n, double dtHalf, double sx, double sy, double sz)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        vx[i] = vx[i] + dtHalf * (ax[i] + 0.0);
-        vy[i] = vy[i] + dtHalf * (ay[i] + 0.0);
-        vz[i] = vz[i] + dtHalf * (az[i] + 0.0);
+        vx[i] = vx[i] + dtHalf * (ax[i] + sx);
+        vy[i] = vy[i] + dtHalf * (ay[i] + sy);
+        vz[i] = vz[i] + dtHalf * (az[i] + sz);
     }
 }
 
@@ -121,6 +121,7 @@ struct NbSlot {
     NbScalars sc{};
     double rsize = 0.0;
     int haveTree = 0, criterion = -1, step = 0, treeIncest = 0, valid = 0;
+    double lmc[6] = {0, 0, 0, 0, 0, 0};   // the LMC's position and velocity (LMC runs)
 };
 
 struct NBodyCudaState {
@@ -158,6 +159,8 @@ struct NBodyCudaState {
     int mixExact = 1;                   // 1: each body's own interaction set (nbSetMixedModeCUDA)
     char* histScratch = nullptr;        // histogram / likelihood buffers
     size_t histScratchBytes = 0;
+    double* lmcDev = nullptr;           // the LMC's {pos, vel} (nbSetLMCCUDA)
+    std::vector<double> lmcShift;       // shiftByLMC: 3 doubles per step
     NbSlot runStart;                    // nbRunSystemCUDA: the initial state of the runs
     NbBestDev* best = nullptr;          // nbRunSystemCUDA: device best-likelihood record
     double* keepPos = nullptr;          // bodies at the best likelihood (3n each)
@@ -267,6 +270,8 @@ static void nb_free_all(NBodyCudaState* st)
     st->histScratch = nullptr;
     cudaFree(st->runStart.mem);
     st->runStart = NbSlot{};
+    cudaFree(st->lmcDev);
+    st->lmcDev = nullptr;
     cudaFree(st->best);
     st->best = nullptr;
     cudaFree(st->keepPos);
@@ -324,6 +329,10 @@ NBodyCudaStatus nb_check_ctx(const NBodyCudaCtx* c, std::string& why)
         if (p.halo.type < NBCUDA_NO_HALO || p.halo.type > NBCUDA_NINKOVIC_HALO ||
             p.halo.type == NBCUDA_CAUSTIC_HALO) { why = "halo type"; return NBODY_UNSUPPORTED; }
     }
+    if (c->lmc && c->potentialType != NBCUDA_POTENTIAL_DEFAULT) {
+        why = "the LMC moves in the default (Milky Way) potential";
+        return NBODY_USER_ERROR;
+    }
     return NBODY_SUCCESS;
 }
 
@@ -331,6 +340,10 @@ NBodyCudaStatus nb_check_ctx(const NBodyCudaCtx* c, std::string& why)
 // Miyamoto-Nagai disks, logarithmic and NFW halos, Hernquist and Plummer bulges.
 static bool nb_pot_basic(const NBodyCudaCtx* c, std::string& why)
 {
+    if (c->lmc) {
+        why = "not implemented with an LMC";
+        return false;
+    }
     if (c->potentialType != NBCUDA_POTENTIAL_DEFAULT) return true;
     const int d2 = c->pot.disk2.type, h = c->pot.halo.type;
     if ((d2 == NBCUDA_NO_DISK || d2 == NBCUDA_MIYAMOTO_NAGAI_DISK) &&
@@ -371,6 +384,33 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
     wp.kick = kick;
     wp.n = n;
     const bool mixed = ctx->precision == NBCUDA_PRECISION_MIXED;
+    // the LMC (nbody/src/nbody_plain.c:329-360): its state, the step's reflex accelerations
+    const bool lmc = ctx->lmc != 0;
+    double shift0[3] = {0.0, 0.0, 0.0}, shift1[3] = {0.0, 0.0, 0.0};
+    if (lmc) {
+        if (!st->lmcDev) {
+            g_lastError = "an LMC context needs the LMC's state (nbSetLMCCUDA)";
+            return NBODY_USER_ERROR;
+        }
+        pot.lmc = st->lmcDev;
+        pot.lmcMass = ctx->lmcMass;
+        pot.lmcScale = ctx->lmcScale;
+        if (drift || kick) {
+            const size_t k = (size_t) st->step;
+            if (3 * (k + 2) > st->lmcShift.size()) {
+                g_lastError = "the LMC's reflex accelerations do not reach this step";
+                return NBODY_USER_ERROR;
+            }
+            for (int c = 0; c < 3; ++c) {
+                shift0[c] = st->lmcShift[3 * k + c];
+                shift1[c] = st->lmcShift[3 * (k + 1) + c];
+            }
+        }
+        for (int c = 0; c < 3; ++c) wp.shift[c] = shift1[c];
+        if (drift)                      // advancePosVel_LMC with the acceleration at its state
+            nb_launch_lmc_half(pot, st->lmcDev, 0, ctx->timestep, shift0, ctx->lmcMass,
+                               ctx->lmcDynaFric, ctx->coulombLog, s);
+    }
 
     for (int attempt = 0; attempt < 4; ++attempt) {
         // reset per-evaluation device scalars (keep rsize)
@@ -383,7 +423,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
         if (ctx->criterion == NBCUDA_EXACT) {
             if (drift) {
                 // advancePosVel without the tree: reuse the bounding-box pass for the drift
-                nb_launch_drift_only(b, n, ctx->timestep, st->numSMs, s);
+                nb_launch_drift_only(b, n, ctx->timestep, st->numSMs, s, shift0);
             }
             NB_CHECK(cudaEventRecord(st->ev0, s));
             nb_launch_direct_fp64(b.px, b.py, b.pz, b.mass, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp,
@@ -393,7 +433,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
             st->haveTree = 0;
         } else {
             nb_build_tree(b, n, ctx->criterion, ctx->theta, ctx->useQuad, drift, ctx->timestep,
-                          st->numSMs, s);
+                          st->numSMs, s, shift0);
             nb_link_and_moments(b, n, st->capNodes, ctx->criterion, ctx->theta, ctx->useQuad, s);
             NB_CHECK(cudaEventRecord(st->ev0, s));
             if (mixed) {
@@ -453,9 +493,15 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
         } else if (kick) {
             // the failed evaluation left the accelerations untouched; the reference still
             // applies advanceVelocities with them
-            k_kick<<<nb_blocks(st, n), 256, 0, s>>>(b.vx, b.vy, b.vz, b.ax, b.ay, b.az, n, wp.dtHalf);
+            k_kick<<<nb_blocks(st, n), 256, 0, s>>>(b.vx, b.vy, b.vz, b.ax, b.ay, b.az, n, wp.dtHalf,
+                                                    shift1[0], shift1[1], shift1[2]);
             nb_count_launch();
             NB_CHECK(cudaStreamSynchronize(s));
+        }
+        if (lmc && kick) {               // advanceVelocities_LMC after the bodies' kick
+            nb_launch_lmc_half(pot, st->lmcDev, 1, ctx->timestep, shift1, ctx->lmcMass,
+                               ctx->lmcDynaFric, ctx->coulombLog, s);
+            NB_CHECK(cudaGetLastError());
         }
         if (st->treeIncest)
             out |= ctx->allowIncest ? NBODY_TREE_INCEST_NONFATAL : NBODY_TREE_INCEST_FATAL;
@@ -938,6 +984,8 @@ static NBodyCudaStatus nb_save_slot(NBodyCudaState* st, NbSlot& sl)
         NB_CHECK(cudaMemcpyAsync(sl.nodeQuad, b.nodeQuad, 6 * nodes * sizeof(double), cudaMemcpyDeviceToDevice, s));
         NB_CHECK(cudaMemcpyAsync(sl.nodeDepth, b.nodeDepth, nodes * sizeof(int), cudaMemcpyDeviceToDevice, s));
     }
+    if (st->lmcDev)
+        NB_CHECK(cudaMemcpyAsync(sl.lmc, st->lmcDev, 6 * sizeof(double), cudaMemcpyDeviceToHost, s));
     NB_CHECK(cudaStreamSynchronize(s));
     sl.sc = *st->scHost;
     sl.rsize = st->rsize;
@@ -982,6 +1030,8 @@ static NBodyCudaStatus nb_restore_slot(NBodyCudaState* st, NbSlot& sl)
     *st->scHost = sl.sc;
     st->scHost->capNodes = st->capNodes;
     NB_CHECK(cudaMemcpyAsync(b.sc, st->scHost, sizeof(NbScalars), cudaMemcpyHostToDevice, s));
+    if (st->lmcDev)
+        NB_CHECK(cudaMemcpyAsync(st->lmcDev, sl.lmc, 6 * sizeof(double), cudaMemcpyHostToDevice, s));
     NB_CHECK(cudaStreamSynchronize(s));
     st->rsize = sl.rsize;
     st->haveTree = sl.haveTree;
@@ -1474,6 +1524,36 @@ NBodyCudaStatus nbSetMixedModeCUDA(NBodyCudaState* st, int exactSet)
     return NBODY_SUCCESS;
 }
 
+NBodyCudaStatus nbSetLMCCUDA(NBodyCudaState* st, const double* pos3, const double* vel3,
+                             const double* shift, int nShift)
+{
+    if (!st || !pos3 || !vel3 || !shift || nShift < 2) {
+        g_lastError = "nbSetLMCCUDA: position, velocity and >= 2 reflex accelerations needed";
+        return NBODY_USER_ERROR;
+    }
+    NB_CHECK(cudaSetDevice(st->device));
+    if (!st->lmcDev) NB_CHECK(cudaMalloc((void**) &st->lmcDev, 6 * sizeof(double)));
+    double h[6] = {pos3[0], pos3[1], pos3[2], vel3[0], vel3[1], vel3[2]};
+    NB_CHECK(cudaMemcpy(st->lmcDev, h, sizeof h, cudaMemcpyHostToDevice));
+    st->lmcShift.assign(shift, shift + 3 * (size_t) nShift);
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbGetLMCCUDA(NBodyCudaState* st, double* pos3, double* vel3)
+{
+    if (!st || !st->lmcDev) {
+        g_lastError = "nbGetLMCCUDA: no LMC set";
+        return NBODY_USER_ERROR;
+    }
+    NB_CHECK(cudaSetDevice(st->device));
+    double h[6];
+    NB_CHECK(cudaMemcpyAsync(h, st->lmcDev, sizeof h, cudaMemcpyDeviceToHost, st->stream));
+    NB_CHECK(cudaStreamSynchronize(st->stream));
+    if (pos3) { pos3[0] = h[0]; pos3[1] = h[1]; pos3[2] = h[2]; }
+    if (vel3) { vel3[0] = h[3]; vel3[1] = h[4]; vel3[2] = h[5]; }
+    return NBODY_SUCCESS;
+}
+
 NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTime)
 {
     if (!st) return NBODY_USER_ERROR;
@@ -1823,6 +1903,10 @@ static NBodyCudaStatus nb_batch_check(const NBodyCudaCtx* ctx, NBodyCudaBatch* b
     if (rc) { g_lastError = why; return rc; }
     if (ctx->criterion == NBCUDA_EXACT) {
         g_lastError = "batched dwarfs use a tree criterion";
+        return NBODY_UNSUPPORTED;
+    }
+    if (ctx->lmc) {
+        g_lastError = "batched dwarfs run without an LMC";
         return NBODY_UNSUPPORTED;
     }
     NB_CHECK(cudaSetDevice(bt->st->device));

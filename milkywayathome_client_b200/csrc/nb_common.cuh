@@ -60,11 +60,14 @@ struct NbPot {
     double haloC1, haloC2, haloC3;                     // triaxial halo constants
     double time;   // the bar's time: step * timestep (nbody/src/nbody_grav.c:141)
     int enabled;   // potentialType == DEFAULT
+    const double* lmc;          // the LMC's {pos, vel} in device memory (nullptr: no LMC)
+    double lmcMass, lmcScale;   // its Plummer sphere
 };
 
 struct NbWalkParams {
     double eps2;
     double dtHalf;
+    double shift[3];   // the Milky Way's reflex acceleration of the second half kick (LMC runs)
     int useQuad;
     int kick;      // 1: v += (a + 0) * dtHalf after the force (advanceVelocities)
     int n;
@@ -280,10 +283,15 @@ void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int c
                           cudaStream_t s, const NbForest* forest = nullptr);
 
 void nb_build_tree(NbTreeBuffers& b, int n, int criterion, double theta, int useQuad, int drift,
-                   double dt, int numSMs, cudaStream_t s);
+                   double dt, int numSMs, cudaStream_t s, const double* shift = nullptr);
 void nb_link_and_moments(NbTreeBuffers& b, int n, int capNodes, int criterion, double theta,
                          int useQuad, cudaStream_t s);
-void nb_launch_drift_only(NbTreeBuffers& b, int n, double dt, int numSMs, cudaStream_t s);
+void nb_launch_drift_only(NbTreeBuffers& b, int n, double dt, int numSMs, cudaStream_t s,
+                          const double* shift = nullptr);
+// One half of the LMC's step (nb_lmc.cu): phase 0 drifts and kicks, phase 1 kicks; shift is
+// the Milky Way's reflex acceleration of that half (3 host doubles).
+void nb_launch_lmc_half(const NbPot& p, double* lmc, int phase, double dt, const double* shift,
+                        double massLMC, int dynaFric, double coulombLog, cudaStream_t s);
 
 // Inclusive prefix sum of n ints in place; tmp needs nb_scan_tmp_ints(n) ints.
 int nb_scan_tmp_ints(int n);

@@ -1,4 +1,4 @@
-// Correctly rounded log and pow for the external potential.
+// Correctly rounded log, pow, sin, cos and atan for the external potential.
 //
 // The reference evaluates its potentials with crlibm's correctly rounded log_rn and pow_rn
 // (milkyway/include/milkyway_math_double.h:43-59: mw_log, mw_pow).  These restatements reach
@@ -181,4 +181,138 @@ NB_HD double nb_pow_rn(double x, double y)
     if (ly.hi > 709.0 || ly.hi < -708.0) return pow(x, y);   // overflow / underflow range
     const NbDD r = nb_exp_dd(ly);
     return r.hi + r.lo;
+}
+
+// ---- sin, cos, atan for the orbiting bar ------------------------------------------------
+//
+// The bar (nbody/src/nbody_potential.c:410-457) rotates positions with crlibm's atan_rn
+// (mw_atan) and the C library's sin and cos, which round correctly but for rare hard cases.
+//
+//   sin(x), cos(x): x = q pi/2 + r, |r| <= ~pi/4 (Cody and Waite's reduction with pi/2 split
+//           into four doubles, each product formed exactly), then the Taylor series of sin(r)
+//           and cos(r) to r^29 and r^28 in double-double; valid for |x| < 2^28.
+//   atan(x): one Newton step on f(y) = sin(y) - x cos(y) from the library's atan (a few
+//           ulps); f'' = -f vanishes at the root, so the step more than triples the correct
+//           bits, and f is formed from the double-double sin and cos of the start value.
+
+// pi/2 = 1.57079632679489661923132169163975144209858469968755291048747229615390820... as four
+// doubles (each the nearest double to the remainder of the previous ones)
+#define NB_PIO2_1 1.5707963267948966
+#define NB_PIO2_2 6.123233995736766e-17
+#define NB_PIO2_3 -1.4973849048591698e-33
+#define NB_PIO2_4 5.562271104316826e-50
+
+// a / d for a double d: the remainder a - q1 d formed exactly, then a second quotient digit
+NB_HD NbDD nb_dd_div_d(NbDD a, double d)
+{
+    const double q1 = a.hi / d;
+    const NbDD p = nb_two_prod(q1, d);
+    NbDD s = nb_two_sum(a.hi, -p.hi);
+    s.lo -= p.lo;
+    s.lo += a.lo;
+    const double q2 = (s.hi + s.lo) / d;
+    return nb_quick_two_sum(q1, q2);
+}
+
+// x = k pi/2 + r for |x| < 2^28: r as a double-double, q = k mod 4
+NB_HD NbDD nb_reduce_pio2(double x, int& q)
+{
+    const double k = nearbyint(x * 0.63661977236758138);     // 2/pi
+    const NbDD p1 = nb_two_prod(k, NB_PIO2_1);
+    NbDD r = nb_two_sum(x, -p1.hi);
+    r = nb_dd_add(r, nb_dd(-p1.lo, 0.0));
+    r = nb_dd_add(r, nb_two_prod(-k, NB_PIO2_2));
+    r = nb_dd_add(r, nb_two_prod(-k, NB_PIO2_3));
+    r = nb_dd_add(r, nb_dd(-k * NB_PIO2_4, 0.0));
+    q = (int) (((long long) k) & 3);
+    return r;
+}
+
+// sin(r) for |r| <= ~0.8: r (1 - r^2/(2 3) (1 - r^2/(4 5) (... (1 - r^2/(28 29)))))
+NB_HD NbDD nb_sin_dd_reduced(NbDD r)
+{
+    const NbDD r2 = nb_dd_mul(r, r);
+    NbDD t = nb_dd(1.0, 0.0);
+    for (int n = 14; n >= 1; --n)
+        t = nb_dd_add(nb_dd(1.0, 0.0), nb_dd_div_d(nb_dd_mul(r2, t), -(double) (2 * n * (2 * n + 1))));
+    return nb_dd_mul(r, t);
+}
+
+// cos(r) for |r| <= ~0.8: 1 - r^2/(1 2) (1 - r^2/(3 4) (... (1 - r^2/(27 28))))
+NB_HD NbDD nb_cos_dd_reduced(NbDD r)
+{
+    const NbDD r2 = nb_dd_mul(r, r);
+    NbDD t = nb_dd(1.0, 0.0);
+    for (int n = 14; n >= 1; --n)
+        t = nb_dd_add(nb_dd(1.0, 0.0), nb_dd_div_d(nb_dd_mul(r2, t), -(double) ((2 * n - 1) * (2 * n))));
+    return t;
+}
+
+NB_HD NbDD nb_dd_neg(NbDD a) { return nb_dd(-a.hi, -a.lo); }
+
+// sin(x) and cos(x) for |x| < 2^28 as double-doubles
+NB_HD void nb_sincos_dd(double x, NbDD& s, NbDD& c)
+{
+    int q = 0;
+    const NbDD r = nb_reduce_pio2(x, q);
+    const NbDD sr = nb_sin_dd_reduced(r), cr = nb_cos_dd_reduced(r);
+    switch (q) {
+    case 0: s = sr; c = cr; break;
+    case 1: s = cr; c = nb_dd_neg(sr); break;
+    case 2: s = nb_dd_neg(sr); c = nb_dd_neg(cr); break;
+    default: s = nb_dd_neg(cr); c = sr; break;
+    }
+}
+
+// correctly rounded sin(x); |x| >= 2^28, inf and nan go to the library's sin
+NB_HD double nb_sin_rn(double x)
+{
+    const double ax = fabs(x);
+    if (!(ax < 268435456.0)) return sin(x);
+    if (ax < 1.4901161193847656e-08) return x;        // |x| < 2^-26: x - x^3/6 rounds to x
+    NbDD s, c;
+    nb_sincos_dd(x, s, c);
+    return s.hi + s.lo;
+}
+
+// correctly rounded cos(x); |x| >= 2^28, inf and nan go to the library's cos
+NB_HD double nb_cos_rn(double x)
+{
+    const double ax = fabs(x);
+    if (!(ax < 268435456.0)) return cos(x);
+    if (ax < 7.4505805969238281e-09) return 1.0;      // |x| < 2^-27: 1 - x^2/2 rounds to 1
+    NbDD s, c;
+    nb_sincos_dd(x, s, c);
+    return c.hi + c.lo;
+}
+
+// correctly rounded atan(x) (crlibm's atan_rn)
+NB_HD double nb_atan_rn(double x)
+{
+    const double ax = fabs(x);
+    if (isnan(x)) return x + x;
+    if (ax < 7.4505805969238281e-09) return x;        // |x| < 2^-27: x - x^3/3 rounds to x
+    if (ax > 1.152921504606846976e18)                  // |x| > 2^60 and inf: pi/2 - 1/x rounds
+        return x > 0.0 ? NB_PIO2_1 : -NB_PIO2_1;      // to the double nearest pi/2
+    const double y0 = atan(x);
+    NbDD s, c;
+    nb_sincos_dd(y0, s, c);
+    const NbDD f = nb_dd_add(s, nb_dd_neg(nb_dd_mul_d(c, x)));    // sin y0 - x cos y0
+    const double fp = c.hi + x * s.hi;                            // cos y0 + x sin y0
+    return y0 + (-(f.hi + f.lo) / fp);
+}
+
+// correctly rounded sin(x) and cos(x) from one reduction
+NB_HD void nb_sincos_rn(double x, double& s, double& c)
+{
+    const double ax = fabs(x);
+    if (!(ax < 268435456.0) || ax < 1.4901161193847656e-08) {
+        s = nb_sin_rn(x);
+        c = nb_cos_rn(x);
+        return;
+    }
+    NbDD sd, cd;
+    nb_sincos_dd(x, sd, cd);
+    s = sd.hi + sd.lo;
+    c = cd.hi + cd.lo;
 }

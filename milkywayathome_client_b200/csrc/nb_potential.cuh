@@ -86,19 +86,25 @@ __device__ __forceinline__ void nb_halo_accel_more(const NbPot& p, double x, dou
 }
 
 // orbitingBarAccel (nbody/src/nbody_potential.c:410-457): the softened needle bar rotating at
-// patternSpeed, at the time p.time; atan, sin and cos are CUDA's.
-__device__ __forceinline__ void nb_bar_accel(const NbPot& p, double x, double y, double z,
+// patternSpeed, at the time p.time; atan, sin and cos correctly rounded (nb_crmath.cuh: the
+// reference's atan is crlibm's atan_rn, its sin and cos the C library's, which agree with the
+// correctly rounded values but for ~0.1 % of arguments).
+// (out of line: its double-double trigonometry would otherwise raise the register count of every
+// kernel that evaluates the potential)
+static __device__ __noinline__ void nb_bar_accel(const NbPot& p, double x, double y, double z,
                                              double& ox, double& oy, double& oz)
 {
     const double amp = p.disk2Mass, a = p.disk2A;
     const double b = 1.4, c = 1;
     const double curAngle = (p.disk2Pattern * p.time * -1) + p.disk2StartAngle;
     double Radi = sqrt(x * x + y * y);
-    double Phi = atan(y / x);
+    double Phi = nb_atan_rn(y / x);
     Phi -= curAngle;
     if (x < 0) Radi = Radi * -1;
-    const double xr = Radi * cos(Phi);
-    const double yr = Radi * sin(Phi);
+    double sPhi, cPhi;
+    nb_sincos_rn(Phi, sPhi, cPhi);
+    const double xr = Radi * cPhi;
+    const double yr = Radi * sPhi;
     const double zr = z;
     const double sq = sqrt(c * c + zr * zr);
     const double secondpart = yr * yr + (b + sq) * (b + sq);
@@ -109,7 +115,8 @@ __device__ __forceinline__ void nb_bar_accel(const NbPot& p, double x, double y,
     const double fy = -yr / 2. / Tp / Tm * (Tp + Tm - 4. * (xr * xr) / (Tp + Tm)) /
                       (yr * yr + (b + sq2) * (b + sq2));
     const double fz = fy * zr / yr * (b + sq2) / sq2;
-    const double cp = cos(curAngle), sp = sin(curAngle);
+    double sp, cp;
+    nb_sincos_rn(curAngle, sp, cp);
     ox = (cp * fx - sp * fy) * amp;
     oy = (sp * fx + cp * fy) * amp;
     oz = fz * amp;
@@ -228,17 +235,30 @@ __device__ __forceinline__ void nb_finish_body(const NbPot& pot, const NbWalkPar
     if (pot.enabled) {
         double ex, ey, ez;
         nb_ext_accel(pot, x0, y0, z0, ex, ey, ez);
-        ex = ex + (0.0 - x0) * 0.0;
-        ey = ey + (0.0 - y0) * 0.0;
-        ez = ez + (0.0 - z0) * 0.0;
+        if (pot.lmc) {
+            // plummerAccel(pos, LMCpos, LMCmass, LMCscale) (nbody/src/nbody_potential.c:145-152)
+            const double lx = pot.lmc[0], ly = pot.lmc[1], lz = pot.lmc[2];
+            const double dist = sqrt((x0 - lx) * (x0 - lx) + (y0 - ly) * (y0 - ly) +
+                                     (z0 - lz) * (z0 - lz));
+            const double tmp = sqrt(pot.lmcScale * pot.lmcScale + dist * dist);
+            const double c = pot.lmcMass / nb_pow_3(tmp);
+            ex = ex + (lx - x0) * c;
+            ey = ey + (ly - y0) * c;
+            ez = ez + (lz - z0) * c;
+        } else {
+            // without an LMC the reference adds a massless one at the origin
+            ex = ex + (0.0 - x0) * 0.0;
+            ey = ey + (0.0 - y0) * 0.0;
+            ez = ez + (0.0 - z0) * 0.0;
+        }
         accx = accx + ex; accy = accy + ey; accz = accz + ez;
     }
     ax[j] = accx; ay[j] = accy; az[j] = accz;
     if (wp.kick) {
         // advanceVelocities (nbody/src/nbody_plain.c:301-315): v += (a + acc_i1) * dtHalf
-        vx[j] = vx[j] + wp.dtHalf * (accx + 0.0);
-        vy[j] = vy[j] + wp.dtHalf * (accy + 0.0);
-        vz[j] = vz[j] + wp.dtHalf * (accz + 0.0);
+        vx[j] = vx[j] + wp.dtHalf * (accx + wp.shift[0]);
+        vy[j] = vy[j] + wp.dtHalf * (accy + wp.shift[1]);
+        vz[j] = vz[j] + wp.dtHalf * (accz + wp.shift[2]);
     }
 }
 

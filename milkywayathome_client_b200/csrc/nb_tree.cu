@@ -36,7 +36,7 @@ __global__ void k_drift_bbox(double* __restrict__ px, double* __restrict__ py, d
                              double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
                              const double* __restrict__ ax, const double* __restrict__ ay,
                              const double* __restrict__ az, int n, int drift, double dt,
-                             NbScalars* __restrict__ sc)
+                             double sx, double sy, double sz, NbScalars* __restrict__ sc)
 {
     double m = 0.0;
     const double dtHalf = 0.5 * dt;
@@ -44,9 +44,11 @@ __global__ void k_drift_bbox(double* __restrict__ px, double* __restrict__ py, d
         double x = px[i], y = py[i], z = pz[i];
         if (drift) {
             double vvx = vx[i], vvy = vy[i], vvz = vz[i];
-            vvx = vvx + dtHalf * (ax[i] + 0.0);
-            vvy = vvy + dtHalf * (ay[i] + 0.0);
-            vvz = vvz + dtHalf * (az[i] + 0.0);
+            // advancePosVel (nbody/src/nbody_plain.c:268-284): v += (a + acc_i) dt/2, acc_i
+            // the Milky Way's reflex acceleration of LMC runs (0 otherwise)
+            vvx = vvx + dtHalf * (ax[i] + sx);
+            vvy = vvy + dtHalf * (ay[i] + sy);
+            vvz = vvz + dtHalf * (az[i] + sz);
             x = x + dt * vvx;
             y = y + dt * vvy;
             z = z + dt * vvz;
@@ -414,14 +416,17 @@ static inline int nb_grid_for(int n, int threads, int cap)
 
 // Kernel sequence of nbMakeTree.  drift != 0 fuses advancePosVel into the bounding box.
 void nb_build_tree(NbTreeBuffers& b, int n, int criterion, double theta, int useQuad,
-                   int drift, double dt, int numSMs, cudaStream_t s)
+                   int drift, double dt, int numSMs, cudaStream_t s, const double* shift)
 {
+    const double sx = shift ? shift[0] : 0.0, sy = shift ? shift[1] : 0.0;
+    const double sz = shift ? shift[2] : 0.0;
     const int T = 256;
     const int gCap = numSMs * 8;
     cudaMemsetAsync(&b.sc->xyzmaxBits, 0, sizeof(unsigned long long), s);
     cudaMemsetAsync(&b.sc->nTree, 0, sizeof(int), s);
     k_drift_bbox<<<nb_grid_for(n, T, gCap), T, 0, s>>>(b.px, b.py, b.pz, b.vx, b.vy, b.vz,
-                                                       b.ax, b.ay, b.az, n, drift, dt, b.sc);
+                                                       b.ax, b.ay, b.az, n, drift, dt, sx, sy,
+                                                       sz, b.sc);
     k_root_size<<<1, 1, 0, s>>>(b.sc);
     k_keys<<<nb_grid_for(n, T, gCap), T, 0, s>>>(b.px, b.py, b.pz, b.mass, n, b.sort.keyA,
                                                  b.sort.idxA, b.sc);
@@ -456,10 +461,14 @@ void nb_link_and_moments(NbTreeBuffers& b, int n, int capNodes, int criterion, d
     nb_count_launch(2);
 }
 
-void nb_launch_drift_only(NbTreeBuffers& b, int n, double dt, int numSMs, cudaStream_t s)
+void nb_launch_drift_only(NbTreeBuffers& b, int n, double dt, int numSMs, cudaStream_t s,
+                          const double* shift)
 {
     const int T = 256;
+    const double sx = shift ? shift[0] : 0.0, sy = shift ? shift[1] : 0.0;
+    const double sz = shift ? shift[2] : 0.0;
     k_drift_bbox<<<nb_grid_for(n, T, numSMs * 8), T, 0, s>>>(b.px, b.py, b.pz, b.vx, b.vy, b.vz,
-                                                             b.ax, b.ay, b.az, n, 1, dt, b.sc);
+                                                             b.ax, b.ay, b.az, n, 1, dt, sx, sy,
+                                                             sz, b.sc);
     nb_count_launch();
 }

@@ -157,7 +157,8 @@ class NBodyCtx:
 
     def __init__(self, timestep, eps2, theta=0.0, criterion="TreeCode", useQuad=True,
                  timeEvolve=None, treeRSize=4.0, allowIncest=False, potential=None,
-                 precision="fp64"):
+                 precision="fp64", LMC=False, LMCmass=0.0, LMCscale=1.0, LMCDynaFric=False,
+                 coulomb_log=0.0):
         crit = CRITERIA[criterion.lower()] if isinstance(criterion, str) else int(criterion)
         self.nStep = 0
         if timeEvolve is not None and timeEvolve > 0.0:
@@ -173,6 +174,9 @@ class NBodyCtx:
             c.potentialType = POTENTIAL_DEFAULT
             c.pot = potential
         c.precision = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}[precision]
+        # the LMC (its state and reflex accelerations: NBodyState.set_lmc)
+        c.lmc, c.lmcDynaFric = int(bool(LMC)), int(bool(LMCDynaFric))
+        c.lmcMass, c.lmcScale, c.coulombLog = float(LMCmass), float(LMCscale), float(coulomb_log)
         self._c = c
 
     @classmethod
@@ -291,6 +295,21 @@ class NBodyState:
         """Mixed-precision walk tuning (nbSetMixedTuningCUDA)."""
         self.check("nbSetMixedTuning", self.lib.nbSetMixedTuningCUDA(
             self._h, int(group_max), int(list_cap), int(blocks_per_sm)))
+
+    def set_lmc(self, position, velocity, shift):
+        """The LMC of an LMC run (nbSetLMCCUDA): its position and velocity and the Milky Way's
+        reflex accelerations shift (k, 3), as the reference's reverseOrbit_LMC leaves them."""
+        p = np.ascontiguousarray(position, dtype=np.float64).reshape(3)
+        v = np.ascontiguousarray(velocity, dtype=np.float64).reshape(3)
+        sh = np.ascontiguousarray(shift, dtype=np.float64).reshape(-1, 3)
+        self.check("nbSetLMC", self.lib.nbSetLMCCUDA(self._h, _lib.ptr(p), _lib.ptr(v),
+                                                     _lib.ptr(sh), len(sh)))
+
+    def lmc(self):
+        """The LMC's current position and velocity (nbGetLMCCUDA)."""
+        p, v = np.empty(3), np.empty(3)
+        self.check("nbGetLMC", self.lib.nbGetLMCCUDA(self._h, _lib.ptr(p), _lib.ptr(v)))
+        return p, v
 
     def set_mixed_mode(self, exact=True):
         """Mixed walk interaction sets (nbSetMixedModeCUDA): exact=True (default) gives every

@@ -93,8 +93,10 @@ def ref():
             "nbref_handle_run_params": (None, [_vp, _ip, _dp, _ip]),
             "nbref_handle_like_params": (None, [_vp, _vp, _vp, _ip, _vp]),
             "nbref_likelihood": (ctypes.c_int, [_vp, _vp]),
+            "nbref_handle_lmc": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int]),
             "nbref_pow_rn": (ctypes.c_double, [ctypes.c_double, ctypes.c_double]),
             "nbref_log_rn": (ctypes.c_double, [ctypes.c_double]),
+            "nbref_atan_rn": (ctypes.c_double, [ctypes.c_double]),
             "nbref_ext_accel": (None, [_vp, _vp, _vp, ctypes.c_int]),
             "nbref_sample_step": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _dp, _dp]),
             "nbref_threads": (ctypes.c_int, []),
@@ -314,6 +316,14 @@ class RefState:
                       (float(x) for x in sun)))
         kw["IterMax"] = it.value
         return kw
+
+    def lmc(self):
+        """(position, velocity, shift (k, 3)) of the state's LMC; shift is empty without one."""
+        p, v = np.zeros(3), np.zeros(3)
+        n = self.lib.nbref_handle_lmc(self.h, _p(p), _p(v), None, 0)
+        sh = np.zeros((max(n, 1), 3))
+        self.lib.nbref_handle_lmc(self.h, _p(p), _p(v), _p(sh), n)
+        return p, v, sh[:n]
 
     def likelihood(self):
         out = np.zeros(10)

@@ -20,6 +20,7 @@
 #include "nbody_potential.h"
 #include "nbody_histogram.h"
 #include "nbody_likelihood.h"
+#include "nbody_orbit_integrator.h"
 #include "nbody_defaults.h"
 #include "milkyway_util.h"
 #include <crlibm.h>
@@ -97,6 +98,11 @@ void nbref_ctx_from_flat(NBodyCtx* ctx, const NBodyCudaCtx* c)
     ctx->pot.halo.gamma = c->pot.halo.gamma;
     ctx->pot.halo.lambda = c->pot.halo.lambda;
     ctx->pot.halo.rho0 = c->pot.halo.rho0;
+    ctx->LMC = (mwbool) c->lmc;
+    ctx->LMCDynaFric = (mwbool) c->lmcDynaFric;
+    ctx->LMCmass = c->lmcMass;
+    ctx->LMCscale = c->lmcScale;
+    ctx->coulomb_log = c->coulombLog;
 }
 
 void nbref_ctx_to_flat(NBodyCudaCtx* c, const NBodyCtx* ctx)
@@ -140,6 +146,11 @@ void nbref_ctx_to_flat(NBodyCudaCtx* c, const NBodyCtx* ctx)
     c->pot.halo.gamma = ctx->pot.halo.gamma;
     c->pot.halo.lambda = ctx->pot.halo.lambda;
     c->pot.halo.rho0 = ctx->pot.halo.rho0;
+    c->lmc = (int) ctx->LMC;
+    c->lmcDynaFric = (int) ctx->LMCDynaFric;
+    c->lmcMass = ctx->LMCmass;
+    c->lmcScale = ctx->LMCscale;
+    c->coulombLog = ctx->coulomb_log;
 }
 
 /* ---- states built from arrays ---- */
@@ -397,7 +408,36 @@ void* nbref_open_lua(const char* luaFile, const char* histFile, unsigned int see
     h->st.useVlos = h->ctx.useVlos;
     h->st.useDist = h->ctx.useDist;
     h->st.usePropMot = h->ctx.usePropMot;
+    /* an LMC run takes the LMC's state and the reflex accelerations that reverseOrbit_LMC
+     * left behind (nbody/src/nbody_plain.c:372-385) */
+    if (h->ctx.LMC && !h->st.shiftByLMC) {
+        mwvector* shift;
+        size_t nShift;
+        mwvector x, v;
+        getLMCArray(&shift, &nShift);
+        setLMCShiftArray(&h->st, shift, nShift);
+        getLMCPosVel(&x, &v);
+        setLMCPosVel(&h->st, x, v);
+    }
     return h;
+}
+
+/* The LMC of the handle's state: its position and velocity (pos3, vel3) and up to cap
+ * reflex accelerations (3 doubles each) into shift; returns their count (0 without an LMC). */
+int nbref_handle_lmc(void* hv, double* pos3, double* vel3, double* shift, int cap)
+{
+    RefHandle* h = (RefHandle*) hv;
+    int k, n;
+    pos3[0] = X(h->st.LMCpos); pos3[1] = Y(h->st.LMCpos); pos3[2] = Z(h->st.LMCpos);
+    vel3[0] = X(h->st.LMCvel); vel3[1] = Y(h->st.LMCvel); vel3[2] = Z(h->st.LMCvel);
+    if (!h->st.shiftByLMC) return 0;
+    n = (int) h->st.nShiftLMC;
+    for (k = 0; k < n && k < cap; ++k) {
+        shift[3 * k] = X(h->st.shiftByLMC[k]);
+        shift[3 * k + 1] = Y(h->st.shiftByLMC[k]);
+        shift[3 * k + 2] = Z(h->st.shiftByLMC[k]);
+    }
+    return n;
 }
 
 void nbref_handle_ctx(void* hv, NBodyCudaCtx* out, int* nStep, double* timeEvolve)
@@ -485,6 +525,7 @@ int nbref_likelihood(void* hv, double* out)
 /* ---- math pins ---- */
 double nbref_pow_rn(double x, double y) { return pow_rn(x, y); }
 double nbref_log_rn(double x) { return log_rn(x); }
+double nbref_atan_rn(double x) { return atan_rn(x); }
 
 void nbref_ext_accel(const NBodyCudaPotential* p, const double* pos, double* acc, int n)
 {

@@ -5,8 +5,7 @@
     (nbody/tests/RunTestUnits.lua refResults) of the single-Plummer Orphan models that
     tests/golden/orphan_dwarf.lua restates (MODELS below: every model whose components this
     build and the reference build here both evaluate -- models 1, 2, 3 and 7 need the
-    exponential disks' Bessel source, which the reference tree lacks, and the LMC models the
-    LMC with dynamical friction);
+    exponential disks' Bessel source, which the reference tree lacks);
   * orphan_model_histogram_3 -- the data histogram those tests match against
     (nbody/tests/orphan_models/orphan_model_histogram_3), copied verbatim (data).
 
@@ -25,12 +24,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 MODELS = {"4": "model_4", "5": "model_5", "5b": "model_5_bounds_test", "6": "model_6",
           "8": "model_8", "9": "model_9", "ninkovic": "model_ninkovic",
           "triaxial": "model_triaxial", "newhist1": "model_newhist1",
-          "newhist2": "model_newhist2", "newhist3": "model_newhist3", "bar": "model_bar"}
+          "newhist2": "model_newhist2", "newhist3": "model_newhist3", "bar": "model_bar",
+          "LMC": "model_LMC", "LMC_bar": "model_LMC_bar"}
 
 
 def parse_results(text, model):
     start = text.index('["%s"]' % model)
-    block = text[start:text.index("\n   },", start)]
+    nxt = text.find('\n   ["', start + 1)         # the next model's entry, or the table's end
+    block = text[start:nxt if nxt >= 0 else len(text)]
     out = {}
     for nb, body in re.findall(r'\["(\d+)"\]\s*=\s*\{(.*?)\}', block, flags=re.S):
         out[nb] = {seed: float(v) for seed, v in re.findall(r'\["(\d+)"\]\s*=\s*([0-9.eE+-]+)', body)}

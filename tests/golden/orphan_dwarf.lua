@@ -4,8 +4,8 @@
 -- golden checks.
 -- Arguments: nbody, variant (a key of `variants` below; default "5"), options.
 --   variant "4", "5", "5b" (model_5_bounds_test), "6", "8", "9", "ninkovic", "triaxial",
---   "newhist1".."newhist3", "bar"; each entry records its potential, dwarf, orbit and the
---   context fields that differ between the models.
+--   "newhist1".."newhist3", "bar", "LMC", "LMC_bar"; each entry records its potential, dwarf,
+--   orbit and the context fields that differ between the models.
 --   options (optional): "allterms" turns on every comparison of the likelihood (velocity
 --   dispersion, line-of-sight velocity, beta average, distance, proper motions); "bestlike"
 --   turns on the best-likelihood scan over the last 5% of the steps.
@@ -82,7 +82,20 @@ local variants = {
                timeEvolve = (2.0 - windowStart) * 3.945, timeBack = 3.945,
                useBestLike = true, bestLikeStart = windowStart / (2.0 - windowStart),
                calibrationRuns = 2 },
+   -- the LMC as a moving Plummer sphere with dynamical friction (reverseOrbit_LMC below)
+   ["LMC"] = { bulge = hernquist(67479.9, 0.6), disk = mn(224933, 4, 0.26),
+               halo = logHalo(155, 22.25, 1.1), eps2Kind = 1, r = 28.8, v = { -170, 94, 108 },
+               lmc = true },
+   ["LMC_bar"] = { bulge = hernquist(67479.9, 0.6), disk = mn(198040, 4, 0.26),
+                   disk2 = function()
+                      return Disk.orbitingBar{ mass = 2.689340798e4, scaleLength = 5.4,
+                                               patternSpeed = 250.61, startAngle = 0.488692 }
+                   end,
+                   halo = logHalo(155, 22.25, 1.1), eps2Kind = 0, r = 28.8, v = { -170, 94, 108 },
+                   lmc = true, timeBack = 3.945 },
 }
+local LMCMASS = 449865.888
+local LMCSCALE = 15.0
 -- newhist1..3: a 12-mass dwarf with the beta-average, line-of-sight and distance comparisons
 local newhist = { { 1, 53.4, 28.7, { -158, 76, 108 } }, { 0, 53.6, 28.5, { -154, 78, 109 } },
                   { 1, 53.8, 28.9, { -159, 80, 105 } } }
@@ -128,6 +141,12 @@ function makeContext()
       IterMax       = 6
    }
    if V.timeBack then c.timeBack = V.timeBack end
+   if V.lmc then
+      c.LMC = true
+      c.LMCmass = LMCMASS
+      c.LMCscale = LMCSCALE
+      c.LMCDynaFric = true
+   end
    if V.calibrationRuns then c.calibrationRuns = V.calibrationRuns end
    if V.useBestLike or bestLike then c.useBestLike = true end
    if V.newhist then
@@ -151,13 +170,31 @@ function makeContext()
 end
 
 function makeBodies(ctx, potential)
-   local finalPosition, finalVelocity = reverseOrbit{
-      potential = potential,
-      position  = lbrToCartesian(ctx, Vector.create(218, V.b or 53.5, V.r)),
-      velocity  = Vector.create(V.v[1], V.v[2], V.v[3]),
-      tstop     = V.tstop or 4.0,
-      dt        = ctx.timestep / 10.0
-   }
+   local finalPosition, finalVelocity
+   if V.lmc then
+      finalPosition, finalVelocity = reverseOrbit_LMC{
+         potential   = potential,
+         position    = lbrToCartesian(ctx, Vector.create(218, 53.5, V.r)),
+         velocity    = Vector.create(V.v[1], V.v[2], V.v[3]),
+         LMCposition = Vector.create(-1.1, -41.1, -27.9),
+         LMCvelocity = Vector.create(-57, -226, 221),
+         LMCmass     = LMCMASS,
+         LMCscale    = LMCSCALE,
+         LMCDynaFric = true,
+         coulomb_log = 0.470003629,
+         ftime       = 4.5,
+         tstop       = 4.0,
+         dt          = ctx.timestep / 10.0
+      }
+   else
+      finalPosition, finalVelocity = reverseOrbit{
+         potential = potential,
+         position  = lbrToCartesian(ctx, Vector.create(218, V.b or 53.5, V.r)),
+         velocity  = Vector.create(V.v[1], V.v[2], V.v[3]),
+         tstop     = V.tstop or 4.0,
+         dt        = ctx.timestep / 10.0
+      }
+   end
 
    return predefinedModels.plummer{
       nbody       = nbody,

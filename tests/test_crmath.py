@@ -1,9 +1,12 @@
-"""Correctly rounded log and pow (milkywayathome_client_b200/csrc/nb_crmath.cuh), no GPU.
+"""Correctly rounded log, pow, sin, cos and atan (milkywayathome_client_b200/csrc/nb_crmath.cuh),
+no GPU.
 
 The header uses only IEEE +, -, *, /, fma and sqrt, so a host build of it computes what the
 device computes, bit for bit.  Its results are compared with Python's decimal module (60
 digits, then rounded once to a double): the correctly rounded values that crlibm's log_rn and
-pow_rn, the reference's mw_log and mw_pow, return.
+pow_rn, the reference's mw_log and mw_pow, return (and its atan_rn, mw_atan).  sin and cos are
+checked the same way; the reference's are the C library's, which round correctly but for about
+0.1 % of the arguments (glibc 2.39).
 """
 import ctypes
 import os
@@ -22,6 +25,14 @@ extern "C" void cr_log(const double* x, int n, double* out)
 { for (int i = 0; i < n; ++i) out[i] = nb_log_rn(x[i]); }
 extern "C" void cr_pow(const double* x, const double* y, int n, double* out)
 { for (int i = 0; i < n; ++i) out[i] = nb_pow_rn(x[i], y[i]); }
+extern "C" void cr_sin(const double* x, int n, double* out)
+{ for (int i = 0; i < n; ++i) out[i] = nb_sin_rn(x[i]); }
+extern "C" void cr_cos(const double* x, int n, double* out)
+{ for (int i = 0; i < n; ++i) out[i] = nb_cos_rn(x[i]); }
+extern "C" void cr_sincos(const double* x, int n, double* out)
+{ for (int i = 0; i < n; ++i) { double s, c; nb_sincos_rn(x[i], s, c); out[i] = s + 2.0 * c; } }
+extern "C" void cr_atan(const double* x, int n, double* out)
+{ for (int i = 0; i < n; ++i) out[i] = nb_atan_rn(x[i]); }
 '''
 
 
@@ -104,3 +115,106 @@ def test_equal_to_the_reference_crlibm(lib):
     py = [rng.uniform(-3, 3) for _ in range(5000)]
     got = _call(lib, "cr_pow", px, py)
     assert all(g == ref.nbref_pow_rn(x, y) for g, x, y in zip(got, px, py))
+
+
+def _dec_pi():
+    def arctan_inv(n):
+        x = Decimal(1) / n
+        x2, s, t, k, sign = x * x, Decimal(0), x, 1, 1
+        while t > Decimal(10) ** -75:
+            s += sign * t / k
+            t *= x2
+            k += 2
+            sign = -sign
+        return s
+    return 16 * arctan_inv(5) - 4 * arctan_inv(239)
+
+
+def _dec_sincos(x, pi):
+    """(sin x, cos x) by Taylor series after reducing x modulo 2 pi, 80 digits."""
+    x = Decimal(x)
+    r = x - (x / (2 * pi)).to_integral_value() * 2 * pi
+    out = []
+    for t, n in ((r, 1), (Decimal(1), 0)):
+        s = Decimal(0)
+        while t and abs(t) > Decimal(10) ** -75 * abs(s + t):
+            s += t
+            t = -t * r * r / ((n + 1) * (n + 2))
+            n += 2
+        out.append(s)
+    return out
+
+
+def _dec_atan(x, pi):
+    """atan x: three halvings x -> x / (1 + sqrt(1 + x^2)), then the series, 80 digits."""
+    x = Decimal(x)
+    neg, x = x < 0, abs(x)
+    inv = x > 1
+    if inv:
+        x = 1 / x
+    for _ in range(3):
+        x = x / (1 + (1 + x * x).sqrt())
+    s, t, k, x2, sign = Decimal(0), x, 1, x * x, 1
+    while t > Decimal(10) ** -75:
+        s += sign * t / k
+        t *= x2
+        k += 2
+        sign = -sign
+    s *= 8
+    if inv:
+        s = pi / 2 - s
+    return -s if neg else s
+
+
+def test_sin_cos_are_correctly_rounded(lib):
+    getcontext().prec = 80
+    pi = _dec_pi()
+    rng = random.Random(13)
+    xs = [rng.uniform(-1200, 1200) for _ in range(3000)]          # the bar's angles
+    xs += [rng.uniform(-2, 2) for _ in range(2000)]
+    xs += [10 ** rng.uniform(-9, 8) * rng.choice([-1, 1]) for _ in range(2000)]
+    xs += [0.0, -0.0, 1e-300, 7.4e-9, 1.5e-8, 0.7853981633974483, 1.5707963267948966, 3.141592653589793]
+    want = [_dec_sincos(x, pi) for x in xs]
+    s, c = _call(lib, "cr_sin", xs), _call(lib, "cr_cos", xs)
+    bad = [(x, g, float(w[0])) for x, g, w in zip(xs, s, want) if g != float(w[0])]
+    assert not bad, bad[:5]
+    bad = [(x, g, float(w[1])) for x, g, w in zip(xs, c, want) if g != float(w[1])]
+    assert not bad, bad[:5]
+    both = _call(lib, "cr_sincos", xs)
+    assert np.array_equal(both, s + 2.0 * c)
+
+
+def test_sin_cos_agree_with_the_c_library_on_most_arguments(lib):
+    """The reference's bar takes the C library's sin and cos: they agree with the correctly
+    rounded values on all but a small fraction of the bar's angles."""
+    rng = np.random.default_rng(1)
+    xs = rng.uniform(-1200, 1200, 50000)
+    s, c = _call(lib, "cr_sin", xs), _call(lib, "cr_cos", xs)
+    assert (s != np.sin(xs)).mean() < 0.01 and (c != np.cos(xs)).mean() < 0.01
+    assert np.max(np.abs(s - np.sin(xs))) <= np.max(np.spacing(np.abs(s)))
+
+
+def test_atan_is_correctly_rounded(lib):
+    getcontext().prec = 80
+    pi = _dec_pi()
+    rng = random.Random(17)
+    xs = [rng.uniform(-30, 30) for _ in range(3000)]
+    xs += [10 ** rng.uniform(-9, 19) * rng.choice([-1, 1]) for _ in range(3000)]
+    xs += [0.0, -0.0, 7.4e-9, 7.5e-9, 1.0, -1.0, 1.2e18, 1e300, float("inf"), -float("inf")]
+    got = _call(lib, "cr_atan", xs)
+    want = [float(_dec_atan(x, pi)) if np.isfinite(x) else float(np.arctan(x)) for x in xs]
+    bad = [(x, g, w) for x, g, w in zip(xs, got, want) if g != w]
+    assert not bad, bad[:5]
+    assert np.isnan(_call(lib, "cr_atan", [float("nan")])[0])
+
+
+def test_atan_equal_to_the_reference_crlibm(lib):
+    from oracle import bindings as ob
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    ref = ob.ref()
+    rng = random.Random(19)
+    xs = [rng.uniform(-30, 30) for _ in range(5000)]
+    xs += [10 ** rng.uniform(-12, 20) * rng.choice([-1, 1]) for _ in range(5000)]
+    got = _call(lib, "cr_atan", xs)
+    assert all(g == ref.nbref_atan_rn(x) for g, x in zip(got, xs))

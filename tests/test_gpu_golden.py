@@ -82,8 +82,10 @@ def _gpu_run_system(variant, nbody, seed, options=()):
     mass, types = r.masses()
     params = HistogramParams(**r.like_params())   # makeHistogram of orphan_dwarf.lua + the ctx
     data = read_histogram(os.path.join(GOLDEN, "orphan_model_histogram_3"))
-    with NBodyState.create(ctx, init["pos"], init["vel"], mass) as st:
+    with NBodyState.create(ctx, init["pos"], init["vel"], mass, gravmap=not c.lmc) as st:
         st.set_types(types)
+        if c.lmc:                  # the LMC's state and reflex accelerations of reverseOrbit_LMC
+            st.set_lmc(*r.lmc())
         rc, res = st.run_system(ctx, nstep, time_evolve, params, data, use_best_like=use_best,
                                 best_like_start=start, calibration_runs=calib,
                                 keep_best_bodies=use_best)
@@ -148,3 +150,63 @@ def test_bar_golden_through_gpu_run_system(nbody, seed):
     res, (use_best, start, calib, nstep) = _gpu_run_system("bar", nbody, seed)
     assert use_best and calib == 2 and res["runs"] == 3
     assert abs(res["result"][0] - want) < 1e-10, (res, want)
+
+
+LMC_CASES = [(v, "100", s) for v in ("LMC", "LMC_bar") for s in ("670828913", "886885833",
+                                                                 "430281807")]
+LMC_CASES += [(v, "1024", "670828913") for v in ("LMC", "LMC_bar")]
+
+
+@pytest.mark.parametrize("variant,nbody,seed", LMC_CASES)
+def test_lmc_golden_through_gpu_run_system(variant, nbody, seed):
+    """model_LMC and model_LMC_bar: the LMC as a moving Plummer sphere with dynamical friction
+    (its orbit integrated beside the bodies on the GPU, the Milky Way's reflex accelerations
+    added to every kick and to the LMC's own), against the reference's golden table."""
+    from oracle import bindings as ob
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    with open(os.path.join(GOLDEN, "golden_likelihoods.json")) as f:
+        want = json.load(f)["models"][variant][nbody][seed]
+    res, (use_best, _, calib, _) = _gpu_run_system(variant, nbody, seed)
+    assert not use_best and calib == 0 and res["runs"] == 1
+    assert abs(res["result"][0] - want) < 1e-10, (res["result"], want)
+
+
+@pytest.mark.parametrize("variant", ["LMC", "LMC_bar"])
+def test_lmc_steps_equal_reference(variant):
+    """200 steps of an LMC run: every body and the LMC's position and velocity equal the
+    reference's bit for bit (model_LMC; model_LMC_bar evaluates the bar's trigonometry with
+    CUDA's functions, so its states agree to a few ulps instead)."""
+    from oracle import bindings as ob
+    from milkywayathome_client_b200 import NBodyCtx, NBodyState, _lib
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    r = ob.RefState.open_lua(os.path.join(GOLDEN, "orphan_dwarf.lua"),
+                             os.path.join(GOLDEN, "orphan_model_histogram_3"), 670828913,
+                             ["1024", variant])
+    c, nstep, time_evolve = r.ctx(_lib.Ctx)
+    assert c.lmc and c.lmcDynaFric
+    ctx = NBodyCtx.from_struct(c, nstep)
+    init = r.get()
+    mass, types = r.masses()
+    lmc_pos, lmc_vel, shift = r.lmc()
+    assert len(shift) > nstep
+    with NBodyState.create(ctx, init["pos"], init["vel"], mass, gravmap=False) as st:
+        st.set_types(types)
+        st.set_time_origin(time_evolve)
+        st.set_lmc(lmc_pos, lmc_vel, shift)
+        assert st.gravMap(ctx) == 0
+        assert r.gravmap() == 0
+        assert st.run_steps(ctx, 200) == 0
+        assert r.step(200) == 0
+        gpos, gvel = st.bodies()
+        p, v = st.lmc()
+    want = r.get()
+    wp, wv, _ = r.lmc()
+    if variant == "LMC":
+        assert np.array_equal(gpos, want["pos"]) and np.array_equal(gvel, want["vel"])
+        assert np.array_equal(p, wp) and np.array_equal(v, wv)
+    else:
+        np.testing.assert_allclose(gpos, want["pos"], rtol=1e-10, atol=1e-12)
+        np.testing.assert_allclose(p, wp, rtol=1e-12)
+        np.testing.assert_allclose(v, wv, rtol=1e-12)

@@ -39,7 +39,8 @@ def test_body_layout_matches_header():
 
 @pytest.mark.parametrize("variant,seed", [("5", "670828913"), ("5", "886885833"),
                                           ("4", "715144259"), ("4", "543966758"),
-                                          ("triaxial", "670828913")])
+                                          ("triaxial", "670828913"), ("LMC", "430281807"),
+                                          ("LMC_bar", "886885833")])
 def test_reference_build_reproduces_golden_likelihood(variant, seed):
     """The from-source reference reproduces RunTestUnits.lua's table (|diff| < 1e-10)."""
     ob = ref_or_skip()
