@@ -94,6 +94,7 @@ def ref():
             "nbref_handle_like_params": (None, [_vp, _vp, _vp, _ip, _vp]),
             "nbref_likelihood": (ctypes.c_int, [_vp, _vp]),
             "nbref_handle_lmc": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int]),
+            "nbref_handle_set_lmc": (None, [_vp, _vp, _vp, _vp, ctypes.c_int]),
             "nbref_pow_rn": (ctypes.c_double, [ctypes.c_double, ctypes.c_double]),
             "nbref_log_rn": (ctypes.c_double, [ctypes.c_double]),
             "nbref_atan_rn": (ctypes.c_double, [ctypes.c_double]),
@@ -324,6 +325,13 @@ class RefState:
         sh = np.zeros((max(n, 1), 3))
         self.lib.nbref_handle_lmc(self.h, _p(p), _p(v), _p(sh), n)
         return p, v, sh[:n]
+
+    def set_lmc(self, position, velocity, shift):
+        """Installs an LMC (position, velocity, reflex accelerations (k, 3)) on the state."""
+        p = np.ascontiguousarray(position, dtype=np.float64).reshape(3)
+        v = np.ascontiguousarray(velocity, dtype=np.float64).reshape(3)
+        sh = np.ascontiguousarray(shift, dtype=np.float64).reshape(-1, 3)
+        self.lib.nbref_handle_set_lmc(self.h, _p(p), _p(v), _p(sh), len(sh))
 
     def likelihood(self):
         out = np.zeros(10)

@@ -422,6 +422,24 @@ void* nbref_open_lua(const char* luaFile, const char* histFile, unsigned int see
     return h;
 }
 
+/* Installs an LMC on the handle's state: position, velocity and n reflex accelerations
+ * (3 doubles each), as nbRunSystemPlain takes them from reverseOrbit_LMC
+ * (nbody/src/nbody_plain.c:372-385); the state frees the array (nbody_types.c:123). */
+void nbref_handle_set_lmc(void* hv, const double* pos3, const double* vel3, const double* shift,
+                          int n)
+{
+    RefHandle* h = (RefHandle*) hv;
+    mwvector x, v;
+    mwvector* arr = (mwvector*) mwCallocA((size_t) (n > 0 ? n : 1), sizeof(mwvector));
+    int k;
+    for (k = 0; k < n; ++k) SET_VECTOR(arr[k], shift[3 * k], shift[3 * k + 1], shift[3 * k + 2]);
+    if (h->st.shiftByLMC) mwFreeA(h->st.shiftByLMC);
+    setLMCShiftArray(&h->st, arr, (size_t) n);
+    SET_VECTOR(x, pos3[0], pos3[1], pos3[2]);
+    SET_VECTOR(v, vel3[0], vel3[1], vel3[2]);
+    setLMCPosVel(&h->st, x, v);
+}
+
 /* The LMC of the handle's state: its position and velocity (pos3, vel3) and up to cap
  * reflex accelerations (3 doubles each) into shift; returns their count (0 without an LMC). */
 int nbref_handle_lmc(void* hv, double* pos3, double* vel3, double* shift, int cap)

@@ -1,0 +1,80 @@
+"""The LMC of the reference's LMC runs on the GPU, against the reference build (oracle/_ref).
+
+The forward runs of model_LMC and model_LMC_bar take coulomb_log from the context, where it is
+0, so their dynamical friction is zero and the golden tests (test_gpu_golden.py) check the LMC's
+orbit bit for bit.  Here the friction is on (coulomb_log 0.470003629, the value
+reverseOrbit_LMC integrates with): Chandrasekhar's formula with the potential's density and
+the quadrature velocity dispersion (dynamicalFriction_LMC, nbody/src/nbody_friction.c:85-132).
+Its erf and exp are the C library's in the reference and CUDA's here, so the LMC's orbit and
+the bodies agree to rounding, not bit for bit.
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _setup(variant, coulomb_log):
+    from oracle import bindings as ob
+    from milkywayathome_client_b200 import _lib
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    r = ob.RefState.open_lua(os.path.join(GOLDEN, "orphan_dwarf.lua"),
+                             os.path.join(GOLDEN, "orphan_model_histogram_3"), 670828913,
+                             ["1024", variant])
+    c, nstep, time_evolve = r.ctx(_lib.Ctx)
+    init = r.get()
+    mass, types = r.masses()
+    lmc = r.lmc()
+    c.coulombLog = coulomb_log
+    ref = ob.RefState.create(c, init["pos"], init["vel"], mass, types)
+    ref.set_lmc(*lmc)
+    r.close()
+    return c, nstep, init, mass, types, lmc, ref
+
+
+@pytest.mark.parametrize("variant", ["LMC", "LMC_bar"])
+def test_lmc_with_friction_against_reference(variant):
+    from milkywayathome_client_b200 import NBodyCtx, NBodyState
+    c, nstep, init, mass, types, (lp, lv, shift), ref = _setup(variant, 0.470003629)
+    ctx = NBodyCtx.from_struct(c, nstep)
+    with NBodyState.create(ctx, init["pos"], init["vel"], mass, gravmap=False) as st:
+        st.set_types(types)
+        st.set_lmc(lp, lv, shift)
+        assert st.gravMap(ctx) == 0
+        assert st.run_steps(ctx, 100) == 0
+        gpos, gvel = st.bodies()
+        p, v = st.lmc()
+    assert ref.gravmap() == 0 and ref.step(100) == 0
+    want = ref.get()
+    wp, wv, _ = ref.lmc()
+    # the friction changes the LMC's velocity by ~0.1 km/s in 100 steps; agreement to rounding
+    np.testing.assert_allclose(p, wp, rtol=1e-12)
+    np.testing.assert_allclose(v, wv, rtol=1e-12)
+    np.testing.assert_allclose(gpos, want["pos"], rtol=1e-9, atol=1e-11)
+    np.testing.assert_allclose(gvel, want["vel"], rtol=1e-9, atol=1e-9)
+    # and it is on: without it the LMC ends elsewhere
+    _, _, _, _, _, _, ref0 = _setup(variant, 0.0)
+    assert ref0.gravmap() == 0 and ref0.step(100) == 0
+    assert np.abs(ref0.lmc()[1] - wv).max() > 1e3 * np.abs(v - wv).max()
+
+
+def test_lmc_state_required_and_shift_bounds():
+    """An LMC context without the LMC's state, or past the end of its reflex accelerations,
+    is refused with an error status (no kernel runs on a missing array)."""
+    from milkywayathome_client_b200 import NBodyCtx, NBodyError, NBodyState
+    c, nstep, init, mass, types, (lp, lv, shift), ref = _setup("LMC", 0.0)
+    ctx = NBodyCtx.from_struct(c, nstep)
+    with NBodyState.create(ctx, init["pos"], init["vel"], mass, gravmap=False) as st:
+        st.set_types(types)
+        with pytest.raises(NBodyError):
+            st.check("nbGravMap", st.gravMap(ctx))
+        st.set_lmc(lp, lv, shift[:4])          # steps k = 0..2 (each takes k and k + 1)
+        assert st.gravMap(ctx) == 0
+        assert st.run_steps(ctx, 3) == 0
+        with pytest.raises(NBodyError):
+            st.check("nbStepSystem", st.step(ctx))
