@@ -371,6 +371,39 @@ typedef struct {
 NBodyCudaStatus nbGenerateDwarfCUDA(NBodyCudaState* st, const NBodyCudaPlummerDwarf* dwarf,
                                     double treeRSize);
 
+/* Dwarf component profiles (dwarf_t, nbody/include/nbody_potential_types.h:136-152).  Einasto
+ * (3) is not sampled: the reference's get_density/get_potential have no case for it. */
+#define NBCUDA_DWARF_PLUMMER 0
+#define NBCUDA_DWARF_NFW 1
+#define NBCUDA_DWARF_GEN_HERNQUIST 2
+#define NBCUDA_DWARF_CORED 4
+
+/* One component: Dwarf.plummer / nfw / general_hernquist {mass, scaleLength} or Dwarf.cored
+ * {mass, scaleLength, r1, rc} (nbody/src/nbody_lua_types/nbody_lua_dwarf.c:57-125).  For NFW
+ * and cored components mass is M200; like the reference the sampler replaces it by the mass
+ * inside its sampling bound 5 r200 (get_extra_nfw_mass, nbody/src/nbody_mixeddwarf.c:728-762). */
+typedef struct {
+    int type, reserved;
+    double mass, scaleLength;
+    double r1, rc;                     /* cored only */
+} NBodyCudaDwarfComponent;
+
+/* A two-component dwarf of any of those profiles (predefinedModels.mixeddwarf with comp1 =
+ * light, comp2 = dark; nbGenerateMixedDwarfCore, nbody/src/nbody_mixeddwarf.c:765-1026),
+ * sampled as NBodyCudaPlummerDwarf is. */
+typedef struct {
+    int nbody, nbodyBaryon;
+    NBodyCudaDwarfComponent light, dark;
+    double position[3], velocity[3];
+    unsigned long long seed;
+} NBodyCudaMixedDwarf;
+NBodyCudaStatus nbGenerateMixedDwarfCUDA(NBodyCudaState* st, const NBodyCudaMixedDwarf* dwarf,
+                                         double treeRSize);
+/* the particle masses the sampler gives the two components: out[0] light, out[1] dark */
+NBodyCudaStatus nbMixedDwarfParticleMassesCUDA(const NBodyCudaMixedDwarf* dwarf, double* out);
+/* every body's mass (nbody doubles) */
+NBodyCudaStatus nbGetBodyMassesCUDA(NBodyCudaState* st, double* mass);
+
 /* ---- batched dwarfs (no reference counterpart: the reference runs one dwarf per process) ----
  * Many independent dwarfs stepped together.  Each dwarf is the reference's simulation (its own
  * root at the origin, root size, octree, softening and time step) and gets the same
@@ -439,6 +472,8 @@ NBodyCudaStatus nbBatchLikelihoodCUDA(NBodyCudaBatch* batch, const NBodyCudaHist
 /* initial conditions of every dwarf of the batch in one launch per phase (one
  * NBodyCudaPlummerDwarf per dwarf, nbody matching the batch); resets root sizes and statuses */
 NBodyCudaStatus nbBatchGenerateDwarfsCUDA(NBodyCudaBatch* batch, const NBodyCudaPlummerDwarf* dwarfs);
+NBodyCudaStatus nbBatchGenerateMixedDwarfsCUDA(NBodyCudaBatch* batch,
+                                               const NBodyCudaMixedDwarf* dwarfs);
 /* mean device time of the steps of the last nbBatchRunStepsCUDA call */
 NBodyCudaStatus nbBatchLastStepTimeCUDA(NBodyCudaBatch* batch, double* stepMs);
 

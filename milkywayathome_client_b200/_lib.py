@@ -93,6 +93,22 @@ class PlummerDwarf(ctypes.Structure):
                 ("seed", ctypes.c_uint64)]
 
 
+DWARF_PLUMMER, DWARF_NFW, DWARF_GEN_HERNQUIST, DWARF_CORED = 0, 1, 2, 4   # NBCUDA_DWARF_*
+
+
+class DwarfComponent(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("reserved", ctypes.c_int),
+                ("mass", ctypes.c_double), ("scaleLength", ctypes.c_double),
+                ("r1", ctypes.c_double), ("rc", ctypes.c_double)]
+
+
+class MixedDwarf(ctypes.Structure):
+    _fields_ = [("nbody", ctypes.c_int), ("nbodyBaryon", ctypes.c_int),
+                ("light", DwarfComponent), ("dark", DwarfComponent),
+                ("position", ctypes.c_double * 3), ("velocity", ctypes.c_double * 3),
+                ("seed", ctypes.c_uint64)]
+
+
 HIST_COMPONENTS = 7       # NBODY_CUDA_HIST_COMPONENTS
 LIKELIHOOD_TERMS = 11     # NBODY_CUDA_LIKELIHOOD_TERMS
 
@@ -204,6 +220,10 @@ SIGNATURES = [
     ("nbBatchSetTimeOriginCUDA", ctypes.c_int, [_vp, ctypes.c_double]),
     ("nbGenerateDwarfCUDA", ctypes.c_int, [_vp, ctypes.POINTER(PlummerDwarf), ctypes.c_double]),
     ("nbBatchGenerateDwarfsCUDA", ctypes.c_int, [_vp, ctypes.POINTER(PlummerDwarf)]),
+    ("nbGenerateMixedDwarfCUDA", ctypes.c_int, [_vp, ctypes.POINTER(MixedDwarf), ctypes.c_double]),
+    ("nbBatchGenerateMixedDwarfsCUDA", ctypes.c_int, [_vp, ctypes.POINTER(MixedDwarf)]),
+    ("nbMixedDwarfParticleMassesCUDA", ctypes.c_int, [ctypes.POINTER(MixedDwarf), _vp]),
+    ("nbGetBodyMassesCUDA", ctypes.c_int, [_vp, _vp]),
     ("nbHistogramCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), _vp, _vp, _vp, _vp]),
     ("nbLikelihoodCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), ctypes.POINTER(DataHist),
                                         _vp]),

@@ -32,10 +32,11 @@ void nb_launch_direct_fp64(const double* px, const double* py, const double* pz,
                            double* vy, double* vz, const NbWalkParams& wp, const NbPot& pot,
                            NbScalars* sc, cudaStream_t s);
 void nb_launch_ext_only(const double* dpos, double* dacc, int n, const NbPot& pot, cudaStream_t s);
-int nb_launch_ic(const NBodyCudaPlummerDwarf* host, int nD, const int* firsts, void* dTable,
+int nb_launch_ic(const NBodyCudaMixedDwarf* host, int nD, const int* firsts, void* dTable,
                  double* scratch, NbTreeBuffers& b, int* types, int n, int numSMs, NbScalars* sc,
                  cudaStream_t s);
 size_t nb_ic_table_bytes(int nD);
+void nb_ic_particle_masses(const NBodyCudaMixedDwarf& h, double out[2]);
 
 static std::atomic<unsigned long long> g_launches{0};
 void nb_count_launch(int n) { g_launches.fetch_add((unsigned long long) n); }
@@ -1452,14 +1453,47 @@ static NBodyCudaStatus nb_set_types(NBodyCudaState* st, const int* types)
 }
 
 // Samples nD dwarfs into the state's bodies (dwarf k from body firsts[k]) and types.
-static NBodyCudaStatus nb_generate(NBodyCudaState* st, const NBodyCudaPlummerDwarf* d, int nD,
+static bool nb_component_ok(const NBodyCudaDwarfComponent& c)
+{
+    switch (c.type) {
+    case NBCUDA_DWARF_PLUMMER:
+    case NBCUDA_DWARF_GEN_HERNQUIST:
+        return c.scaleLength > 0.0 && c.mass >= 0.0;
+    case NBCUDA_DWARF_NFW:                           // r200 from the M200 mass
+        return c.scaleLength > 0.0 && c.mass > 0.0;
+    case NBCUDA_DWARF_CORED:
+        return c.scaleLength > 0.0 && c.mass > 0.0 && c.r1 > 0.0 && c.rc > 0.0;
+    default:
+        return false;
+    }
+}
+
+static bool nb_mixed_dwarf_ok(const NBodyCudaMixedDwarf& w)
+{
+    return w.nbody >= 1 && w.nbodyBaryon >= 0 && w.nbodyBaryon <= w.nbody &&
+           nb_component_ok(w.light) && nb_component_ok(w.dark);
+}
+
+static NBodyCudaMixedDwarf nb_mixed_from_plummer(const NBodyCudaPlummerDwarf& p)
+{
+    NBodyCudaMixedDwarf m{};
+    m.nbody = p.nbody;
+    m.nbodyBaryon = p.nbodyBaryon;
+    m.light.type = m.dark.type = NBCUDA_DWARF_PLUMMER;
+    m.light.mass = p.massLight;
+    m.light.scaleLength = p.scaleLight;
+    m.dark.mass = p.massDark;
+    m.dark.scaleLength = p.scaleDark;
+    for (int c = 0; c < 3; ++c) { m.position[c] = p.position[c]; m.velocity[c] = p.velocity[c]; }
+    m.seed = p.seed;
+    return m;
+}
+
+static NBodyCudaStatus nb_generate(NBodyCudaState* st, const NBodyCudaMixedDwarf* d, int nD,
                                    const int* firsts)
 {
     for (int k = 0; k < nD; ++k) {
-        const NBodyCudaPlummerDwarf& w = d[k];
-        if (w.nbody < 1 || w.nbodyBaryon < 0 || w.nbodyBaryon > w.nbody ||
-            !(w.scaleLight > 0.0) || !(w.scaleDark > 0.0) || !(w.massLight >= 0.0) ||
-            !(w.massDark >= 0.0)) {
+        if (!nb_mixed_dwarf_ok(d[k])) {
             g_lastError = "invalid dwarf parameters";
             return NBODY_USER_ERROR;
         }
@@ -1496,14 +1530,45 @@ static NBodyCudaStatus nb_generate(NBodyCudaState* st, const NBodyCudaPlummerDwa
 
 extern "C" {
 
-NBodyCudaStatus nbGenerateDwarfCUDA(NBodyCudaState* st, const NBodyCudaPlummerDwarf* dwarf,
-                                    double treeRSize)
+NBodyCudaStatus nbGenerateMixedDwarfCUDA(NBodyCudaState* st, const NBodyCudaMixedDwarf* dwarf,
+                                         double treeRSize)
 {
     if (!st || !dwarf || dwarf->nbody != st->nbody) return NBODY_USER_ERROR;
     NBodyCudaStatus rc = nb_reset_run(st, treeRSize);
     if (rc) return rc;
     const int first = 0;
     return nb_generate(st, dwarf, 1, &first);
+}
+
+NBodyCudaStatus nbGenerateDwarfCUDA(NBodyCudaState* st, const NBodyCudaPlummerDwarf* dwarf,
+                                    double treeRSize)
+{
+    if (!dwarf) return NBODY_USER_ERROR;
+    const NBodyCudaMixedDwarf m = nb_mixed_from_plummer(*dwarf);
+    return nbGenerateMixedDwarfCUDA(st, &m, treeRSize);
+}
+
+NBodyCudaStatus nbMixedDwarfParticleMassesCUDA(const NBodyCudaMixedDwarf* dwarf, double* out)
+{
+    if (!dwarf || !out) return NBODY_USER_ERROR;
+    if (!nb_mixed_dwarf_ok(*dwarf)) {
+        g_lastError = "invalid dwarf parameters";
+        return NBODY_USER_ERROR;
+    }
+    nb_ic_particle_masses(*dwarf, out);
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbGetBodyMassesCUDA(NBodyCudaState* st, double* mass)
+{
+    if (!st || !mass) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(st->device));
+    if (st->nbody) {
+        NB_CHECK(cudaMemcpyAsync(mass, st->b.mass, sizeof(double) * (size_t) st->nbody,
+                                 cudaMemcpyDeviceToHost, st->stream));
+        NB_CHECK(cudaStreamSynchronize(st->stream));
+    }
+    return NBODY_SUCCESS;
 }
 
 NBodyCudaStatus nbSetMixedTuningCUDA(NBodyCudaState* st, int groupMax, int listCap, int blocksPerSM)
@@ -2185,6 +2250,14 @@ NBodyCudaStatus nbBatchLikelihoodCUDA(NBodyCudaBatch* bt, const NBodyCudaHistogr
 }
 
 NBodyCudaStatus nbBatchGenerateDwarfsCUDA(NBodyCudaBatch* bt, const NBodyCudaPlummerDwarf* dwarfs)
+{
+    if (!bt || !dwarfs) return NBODY_USER_ERROR;
+    std::vector<NBodyCudaMixedDwarf> m(bt->nDwarfs);
+    for (int d = 0; d < bt->nDwarfs; ++d) m[d] = nb_mixed_from_plummer(dwarfs[d]);
+    return nbBatchGenerateMixedDwarfsCUDA(bt, m.data());
+}
+
+NBodyCudaStatus nbBatchGenerateMixedDwarfsCUDA(NBodyCudaBatch* bt, const NBodyCudaMixedDwarf* dwarfs)
 {
     if (!bt || !dwarfs) return NBODY_USER_ERROR;
     std::vector<int> firsts(bt->nDwarfs);

@@ -1,15 +1,20 @@
-// Two-component Plummer dwarf initial conditions on the GPU, one thread per body.
+// Two-component dwarf initial conditions on the GPU, one thread per body.
 //
 // Restates the sampler of nbGenerateMixedDwarfCore (nbody/src/nbody_mixeddwarf.c:765-1026)
-// for Plummer components (Dwarf.plummer, nbody/src/nbody_dwarf_potential.c): radii by rejection
-// from r^2 rho(r) of the body's own component (r_mag, :538-574), speeds by rejection from the
-// Eddington distribution function of that component in the combined potential (vel_mag,
-// :576-618, dist_fun :471-535), the DF evaluated as the reference does -- five-point stencil
-// derivatives (:63-95), the d^2rho/dpsi^2 integrand (fun, :368-445), a bisection root finder for
-// the integration limit (:247-366) and its composite three-point Gauss quadrature (:97-209),
-// the DF maximum by golden-section search (:211-245) -- then isotropic directions by rejection in
-// the unit cube (get_components, :620-647), and each component recentred on its own centre of
-// mass and velocity and shifted onto the orbit (cm_correction_by_comp, :649-694).
+// for the reference's dwarf profiles (Dwarf.plummer, nfw, general_hernquist and cored,
+// nbody/src/nbody_dwarf_potential.c:36-175; Einasto has no case in the reference's
+// get_density/get_potential): radii by rejection from r^2 rho(r) of the body's own component
+// (r_mag, :538-574), speeds by rejection from the Eddington distribution function of that
+// component in the combined potential (vel_mag, :576-618, dist_fun :471-535), the DF evaluated
+// as the reference does -- five-point stencil derivatives (:63-95), the d^2rho/dpsi^2 integrand
+// (fun, :368-445), a bisection root finder for the integration limit (:247-366) and its
+// composite three-point Gauss quadrature (:97-209), the DF maximum by golden-section search
+// (:211-245) -- then isotropic directions by rejection in the unit cube (get_components,
+// :620-647), and each component recentred on its own centre of mass and velocity and shifted
+// onto the orbit (cm_correction_by_comp, :649-694).  The per-component constants -- r200, the
+// NFW/cored normalisations (set_vars, :696-726), the NFW/cored mass reset to the mass inside
+// the sampling bound (get_extra_nfw_mass, :728-762), the bounds and the r^2 rho maxima
+// (:797-903) -- are computed once on the host in the reference's order.
 //
 // The random numbers are not the reference's dSFMT stream: every body draws from its own
 // counter-based stream (splitmix64 of the seed and the body index), so the samples agree with
@@ -17,13 +22,68 @@
 // evaluations of ~330 integrand points each) is what makes the reference's sampler take ~12 min
 // per 10^6 bodies on one core; here the bodies are independent threads.
 #include "nb_common.cuh"
+#include "nb_crmath.cuh"
 #include <vector>
 
 namespace {
 
+// pcrit and vol_pcrit = 200 pcrit 4 pi / 3 (milkyway/include/milkyway_math_supplemental.h:224-225)
+constexpr double kPcrit = 0.000679087369829744220469326744094105320596648627735869652;
+constexpr double kVolPcrit = 0.568910904587397184785763397846734505212216314432372653620;
+
+// One component of the dwarf with the constants its density and potential need.
+struct NbIcComp {
+    int type;                    // NBCUDA_DWARF_*
+    double M, a;                 // mass (after the NFW/cored reset) and scale length
+    double p0, ps, r1, rc;       // NFW/cored normalisations, cored radii
+    double C2, C3;               // cored potential constants (cored_pot)
+    double bound, rhoMax;        // r_mag's sampling bound and maximum of r^2 rho
+
+    // get_density (nbody_dwarf_potential.c:207-236)
+    NB_HD double den(double r) const
+    {
+        switch (type) {
+        case NBCUDA_DWARF_NFW: {
+            const double R = r / a;
+            return p0 * (1.0 / R) * (1.0 / ((1.0 + R) * (1.0 + R)));
+        }
+        case NBCUDA_DWARF_GEN_HERNQUIST:
+            return (1.0 / (2.0 * M_PI)) * M * a / (r * ((r + a) * (r + a) * (r + a)));
+        case NBCUDA_DWARF_CORED:
+            if (r <= r1) return p0 / (1.0 + (r / rc) * (r / rc));
+            return ps / ((r / a) * ((1.0 + r / a) * (1.0 + r / a)));
+        default: {                                   // Plummer
+            const double x = 1.0 + (r / a) * (r / a);
+            return (3.0 / (4.0 * M_PI)) * (M / (a * a * a)) * (1.0 / sqrt(x * x * x * x * x));
+        }
+        }
+    }
+    // get_potential (nbody_dwarf_potential.c:176-205), the positive psi; its log and atan are
+    // the CUDA library's (the samples match the reference's in distribution only, and psi is
+    // evaluated ~10^5 times per body), the set-up's below correctly rounded as the reference's
+    NB_HD double pot(double r) const
+    {
+        switch (type) {
+        case NBCUDA_DWARF_NFW: {
+            const double R = r / a;
+            return 4.0 * M_PI * (a * a) * p0 * (1.0 / R) * log(1.0 + R);
+        }
+        case NBCUDA_DWARF_GEN_HERNQUIST:
+            return M / (r + a);
+        case NBCUDA_DWARF_CORED:
+            if (r <= r1)
+                return -1.0 * (4.0 * M_PI * p0 * ((rc * rc) / 2.0 * log(r * r + rc * rc) +
+                                                  (rc * rc * rc) / r * atan(r / rc)) + C2);
+            return -1.0 * (-4.0 * M_PI * ps * (a * a * a) / r * log(1.0 + r / a) + C3 / r);
+        default:
+            return M / sqrt(r * r + a * a);
+        }
+    }
+};
+
 struct NbIcDwarf {
     int first, count, nBaryon;
-    double massL, rsL, massD, rsD;
+    NbIcComp L, D;
     double pos[3], vel[3];
     unsigned long long seed;
 };
@@ -42,25 +102,10 @@ struct NbRng {
     }
 };
 
-// ---- the Plummer model of nbody_dwarf_potential.c (psi: the positive potential) ----
-__device__ __forceinline__ double pl_den(double M, double a, double r)
-{
-    const double x = 1.0 + (r / a) * (r / a);
-    const double x5 = x * x * x * x * x;
-    return (3.0 / (4.0 * M_PI)) * (M / (a * a * a)) * (1.0 / sqrt(x5));
-}
-__device__ __forceinline__ double pl_pot(double M, double a, double r)
-{
-    return M / sqrt(r * r + a * a);
-}
-
 struct NbIcModel {
-    double ML, aL, MD, aD;
-    __device__ double psi(double r) const { return pl_pot(ML, aL, r) + pl_pot(MD, aD, r); }
-    __device__ double den(bool dark, double r) const
-    {
-        return dark ? pl_den(MD, aD, r) : pl_den(ML, aL, r);
-    }
+    NbIcComp L, D;
+    __device__ double psi(double r) const { return L.pot(r) + D.pot(r); }
+    __device__ double den(bool dark, double r) const { return dark ? D.den(r) : L.den(r); }
 };
 
 // five-point stencils with h = 0.001 (first_derivative / second_derivative)
@@ -84,8 +129,8 @@ __device__ __forceinline__ double d2(F f, double x)
 // the DF integrand d^2 rho / d psi^2 / sqrt(|E - psi|) at radius ri (fun)
 __device__ double ic_integrand(const NbIcModel& m, double ri, double energy, bool dark)
 {
-    auto potL = [&](double r) { return pl_pot(m.ML, m.aL, r); };
-    auto potD = [&](double r) { return pl_pot(m.MD, m.aD, r); };
+    auto potL = [&](double r) { return m.L.pot(r); };
+    auto potD = [&](double r) { return m.D.pot(r); };
     auto denC = [&](double r) { return m.den(dark, r); };
     double dpsi = d1(potL, ri) + d1(potD, ri);
     const double d2psi = d2(potL, ri) + d2(potD, ri);
@@ -158,11 +203,11 @@ __device__ double ic_df(const NbIcModel& m, double v, double r, bool dark)
 {
     const double cons = 0.03582244801567226;
     const double energy = m.psi(r) - 0.5 * v * v;
-    double range = m.MD == 0 ? 20.0 * sqrt(fabs((m.ML / energy) * (m.ML / energy) - m.aL * m.aL))
-                             : 20.0 * sqrt(fabs((m.MD / energy) * (m.MD / energy) - m.aD * m.aD));
+    double range = m.D.M == 0 ? 20.0 * sqrt(fabs((m.L.M / energy) * (m.L.M / energy) - m.L.a * m.L.a))
+                              : 20.0 * sqrt(fabs((m.D.M / energy) * (m.D.M / energy) - m.D.a * m.D.a));
     for (int counter = 0; m.psi(range) > energy; ++counter) {
         range = 100.0 * range;
-        if (counter > 100) { range = 100.0 * (m.aL + m.aD); break; }
+        if (counter > 100) { range = 100.0 * (m.L.a + m.D.a); break; }
     }
     double up = ic_root(m, energy, 0.0, range);
     if (isinf(up) || up == 0.0 || isnan(up)) up = r;        // find_upperlimit_r's fallback
@@ -238,19 +283,16 @@ __global__ void k_ic_sample(const NbIcDwarf* __restrict__ dwarfs, int nD, int n,
         const NbIcDwarf& d = dwarfs[ic_dwarf_of(dwarfs, nD, i)];
         const int k = i - d.first;
         const bool dark = k >= d.nBaryon;
-        const NbIcModel m{d.massL, d.rsL, d.massD, d.rsD};
+        const NbIcModel m{d.L, d.D};
         NbRng rng{ic_mix(d.seed ^ ic_mix((unsigned long long) k + 0x51ED27ull))};
-        const double M = dark ? d.massD : d.massL, a = dark ? d.rsD : d.rsL;
-        const double bound = 50.0 * (d.rsL + d.rsD);
-        const double rmax = sqrt(2.0 / 3.0) * a;
-        const double rhoMax = rmax * rmax * pl_den(M, a, rmax);
+        const NbIcComp& comp = dark ? d.D : d.L;
         double r = 0.0;
         for (int tries = 0; tries <= 1000 && !(isfinite(r) && r != 0.0); ++tries) {
             r = 0.0;
             for (int counter = 0; counter <= 1000; ++counter) {      // r_mag
-                const double rr = rng.uniform() * bound;
+                const double rr = rng.uniform() * comp.bound;
                 const double u = rng.uniform();
-                if (rr * rr * pl_den(M, a, rr) / rhoMax > u) { r = rr; break; }
+                if (rr * rr * comp.den(rr) / comp.rhoMax > u) { r = rr; break; }
             }
         }
         double v = 0.0;
@@ -276,8 +318,8 @@ __global__ void k_ic_sample(const NbIcDwarf* __restrict__ dwarfs, int nD, int n,
         px[i] = dr[0]; py[i] = dr[1]; pz[i] = dr[2];
         vx[i] = dv[0]; vy[i] = dv[1]; vz[i] = dv[2];
         const int nDark = d.count - d.nBaryon;
-        mass[i] = dark ? (nDark ? d.massD / (double) nDark : 0.0)
-                       : (d.nBaryon ? d.massL / (double) d.nBaryon : 0.0);
+        mass[i] = dark ? (nDark ? d.D.M / (double) nDark : 0.0)
+                       : (d.nBaryon ? d.L.M / (double) d.nBaryon : 0.0);
         types[i] = dark ? -1 : 1;
     }
 }
@@ -329,7 +371,7 @@ __global__ void k_ic_shift(const NbIcDwarf* __restrict__ dwarfs, int nD, int n,
         const int dwi = ic_dwarf_of(dwarfs, nD, i);
         const NbIcDwarf& d = dwarfs[dwi];
         const bool dark = i - d.first >= d.nBaryon;
-        const double cm = dark ? d.massD : d.massL;
+        const double cm = dark ? d.D.M : d.L.M;
         const double* s = sums + 6 * (size_t) (2 * dwi + dark);
         px[i] = px[i] - s[0] / cm + d.pos[0];
         py[i] = py[i] - s[1] / cm + d.pos[1];
@@ -342,22 +384,100 @@ __global__ void k_ic_shift(const NbIcDwarf* __restrict__ dwarfs, int nD, int n,
 
 }  // namespace
 
+namespace {
+
+// The component's constants as nbGenerateMixedDwarfCore sets them up: set_vars
+// (nbody_mixeddwarf.c:696-726), the sampling bound with get_extra_nfw_mass for NFW and cored
+// components (:728-762, :797-831), the cored potential's constants (cored_pot,
+// nbody_dwarf_potential.c:139-175) and the maximum of r^2 rho at its analytic radius (:873-903).
+// rscaleL and rscaleD: both components' scale lengths (the Plummer/Hernquist bound).
+NbIcComp nb_ic_setup(const NBodyCudaDwarfComponent& in, double rscaleL, double rscaleD)
+{
+    NbIcComp c{};
+    c.type = in.type;
+    c.M = in.mass;
+    c.a = in.scaleLength;
+    c.r1 = in.r1;
+    c.rc = in.rc;
+    const double rs = c.a, r1 = c.r1, rc = c.rc;
+    const bool cored = c.type == NBCUDA_DWARF_CORED;
+    const double r200 = cbrt(c.M / kVolPcrit);
+    if (cored) {
+        const double D1 = r1 * ((1.0 + r1 / rs) * (1.0 + r1 / rs)) / (rs + rs * ((r1 / rc) * (r1 / rc)));
+        const double D2 = (rs * rs * rs) * (nb_log_rn(1.0 + r200 / rs) - nb_log_rn(1.0 + r1 / rs) -
+                                            r200 / (rs + r200) + r1 / (rs + r1));
+        const double D3 = (rc * rc) * (r1 - rc * nb_atan_rn(r1 / rc));
+        c.p0 = c.M / (4.0 * M_PI * (D1 * D2 + D3));
+        c.ps = c.p0 * D1;
+    } else {
+        const double conc = r200 / rs;
+        const double term = nb_log_rn(1.0 + conc) - conc / (1.0 + conc);
+        c.p0 = 200.0 * (conc * conc * conc) * kPcrit / (3.0 * term);
+    }
+    if (c.type == NBCUDA_DWARF_NFW || cored) {
+        c.bound = 5.0 * r200;
+        const double r = c.bound;                    // the mass inside the bound
+        if (cored) {
+            const double C1 = 0;
+            const double C3 = C1 + 4 * M_PI * (c.ps * (rs * rs * rs) * (nb_log_rn((1 + r1 / rs)) - r1 / (rs + r1)) -
+                                               c.p0 * (rc * rc) * (r1 - rc * nb_atan_rn(r1 / rc)));
+            if (r <= r1)
+                c.M = 4.0 * M_PI * c.p0 * (rc * rc) * (r - rc * nb_atan_rn(r / rc)) - C1;
+            else
+                c.M = 4.0 * M_PI * c.ps * (rs * rs * rs) * (nb_log_rn((rs + r) / rs) - r / (rs + r)) - C3;
+        } else {
+            c.M = 4.0 * M_PI * c.p0 * (rs * rs * rs) * (nb_log_rn((rs + r) / rs) - r / (rs + r));
+        }
+    } else {
+        c.bound = 50.0 * (rscaleL + rscaleD);
+    }
+    if (cored) {
+        c.C3 = 4.0 * M_PI * (c.ps * (rs * rs * rs) * (nb_log_rn((1.0 + r1 / rs)) - r1 / (rs + r1)) -
+                             c.p0 * (rc * rc) * (r1 - rc * nb_atan_rn(r1 / rc)));
+        c.C2 = c.C3 / r1 - (4.0 * M_PI) / r1 *
+                               (c.ps * (rs * rs * rs) * nb_log_rn(1 + r1 / rs) +
+                                c.p0 * (((rc * rc) * r1) / 2.0 * nb_log_rn((r1 * r1) + (rc * rc)) +
+                                        (rc * rc * rc) * nb_atan_rn(r1 / rc)));
+    }
+    double rmax;
+    switch (c.type) {
+    case NBCUDA_DWARF_NFW: rmax = rs; break;
+    case NBCUDA_DWARF_GEN_HERNQUIST: rmax = rs / 2.0; break;
+    case NBCUDA_DWARF_CORED: rmax = rs > r1 ? rs : r1; break;
+    default: rmax = sqrt(2.0 / 3.0) * rs; break;
+    }
+    c.rhoMax = (rmax * rmax) * c.den(rmax);
+    return c;
+}
+
+}  // namespace
+
+// The two components' particle masses as the sampler assigns them (after the NFW/cored reset).
+void nb_ic_particle_masses(const NBodyCudaMixedDwarf& h, double out[2])
+{
+    const NbIcComp L = nb_ic_setup(h.light, h.light.scaleLength, h.dark.scaleLength);
+    const NbIcComp D = nb_ic_setup(h.dark, h.light.scaleLength, h.dark.scaleLength);
+    const int nDark = h.nbody - h.nbodyBaryon;
+    out[0] = h.nbodyBaryon ? L.M / (double) h.nbodyBaryon : 0.0;
+    out[1] = nDark ? D.M / (double) nDark : 0.0;
+}
+
 // Samples every dwarf of the table into the SoA body arrays (bodies [first, first + count) of
 // each dwarf) and their types; scratch needs 12 doubles per dwarf.  One launch per phase for all
 // dwarfs.  Returns the number of launches.
-int nb_launch_ic(const NBodyCudaPlummerDwarf* host, int nD, const int* firsts, void* dTable,
+int nb_launch_ic(const NBodyCudaMixedDwarf* host, int nD, const int* firsts, void* dTable,
                  double* scratch, NbTreeBuffers& b, int* types, int n, int numSMs, NbScalars* sc,
                  cudaStream_t s)
 {
     std::vector<NbIcDwarf> t(nD);
     for (int k = 0; k < nD; ++k) {
-        const NBodyCudaPlummerDwarf& h = host[k];
+        const NBodyCudaMixedDwarf& h = host[k];
         NbIcDwarf& d = t[k];
         d.first = firsts[k];
         d.count = h.nbody;
         d.nBaryon = h.nbodyBaryon;
-        d.massL = h.massLight; d.rsL = h.scaleLight;
-        d.massD = h.massDark; d.rsD = h.scaleDark;
+        d.L = nb_ic_setup(h.light, h.light.scaleLength, h.dark.scaleLength);
+        d.D = nb_ic_setup(h.dark, h.light.scaleLength, h.dark.scaleLength);
         for (int c = 0; c < 3; ++c) { d.pos[c] = h.position[c]; d.vel[c] = h.velocity[c]; }
         d.seed = h.seed;
     }

@@ -223,6 +223,57 @@ def plummer_dwarf_struct(nbody, seed, nbody_baryon=None, mass_l=12.0, rscale_l=0
     return d
 
 
+class Dwarf:
+    """The components of a two-component dwarf, as the reference's Lua Dwarf.plummer, nfw,
+    general_hernquist and cored (nbody/src/nbody_lua_types/nbody_lua_dwarf.c:57-125): for nfw
+    and cored, mass is M200 (the sampler takes the mass inside its bound 5 r200 instead)."""
+
+    @staticmethod
+    def _make(kind, mass, scaleLength, r1=0.0, rc=0.0):
+        c = _lib.DwarfComponent()
+        c.type, c.mass, c.scaleLength, c.r1, c.rc = kind, float(mass), float(scaleLength), float(r1), float(rc)
+        return c
+
+    @staticmethod
+    def plummer(mass, scaleLength):
+        return Dwarf._make(_lib.DWARF_PLUMMER, mass, scaleLength)
+
+    @staticmethod
+    def nfw(mass, scaleLength):
+        return Dwarf._make(_lib.DWARF_NFW, mass, scaleLength)
+
+    @staticmethod
+    def general_hernquist(mass, scaleLength):
+        return Dwarf._make(_lib.DWARF_GEN_HERNQUIST, mass, scaleLength)
+
+    @staticmethod
+    def cored(mass, scaleLength, r1, rc):
+        return Dwarf._make(_lib.DWARF_CORED, mass, scaleLength, r1, rc)
+
+
+def mixed_dwarf_struct(nbody, seed, comp1, comp2, nbody_baryon=None, position=None, velocity=None):
+    """NBodyCudaMixedDwarf: predefinedModels.mixeddwarf{nbody, nbody_baryon, comp1 (light),
+    comp2 (dark), position, velocity} with the GPU sampler's seed."""
+    d = _lib.MixedDwarf()
+    d.nbody = int(nbody)
+    d.nbodyBaryon = int(nbody // 2 if nbody_baryon is None else nbody_baryon)
+    d.light, d.dark = comp1, comp2
+    pos = np.zeros(3) if position is None else np.asarray(position, dtype=np.float64)
+    vel = np.zeros(3) if velocity is None else np.asarray(velocity, dtype=np.float64)
+    for c in range(3):
+        d.position[c], d.velocity[c] = float(pos[c]), float(vel[c])
+    d.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    return d
+
+
+def mixed_dwarf_particle_masses(dwarf):
+    """(light, dark) particle masses the sampler assigns (nbMixedDwarfParticleMassesCUDA)."""
+    out = np.zeros(2)
+    NBodyState.check("nbMixedDwarfParticleMasses",
+                     _lib.load().nbMixedDwarfParticleMassesCUDA(ctypes.byref(dwarf), _lib.ptr(out)))
+    return float(out[0]), float(out[1])
+
+
 class NBodyState:
     """Device-resident N-body state: NBodyState.create(ctx, bodies) and state:step(ctx)
     (nbody/src/nbody_lua_types/nbody_lua_nbodystate.c:60-147) over the CUDA library.
@@ -290,6 +341,25 @@ class NBodyState:
         if gravmap:
             st.check("nbGravMap", st.gravMap(ctx))
         return st
+
+    @classmethod
+    def generate_mixed(cls, ctx, nbody, seed, comp1, comp2, nbody_baryon=None, position=None,
+                       velocity=None, device=0, gravmap=True):
+        """A two-component dwarf of any of the reference's profiles (Dwarf.*) sampled on the
+        GPU (nbGenerateMixedDwarfCUDA), then nbGravMap."""
+        st = cls(nbody, device)
+        d = mixed_dwarf_struct(nbody, seed, comp1, comp2, nbody_baryon, position, velocity)
+        st.check("nbGenerateMixedDwarf", st.lib.nbGenerateMixedDwarfCUDA(
+            st._h, ctypes.byref(d), float(ctx.treeRSize)))
+        if gravmap:
+            st.check("nbGravMap", st.gravMap(ctx))
+        return st
+
+    def masses(self):
+        """Every body's mass (nbGetBodyMassesCUDA)."""
+        m = np.empty(self.nbody)
+        self.check("nbGetBodyMasses", self.lib.nbGetBodyMassesCUDA(self._h, _lib.ptr(m)))
+        return m
 
     def set_mixed_tuning(self, group_max=32, list_cap=64, blocks_per_sm=0):
         """Mixed-precision walk tuning (nbSetMixedTuningCUDA)."""
@@ -618,7 +688,13 @@ class NBodyBatch:
 
     def generate(self, dwarfs):
         """Sample every dwarf on the GPU in one launch per phase (nbBatchGenerateDwarfsCUDA):
-        dwarfs is a list of plummer_dwarf_struct()s matching the batch's sizes."""
+        dwarfs is a list of plummer_dwarf_struct()s or mixed_dwarf_struct()s matching the
+        batch's sizes."""
+        if dwarfs and isinstance(dwarfs[0], _lib.MixedDwarf):
+            arr = (_lib.MixedDwarf * len(dwarfs))(*dwarfs)
+            self.check("nbBatchGenerateMixedDwarfs",
+                       self.lib.nbBatchGenerateMixedDwarfsCUDA(self._h, arr))
+            return
         arr = (_lib.PlummerDwarf * len(dwarfs))(*dwarfs)
         self.check("nbBatchGenerateDwarfs", self.lib.nbBatchGenerateDwarfsCUDA(self._h, arr))
 

@@ -1,8 +1,9 @@
--- Two-component Plummer dwarf for the initial-condition checks: the reference's mixed-dwarf
--- sampler (predefinedModels.mixeddwarf with two Dwarf.plummer components, as the sample
+-- Two-component dwarf for the initial-condition checks: the reference's mixed-dwarf sampler
+-- (predefinedModels.mixeddwarf with two Dwarf components, by default Dwarf.plummer as the sample
 -- workunit nbody/sample_workunits/for_developers.lua builds it) placed at a fixed position and
 -- velocity, without the reverse orbit, so that only the sampler is exercised.
--- Arguments: nbody, nbody_baryon, mass_l, rscale_l, mass_d, rscale_d.
+-- Arguments: nbody, nbody_baryon, mass_l, rscale_l, mass_d, rscale_d, and optionally
+-- type_l, type_d (plummer, nfw, general_hernquist or cored) and r1, rc (of cored components).
 
 arg = {...}
 
@@ -15,6 +16,17 @@ massL = tonumber(arg[3])
 rscaleL = tonumber(arg[4])
 massD = tonumber(arg[5])
 rscaleD = tonumber(arg[6])
+typeL = arg[7] or "plummer"
+typeD = arg[8] or "plummer"
+coreR1 = tonumber(arg[9] or "0")
+coreRc = tonumber(arg[10] or "0")
+
+local function component(kind, m, a)
+   if kind == "cored" then
+      return Dwarf.cored{ mass = m, scaleLength = a, r1 = coreR1, rc = coreRc }
+   end
+   return Dwarf[kind]{ mass = m, scaleLength = a }
+end
 
 function makePotential()
    return Potential.create{
@@ -46,8 +58,8 @@ function makeContext()
 end
 
 function makeBodies(ctx, potential)
-   local comp1 = Dwarf.plummer{ mass = massL, scaleLength = rscaleL }
-   local comp2 = Dwarf.plummer{ mass = massD, scaleLength = rscaleD }
+   local comp1 = component(typeL, massL, rscaleL)
+   local comp2 = component(typeD, massD, rscaleD)
    return predefinedModels.mixeddwarf{
       nbody        = nbody,
       nbody_baryon = nbodyBaryon,
