@@ -474,6 +474,20 @@ NBodyCudaStatus nbBatchLikelihoodCUDA(NBodyCudaBatch* batch, const NBodyCudaHist
 NBodyCudaStatus nbBatchGenerateDwarfsCUDA(NBodyCudaBatch* batch, const NBodyCudaPlummerDwarf* dwarfs);
 NBodyCudaStatus nbBatchGenerateMixedDwarfsCUDA(NBodyCudaBatch* batch,
                                                const NBodyCudaMixedDwarf* dwarfs);
+/* nbRunSystemCUDA for every dwarf at once (rp shared: nStep, the best-likelihood window from
+ * bestLikeStart, timeEvolve): steps through the batch's step (captured graphs when useGraph),
+ * each step of the window one histogram pass, likelihood and best-record update for all
+ * dwarfs; res[ndwarfs] as nbRunSystemCUDA's per dwarf.  Types must be set
+ * (nbBatchSetTypesCUDA).  With an orbiting bar, calibrationRuns must be 0 (the batch shares
+ * one time origin): NBODY_UNSUPPORTED otherwise. */
+NBodyCudaStatus nbBatchRunSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* batch,
+                                     const NBodyCudaRunParams* rp,
+                                     const NBodyCudaHistogramParams* hp,
+                                     const NBodyCudaDataHistogram* data, int useGraph,
+                                     NBodyCudaRunResult* res);
+/* every dwarf's bodies at its best likelihood (keepBestBodies; valid for dwarfs with
+ * bestCount > 0), all bodies of the batch in order */
+NBodyCudaStatus nbBatchGetBestBodiesCUDA(NBodyCudaBatch* batch, double* pos, double* vel);
 /* mean device time of the steps of the last nbBatchRunStepsCUDA call */
 NBodyCudaStatus nbBatchLastStepTimeCUDA(NBodyCudaBatch* batch, double* stepMs);
 

@@ -222,6 +222,8 @@ SIGNATURES = [
     ("nbBatchGenerateDwarfsCUDA", ctypes.c_int, [_vp, ctypes.POINTER(PlummerDwarf)]),
     ("nbGenerateMixedDwarfCUDA", ctypes.c_int, [_vp, ctypes.POINTER(MixedDwarf), ctypes.c_double]),
     ("nbBatchGenerateMixedDwarfsCUDA", ctypes.c_int, [_vp, ctypes.POINTER(MixedDwarf)]),
+    ("nbBatchRunSystemCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
+    ("nbBatchGetBestBodiesCUDA", ctypes.c_int, [_vp, _vp, _vp]),
     ("nbMixedDwarfParticleMassesCUDA", ctypes.c_int, [ctypes.POINTER(MixedDwarf), _vp]),
     ("nbGetBodyMassesCUDA", ctypes.c_int, [_vp, _vp]),
     ("nbHistogramCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), _vp, _vp, _vp, _vp]),

@@ -1807,6 +1807,8 @@ struct NBodyCudaBatch {
     NbBatchTuning graphTune;
     double lastStepMs = 0.0;
     int lastSteps = 0;
+    NbBestDev* best = nullptr;          // nbBatchRunSystemCUDA: per-dwarf best-likelihood records
+    bool haveKeep = false;              // keepPos/keepVel of the state hold best bodies
 };
 
 static NbForest nb_forest_of(NBodyCudaBatch* bt)
@@ -2051,6 +2053,7 @@ NBodyCudaStatus nbBatchDestroyCUDA(NBodyCudaBatch* bt)
     if (!bt) return NBODY_SUCCESS;
     if (bt->st) cudaSetDevice(bt->st->device);
     nb_batch_drop_graph(bt);
+    cudaFree(bt->best);
     cudaFree(bt->dDwarfs);
     cudaFree(bt->bodyDwarf);
     if (bt->hDwarfs) cudaFreeHost(bt->hDwarfs);
@@ -2273,6 +2276,141 @@ NBodyCudaStatus nbBatchGenerateMixedDwarfsCUDA(NBodyCudaBatch* bt, const NBodyCu
     NBodyCudaStatus rc = nb_generate(bt->st, dwarfs, bt->nDwarfs, firsts.data());
     if (rc) return rc;
     return nb_batch_reset_table(bt);
+}
+
+// nbRunSystemCUDA for every dwarf of the batch at once: the steps through the batch's step
+// (captured graphs when useGraph), then with the best-likelihood scan each step of the window
+// one histogram pass, one likelihood and one best-record update for all dwarfs; res[d] as
+// nbRunSystemCUDA's for dwarf d.  The orbiting bar's calibration runs need a time origin per
+// dwarf and are not run for a batch.
+NBodyCudaStatus nbBatchRunSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt,
+                                     const NBodyCudaRunParams* rp,
+                                     const NBodyCudaHistogramParams* hp,
+                                     const NBodyCudaDataHistogram* data, int useGraph,
+                                     NBodyCudaRunResult* res)
+{
+    if (!bt || !ctx || !rp || !res || rp->nStep < 0 || rp->calibrationRuns < 0) {
+        g_lastError = "nbBatchRunSystemCUDA: invalid arguments";
+        return NBODY_USER_ERROR;
+    }
+    NBodyCudaStatus rc = nb_batch_check(ctx, bt);
+    if (rc) return rc;
+    if ((rp->useBestLike || rp->keepBestBodies) && (!hp || !data)) {
+        g_lastError = "nbBatchRunSystemCUDA: the best-likelihood scan needs histogram parameters and data";
+        return NBODY_USER_ERROR;
+    }
+    const bool bar = ctx->potentialType == NBCUDA_POTENTIAL_DEFAULT &&
+                     ctx->pot.disk2.type == NBCUDA_ORBITING_BAR;
+    if (bar && rp->calibrationRuns > 0) {
+        g_lastError = "nbBatchRunSystemCUDA: the bar's calibration runs need a time origin per dwarf";
+        return NBODY_UNSUPPORTED;
+    }
+    NBodyCudaState* st = bt->st;
+    if (st->step > rp->nStep) {
+        g_lastError = "nbBatchRunSystemCUDA: the batch is past nStep";
+        return NBODY_USER_ERROR;
+    }
+    NB_CHECK(cudaSetDevice(st->device));
+    const int D = bt->nDwarfs;
+    const cudaStream_t s = st->stream;
+    for (int d = 0; d < D; ++d) {
+        res[d] = NBodyCudaRunResult{};
+        for (int t = 0; t < NB_LIKELIHOOD_TERMS; ++t) res[d].result[t] = res[d].final[t] = NAN;
+    }
+    NbHistRun hr;
+    const bool like = hp && data;
+    if (like) {
+        rc = nb_hist_prepare(st, nb_batch_sizes(bt), hp, data, false, hr);
+        if (rc != NBODY_SUCCESS) return rc;
+    }
+    if (!bt->best) NB_CHECK(cudaMalloc((void**) &bt->best, sizeof(NbBestDev) * (size_t) D));
+    if (rp->keepBestBodies && !st->keepPos) {
+        NB_CHECK(nb_alloc(&st->keepPos, 3 * (size_t) st->nbody));
+        NB_CHECK(nb_alloc(&st->keepVel, 3 * (size_t) st->nbody));
+    }
+    NbBestDev init{};
+    init.best[0] = 9999999.9;                       // st->bestLikelihood = DEFAULT_WORST_CASE
+    init.timeEvolve = rp->timeEvolve;
+    std::vector<NbBestDev> bestHost(D, init);
+    NB_CHECK(cudaMemcpyAsync(bt->best, bestHost.data(), sizeof(NbBestDev) * (size_t) D,
+                             cudaMemcpyHostToDevice, s));
+    // nbody.c:436-447: the bar's time origin of the first (here the only) run
+    const double og = (2 * rp->bestLikeStart) / (rp->bestLikeStart + 1);
+    const double pft = rp->useBestLike ? rp->timeEvolve / (2 - og) : rp->timeEvolve;
+    st->timeOrigin = pft;
+    bt->haveKeep = false;
+    NBodyCudaStatus all = nb_batch_eval(ctx, bt, 0, 0, false);   // nbGravMap
+    const bool scan = like && rp->useBestLike;
+    double total = 0.0;
+    int steps = 0;
+    if (!(all & ~(int) NBODY_STATUS_WARNINGS_MASK)) {
+        while (st->step < rp->nStep) {
+            const NBodyCudaStatus rcStep = nb_batch_eval(ctx, bt, 1, 1, useGraph != 0);
+            all |= rcStep;
+            total += st->stepMs;
+            ++steps;
+            st->step++;
+            if (rcStep & ~(int) NBODY_STATUS_WARNINGS_MASK) break;
+            if (scan && (double) st->step / (double) rp->nStep >= rp->bestLikeStart) {
+                nb_hist_launch(st, bt->bodyDwarf, hr, true);
+                nb_launch_best_update(hr.out, bt->best, D, st->step, rp->nStep, hr.f, s);
+                if (rp->keepBestBodies) {
+                    NbTreeBuffers& b = st->b;
+                    nb_launch_keep_best(bt->best, bt->bodyDwarf, b.px, b.py, b.pz, b.vx, b.vy,
+                                        b.vz, st->nbody, st->keepPos, st->keepVel, st->numSMs, s);
+                }
+            }
+        }
+    }
+    bt->lastStepMs = steps ? total / steps : 0.0;
+    bt->lastSteps = steps;
+    std::vector<double> fin((size_t) NB_LIKELIHOOD_TERMS * D, NAN);
+    const bool ok = !(all & ~(int) NBODY_STATUS_WARNINGS_MASK);
+    if (like && ok) {
+        nb_hist_launch(st, bt->bodyDwarf, hr, true);
+        NB_CHECK(cudaMemcpyAsync(fin.data(), hr.out, 8 * fin.size(), cudaMemcpyDeviceToHost, s));
+    }
+    NB_CHECK(cudaMemcpyAsync(bestHost.data(), bt->best, sizeof(NbBestDev) * (size_t) D,
+                             cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaGetLastError());
+    NB_CHECK(cudaStreamSynchronize(s));
+    for (int d = 0; d < D; ++d) {
+        NBodyCudaRunResult& r = res[d];
+        const NbBestDev& b = bestHost[d];
+        r.runs = 1;
+        r.previousForwardTime = pft;
+        r.bestTime = b.bestTime;
+        r.bestStep = b.bestStep;
+        r.bestCount = b.count;
+        bt->haveKeep = bt->haveKeep || (rp->keepBestBodies && b.count > 0);
+        for (int t = 0; t < NB_LIKELIHOOD_TERMS; ++t) r.best[t] = b.best[t];
+        if (!(like && ok)) continue;
+        // nbody.c:308-345: clamp the final likelihood, then the best one replaces it if better
+        for (int t = 0; t < NB_LIKELIHOOD_TERMS; ++t) r.final[t] = fin[(size_t) NB_LIKELIHOOD_TERMS * d + t];
+        double& l = r.final[0];
+        const double worst = 9999999.9;
+        if (l > worst || l < -1 * worst) l = worst;
+        else if (l == 0.0) l = 1e-9;
+        const bool useBest = rp->useBestLike && fabs(r.final[0]) > fabs(b.best[0]);
+        for (int t = 0; t < NB_LIKELIHOOD_TERMS; ++t) r.result[t] = useBest ? b.best[t] : r.final[t];
+    }
+    return all;
+}
+
+// The bodies of every dwarf at its best likelihood (valid for the dwarfs whose bestCount > 0).
+NBodyCudaStatus nbBatchGetBestBodiesCUDA(NBodyCudaBatch* bt, double* pos, double* vel)
+{
+    if (!bt || !bt->haveKeep) {
+        g_lastError = "nbBatchGetBestBodiesCUDA: no best-likelihood bodies kept";
+        return NBODY_USER_ERROR;
+    }
+    NBodyCudaState* st = bt->st;
+    NB_CHECK(cudaSetDevice(st->device));
+    const size_t bytes = 3 * (size_t) st->nbody * sizeof(double);
+    if (pos) NB_CHECK(cudaMemcpyAsync(pos, st->keepPos, bytes, cudaMemcpyDeviceToHost, st->stream));
+    if (vel) NB_CHECK(cudaMemcpyAsync(vel, st->keepVel, bytes, cudaMemcpyDeviceToHost, st->stream));
+    NB_CHECK(cudaStreamSynchronize(st->stream));
+    return NBODY_SUCCESS;
 }
 
 NBodyCudaStatus nbBatchLastStepTimeCUDA(NBodyCudaBatch* bt, double* stepMs)

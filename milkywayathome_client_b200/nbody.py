@@ -698,6 +698,33 @@ class NBodyBatch:
         arr = (_lib.PlummerDwarf * len(dwarfs))(*dwarfs)
         self.check("nbBatchGenerateDwarfs", self.lib.nbBatchGenerateDwarfsCUDA(self._h, arr))
 
+    def run_system(self, ctx, nstep, time_evolve, params=None, data=None, use_best_like=False,
+                   best_like_start=0.95, keep_best_bodies=False, graph=True):
+        """NBodyState.run_system for every dwarf at once (nbBatchRunSystemCUDA): returns
+        (status, [dict per dwarf]) with the keys of NBodyState.run_system."""
+        rp = _lib.RunParams(int(nstep), int(bool(use_best_like)), float(time_evolve),
+                            float(best_like_start), 0, int(bool(keep_best_bodies)))
+        res = (_lib.RunResult * self.ndwarfs)()
+        hp = params.struct() if params is not None else None
+        dh = data.struct() if data is not None else None
+        rc = self.lib.nbBatchRunSystemCUDA(ctypes.byref(ctx.struct), self._h, ctypes.byref(rp),
+                                           ctypes.byref(hp) if hp is not None else None,
+                                           ctypes.byref(dh) if dh is not None else None,
+                                           int(bool(graph)), res)
+        out = [{"result": np.array(r.result[:]), "final": np.array(r.final[:]),
+                "best": np.array(r.best[:]), "best_time": r.bestTime, "best_step": r.bestStep,
+                "best_count": r.bestCount, "previous_forward_time": r.previousForwardTime,
+                "runs": r.runs} for r in res]
+        return rc, out
+
+    def best_bodies(self):
+        """Every dwarf's bodies at its best likelihood (nbBatchGetBestBodiesCUDA)."""
+        n = int(self.offsets[-1])
+        pos, vel = np.empty((n, 3)), np.empty((n, 3))
+        self.check("nbBatchGetBestBodies", self.lib.nbBatchGetBestBodiesCUDA(
+            self._h, _lib.ptr(pos), _lib.ptr(vel)))
+        return pos, vel
+
     def set_time_origin(self, previous_forward_time):
         self.check("nbBatchSetTimeOrigin", self.lib.nbBatchSetTimeOriginCUDA(
             self._h, float(previous_forward_time)))

@@ -210,3 +210,61 @@ def test_lmc_steps_equal_reference(variant):
         np.testing.assert_allclose(gpos, want["pos"], rtol=1e-10, atol=1e-12)
         np.testing.assert_allclose(p, wp, rtol=1e-12)
         np.testing.assert_allclose(v, wv, rtol=1e-12)
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_batch_run_system_with_best_likelihood_scan(graph):
+    """nbBatchRunSystemCUDA on three model-5 dwarfs (three seeds) with the best-likelihood scan
+    over the last 5 % of the steps and the best bodies kept: every dwarf's result, best step,
+    best count and best bodies equal those of its own nbRunSystemCUDA run (FP64 batches step
+    bit for bit like single states), and the final likelihood is the golden one when the scan
+    is off."""
+    from oracle import bindings as ob
+    from milkywayathome_client_b200 import (HistogramParams, NBodyBatch, NBodyCtx, NBodyState,
+                                            _lib, read_histogram)
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    seeds = ("670828913", "886885833", "715144259")
+    data = read_histogram(os.path.join(GOLDEN, "orphan_model_histogram_3"))
+    dwarfs = []
+    for seed in seeds:
+        r = ob.RefState.open_lua(os.path.join(GOLDEN, "orphan_dwarf.lua"),
+                                 os.path.join(GOLDEN, "orphan_model_histogram_3"), int(seed),
+                                 ["100", "5", "bestlike"])
+        c, nstep, time_evolve = r.ctx(_lib.Ctx)
+        use_best, start, _ = r.run_params()
+        init = r.get()
+        mass, types = r.masses()
+        dwarfs.append((c, nstep, time_evolve, start, init, mass, types,
+                       HistogramParams(**r.like_params())))
+    c, nstep, time_evolve, start, _, _, _, params = dwarfs[0]
+    ctx = NBodyCtx.from_struct(c, nstep)
+    want = []
+    for c_, _, _, _, init, mass, types, _ in dwarfs:
+        assert c_.timestep == c.timestep and c_.eps2 == c.eps2
+        with NBodyState.create(ctx, init["pos"], init["vel"], mass) as st:
+            st.set_types(types)
+            rc, res = st.run_system(ctx, nstep, time_evolve, params, data, use_best_like=True,
+                                    best_like_start=start, keep_best_bodies=True)
+            assert rc == 0
+            want.append((res, st.best_bodies()))
+    spec = [(len(d[5]), c.eps2, c.timestep, 4.0) for d in dwarfs]
+    with NBodyBatch(spec) as bt:
+        bt.set_bodies(np.concatenate([d[4]["pos"] for d in dwarfs]),
+                      np.concatenate([d[4]["vel"] for d in dwarfs]),
+                      np.concatenate([d[5] for d in dwarfs]))
+        bt.set_types(np.concatenate([d[6] for d in dwarfs]))
+        rc, got = bt.run_system(ctx, nstep, time_evolve, params, data, use_best_like=True,
+                                best_like_start=start, keep_best_bodies=True, graph=graph)
+        assert rc == 0
+        bpos, bvel = bt.best_bodies()
+        offs = bt.offsets
+    for k, ((w, (wpos, wvel)), g) in enumerate(zip(want, got)):
+        assert w["best_count"] >= 1
+        for key in ("best_step", "best_count", "runs"):
+            assert g[key] == w[key], (k, key, g[key], w[key])
+        assert g["best_time"] == w["best_time"]
+        for key in ("result", "final", "best"):
+            assert np.array_equal(g[key], w[key], equal_nan=True), (k, key, g[key], w[key])
+        s = slice(offs[k], offs[k + 1])
+        assert np.array_equal(bpos[s], wpos) and np.array_equal(bvel[s], wvel)
