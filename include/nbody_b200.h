@@ -261,6 +261,14 @@ typedef struct {                       /* a data histogram as nbReadHistogram re
      * each, NULL where the file holds none */
     const double* compVariable[NBODY_CUDA_HIST_COMPONENTS];
     const double* compErr[NBODY_CUDA_HIST_COMPONENTS];
+    /* the lambda ranges of the EMD ("EMDRange = {start, end, ...}", the values as strtof
+     * parses them, params.EMDRange of nbody/src/nbody_histogram.c:1547-1561): nRange values,
+     * pairs of inclusive bounds; nRange 0: one range over every bin (the file's default).  The
+     * EMD is taken per range over its used bins, each renormalised, weighted by the range's
+     * share of the data counts (nbMatchEMD, nbody/src/nbody_emd.c:1332-1402). */
+    int nRange;
+    int reserved2;
+    const double* emdRange;
 } NBodyCudaDataHistogram;
 /* ---- nbRunSystem: the run loop with the best-likelihood scan and the bar's calibration ----
  * The forward evolution of nbody/src/nbody.c:420-520 around nbRunSystemPlain

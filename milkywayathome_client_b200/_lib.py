@@ -141,7 +141,9 @@ class DataHist(ctypes.Structure):
                 ("err", ctypes.POINTER(ctypes.c_double)),
                 ("betaDispBins", ctypes.c_int), ("reserved", ctypes.c_int),
                 ("compVariable", ctypes.POINTER(ctypes.c_double) * HIST_COMPONENTS),
-                ("compErr", ctypes.POINTER(ctypes.c_double) * HIST_COMPONENTS)]
+                ("compErr", ctypes.POINTER(ctypes.c_double) * HIST_COMPONENTS),
+                ("nRange", ctypes.c_int), ("reserved2", ctypes.c_int),
+                ("emdRange", ctypes.POINTER(ctypes.c_double))]
 
 
 class RunParams(ctypes.Structure):

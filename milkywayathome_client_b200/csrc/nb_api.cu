@@ -1245,6 +1245,10 @@ static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int
             g_lastError = "data histogram does not match the histogram parameters";
             return NBODY_USER_ERROR;
         }
+        if (data->nRange < 0 || data->nRange > 1024 || (data->nRange > 0 && !data->emdRange)) {
+            g_lastError = "data histogram: invalid EMD ranges";
+            return NBODY_USER_ERROR;
+        }
         if (hp->betaBins != 1) {
             g_lastError = "the likelihood is implemented for one beta bin";
             return NBODY_UNSUPPORTED;
@@ -1322,7 +1326,8 @@ static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int
                         nb_al(4 * chunks.size() * Bz) + nb_al(4 * Dz * Bz) + nb_al(4 * nz) +
                         5 * nb_al(8 * QDB) + nb_al(4 * Dz) + nb_al(8 * NB_LIKELIHOOD_TERMS * Dz) +
                         nb_al(8 * Dz * NB_HIST_COMPONENTS * 2 * Bz) + nb_al(4 * Bz) +
-                        (3 + 2 * NB_HIST_COMPONENTS) * nb_al(8 * Bz) + 256;
+                        (3 + 2 * NB_HIST_COMPONENTS) * nb_al(8 * Bz) +
+                        nb_al(8 * (size_t) (data && data->nRange > 0 ? data->nRange : 0)) + 256;
     NB_CHECK(cudaSetDevice(st->device));
     if (st->histScratchBytes < need) {
         cudaFree(st->histScratch);
@@ -1382,6 +1387,13 @@ static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int
         dh.totalNum = data->totalNum;
         dh.nBins = B;
         dh.betaDispBins = data->betaDispBins;
+        dh.nRange = data->nRange;
+        dh.emdRange = nullptr;
+        if (data->nRange > 0) {
+            double* dst = (double*) carve(8 * (size_t) data->nRange);
+            cudaMemcpyAsync(dst, data->emdRange, 8 * (size_t) data->nRange, cudaMemcpyHostToDevice, s);
+            dh.emdRange = dst;
+        }
         NB_CHECK(cudaGetLastError());
     }
     return NBODY_SUCCESS;

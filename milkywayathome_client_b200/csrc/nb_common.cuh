@@ -189,6 +189,8 @@ struct NbDataHistDev {
     unsigned int totalNum;
     int nBins;
     int betaDispBins;
+    int nRange;                     // EMD lambda ranges (0: one over every bin)
+    const double* emdRange;
 };
 // Which comparison terms nbSystemLikelihood adds (the reference's st->use* flags).
 struct NbLikeFlags {

@@ -412,30 +412,54 @@ __global__ void k_likelihood(NbHistPlan p, const double* __restrict__ mass,
         emdComp = INFINITY;
     } else if (histMass <= 0.0 || dh.massPerParticle <= 0.0) {
         emdComp = NAN;
+    } else if (dh.nRange % 2 != 0) {
+        emdComp = NAN;                                  // an odd number of range bounds
     } else {
-        // weights of the used bins, as nbMatchEMD forms them
-        unsigned simRange = 0, dataRange = 0;
-        for (int j = 0; j < nb; ++j) {
-            if (!dh.useBin[j]) continue;
-            const double var = (double) c[j] / (double) nSimU;
-            simRange += (unsigned) round(var * (double) nSimU);
-            dataRange += (unsigned) round(dh.variable[j] * (double) nData);
+        // per lambda range (one over every bin by default): the used bins whose centres lie in
+        // it -- the simulated histogram's centres (i + 0.5) lambdaSize + lambdaStart, the data
+        // file's own -- each side renormalised to the range, the range's EMD weighted by its
+        // share of the data counts
+        // (without ranges every used bin counts: the file's default range reaches half a bin
+        // beyond the outer centres)
+        const bool every = dh.nRange == 0;
+        const int nR = every ? 2 : dh.nRange;
+        double emdSum = 0.0;
+        unsigned totalRange = 0;
+        bool bad = false;
+        for (int r = 0; r < nR && !bad; r += 2) {
+            const double lo = every ? 0.0 : dh.emdRange[r];
+            const double hi = every ? 0.0 : dh.emdRange[r + 1];
+            if (lo > hi) { bad = true; break; }
+            unsigned simRange = 0, dataRange = 0;
+            for (int j = 0; j < nb; ++j) {
+                if (!dh.useBin[j]) continue;
+                const double simL = ((double) (j / p.h.betaBins) + 0.5) * p.h.lambdaSize + p.h.lambdaStart;
+                if (every || (simL >= lo && simL <= hi))
+                    simRange += (unsigned) round(((double) c[j] / (double) nSimU) * (double) nSimU);
+                if (every || (dh.lambda[j] >= lo && dh.lambda[j] <= hi))
+                    dataRange += (unsigned) round(dh.variable[j] * (double) nData);
+            }
+            double Fs = 0.0, Fd = 0.0, cost = 0.0, prevL = 0.0;
+            bool first = true;
+            for (int j = 0; j < nb; ++j) {
+                if (!dh.useBin[j] || !(every || (dh.lambda[j] >= lo && dh.lambda[j] <= hi))) continue;
+                if (!first) cost += fabs(Fs - Fd) * (dh.lambda[j] - prevL);
+                const double var = (double) c[j] / (double) nSimU;
+                Fs += var * (double) nSimU / (1.0 * simRange);
+                Fd += dh.variable[j] * (double) nData / (1.0 * dataRange);
+                prevL = dh.lambda[j];
+                first = false;
+            }
+            totalRange += dataRange;
+            emdSum += cost * ((double) dataRange / (1.0 * nData));
         }
-        double Fs = 0.0, Fd = 0.0, cost = 0.0, prevL = 0.0;
-        bool first = true;
-        for (int j = 0; j < nb; ++j) {
-            if (!dh.useBin[j]) continue;
-            if (!first) cost += fabs(Fs - Fd) * (dh.lambda[j] - prevL);
-            const double var = (double) c[j] / (double) nSimU;
-            Fs += var * (double) nSimU / (1.0 * simRange);
-            Fd += dh.variable[j] * (double) nData / (1.0 * dataRange);
-            prevL = dh.lambda[j];
-            first = false;
+        if (bad || totalRange == 0) {
+            emdComp = NAN;
+        } else {
+            emd = emdSum * (double) (nData / totalRange);   // integer division, as the reference
+            emd = round(emd * 1.0e9) * 1.0e-9;
+            emdComp = emd > 50.0 ? NAN : -(300.0 * nb_log_rn(1.0 - emd / 50.0));   // mw_log
         }
-        emd = cost * ((double) dataRange / (1.0 * nData));
-        emd = emd * (double) (nData / dataRange);       // integer division, as the reference
-        emd = round(emd * 1.0e9) * 1.0e-9;
-        emdComp = emd > 50.0 ? NAN : -(300.0 * nb_log_rn(1.0 - emd / 50.0));   // mw_log
     }
     double costComp;
     if (nSimU == 0 || nData == 0) {

@@ -16,6 +16,7 @@ a simulation (the likelihood target of a parameter fit).
 """
 import ctypes
 import math
+import re
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -108,6 +109,8 @@ class DataHistogram:
     # histograms 1..7 (COMPONENTS order): (values, errors) or None where the file has none
     components: list = field(default_factory=lambda: [None] * 7)
     betaDispBins: int = 0
+    # "EMDRange = {...}": the EMD's lambda ranges as pairs of bounds (None: every bin)
+    emdRange: np.ndarray = None
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -144,8 +147,39 @@ class DataHistogram:
             keep += [v, e]
             d.compVariable[k] = v.ctypes.data_as(dp)
             d.compErr[k] = e.ctypes.data_as(dp)
+        d.nRange = 0
+        if self.emdRange is not None:
+            rng = np.ascontiguousarray(self.emdRange, dtype=np.float64)
+            keep.append(rng)
+            d.nRange = len(rng)
+            d.emdRange = rng.ctypes.data_as(dp)
         self._keep = keep
         return d
+
+
+_libc = None
+
+
+def _strtof(text):
+    """The C library's strtof (decimal to the nearest float, then exactly to double)."""
+    global _libc
+    if _libc is None:
+        _libc = ctypes.CDLL(None)
+        _libc.strtof.restype = ctypes.c_float
+        _libc.strtof.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+    return float(_libc.strtof(text.encode(), None))
+
+
+def parse_emd_range(value):
+    """params.EMDRange as nbReadHistogram reads an "EMDRange = {...}" line
+    (nbody/src/nbody_histogram.c:1290-1301 and 1547-1561): the first token without white space
+    after the brace, cut at any of {}()[], and space, each piece parsed by strtof."""
+    v = value.strip()
+    if not v.startswith("{"):
+        return None
+    words = v[1:].split()
+    token = words[0] if words else ""
+    return np.array([_strtof(t) for t in re.split(r"[{}()\[\], ]", token) if t])
 
 
 def read_histogram(path):
@@ -174,9 +208,6 @@ def read_histogram(path):
                 header[k] = v
                 continue
             rows.append([float(t) for t in s.split()])
-    if "EMDRange" in header:
-        raise ValueError("%s: an EMDRange restricts the EMD, which this build does not support"
-                         % path)
     has_pm = int(header.get("hasPM", 0)) == 1
     ncols = (19 if has_pm else 15) if extended else 9
     rows = np.array(rows)
@@ -190,7 +221,9 @@ def read_histogram(path):
                          totalSimulated=int(header.get("totalSimulated", 0)),
                          useBin=rows[:, 0].astype(np.int32), lambda_=rows[:, 1], beta=rows[:, 2],
                          variable=rows[:, 3], err=rows[:, 4], components=comps,
-                         betaDispBins=int(header.get("betaDispBins", 0)))
+                         betaDispBins=int(header.get("betaDispBins", 0)),
+                         emdRange=(parse_emd_range(header["EMDRange"])
+                                   if "EMDRange" in header else None))
 
 
 def write_histogram(path, params, data):
@@ -207,6 +240,9 @@ def write_histogram(path, params, data):
         f.write("betaBins = %u\n" % params.betaBins)
         if data.betaDispBins:
             f.write("betaDispBins = %u\n" % data.betaDispBins)
+        if data.emdRange is not None:         # float values, written to parse back exactly
+            f.write("EMDRange = {%s}\n" % ",".join(repr(float(np.float32(v)))
+                                                    for v in data.emdRange))
         if full:
             f.write("hasPM = 1\n!\n")
         ncomp = 7 if full else 2

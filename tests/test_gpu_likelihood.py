@@ -51,10 +51,10 @@ def _assert_terms(got, ref):
             assert abs(got[k] - ref[k]) <= 1e-9 * max(1.0, abs(ref[k])), (k, got, ref)
 
 
-def _run_case(variant, nbody, seed, extra=()):
+def _run_case(variant, nbody, seed, extra=(), hist=HIST):
     from oracle import bindings as ob
     from milkywayathome_client_b200 import NBodyCtx, NBodyState, _lib
-    r = ob.RefState.open_lua(LUA, HIST, int(seed), [nbody, variant] + list(extra))
+    r = ob.RefState.open_lua(LUA, hist, int(seed), [nbody, variant] + list(extra))
     c, nstep, _ = r.ctx(_lib.Ctx)
     ctx = NBodyCtx.from_struct(c, nstep)
     init = r.get()
@@ -83,6 +83,31 @@ def test_likelihood_matches_reference(variant, nbody, seed):
     assert totals[0, 0] == counts.sum()
     assert np.isfinite(ref[3])                 # the beta-dispersion term is compared
     _assert_terms(got, ref)
+
+
+@pytest.mark.parametrize("ranges", ["{-40,-10.3,10.3,40}", "{-30,0}", "{-45,-20,-15,5,12,48}",
+                                    "{-50,50}", "{-40,-10}"])
+def test_emd_ranges_match_reference(tmp_path, ranges):
+    """A data file with an EMDRange line: the EMD per lambda range, each renormalised and
+    weighted by its share of the data counts, rescaled by the integer ratio of all data counts
+    to those in the ranges (nbMatchEMD, nbody/src/nbody_emd.c:1332-1427)."""
+    from oracle import bindings as ob
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    from milkywayathome_client_b200 import read_histogram
+    path = tmp_path / "ranged_histogram"
+    path.write_text(open(HIST).read().replace("betaBins = 1\n",
+                                              "betaBins = 1\nEMDRange = %s\n" % ranges))
+    r, st, _ = _run_case("5", "1024", "886885833", hist=str(path))
+    data = read_histogram(str(path))
+    assert data.emdRange is not None
+    ref = r.likelihood()
+    got = st.likelihood(_orphan_params(), data)[0]
+    full = st.likelihood(_orphan_params(), read_histogram(HIST))[0]
+    st.close()
+    _assert_terms(got, ref)
+    if ranges != "{-50,50}":
+        assert got[1] != full[1]               # the ranges change the EMD term
 
 
 @pytest.mark.parametrize("beta_disp_bins", [0, 3, 4])

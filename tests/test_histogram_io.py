@@ -59,10 +59,21 @@ def test_parameter_struct_defaults():
     assert (h.sunVelx, h.sunVely, h.sunVelz) == (10.3, 229.2, 6.9)
 
 
-def test_emd_range_is_rejected(tmp_path):
-    from milkywayathome_client_b200 import read_histogram
+def test_emd_range_is_read_as_the_reference_reads_it(tmp_path):
+    """EMDRange lines (nbReadHistogram: sscanf " EMDRange = {%s}", strtok, strtof): float
+    values, the first white-space-free token only, and a write/read round trip."""
+    import numpy as np
+    from milkywayathome_client_b200 import HistogramParams, read_histogram, write_histogram
     src = open(os.path.join(GOLDEN, "orphan_model_histogram_3")).read()
     path = tmp_path / "h"
-    path.write_text(src.replace("betaBins = 1\n", "betaBins = 1\nEMDRange = {-20,20}\n"))
-    with pytest.raises(ValueError):
-        read_histogram(str(path))
+    path.write_text(src.replace("betaBins = 1\n", "betaBins = 1\nEMDRange = {-40,-10.3,10.3,40}\n"))
+    h = read_histogram(str(path))
+    assert list(h.emdRange) == [-40.0, float(np.float32(-10.3)), float(np.float32(10.3)), 40.0]
+    d = h.struct()
+    assert d.nRange == 4 and d.emdRange[1] == float(np.float32(-10.3))
+    out = tmp_path / "h2"
+    write_histogram(str(out), HistogramParams(lambdaBins=h.nbins), h)
+    assert np.array_equal(read_histogram(str(out)).emdRange, h.emdRange)
+    path.write_text(src.replace("betaBins = 1\n", "betaBins = 1\nEMDRange = { -40, -10 }\n"))
+    assert list(read_histogram(str(path)).emdRange) == [-40.0]     # an odd count: NaN EMD
+    assert read_histogram(os.path.join(GOLDEN, "orphan_model_histogram_3")).struct().nRange == 0
