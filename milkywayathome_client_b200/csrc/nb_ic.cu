@@ -39,8 +39,23 @@ struct NbIcComp {
     double C2, C3;               // cored potential constants (cored_pot)
     double bound, rhoMax;        // r_mag's sampling bound and maximum of r^2 rho
 
-    // get_density (nbody_dwarf_potential.c:207-236)
+    // get_density (nbody_dwarf_potential.c:207-236); the Plummer case inline, the others out of
+    // line, so that the DF integrand's many evaluations keep the Plummer sampler's registers
     NB_HD double den(double r) const
+    {
+        if (type == NBCUDA_DWARF_PLUMMER) {
+            const double x = 1.0 + (r / a) * (r / a);
+            return (3.0 / (4.0 * M_PI)) * (M / (a * a * a)) * (1.0 / sqrt(x * x * x * x * x));
+        }
+        return den_profile(r);
+    }
+    // get_potential (nbody_dwarf_potential.c:176-205), the positive psi
+    NB_HD double pot(double r) const
+    {
+        if (type == NBCUDA_DWARF_PLUMMER) return M / sqrt(r * r + a * a);
+        return pot_profile(r);
+    }
+    __host__ __device__ __noinline__ double den_profile(double r) const
     {
         switch (type) {
         case NBCUDA_DWARF_NFW: {
@@ -49,19 +64,15 @@ struct NbIcComp {
         }
         case NBCUDA_DWARF_GEN_HERNQUIST:
             return (1.0 / (2.0 * M_PI)) * M * a / (r * ((r + a) * (r + a) * (r + a)));
-        case NBCUDA_DWARF_CORED:
+        default:                                     // cored
             if (r <= r1) return p0 / (1.0 + (r / rc) * (r / rc));
             return ps / ((r / a) * ((1.0 + r / a) * (1.0 + r / a)));
-        default: {                                   // Plummer
-            const double x = 1.0 + (r / a) * (r / a);
-            return (3.0 / (4.0 * M_PI)) * (M / (a * a * a)) * (1.0 / sqrt(x * x * x * x * x));
-        }
         }
     }
-    // get_potential (nbody_dwarf_potential.c:176-205), the positive psi; its log and atan are
-    // the CUDA library's (the samples match the reference's in distribution only, and psi is
-    // evaluated ~10^5 times per body), the set-up's below correctly rounded as the reference's
-    NB_HD double pot(double r) const
+    // log and atan are the CUDA library's here (the samples match the reference's in
+    // distribution only, and psi is evaluated ~10^5 times per body); the set-up's below are
+    // correctly rounded as the reference's
+    __host__ __device__ __noinline__ double pot_profile(double r) const
     {
         switch (type) {
         case NBCUDA_DWARF_NFW: {
@@ -70,13 +81,11 @@ struct NbIcComp {
         }
         case NBCUDA_DWARF_GEN_HERNQUIST:
             return M / (r + a);
-        case NBCUDA_DWARF_CORED:
+        default:                                     // cored
             if (r <= r1)
                 return -1.0 * (4.0 * M_PI * p0 * ((rc * rc) / 2.0 * log(r * r + rc * rc) +
                                                   (rc * rc * rc) / r * atan(r / rc)) + C2);
             return -1.0 * (-4.0 * M_PI * ps * (a * a * a) / r * log(1.0 + r / a) + C3 / r);
-        default:
-            return M / sqrt(r * r + a * a);
         }
     }
 };
@@ -102,10 +111,37 @@ struct NbRng {
     }
 };
 
+// The two components of the body's dwarf as the DF evaluation sees them: potL/potD/psi/den
+// and the masses and scale lengths.  Two forms: both components Plummer, held in four
+// registers (the common case; the potential is evaluated ~10^5 times per body), and any
+// profiles, read from the device table.
+struct NbIcPlummerModel {
+    double ML, aL, MD, aD;
+    __device__ double potL(double r) const { return ML / sqrt(r * r + aL * aL); }
+    __device__ double potD(double r) const { return MD / sqrt(r * r + aD * aD); }
+    __device__ double psi(double r) const { return potL(r) + potD(r); }
+    __device__ double den(bool dark, double r) const
+    {
+        const double M = dark ? MD : ML, a = dark ? aD : aL;
+        const double x = 1.0 + (r / a) * (r / a);
+        return (3.0 / (4.0 * M_PI)) * (M / (a * a * a)) * (1.0 / sqrt(x * x * x * x * x));
+    }
+    __device__ double massL() const { return ML; }
+    __device__ double massD() const { return MD; }
+    __device__ double scaleL() const { return aL; }
+    __device__ double scaleD() const { return aD; }
+};
 struct NbIcModel {
-    NbIcComp L, D;
-    __device__ double psi(double r) const { return L.pot(r) + D.pot(r); }
-    __device__ double den(bool dark, double r) const { return dark ? D.den(r) : L.den(r); }
+    const NbIcComp* __restrict__ L;
+    const NbIcComp* __restrict__ D;
+    __device__ double potL(double r) const { return L->pot(r); }
+    __device__ double potD(double r) const { return D->pot(r); }
+    __device__ double psi(double r) const { return L->pot(r) + D->pot(r); }
+    __device__ double den(bool dark, double r) const { return dark ? D->den(r) : L->den(r); }
+    __device__ double massL() const { return L->M; }
+    __device__ double massD() const { return D->M; }
+    __device__ double scaleL() const { return L->a; }
+    __device__ double scaleD() const { return D->a; }
 };
 
 // five-point stencils with h = 0.001 (first_derivative / second_derivative)
@@ -127,10 +163,11 @@ __device__ __forceinline__ double d2(F f, double x)
 }
 
 // the DF integrand d^2 rho / d psi^2 / sqrt(|E - psi|) at radius ri (fun)
-__device__ double ic_integrand(const NbIcModel& m, double ri, double energy, bool dark)
+template <typename Model>
+__device__ double ic_integrand(const Model& m, double ri, double energy, bool dark)
 {
-    auto potL = [&](double r) { return m.L.pot(r); };
-    auto potD = [&](double r) { return m.D.pot(r); };
+    auto potL = [&](double r) { return m.potL(r); };
+    auto potD = [&](double r) { return m.potD(r); };
     auto denC = [&](double r) { return m.den(dark, r); };
     double dpsi = d1(potL, ri) + d1(potD, ri);
     const double d2psi = d2(potL, ri) + d2(potD, ri);
@@ -144,7 +181,8 @@ __device__ double ic_integrand(const NbIcModel& m, double ri, double energy, boo
 }
 
 // composite three-point Gauss quadrature: 100 panels over [a, 1.5 a], then 10 up to b
-__device__ double ic_gauss_quad(const NbIcModel& m, double lower, double upper, double energy,
+template <typename Model>
+__device__ double ic_gauss_quad(const Model& m, double lower, double upper, double energy,
                                 bool dark)
 {
     const double a = lower > upper ? upper : lower, b = lower > upper ? lower : upper;
@@ -172,7 +210,8 @@ __device__ double ic_gauss_quad(const NbIcModel& m, double lower, double upper, 
 }
 
 // bisection for psi(r) = value on [lo, hi] split in 4 intervals (root_finder); 0 if none
-__device__ double ic_root(const NbIcModel& m, double value, double lo, double hi)
+template <typename Model>
+__device__ double ic_root(const Model& m, double value, double lo, double hi)
 {
     double vals[5], bounds[5];
     for (int i = 0; i < 5; ++i) {
@@ -199,15 +238,17 @@ __device__ double ic_root(const NbIcModel& m, double value, double lo, double hi
 }
 
 // the Eddington DF at speed v and radius r (dist_fun)
-__device__ double ic_df(const NbIcModel& m, double v, double r, bool dark)
+template <typename Model>
+__device__ double ic_df(const Model& m, double v, double r, bool dark)
 {
     const double cons = 0.03582244801567226;
     const double energy = m.psi(r) - 0.5 * v * v;
-    double range = m.D.M == 0 ? 20.0 * sqrt(fabs((m.L.M / energy) * (m.L.M / energy) - m.L.a * m.L.a))
-                              : 20.0 * sqrt(fabs((m.D.M / energy) * (m.D.M / energy) - m.D.a * m.D.a));
+    const double ML = m.massL(), MD = m.massD(), aL = m.scaleL(), aD = m.scaleD();
+    double range = MD == 0 ? 20.0 * sqrt(fabs((ML / energy) * (ML / energy) - aL * aL))
+                           : 20.0 * sqrt(fabs((MD / energy) * (MD / energy) - aD * aD));
     for (int counter = 0; m.psi(range) > energy; ++counter) {
         range = 100.0 * range;
-        if (counter > 100) { range = 100.0 * (m.L.a + m.D.a); break; }
+        if (counter > 100) { range = 100.0 * (aL + aD); break; }
     }
     double up = ic_root(m, energy, 0.0, range);
     if (isinf(up) || up == 0.0 || isnan(up)) up = r;        // find_upperlimit_r's fallback
@@ -217,7 +258,8 @@ __device__ double ic_df(const NbIcModel& m, double v, double r, bool dark)
 }
 
 // golden-section search for the DF maximum over speeds (max_finder)
-__device__ double ic_df_max(const NbIcModel& m, double r, bool dark, double a, double b,
+template <typename Model>
+__device__ double ic_df_max(const Model& m, double r, bool dark, double a, double b,
                             double c, int limit, double tol)
 {
     const double R = 0.61803399, C = 1.0 - R;
@@ -271,7 +313,40 @@ __device__ int ic_dwarf_of(const NbIcDwarf* dw, int nD, int i)
     return lo;
 }
 
-// One body per thread: radius and speed by rejection, isotropic directions.
+// The radius and speed of one body by rejection (r_mag, vel_mag); r = v = 0 when either fails.
+template <typename Model>
+__device__ void ic_sample_rv(const Model& m, const NbIcComp& comp, bool dark, NbRng& rng,
+                             double& rOut, double& vOut)
+{
+    double r = 0.0;
+    for (int tries = 0; tries <= 1000 && !(isfinite(r) && r != 0.0); ++tries) {
+        r = 0.0;
+        for (int counter = 0; counter <= 1000; ++counter) {      // r_mag
+            const double rr = rng.uniform() * comp.bound;
+            const double u = rng.uniform();
+            if (rr * rr * m.den(dark, rr) / comp.rhoMax > u) { r = rr; break; }
+        }
+    }
+    double v = 0.0;
+    if (isfinite(r) && r != 0.0) {
+        const double vesc = 0.99 * sqrt(fabs(2.0 * m.psi(r)));
+        const double dfMax = ic_df_max(m, r, dark, 0.0, 0.5 * vesc, vesc, 10, 1.0e-2);
+        for (int tries = 0; tries <= 1000 && !(isfinite(v) && v != 0.0); ++tries) {
+            v = 0.0;
+            for (int counter = 0; counter <= 1000; ++counter) {  // vel_mag
+                const double vv = rng.uniform() * vesc;
+                const double u = rng.uniform();
+                if (fabs(ic_df(m, vv, r, dark) / dfMax) > u) { v = vv; break; }
+            }
+        }
+    }
+    rOut = r;
+    vOut = v;
+}
+
+// One body per thread: radius and speed by rejection, isotropic directions.  ALL_PLUMMER: every
+// dwarf of the table has two Plummer components (their model in registers).
+template <bool ALL_PLUMMER>
 __global__ void k_ic_sample(const NbIcDwarf* __restrict__ dwarfs, int nD, int n,
                             double* __restrict__ px, double* __restrict__ py,
                             double* __restrict__ pz, double* __restrict__ vx,
@@ -283,30 +358,15 @@ __global__ void k_ic_sample(const NbIcDwarf* __restrict__ dwarfs, int nD, int n,
         const NbIcDwarf& d = dwarfs[ic_dwarf_of(dwarfs, nD, i)];
         const int k = i - d.first;
         const bool dark = k >= d.nBaryon;
-        const NbIcModel m{d.L, d.D};
         NbRng rng{ic_mix(d.seed ^ ic_mix((unsigned long long) k + 0x51ED27ull))};
         const NbIcComp& comp = dark ? d.D : d.L;
-        double r = 0.0;
-        for (int tries = 0; tries <= 1000 && !(isfinite(r) && r != 0.0); ++tries) {
-            r = 0.0;
-            for (int counter = 0; counter <= 1000; ++counter) {      // r_mag
-                const double rr = rng.uniform() * comp.bound;
-                const double u = rng.uniform();
-                if (rr * rr * comp.den(rr) / comp.rhoMax > u) { r = rr; break; }
-            }
-        }
-        double v = 0.0;
-        if (isfinite(r) && r != 0.0) {
-            const double vesc = 0.99 * sqrt(fabs(2.0 * m.psi(r)));
-            const double dfMax = ic_df_max(m, r, dark, 0.0, 0.5 * vesc, vesc, 10, 1.0e-2);
-            for (int tries = 0; tries <= 1000 && !(isfinite(v) && v != 0.0); ++tries) {
-                v = 0.0;
-                for (int counter = 0; counter <= 1000; ++counter) {  // vel_mag
-                    const double vv = rng.uniform() * vesc;
-                    const double u = rng.uniform();
-                    if (fabs(ic_df(m, vv, r, dark) / dfMax) > u) { v = vv; break; }
-                }
-            }
+        double r, v;
+        if (ALL_PLUMMER) {
+            const NbIcPlummerModel m{d.L.M, d.L.a, d.D.M, d.D.a};
+            ic_sample_rv(m, comp, dark, rng, r, v);
+        } else {
+            const NbIcModel m{&d.L, &d.D};
+            ic_sample_rv(m, comp, dark, rng, r, v);
         }
         if (!(isfinite(r) && r != 0.0 && isfinite(v) && v != 0.0)) {
             nb_raise(sc, NBODY_ERROR);                // the reference exits here
@@ -486,7 +546,13 @@ int nb_launch_ic(const NBodyCudaMixedDwarf* host, int nD, const int* firsts, voi
     const NbIcDwarf* dt = (const NbIcDwarf*) dTable;
     // few bodies per thread, many threads: the per-body work is long and uneven
     const int g = min((n + 127) / 128, numSMs * 64);
-    k_ic_sample<<<g, 128, 0, s>>>(dt, nD, n, b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.mass, types, sc);
+    bool allPlummer = true;
+    for (const NbIcDwarf& d : t)
+        allPlummer = allPlummer && d.L.type == NBCUDA_DWARF_PLUMMER && d.D.type == NBCUDA_DWARF_PLUMMER;
+    if (allPlummer)
+        k_ic_sample<true><<<g, 128, 0, s>>>(dt, nD, n, b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.mass, types, sc);
+    else
+        k_ic_sample<false><<<g, 128, 0, s>>>(dt, nD, n, b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.mass, types, sc);
     const int g2 = min((n + 255) / 256, numSMs * 8);
     k_ic_moments<<<g2, 256, 0, s>>>(dt, nD, n, b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.mass, scratch);
     k_ic_shift<<<g2, 256, 0, s>>>(dt, nD, n, b.px, b.py, b.pz, b.vx, b.vy, b.vz, scratch);
