@@ -486,8 +486,8 @@ NBodyCudaStatus nbBatchGenerateMixedDwarfsCUDA(NBodyCudaBatch* batch,
  * bestLikeStart, timeEvolve): steps through the batch's step (captured graphs when useGraph),
  * each step of the window one histogram pass, likelihood and best-record update for all
  * dwarfs; res[ndwarfs] as nbRunSystemCUDA's per dwarf.  Types must be set
- * (nbBatchSetTypesCUDA).  With an orbiting bar, calibrationRuns must be 0 (the batch shares
- * one time origin): NBODY_UNSUPPORTED otherwise. */
+ * (nbBatchSetTypesCUDA).  With an orbiting bar, the calibrationRuns restart the whole batch
+ * from its initial state, each dwarf with its own previous best time as its bar's origin. */
 NBodyCudaStatus nbBatchRunSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* batch,
                                      const NBodyCudaRunParams* rp,
                                      const NBodyCudaHistogramParams* hp,

@@ -2290,11 +2290,74 @@ NBodyCudaStatus nbBatchGenerateMixedDwarfsCUDA(NBodyCudaBatch* bt, const NBodyCu
     return nb_batch_reset_table(bt);
 }
 
+// Sets every dwarf's own bar time origin (origins: nDwarfs values) in the device table.
+static NBodyCudaStatus nb_batch_set_origins(NBodyCudaBatch* bt, const double* origins)
+{
+    NB_CHECK(cudaMemcpy2DAsync(&bt->dDwarfs[0].timeOrigin, sizeof(NbDwarfDev), origins,
+                               sizeof(double), sizeof(double), (size_t) bt->nDwarfs,
+                               cudaMemcpyHostToDevice, bt->st->stream));
+    NB_CHECK(cudaStreamSynchronize(bt->st->stream));
+    return NBODY_SUCCESS;
+}
+
+// One run of the batch (nbGravMap, the steps with the scan) into bestHost / fin (per dwarf).
+static NBodyCudaStatus nb_batch_run_once(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt,
+                                         const NBodyCudaRunParams* rp, NbHistRun* hr, bool like,
+                                         int useGraph, std::vector<NbBestDev>& bestHost,
+                                         std::vector<double>& fin)
+{
+    NBodyCudaState* st = bt->st;
+    const int D = bt->nDwarfs;
+    const cudaStream_t s = st->stream;
+    NbBestDev init{};
+    init.best[0] = 9999999.9;                       // st->bestLikelihood = DEFAULT_WORST_CASE
+    init.timeEvolve = rp->timeEvolve;
+    bestHost.assign(D, init);
+    NB_CHECK(cudaMemcpyAsync(bt->best, bestHost.data(), sizeof(NbBestDev) * (size_t) D,
+                             cudaMemcpyHostToDevice, s));
+    NBodyCudaStatus all = nb_batch_eval(ctx, bt, 0, 0, false);   // nbGravMap
+    const bool scan = like && rp->useBestLike;
+    double total = 0.0;
+    int steps = 0;
+    if (!(all & ~(int) NBODY_STATUS_WARNINGS_MASK)) {
+        while (st->step < rp->nStep) {
+            const NBodyCudaStatus rcStep = nb_batch_eval(ctx, bt, 1, 1, useGraph != 0);
+            all |= rcStep;
+            total += st->stepMs;
+            ++steps;
+            st->step++;
+            if (rcStep & ~(int) NBODY_STATUS_WARNINGS_MASK) break;
+            if (scan && (double) st->step / (double) rp->nStep >= rp->bestLikeStart) {
+                nb_hist_launch(st, bt->bodyDwarf, *hr, true);
+                nb_launch_best_update(hr->out, bt->best, D, st->step, rp->nStep, hr->f, s);
+                if (rp->keepBestBodies) {
+                    NbTreeBuffers& b = st->b;
+                    nb_launch_keep_best(bt->best, bt->bodyDwarf, b.px, b.py, b.pz, b.vx, b.vy,
+                                        b.vz, st->nbody, st->keepPos, st->keepVel, st->numSMs, s);
+                }
+            }
+        }
+    }
+    bt->lastStepMs = steps ? total / steps : 0.0;
+    bt->lastSteps = steps;
+    fin.assign((size_t) NB_LIKELIHOOD_TERMS * D, NAN);
+    if (like && !(all & ~(int) NBODY_STATUS_WARNINGS_MASK)) {
+        nb_hist_launch(st, bt->bodyDwarf, *hr, true);
+        NB_CHECK(cudaMemcpyAsync(fin.data(), hr->out, 8 * fin.size(), cudaMemcpyDeviceToHost, s));
+    }
+    NB_CHECK(cudaMemcpyAsync(bestHost.data(), bt->best, sizeof(NbBestDev) * (size_t) D,
+                             cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaGetLastError());
+    NB_CHECK(cudaStreamSynchronize(s));
+    return all;
+}
+
 // nbRunSystemCUDA for every dwarf of the batch at once: the steps through the batch's step
 // (captured graphs when useGraph), then with the best-likelihood scan each step of the window
-// one histogram pass, one likelihood and one best-record update for all dwarfs; res[d] as
-// nbRunSystemCUDA's for dwarf d.  The orbiting bar's calibration runs need a time origin per
-// dwarf and are not run for a batch.
+// one histogram pass, one likelihood and one best-record update for all dwarfs; with an
+// orbiting bar the calibration runs restart the whole batch from its initial state, each dwarf
+// with its own previous best time as its bar's time origin.  res[d] as nbRunSystemCUDA's for
+// dwarf d.
 NBodyCudaStatus nbBatchRunSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt,
                                      const NBodyCudaRunParams* rp,
                                      const NBodyCudaHistogramParams* hp,
@@ -2310,12 +2373,6 @@ NBodyCudaStatus nbBatchRunSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt
     if ((rp->useBestLike || rp->keepBestBodies) && (!hp || !data)) {
         g_lastError = "nbBatchRunSystemCUDA: the best-likelihood scan needs histogram parameters and data";
         return NBODY_USER_ERROR;
-    }
-    const bool bar = ctx->potentialType == NBCUDA_POTENTIAL_DEFAULT &&
-                     ctx->pot.disk2.type == NBCUDA_ORBITING_BAR;
-    if (bar && rp->calibrationRuns > 0) {
-        g_lastError = "nbBatchRunSystemCUDA: the bar's calibration runs need a time origin per dwarf";
-        return NBODY_UNSUPPORTED;
     }
     NBodyCudaState* st = bt->st;
     if (st->step > rp->nStep) {
@@ -2340,57 +2397,53 @@ NBodyCudaStatus nbBatchRunSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt
         NB_CHECK(nb_alloc(&st->keepPos, 3 * (size_t) st->nbody));
         NB_CHECK(nb_alloc(&st->keepVel, 3 * (size_t) st->nbody));
     }
-    NbBestDev init{};
-    init.best[0] = 9999999.9;                       // st->bestLikelihood = DEFAULT_WORST_CASE
-    init.timeEvolve = rp->timeEvolve;
-    std::vector<NbBestDev> bestHost(D, init);
-    NB_CHECK(cudaMemcpyAsync(bt->best, bestHost.data(), sizeof(NbBestDev) * (size_t) D,
-                             cudaMemcpyHostToDevice, s));
-    // nbody.c:436-447: the bar's time origin of the first (here the only) run
+    // nbody.c:436-447: the bar's first time origin; calibration only with an orbiting bar
     const double og = (2 * rp->bestLikeStart) / (rp->bestLikeStart + 1);
     const double pft = rp->useBestLike ? rp->timeEvolve / (2 - og) : rp->timeEvolve;
-    st->timeOrigin = pft;
-    bt->haveKeep = false;
-    NBodyCudaStatus all = nb_batch_eval(ctx, bt, 0, 0, false);   // nbGravMap
-    const bool scan = like && rp->useBestLike;
-    double total = 0.0;
-    int steps = 0;
-    if (!(all & ~(int) NBODY_STATUS_WARNINGS_MASK)) {
-        while (st->step < rp->nStep) {
-            const NBodyCudaStatus rcStep = nb_batch_eval(ctx, bt, 1, 1, useGraph != 0);
-            all |= rcStep;
-            total += st->stepMs;
-            ++steps;
-            st->step++;
-            if (rcStep & ~(int) NBODY_STATUS_WARNINGS_MASK) break;
-            if (scan && (double) st->step / (double) rp->nStep >= rp->bestLikeStart) {
-                nb_hist_launch(st, bt->bodyDwarf, hr, true);
-                nb_launch_best_update(hr.out, bt->best, D, st->step, rp->nStep, hr.f, s);
-                if (rp->keepBestBodies) {
-                    NbTreeBuffers& b = st->b;
-                    nb_launch_keep_best(bt->best, bt->bodyDwarf, b.px, b.py, b.pz, b.vx, b.vy,
-                                        b.vz, st->nbody, st->keepPos, st->keepVel, st->numSMs, s);
-                }
-            }
+    const bool bar = ctx->potentialType == NBCUDA_POTENTIAL_DEFAULT &&
+                     ctx->pot.disk2.type == NBCUDA_ORBITING_BAR;
+    const int runs = 1 + (bar ? rp->calibrationRuns : 0);
+    std::vector<double> origin(D, 0.0);             // the first run: the shared origin pft
+    rc = nb_batch_set_origins(bt, origin.data());
+    if (rc) return rc;
+    std::vector<NbDwarfDev> tableStart;
+    if (runs > 1) {
+        rc = nb_save_slot(st, st->runStart);
+        if (rc != NBODY_SUCCESS) return rc;
+        tableStart.resize(D);
+        NB_CHECK(cudaMemcpyAsync(tableStart.data(), bt->dDwarfs, sizeof(NbDwarfDev) * (size_t) D,
+                                 cudaMemcpyDeviceToHost, s));
+        NB_CHECK(cudaStreamSynchronize(s));
+    }
+    NBodyCudaStatus all = NBODY_SUCCESS;
+    std::vector<NbBestDev> bestHost;
+    std::vector<double> fin;
+    std::vector<double> used(D, pft);               // each dwarf's origin in the last run
+    int done = 0;
+    for (int i = 0; i < runs; ++i) {
+        if (i > 0) {
+            rc = nb_restore_slot(st, st->runStart);
+            if (rc != NBODY_SUCCESS) return rc;
+            NB_CHECK(cudaMemcpyAsync(bt->dDwarfs, tableStart.data(), sizeof(NbDwarfDev) * (size_t) D,
+                                     cudaMemcpyHostToDevice, s));
+            for (int d = 0; d < D; ++d) origin[d] = used[d] = bestHost[d].bestTime;  // nbody.c:508-516
+            st->timeOrigin = 0.0;
+            rc = nb_batch_set_origins(bt, origin.data());
+            if (rc) return rc;
+        } else {
+            st->timeOrigin = pft;
         }
+        bt->haveKeep = false;
+        all |= nb_batch_run_once(ctx, bt, rp, like ? &hr : nullptr, like, useGraph, bestHost, fin);
+        done = i + 1;
+        if (all & ~(int) NBODY_STATUS_WARNINGS_MASK) break;
     }
-    bt->lastStepMs = steps ? total / steps : 0.0;
-    bt->lastSteps = steps;
-    std::vector<double> fin((size_t) NB_LIKELIHOOD_TERMS * D, NAN);
     const bool ok = !(all & ~(int) NBODY_STATUS_WARNINGS_MASK);
-    if (like && ok) {
-        nb_hist_launch(st, bt->bodyDwarf, hr, true);
-        NB_CHECK(cudaMemcpyAsync(fin.data(), hr.out, 8 * fin.size(), cudaMemcpyDeviceToHost, s));
-    }
-    NB_CHECK(cudaMemcpyAsync(bestHost.data(), bt->best, sizeof(NbBestDev) * (size_t) D,
-                             cudaMemcpyDeviceToHost, s));
-    NB_CHECK(cudaGetLastError());
-    NB_CHECK(cudaStreamSynchronize(s));
     for (int d = 0; d < D; ++d) {
         NBodyCudaRunResult& r = res[d];
         const NbBestDev& b = bestHost[d];
-        r.runs = 1;
-        r.previousForwardTime = pft;
+        r.runs = done;
+        r.previousForwardTime = used[d];
         r.bestTime = b.bestTime;
         r.bestStep = b.bestStep;
         r.bestCount = b.count;

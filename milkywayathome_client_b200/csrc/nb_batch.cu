@@ -44,7 +44,8 @@ __global__ void k_b_reset(NbScalars* __restrict__ sc, NbDwarfDev* __restrict__ d
     }
     for (int d = t; d < nDwarfs; d += gridDim.x * blockDim.x) {
         dw[d].xyzmaxBits = 0;
-        dw[d].time = sc->step * dw[d].dt - sc->timeOrigin;   // barTime of this evaluation
+        // barTime of this evaluation: the shared origin, or the dwarf's own (the other is 0)
+        dw[d].time = sc->step * dw[d].dt - sc->timeOrigin - dw[d].timeOrigin;
     }
 }
 

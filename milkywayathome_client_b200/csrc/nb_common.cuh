@@ -127,7 +127,8 @@ struct NbDwarfDev {
     int rootNode, rootEnd;          // root node and Next(root)
     int depthEps;                   // first depth whose cell size is <= DBL_EPSILON
     int status;                     // status bits raised while building this dwarf's tree
-    double time;                    // the bar's time of this evaluation: step * dt
+    double time;                    // the bar's time of this evaluation: step * dt - origin
+    double timeOrigin;              // this dwarf's own bar time origin (calibration runs; else 0)
 };
 struct NbForest {
     const int* bodyDwarf;           // dwarf of every body (input = sorted position)

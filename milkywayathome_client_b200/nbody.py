@@ -699,11 +699,12 @@ class NBodyBatch:
         self.check("nbBatchGenerateDwarfs", self.lib.nbBatchGenerateDwarfsCUDA(self._h, arr))
 
     def run_system(self, ctx, nstep, time_evolve, params=None, data=None, use_best_like=False,
-                   best_like_start=0.95, keep_best_bodies=False, graph=True):
+                   best_like_start=0.95, calibration_runs=0, keep_best_bodies=False, graph=True):
         """NBodyState.run_system for every dwarf at once (nbBatchRunSystemCUDA): returns
         (status, [dict per dwarf]) with the keys of NBodyState.run_system."""
         rp = _lib.RunParams(int(nstep), int(bool(use_best_like)), float(time_evolve),
-                            float(best_like_start), 0, int(bool(keep_best_bodies)))
+                            float(best_like_start), int(calibration_runs),
+                            int(bool(keep_best_bodies)))
         res = (_lib.RunResult * self.ndwarfs)()
         hp = params.struct() if params is not None else None
         dh = data.struct() if data is not None else None

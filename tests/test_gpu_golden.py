@@ -268,3 +268,56 @@ def test_batch_run_system_with_best_likelihood_scan(graph):
             assert np.array_equal(g[key], w[key], equal_nan=True), (k, key, g[key], w[key])
         s = slice(offs[k], offs[k + 1])
         assert np.array_equal(bpos[s], wpos) and np.array_equal(bvel[s], wvel)
+
+
+def test_batch_run_system_bar_calibration_runs():
+    """model_bar dwarfs (three seeds) as one batch: the best-likelihood window and the two
+    calibration runs, each dwarf's bar with its own time origin from its previous run's best
+    time; every dwarf's result equals its own nbRunSystemCUDA run and the golden value."""
+    from oracle import bindings as ob
+    from milkywayathome_client_b200 import (HistogramParams, NBodyBatch, NBodyCtx, NBodyState,
+                                            _lib, read_histogram)
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    seeds = ("670828913", "886885833", "715144259")
+    with open(os.path.join(GOLDEN, "golden_likelihoods.json")) as f:
+        golden = json.load(f)["models"]["bar"]["100"]
+    data = read_histogram(os.path.join(GOLDEN, "orphan_model_histogram_3"))
+    dwarfs = []
+    for seed in seeds:
+        r = ob.RefState.open_lua(os.path.join(GOLDEN, "orphan_dwarf.lua"),
+                                 os.path.join(GOLDEN, "orphan_model_histogram_3"), int(seed),
+                                 ["100", "bar"])
+        c, nstep, time_evolve = r.ctx(_lib.Ctx)
+        use_best, start, calib = r.run_params()
+        init = r.get()
+        mass, types = r.masses()
+        dwarfs.append((c, init, mass, types))
+    assert use_best and calib == 2
+    c = dwarfs[0][0]
+    ctx = NBodyCtx.from_struct(c, nstep)
+    params = HistogramParams(**r.like_params())
+    want = []
+    for _, init, mass, types in dwarfs:
+        with NBodyState.create(ctx, init["pos"], init["vel"], mass) as st:
+            st.set_types(types)
+            rc, res = st.run_system(ctx, nstep, time_evolve, params, data, use_best_like=True,
+                                    best_like_start=start, calibration_runs=calib)
+            assert rc == 0 and res["runs"] == 3
+            want.append(res)
+    spec = [(len(d[2]), c.eps2, c.timestep, 4.0) for d in dwarfs]
+    with NBodyBatch(spec) as bt:
+        bt.set_bodies(np.concatenate([d[1]["pos"] for d in dwarfs]),
+                      np.concatenate([d[1]["vel"] for d in dwarfs]),
+                      np.concatenate([d[2] for d in dwarfs]))
+        bt.set_types(np.concatenate([d[3] for d in dwarfs]))
+        rc, got = bt.run_system(ctx, nstep, time_evolve, params, data, use_best_like=True,
+                                best_like_start=start, calibration_runs=calib)
+        assert rc == 0
+    for k, (seed, w, g) in enumerate(zip(seeds, want, got)):
+        assert g["runs"] == 3
+        assert g["previous_forward_time"] == w["previous_forward_time"], k
+        for key in ("best_step", "best_count", "best_time"):
+            assert g[key] == w[key], (k, key, g[key], w[key])
+        assert np.array_equal(g["result"], w["result"], equal_nan=True), (k, g["result"], w["result"])
+        assert abs(g["result"][0] - golden[seed]) < 1e-10

@@ -78,3 +78,24 @@ def test_lmc_state_required_and_shift_bounds():
         assert st.run_steps(ctx, 3) == 0
         with pytest.raises(NBodyError):
             st.check("nbStepSystem", st.step(ctx))
+
+
+def test_lmc_in_the_mixed_form():
+    """The mixed-precision walk with an LMC: the LMC's own orbit does not depend on the bodies,
+    so it equals the FP64 run's bit for bit; the bodies agree to the mixed walk's accuracy."""
+    from milkywayathome_client_b200 import NBodyCtx, NBodyState
+    c, nstep, init, mass, types, (lp, lv, shift), ref = _setup("LMC", 0.470003629)
+    out = {}
+    for precision in ("fp64", "mixed"):
+        ctx = NBodyCtx.from_struct(c, nstep).with_precision(precision)
+        with NBodyState.create(ctx, init["pos"], init["vel"], mass, gravmap=False) as st:
+            st.set_types(types)
+            st.set_lmc(lp, lv, shift)
+            assert st.gravMap(ctx) == 0
+            assert st.run_steps(ctx, 50) == 0
+            out[precision] = (st.bodies(), st.lmc())
+    (p64, v64), (l64p, l64v) = out["fp64"]
+    (pmx, vmx), (lmxp, lmxv) = out["mixed"]
+    assert np.array_equal(l64p, lmxp) and np.array_equal(l64v, lmxv)
+    scale = np.abs(p64).max()
+    assert np.abs(pmx - p64).max() < 1e-6 * scale
