@@ -496,6 +496,14 @@ NBodyCudaStatus nbBatchRunSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* ba
 /* every dwarf's bodies at its best likelihood (keepBestBodies; valid for dwarfs with
  * bestCount > 0), all bodies of the batch in order */
 NBodyCudaStatus nbBatchGetBestBodiesCUDA(NBodyCudaBatch* batch, double* pos, double* vel);
+/* LMC runs of a batch (a context with lmc set): every dwarf's LMC as nbSetLMCCUDA takes one --
+ * pos3/vel3 3 doubles per dwarf, shift nShift reflex accelerations of 3 doubles per dwarf,
+ * dwarf after dwarf.  Each dwarf's LMC moves with its own time step and bar time; set the
+ * LMCs after the bodies (nbBatchSetBodiesCUDA and the generators restore the LMC states given
+ * here). */
+NBodyCudaStatus nbBatchSetLMCCUDA(NBodyCudaBatch* batch, const double* pos3, const double* vel3,
+                                  const double* shift, int nShift);
+NBodyCudaStatus nbBatchGetLMCCUDA(NBodyCudaBatch* batch, double* pos3, double* vel3);
 /* mean device time of the steps of the last nbBatchRunStepsCUDA call */
 NBodyCudaStatus nbBatchLastStepTimeCUDA(NBodyCudaBatch* batch, double* stepMs);
 

@@ -226,6 +226,8 @@ SIGNATURES = [
     ("nbBatchGenerateMixedDwarfsCUDA", ctypes.c_int, [_vp, ctypes.POINTER(MixedDwarf)]),
     ("nbBatchRunSystemCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
     ("nbBatchGetBestBodiesCUDA", ctypes.c_int, [_vp, _vp, _vp]),
+    ("nbBatchSetLMCCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int]),
+    ("nbBatchGetLMCCUDA", ctypes.c_int, [_vp, _vp, _vp]),
     ("nbMixedDwarfParticleMassesCUDA", ctypes.c_int, [ctypes.POINTER(MixedDwarf), _vp]),
     ("nbGetBodyMassesCUDA", ctypes.c_int, [_vp, _vp]),
     ("nbHistogramCUDA", ctypes.c_int, [_vp, ctypes.POINTER(HistParams), _vp, _vp, _vp, _vp]),

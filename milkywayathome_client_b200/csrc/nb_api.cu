@@ -1794,7 +1794,8 @@ NBodyCudaStatus nbGetBestBodiesCUDA(NBodyCudaState* st, double* pos, double* vel
 // Batched dwarfs (nb_batch.cu builds the forest; the walks take the forest description)
 // =============================================================================================
 int nb_build_forest(NbTreeBuffers& b, const NbForest& f, int n, int capNodes, int criterion,
-                    double theta, int useQuad, int drift, int numSMs, cudaStream_t s);
+                    double theta, int useQuad, int drift, int numSMs, cudaStream_t s,
+                    const NbBatchLMC* lmc);
 
 struct NbBatchTuning {
     int groupMax = 32;      // bodies per walk group of the mixed walk
@@ -1821,11 +1822,16 @@ struct NBodyCudaBatch {
     int lastSteps = 0;
     NbBestDev* best = nullptr;          // nbBatchRunSystemCUDA: per-dwarf best-likelihood records
     bool haveKeep = false;              // keepPos/keepVel of the state hold best bodies
+    double* lmcShiftDev = nullptr;      // LMC runs: every dwarf's reflex accelerations
+    int nShift = 0;                     // (nShift vectors per dwarf)
+    std::vector<double> lmcHost;        // the LMC states nbBatchSetLMCCUDA gave, 6 per dwarf
 };
 
-static NbForest nb_forest_of(NBodyCudaBatch* bt)
+static NbForest nb_forest_of(NBodyCudaBatch* bt, const NBodyCudaCtx* ctx = nullptr)
 {
-    return NbForest{bt->bodyDwarf, bt->dDwarfs, bt->nDwarfs};
+    const bool lmc = ctx && ctx->lmc && bt->lmcShiftDev;
+    return NbForest{bt->bodyDwarf, bt->dDwarfs, bt->nDwarfs, lmc ? bt->lmcShiftDev : nullptr,
+                    lmc ? bt->nShift : 0};
 }
 
 static void nb_batch_drop_graph(NBodyCudaBatch* bt)
@@ -1862,14 +1868,25 @@ static int nb_batch_enqueue(NBodyCudaBatch* bt, const NBodyCudaCtx* ctx, int dri
     NBodyCudaState* st = bt->st;
     NbTreeBuffers& b = st->b;
     const cudaStream_t s = st->stream;
-    const NbForest f = nb_forest_of(bt);
+    const NbForest f = nb_forest_of(bt, ctx);
     NbWalkParams wp{};
     wp.useQuad = ctx->useQuad;
     wp.kick = kick;
     wp.n = st->nbody;
-    const NbPot pot = nb_pot_from(ctx);
+    NbPot pot = nb_pot_from(ctx);
+    NbBatchLMC lmc{};
+    const bool withLMC = f.lmcShift != nullptr;
+    if (withLMC) {                      // each dwarf's LMC: its Plummer sphere on its bodies
+        pot.lmcMass = ctx->lmcMass;
+        pot.lmcScale = ctx->lmcScale;
+        lmc.pot = nb_pot_from(ctx);
+        lmc.mass = ctx->lmcMass;
+        lmc.dynaFric = ctx->lmcDynaFric;
+        lmc.coulombLog = ctx->coulombLog;
+    }
     int launches = nb_build_forest(b, f, st->nbody, st->capNodes, ctx->criterion, ctx->theta,
-                                   ctx->useQuad, drift, st->numSMs, s);
+                                   ctx->useQuad, drift, st->numSMs, s, withLMC ? &lmc : nullptr);
+    if (withLMC && drift) launches += 1;
     cudaEventRecord(st->ev0, s);
     if (ctx->precision == NBCUDA_PRECISION_MIXED) {
         nb_launch_walk_mixed(b, st->mx, st->capNodes, wp, pot, false, st->numSMs, s, &f);
@@ -1881,6 +1898,10 @@ static int nb_batch_enqueue(NBodyCudaBatch* bt, const NBodyCudaCtx* ctx, int dri
         launches += 1;
     }
     cudaEventRecord(st->ev1, s);
+    if (withLMC && kick) {              // advanceVelocities_LMC after the bodies' kick
+        nb_launch_b_lmc_half(lmc, f, b.sc, 1, s);
+        launches += 1;
+    }
     cudaMemcpyAsync(st->scHost, b.sc, sizeof(NbScalars), cudaMemcpyDeviceToHost, s);
     return launches;
 }
@@ -1900,6 +1921,10 @@ static NBodyCudaStatus nb_batch_eval(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt
     const cudaStream_t s = st->stream;
     NbTreeBuffers& b = st->b;
     const bool mixed = ctx->precision == NBCUDA_PRECISION_MIXED;
+    if (ctx->lmc && (drift || kick) && st->step + 2 > bt->nShift) {
+        g_lastError = "the LMC's reflex accelerations do not reach this step";
+        return NBODY_USER_ERROR;
+    }
     for (int attempt = 0; attempt < 4; ++attempt) {
         if (mixed) {
             NBodyCudaStatus rc = nb_batch_mixed_buffers(bt);
@@ -1984,9 +2009,9 @@ static NBodyCudaStatus nb_batch_check(const NBodyCudaCtx* ctx, NBodyCudaBatch* b
         g_lastError = "batched dwarfs use a tree criterion";
         return NBODY_UNSUPPORTED;
     }
-    if (ctx->lmc) {
-        g_lastError = "batched dwarfs run without an LMC";
-        return NBODY_UNSUPPORTED;
+    if (ctx->lmc && !bt->lmcShiftDev) {
+        g_lastError = "an LMC context needs every dwarf's LMC state (nbBatchSetLMCCUDA)";
+        return NBODY_USER_ERROR;
     }
     NB_CHECK(cudaSetDevice(bt->st->device));
     return NBODY_SUCCESS;
@@ -2005,6 +2030,8 @@ static NBodyCudaStatus nb_batch_reset_table(NBodyCudaBatch* bt)
         h.first = first;
         h.count = bt->dwarfs[d].nbody;
         first += h.count;
+        if (!bt->lmcHost.empty())
+            for (int c = 0; c < 6; ++c) h.lmc[c] = bt->lmcHost[6 * (size_t) d + c];
     }
     NB_CHECK(cudaMemcpyAsync(bt->dDwarfs, bt->hDwarfs, sizeof(NbDwarfDev) * bt->nDwarfs,
                              cudaMemcpyHostToDevice, bt->st->stream));
@@ -2066,6 +2093,7 @@ NBodyCudaStatus nbBatchDestroyCUDA(NBodyCudaBatch* bt)
     if (bt->st) cudaSetDevice(bt->st->device);
     nb_batch_drop_graph(bt);
     cudaFree(bt->best);
+    cudaFree(bt->lmcShiftDev);
     cudaFree(bt->dDwarfs);
     cudaFree(bt->bodyDwarf);
     if (bt->hDwarfs) cudaFreeHost(bt->hDwarfs);
@@ -2460,6 +2488,62 @@ NBodyCudaStatus nbBatchRunSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaBatch* bt
         for (int t = 0; t < NB_LIKELIHOOD_TERMS; ++t) r.result[t] = useBest ? b.best[t] : r.final[t];
     }
     return all;
+}
+
+// Every dwarf's LMC: pos3/vel3 3 doubles per dwarf, shift nShift vectors of 3 doubles per
+// dwarf (dwarf-major), as each dwarf's reverseOrbit_LMC leaves them.
+NBodyCudaStatus nbBatchSetLMCCUDA(NBodyCudaBatch* bt, const double* pos3, const double* vel3,
+                                  const double* shift, int nShift)
+{
+    if (!bt || !pos3 || !vel3 || !shift || nShift < 2) {
+        g_lastError = "nbBatchSetLMCCUDA: positions, velocities and >= 2 reflex accelerations needed";
+        return NBODY_USER_ERROR;
+    }
+    NBodyCudaState* st = bt->st;
+    NB_CHECK(cudaSetDevice(st->device));
+    const int D = bt->nDwarfs;
+    const size_t bytes = sizeof(double) * 3 * (size_t) nShift * D;
+    if (bt->lmcShiftDev && bt->nShift != nShift) {
+        cudaFree(bt->lmcShiftDev);
+        bt->lmcShiftDev = nullptr;
+    }
+    if (!bt->lmcShiftDev) NB_CHECK(cudaMalloc((void**) &bt->lmcShiftDev, bytes));
+    bt->nShift = nShift;
+    NB_CHECK(cudaMemcpyAsync(bt->lmcShiftDev, shift, bytes, cudaMemcpyHostToDevice, st->stream));
+    bt->lmcHost.assign(6 * (size_t) D, 0.0);
+    for (int d = 0; d < D; ++d)
+        for (int c = 0; c < 3; ++c) {
+            bt->lmcHost[6 * (size_t) d + c] = pos3[3 * (size_t) d + c];
+            bt->lmcHost[6 * (size_t) d + 3 + c] = vel3[3 * (size_t) d + c];
+        }
+    NB_CHECK(cudaMemcpy2DAsync(&bt->dDwarfs[0].lmc[0], sizeof(NbDwarfDev), bt->lmcHost.data(),
+                               6 * sizeof(double), 6 * sizeof(double), (size_t) D,
+                               cudaMemcpyHostToDevice, st->stream));
+    NB_CHECK(cudaStreamSynchronize(st->stream));
+    nb_batch_drop_graph(bt);
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbBatchGetLMCCUDA(NBodyCudaBatch* bt, double* pos3, double* vel3)
+{
+    if (!bt || !bt->lmcShiftDev) {
+        g_lastError = "nbBatchGetLMCCUDA: no LMC set";
+        return NBODY_USER_ERROR;
+    }
+    NBodyCudaState* st = bt->st;
+    NB_CHECK(cudaSetDevice(st->device));
+    const int D = bt->nDwarfs;
+    std::vector<double> h(6 * (size_t) D);
+    NB_CHECK(cudaMemcpy2DAsync(h.data(), 6 * sizeof(double), &bt->dDwarfs[0].lmc[0],
+                               sizeof(NbDwarfDev), 6 * sizeof(double), (size_t) D,
+                               cudaMemcpyDeviceToHost, st->stream));
+    NB_CHECK(cudaStreamSynchronize(st->stream));
+    for (int d = 0; d < D; ++d)
+        for (int c = 0; c < 3; ++c) {
+            if (pos3) pos3[3 * (size_t) d + c] = h[6 * (size_t) d + c];
+            if (vel3) vel3[3 * (size_t) d + c] = h[6 * (size_t) d + 3 + c];
+        }
+    return NBODY_SUCCESS;
 }
 
 // The bodies of every dwarf at its best likelihood (valid for the dwarfs whose bestCount > 0).

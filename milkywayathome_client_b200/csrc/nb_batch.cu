@@ -57,7 +57,9 @@ __global__ void k_b_drift_bbox(double* __restrict__ px, double* __restrict__ py,
                                double* __restrict__ vy, double* __restrict__ vz,
                                const double* __restrict__ ax, const double* __restrict__ ay,
                                const double* __restrict__ az, const int* __restrict__ bodyDwarf,
-                               NbDwarfDev* __restrict__ dw, int n, int drift)
+                               NbDwarfDev* __restrict__ dw, int n, int drift,
+                               const double* __restrict__ lmcShift, int nShift,
+                               const NbScalars* __restrict__ sc)
 {
     const int lane = threadIdx.x & 31;
     const int warpsTotal = (gridDim.x * blockDim.x) >> 5;
@@ -72,10 +74,16 @@ __global__ void k_b_drift_bbox(double* __restrict__ px, double* __restrict__ py,
             if (drift) {
                 const double dt = dw[d].dt;
                 const double dtHalf = 0.5 * dt;
+                // the Milky Way's reflex acceleration of LMC runs (acc_i), else 0
+                double sx = 0.0, sy = 0.0, sz = 0.0;
+                if (lmcShift) {
+                    const double* sh = lmcShift + 3 * ((size_t) d * nShift + sc->step);
+                    sx = sh[0]; sy = sh[1]; sz = sh[2];
+                }
                 double vvx = vx[i], vvy = vy[i], vvz = vz[i];
-                vvx = vvx + dtHalf * (ax[i] + 0.0);
-                vvy = vvy + dtHalf * (ay[i] + 0.0);
-                vvz = vvz + dtHalf * (az[i] + 0.0);
+                vvx = vvx + dtHalf * (ax[i] + sx);
+                vvy = vvy + dtHalf * (ay[i] + sy);
+                vvz = vvz + dtHalf * (az[i] + sz);
                 x = x + dt * vvx;
                 y = y + dt * vvy;
                 z = z + dt * vvz;
@@ -416,15 +424,20 @@ static inline int nb_b_grid(int n, int threads, int cap)
 // dwarfs; nothing here synchronises with the host (the sequence is captured in a graph).
 // Requires every dwarf to hold >= 2 bodies.  Returns the number of launches issued.
 int nb_build_forest(NbTreeBuffers& b, const NbForest& f, int n, int capNodes, int criterion,
-                    double theta, int useQuad, int drift, int numSMs, cudaStream_t s)
+                    double theta, int useQuad, int drift, int numSMs, cudaStream_t s,
+                    const NbBatchLMC* lmc)
 {
     const int T = 256;
     const int gB = nb_b_grid(n, T, numSMs * 8);
     const int g = nb_b_grid(n, T, 1 << 20);
     int launches = 0;
     k_b_reset<<<nb_b_grid(f.nDwarfs, T, 64), T, 0, s>>>(b.sc, f.dwarfs, f.nDwarfs, n);
+    // LMC runs: each LMC drifts and takes its first half kick before the bodies drift
+    // (nbStepSystemPlain's advancePosVel_LMC follows advancePosVel but reads no body)
+    if (lmc && drift) nb_launch_b_lmc_half(*lmc, f, b.sc, 0, s);
     k_b_drift_bbox<<<gB, T, 0, s>>>(b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.ax, b.ay, b.az,
-                                    f.bodyDwarf, f.dwarfs, n, drift);
+                                    f.bodyDwarf, f.dwarfs, n, drift,
+                                    lmc && drift ? f.lmcShift : nullptr, f.nShift, b.sc);
     k_b_root_size<<<nb_b_grid(f.nDwarfs, 128, 64), 128, 0, s>>>(f.dwarfs, f.nDwarfs, b.sc);
     k_b_keys<<<gB, T, 0, s>>>(b.px, b.py, b.pz, b.mass, f.bodyDwarf, f.dwarfs, n, b.sort.keyA,
                               b.sort.idxA, b.sc);

@@ -129,11 +129,23 @@ struct NbDwarfDev {
     int status;                     // status bits raised while building this dwarf's tree
     double time;                    // the bar's time of this evaluation: step * dt - origin
     double timeOrigin;              // this dwarf's own bar time origin (calibration runs; else 0)
+    double lmc[6];                  // LMC runs: this dwarf's LMC position and velocity
 };
 struct NbForest {
     const int* bodyDwarf;           // dwarf of every body (input = sorted position)
     NbDwarfDev* dwarfs;
     int nDwarfs;
+    // LMC runs: each dwarf's reflex accelerations, nShift vectors of 3 doubles from
+    // lmcShift + 3 nShift d (shiftByLMC; step k takes k in the drift and k + 1 in the kick)
+    const double* lmcShift;
+    int nShift;
+};
+// The LMC of a batch's LMC runs: the context's LMC parameters and the potential it moves in.
+struct NbBatchLMC {
+    NbPot pot;
+    double mass;
+    int dynaFric;
+    double coulombLog;
 };
 
 // ---- Lambda-Beta histograms and the likelihood (nb_likelihood.cu) ----
@@ -293,6 +305,8 @@ void nb_launch_drift_only(NbTreeBuffers& b, int n, double dt, int numSMs, cudaSt
                           const double* shift = nullptr);
 // One half of the LMC's step (nb_lmc.cu): phase 0 drifts and kicks, phase 1 kicks; shift is
 // the Milky Way's reflex acceleration of that half (3 host doubles).
+void nb_launch_b_lmc_half(const NbBatchLMC& lmc, const NbForest& f, const NbScalars* sc, int phase,
+                          cudaStream_t s);
 void nb_launch_lmc_half(const NbPot& p, double* lmc, int phase, double dt, const double* shift,
                         double massLMC, int dynaFric, double coulombLog, cudaStream_t s);
 

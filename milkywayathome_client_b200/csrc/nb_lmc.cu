@@ -227,10 +227,12 @@ __device__ void nb_dyn_friction(const NbPot& p, double x, double y, double z, do
 // the LMC's current state; phase 0 (advancePosVel_LMC, :286-299) drifts the LMC with its
 // velocity and then kicks it by (acc + shift) dt/2, phase 1 (advanceVelocities_LMC, :317-327)
 // only kicks.
-__global__ void k_lmc_half(NbPot p, double* __restrict__ lmc, int phase, double dt, double sx,
-                           double sy, double sz, double massLMC, int dynaFric, double coulombLog)
+// advancePosVel_LMC (phase 0: drift with the old velocity, then half kick) or
+// advanceVelocities_LMC (phase 1: half kick) with the external potential, the friction and the
+// step's reflex acceleration (sx, sy, sz) (nbody/src/nbody_plain.c:286-325, :338-352).
+__device__ void nb_lmc_update(const NbPot& p, double* lmc, int phase, double dt, double sx,
+                              double sy, double sz, double massLMC, int dynaFric, double coulombLog)
 {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
     const double x = lmc[0], y = lmc[1], z = lmc[2];
     const double vx = lmc[3], vy = lmc[4], vz = lmc[5];
     double ex, ey, ez, fx, fy, fz;
@@ -248,7 +250,39 @@ __global__ void k_lmc_half(NbPot p, double* __restrict__ lmc, int phase, double 
     lmc[5] = vz + (az + sz) * dtHalf;
 }
 
+__global__ void k_lmc_half(NbPot p, double* __restrict__ lmc, int phase, double dt, double sx,
+                           double sy, double sz, double massLMC, int dynaFric, double coulombLog)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    nb_lmc_update(p, lmc, phase, dt, sx, sy, sz, massLMC, dynaFric, coulombLog);
+}
+
+// Every dwarf's LMC of a batch, one thread per dwarf: the dwarf's time step and bar time, its
+// reflex acceleration of the step (sc->step in phase 0, sc->step + 1 in phase 1).  Phase 1
+// follows the bodies' kick and is skipped when the evaluation failed (it is redone).
+__global__ void k_b_lmc_half(NbBatchLMC L, NbForest f, const NbScalars* __restrict__ sc,
+                             int phase)
+{
+    if (phase == 1 && nb_failed(sc)) return;
+    const int k = sc->step + phase;
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < f.nDwarfs; d += gridDim.x * blockDim.x) {
+        NbDwarfDev& dw = f.dwarfs[d];
+        NbPot p = L.pot;
+        p.time = dw.time;
+        const double* sh = f.lmcShift + 3 * ((size_t) d * f.nShift + k);
+        nb_lmc_update(p, dw.lmc, phase, dw.dt, sh[0], sh[1], sh[2], L.mass, L.dynaFric,
+                      L.coulombLog);
+    }
+}
+
 }  // namespace
+
+void nb_launch_b_lmc_half(const NbBatchLMC& lmc, const NbForest& f, const NbScalars* sc, int phase,
+                          cudaStream_t s)
+{
+    k_b_lmc_half<<<(f.nDwarfs + 127) / 128, 128, 0, s>>>(lmc, f, sc, phase);
+    nb_count_launch();
+}
 
 void nb_launch_lmc_half(const NbPot& p, double* lmc, int phase, double dt, const double* shift,
                         double massLMC, int dynaFric, double coulombLog, cudaStream_t s)

@@ -156,9 +156,17 @@ __global__ void k_body_epilogue(const double* __restrict__ px, const double* __r
         NbWalkParams w = wp;
         NbPot p = pot;
         if (FOREST) {
-            const NbDwarfDev& d = forest.dwarfs[forest.bodyDwarf[j]];
+            const int dj = forest.bodyDwarf[j];
+            NbDwarfDev& d = forest.dwarfs[dj];
             w.dtHalf = 0.5 * d.dt;
             p.time = d.time;
+            if (forest.lmcShift) {                   // LMC runs: this dwarf's LMC and acc_i1
+                p.lmc = d.lmc;
+                if (w.kick) {
+                    const double* sh = forest.lmcShift + 3 * ((size_t) dj * forest.nShift + sc->step + 1);
+                    w.shift[0] = sh[0]; w.shift[1] = sh[1]; w.shift[2] = sh[2];
+                }
+            }
         }
         nb_finish_body(p, w, (unsigned) j, px[j], py[j], pz[j], ax[j], ay[j], az[j], ax, ay, az,
                        vx, vy, vz);
@@ -177,7 +185,7 @@ void nb_launch_body_epilogue(const double* px, const double* py, const double* p
                                                 *forest);
     else
         k_body_epilogue<false><<<g, 256, 0, s>>>(px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc,
-                                                 NbForest{nullptr, nullptr, 0});
+                                                 NbForest{nullptr, nullptr, 0, nullptr, 0});
     nb_count_launch();
 }
 

@@ -718,6 +718,21 @@ class NBodyBatch:
                 "runs": r.runs} for r in res]
         return rc, out
 
+    def set_lmc(self, positions, velocities, shifts):
+        """Every dwarf's LMC (nbBatchSetLMCCUDA): positions and velocities (ndwarfs, 3), reflex
+        accelerations (ndwarfs, k, 3)."""
+        p = np.ascontiguousarray(positions, dtype=np.float64).reshape(self.ndwarfs, 3)
+        v = np.ascontiguousarray(velocities, dtype=np.float64).reshape(self.ndwarfs, 3)
+        sh = np.ascontiguousarray(shifts, dtype=np.float64).reshape(self.ndwarfs, -1, 3)
+        self.check("nbBatchSetLMC", self.lib.nbBatchSetLMCCUDA(self._h, _lib.ptr(p), _lib.ptr(v),
+                                                               _lib.ptr(sh), sh.shape[1]))
+
+    def lmc(self):
+        """Every dwarf's LMC position and velocity, (ndwarfs, 3) each (nbBatchGetLMCCUDA)."""
+        p, v = np.empty((self.ndwarfs, 3)), np.empty((self.ndwarfs, 3))
+        self.check("nbBatchGetLMC", self.lib.nbBatchGetLMCCUDA(self._h, _lib.ptr(p), _lib.ptr(v)))
+        return p, v
+
     def best_bodies(self):
         """Every dwarf's bodies at its best likelihood (nbBatchGetBestBodiesCUDA)."""
         n = int(self.offsets[-1])

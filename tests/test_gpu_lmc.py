@@ -99,3 +99,54 @@ def test_lmc_in_the_mixed_form():
     assert np.array_equal(l64p, lmxp) and np.array_equal(l64v, lmxv)
     scale = np.abs(p64).max()
     assert np.abs(pmx - p64).max() < 1e-6 * scale
+
+
+@pytest.mark.parametrize("variant", ["LMC", "LMC_bar"])
+def test_batch_of_lmc_dwarfs_equals_single_states(variant):
+    """Three LMC-run dwarfs (three seeds, each with its own LMC orbit and reflex accelerations)
+    as one batch, friction on: after 60 steps through captured graphs every body and every
+    LMC equal the single-state runs bit for bit."""
+    from oracle import bindings as ob
+    from milkywayathome_client_b200 import NBodyBatch, NBodyCtx, NBodyState, _lib
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    dwarfs = []
+    for seed in (670828913, 886885833, 430281807):
+        r = ob.RefState.open_lua(os.path.join(GOLDEN, "orphan_dwarf.lua"),
+                                 os.path.join(GOLDEN, "orphan_model_histogram_3"), seed,
+                                 ["100", variant])
+        c, nstep, time_evolve = r.ctx(_lib.Ctx)
+        c.coulombLog = 0.470003629
+        init = r.get()
+        mass, types = r.masses()
+        dwarfs.append((init, mass, types, r.lmc()))
+        r.close()
+    ctx = NBodyCtx.from_struct(c, nstep)
+    k = min(len(d[3][2]) for d in dwarfs)
+    want = []
+    for init, mass, types, (lp, lv, sh) in dwarfs:
+        with NBodyState.create(ctx, init["pos"], init["vel"], mass, gravmap=False) as st:
+            st.set_types(types)
+            st.set_time_origin(time_evolve)
+            st.set_lmc(lp, lv, sh[:k])
+            assert st.gravMap(ctx) == 0
+            assert st.run_steps(ctx, 60) == 0
+            want.append((st.bodies(), st.lmc()))
+    spec = [(len(d[1]), c.eps2, c.timestep, 4.0) for d in dwarfs]
+    with NBodyBatch(spec) as bt:
+        bt.set_bodies(np.concatenate([d[0]["pos"] for d in dwarfs]),
+                      np.concatenate([d[0]["vel"] for d in dwarfs]),
+                      np.concatenate([d[1] for d in dwarfs]))
+        bt.set_types(np.concatenate([d[2] for d in dwarfs]))
+        bt.set_time_origin(time_evolve)
+        bt.set_lmc([d[3][0] for d in dwarfs], [d[3][1] for d in dwarfs],
+                   np.stack([d[3][2][:k] for d in dwarfs]))
+        assert bt.gravMap(ctx) == 0
+        assert bt.run_steps(ctx, 60, graph=True) == 0
+        pos, vel = bt.bodies()
+        lp, lv = bt.lmc()
+        offs = bt.offsets
+    for j, ((wpos, wvel), (wlp, wlv)) in enumerate(want):
+        s = slice(offs[j], offs[j + 1])
+        assert np.array_equal(pos[s], wpos) and np.array_equal(vel[s], wvel), j
+        assert np.array_equal(lp[j], wlp) and np.array_equal(lv[j], wlv), j
