@@ -326,9 +326,11 @@ NBodyCudaStatus nb_check_ctx(const NBodyCudaCtx* c, std::string& why)
         if (p.disk.type != NBCUDA_NO_DISK && p.disk.type != NBCUDA_MIYAMOTO_NAGAI_DISK) { why = "disk type"; return NBODY_UNSUPPORTED; }
         if (p.disk2.type != NBCUDA_NO_DISK && p.disk2.type != NBCUDA_MIYAMOTO_NAGAI_DISK &&
             p.disk2.type != NBCUDA_ORBITING_BAR) { why = "disk2 type"; return NBODY_UNSUPPORTED; }
-        // the caustic halo is not evaluated on the GPU; every other halo of the reference is
-        if (p.halo.type < NBCUDA_NO_HALO || p.halo.type > NBCUDA_NINKOVIC_HALO ||
-            p.halo.type == NBCUDA_CAUSTIC_HALO) { why = "halo type"; return NBODY_UNSUPPORTED; }
+        // every halo of the reference
+        if (p.halo.type < NBCUDA_NO_HALO || p.halo.type > NBCUDA_NINKOVIC_HALO) {
+            why = "halo type";
+            return NBODY_UNSUPPORTED;
+        }
     }
     if (c->lmc && c->potentialType != NBCUDA_POTENTIAL_DEFAULT) {
         why = "the LMC moves in the default (Milky Way) potential";

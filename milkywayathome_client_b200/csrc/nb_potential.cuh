@@ -5,19 +5,215 @@
 #include "nb_common.cuh"
 #include "nb_crmath.cuh"
 
-// The halos of nbody/src/nbody_potential.c:518-625 beyond the logarithmic and NFW ones
-// (the caustic halo is not supported): triaxial logarithmic (:518-541, constants c1..c3 as
+// ---- the caustic halo (causticHaloAccel, nbody/src/nbody_caustic.c) ----
+// Twenty cold dark-matter flows, each a ring caustic of radius a_n, speed V_n, infall rate
+// rate_n and width p_n (the reference's tables, :32-35; the halo's Lua parameters are not
+// used).  Far from a caustic a flow's field has a closed form (gfield_far, :46-62); near one
+// (inside the tricusp, :286-292) it is a sum over the real roots of a quartic, found in
+// complex arithmetic as the reference does it (T1..T4, f1..f5, gfield_close, :65-250):
+// principal square roots, and powers as exp(c log z) with the principal logarithm (C99's
+// cpow).  The reference's T2 applies the real sqrt to a complex value in its near-zero branch,
+// which takes the real part (C99 6.3.1.7); that is kept.  Complex arithmetic and the library's
+// log/exp/sin/cos/atan2 round differently from the C library's, so the field agrees with the
+// reference's to rounding (a root-count or tricusp test that sits on its threshold can differ).
+struct NbCx {
+    double re, im;
+};
+__device__ __forceinline__ NbCx nb_cx(double re, double im = 0.0) { NbCx c; c.re = re; c.im = im; return c; }
+__device__ __forceinline__ NbCx operator+(NbCx a, NbCx b) { return nb_cx(a.re + b.re, a.im + b.im); }
+__device__ __forceinline__ NbCx operator-(NbCx a, NbCx b) { return nb_cx(a.re - b.re, a.im - b.im); }
+__device__ __forceinline__ NbCx operator*(NbCx a, NbCx b)
+{
+    return nb_cx(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+__device__ __forceinline__ NbCx operator*(double s, NbCx a) { return nb_cx(s * a.re, s * a.im); }
+__device__ __forceinline__ NbCx nb_cx_divr(NbCx a, double s) { return nb_cx(a.re / s, a.im / s); }
+// a / b by Smith's method
+__device__ __forceinline__ NbCx operator/(NbCx a, NbCx b)
+{
+    if (fabs(b.re) >= fabs(b.im)) {
+        const double r = b.im / b.re, d = b.re + b.im * r;
+        return nb_cx((a.re + a.im * r) / d, (a.im - a.re * r) / d);
+    }
+    const double r = b.re / b.im, d = b.re * r + b.im;
+    return nb_cx((a.re * r + a.im) / d, (a.im * r - a.re) / d);
+}
+__device__ __forceinline__ double nb_cx_abs(NbCx a) { return hypot(a.re, a.im); }
+// principal square root
+__device__ __forceinline__ NbCx nb_cx_sqrt(NbCx a)
+{
+    if (a.im == 0.0) {
+        if (a.re < 0.0) return nb_cx(0.0, copysign(sqrt(-a.re), a.im));
+        return nb_cx(fabs(sqrt(a.re)), copysign(0.0, a.im));
+    }
+    const double d = hypot(a.re, a.im);
+    if (a.re > 0.0) {
+        const double r = sqrt(0.5 * (d + a.re));
+        return nb_cx(r, 0.5 * (a.im / r));
+    }
+    const double t = sqrt(0.5 * (d - a.re));
+    return nb_cx(fabs(0.5 * (a.im / t)), copysign(t, a.im));
+}
+// a^c for a real exponent c: exp(c log a), principal branch
+__device__ __forceinline__ NbCx nb_cx_pow(NbCx a, double c)
+{
+    if (a.re == 0.0 && a.im == 0.0) return nb_cx(0.0, 0.0);
+    const double lr = log(hypot(a.re, a.im)), li = atan2(a.im, a.re);
+    const double m = exp(c * lr);
+    double sn, cs;
+    sincos(c * li, &sn, &cs);
+    return nb_cx(m * cs, m * sn);
+}
+
+__device__ const double kCauA[21] = {1.0, 40.1, 20.1, 13.6, 10.4, 8.4, 7.0, 6.1, 5.3, 4.8, 4.3,
+                                     4.0, 3.7, 3.4, 3.2, 3.0, 2.8, 2.7, 2.5, 2.4, 2.3};
+__device__ const double kCauV[21] = {1.0, 517, 523, 523, 523, 522, 521, 521, 520, 517, 515,
+                                     512, 510, 507, 505, 503, 501, 499, 497, 496, 494};
+__device__ const double kCauRate[21] = {1.0, 53, 23, 14, 10, 7.8, 6.3, 5.3, 4.5, 3.9, 3.4,
+                                        3.1, 2.8, 2.5, 2.3, 2.1, 2.0, 1.8, 1.7, 1.6, 1.5};
+__device__ const double kCauP[21] = {1.0, 0.3, 0.3, 1.0, 0.3, 0.15, 0.12, 0.6, 0.23, 0.41, 0.25,
+                                     0.19, 0.17, 0.11, 0.09, 0.09, 0.09, 0.09, 0.09, 0.09, 0.09};
+
+__device__ __forceinline__ NbCx nb_cau_f1(NbCx x) { return nb_cx_divr(nb_cx(2.0) + 4.0 * x, 3.0); }
+__device__ __forceinline__ NbCx nb_cau_f2(NbCx x, NbCx z)
+{
+    const NbCx om = nb_cx(1.0) - x;
+    return 4.0 * (om * om - 3.0 * z * z);
+}
+__device__ __forceinline__ NbCx nb_cau_f3(NbCx x, NbCx z)
+{
+    const NbCx xm = x - nb_cx(1.0);
+    return -128.0 * nb_cx_pow(xm, 3.0) - 1728.0 * z * z - 1152.0 * xm * z * z;
+}
+__device__ __forceinline__ NbCx nb_cau_f4(NbCx x, NbCx z)
+{
+    const NbCx f2 = nb_cau_f2(x, z), f3 = nb_cau_f3(x, z);
+    const NbCx disc = nb_cx_sqrt(-256.0 * f2 * f2 * f2 + f3 * f3);
+    return nb_cx_pow(nb_cx_divr(f3 + disc, 2.0), 1.0 / 3.0);
+}
+// T1..T4 (k = 0..3): the roots of the quartic, the signs of the reference's four forms
+__device__ __forceinline__ NbCx nb_cau_T(int k, NbCx x, NbCx z)
+{
+    const double sA = (k < 2) ? -1.0 : 1.0;              // before the first square root
+    const double sB = (k == 0 || k == 2) ? -1.0 : 1.0;   // before the second
+    const double sX = (k < 2) ? -1.0 : 1.0;              // before 2 x / (first root)
+    const NbCx f1 = nb_cau_f1(x), f4 = nb_cau_f4(x, z);
+    if (x.re >= -0.125 && nb_cx_abs(f4) < 0.001) {
+        const NbCx poly = nb_cx(-1.0) - 6.0 * x + 15.0 * x * x - 8.0 * x * x * x;
+        const NbCx temp = nb_cx_divr(nb_cx_pow(poly, 1.0 / 3.0), 3.0);
+        const NbCx half = nb_cx_divr(f1, 2.0) + temp;
+        NbCx inner;
+        if (k == 1)                                      // T2: the real sqrt of the real part
+            inner = f1 - temp - nb_cx_divr(2.0 * x, sqrt(half.re));
+        else
+            inner = f1 - temp + sX * (2.0 * x / nb_cx_sqrt(half));
+        return 0.5 * (nb_cx(1.0) + sA * nb_cx_sqrt(half) + sB * nb_cx_sqrt(inner));
+    }
+    const NbCx f2 = nb_cau_f2(x, z);
+    const NbCx temp = nb_cx_sqrt(nb_cx_divr(f1, 2.0) + f2 / (3.0 * f4) + nb_cx_divr(f4, 12.0));
+    const NbCx inner = f1 - f2 / (3.0 * f4) - nb_cx_divr(f4, 12.0) + sX * (2.0 * x / temp);
+    return 0.5 * (nb_cx(1.0) + sA * temp + sB * nb_cx_sqrt(inner));
+}
+__device__ __forceinline__ NbCx nb_cau_f5(NbCx x, NbCx z, double T)
+{
+    return nb_cx_divr(nb_cx_sqrt(nb_cx(2.0 * T - 1.0) + x - nb_cx(0.0, 1.0) * z), 2.0);
+}
+
+__device__ __forceinline__ void nb_cau_far(double rho, double z, int n, double& rf, double& zf)
+{
+    const double rsq = rho * rho + z * z;
+    const double shift = kCauA[n] + kCauP[n] / 4.0;
+    const double An = (8.0 * M_PI * 1.0 * kCauRate[n] * 4498.6589) / (kCauV[n] * 1.0226831);
+    const double sv = hypot(rsq - shift * shift, 2.0 * shift * z);
+    const double factor = (-An) / (sv * (2.0 * shift * shift + sv));
+    rf += factor * (rsq * rho - shift * shift * rho);
+    zf += factor * (rsq * z + shift * shift * z);
+}
+
+static __device__ __noinline__ void nb_cau_close(double rho, double zIn, int n, double& rf,
+                                                 double& zf)
+{
+    const NbCx z = nb_cx(zIn / kCauP[n]);
+    const NbCx x = nb_cx((rho - kCauA[n]) / kCauP[n]);
+    double im[4], re[4];
+    for (int k = 0; k < 4; ++k) {
+        const NbCx t = nb_cau_T(k, x, z);
+        im[k] = fabs(t.im);
+        re[k] = t.re;
+    }
+    int count = 0;
+    for (int i = 0; i < 4; ++i) if (im[i] < 0.00001) count++;
+    if (count == 4)                                      // ascending
+        for (int i = 0; i < 4; ++i)
+            for (int j = i + 1; j < 4; ++j)
+                if (re[i] > re[j]) { const double t = re[i]; re[i] = re[j]; re[j] = t; }
+    double re2[2] = {0.0, 0.0};
+    if (count == 2) {
+        int c = 0;
+        for (int i = 0; i < 4; ++i)
+            if (im[i] < 0.00001 && c < 2) re2[c++] = re[i];
+        if (re2[0] > re2[1]) { const double t = re2[0]; re2[0] = re2[1]; re2[1] = t; }
+    }
+    const double factor = -8.0 * M_PI * 1.0 * kCauRate[n] * 4498.6589 / (rho * kCauV[n] * 1.0226831);
+    if (count == 2) {                                    // outside the caustic
+        const NbCx a = nb_cau_f5(x, z, re2[1]), b = nb_cau_f5(x, z, re2[0]);
+        rf += factor * (a.re - b.re - 0.5);
+        zf += factor * (a.im - b.im);
+    } else {                                             // inside: four roots
+        const NbCx a = nb_cau_f5(x, z, re[3]), b = nb_cau_f5(x, z, re[2]);
+        const NbCx c = nb_cau_f5(x, z, re[1]), d = nb_cau_f5(x, z, re[0]);
+        rf += factor * (a.re - b.re + c.re - d.re - 0.5);
+        zf += factor * (a.im - b.im + c.im - d.im);
+    }
+}
+
+static __device__ __noinline__ double3 nb_caustic_accel(double x, double y, double z)
+{
+    double rf = 0.0, zf = 0.0;
+    const double rho = sqrt(x * x + y * y);
+    for (int n = 1; n <= 20; ++n) {
+        const double an = kCauA[n], pn = kCauP[n];
+        const double root = sqrt(1.0 + (8.0 / pn) * (rho - an));
+        const double R = (3.0 - root) / 4.0, l = (3.0 + root) / 4.0;
+        const double tr = 2.0 * pn * sqrt((R * R * R) * (1.0 - R));
+        const double tl = 2.0 * pn * sqrt((l * l * l) * (1.0 - l));
+        if ((z <= tr && z >= 0.0 && rho >= an && rho <= an + pn) ||
+            (z >= tl && z <= tr && rho >= (an - pn / 8.0) && rho <= an) ||
+            (z >= -tr && z <= 0.0 && rho >= an && rho <= an + pn) ||
+            (z <= -tl && z >= -tr && rho >= (an - pn / 8.0) && rho <= an))
+            nb_cau_close(rho, z, n, rf, zf);
+        else
+            nb_cau_far(rho, z, n, rf, zf);
+    }
+    if (rho < 0.000001) return make_double3(0.0, 0.0, zf);
+    return make_double3((rf * x) / rho, (rf * y) / rho, zf);
+}
+
+// The halos of nbody/src/nbody_potential.c:518-625 beyond the logarithmic and NFW ones:
+// the caustic halo (above), triaxial logarithmic (:518-541, constants c1..c3 as
 // nbody/src/nbody_check_params.c:182-194 sets them), Allen-Santillan (:543-561),
 // Wilkinson-Evans (:563-573), NFW by mass (:575-585), Plummer (:587-592), Hernquist
 // (:594-599) and the Ninkovic special case (:601-625), in the reference's operation order.
 // Their powers and logarithms are correctly rounded (nb_crmath.cuh), as crlibm's pow_rn and
 // log_rn in the reference, so these halos reproduce the reference bit for bit.
+// CAUSTIC = false leaves the caustic halo's code out (callers that never meet it: its register
+// demand would otherwise set the allocation of the whole kernel).
+template <bool CAUSTIC = true>
 __device__ __forceinline__ void nb_halo_accel_more(const NbPot& p, double x, double y, double z,
                                                    double r, double& tx, double& ty, double& tz)
 {
     const double a = p.haloA, M = p.haloMass;
     double c = 0.0;                    // acceleration = pos * c for the spherical halos
     switch (p.haloType) {
+    case NBCUDA_CAUSTIC_HALO: {
+        if (CAUSTIC) {
+            const double3 t = nb_caustic_accel(x, y, z);
+            tx = t.x; ty = t.y; tz = t.z;
+        } else {
+            tx = ty = tz = 0.0;
+        }
+        return;
+    }
     case NBCUDA_TRIAXIAL_HALO: {
         const double qzs = p.haloQz * p.haloQz;
         const double rhalosqr = a * a;
@@ -125,6 +321,7 @@ static __device__ __noinline__ void nb_bar_accel(const NbPot& p, double x, doubl
 // nbExtAcceleration (nbody/src/nbody_potential.c:627-762) for the supported components:
 // Miyamoto-Nagai disks (:173-194), logarithmic (:488-504) and NFW (:506-515) halos,
 // Hernquist (:157-162) and Plummer (:164-169) bulges.
+template <bool CAUSTIC = true>
 __device__ __forceinline__ void nb_ext_accel(const NbPot& p, double x, double y, double z,
                                              double& ox, double& oy, double& oz)
 {
@@ -171,7 +368,7 @@ __device__ __forceinline__ void nb_ext_accel(const NbPot& p, double x, double y,
             const double c = (-M / (r * r)) * (nb_log_rn(ar / a) / r - 1 / ar);
             tx = c * x; ty = c * y; tz = c * z;
         } else if (p.haloType != NBCUDA_NO_HALO) {
-            nb_halo_accel_more(p, x, y, z, r, tx, ty, tz);
+            nb_halo_accel_more<CAUSTIC>(p, x, y, z, r, tx, ty, tz);
         }
         axx = axx + tx; ayy = ayy + ty; azz = azz + tz;
     }
@@ -225,6 +422,7 @@ __device__ __forceinline__ double nb_ext_potential(const NbPot& p, double x, dou
 
 // nbMapForceBody's epilogue (nbody/src/nbody_grav.c:167-176): a += nbExtAcceleration(pos)
 // + plummerAccel(pos, LMC at the origin, mass 0, scale 1), whose value is (0 - pos) * 0.
+template <bool CAUSTIC = true>
 __device__ __forceinline__ void nb_finish_body(const NbPot& pot, const NbWalkParams& wp, unsigned j,
                                                double x0, double y0, double z0, double accx,
                                                double accy, double accz, double* __restrict__ ax,
@@ -234,7 +432,7 @@ __device__ __forceinline__ void nb_finish_body(const NbPot& pot, const NbWalkPar
 {
     if (pot.enabled) {
         double ex, ey, ez;
-        nb_ext_accel(pot, x0, y0, z0, ex, ey, ez);
+        nb_ext_accel<CAUSTIC>(pot, x0, y0, z0, ex, ey, ez);
         if (pot.lmc) {
             // plummerAccel(pos, LMCpos, LMCmass, LMCscale) (nbody/src/nbody_potential.c:145-152)
             const double lx = pot.lmc[0], ly = pot.lmc[1], lz = pot.lmc[2];

@@ -143,7 +143,8 @@ k_walk_fp64(const double4* __restrict__ rec,
 // nbMapForceBody's epilogue for every body after a tree walk: a = self-gravity (as the walk
 // stored it) + nbExtAcceleration + the zero LMC term, then the optional kick (nb_finish_body).
 // FOREST: each body with its dwarf's time step and the bar's time of its dwarf.
-template <bool FOREST>
+// CAUSTIC: the potential's halo is the caustic one (its code compiled in only then).
+template <bool FOREST, bool CAUSTIC>
 __global__ void k_body_epilogue(const double* __restrict__ px, const double* __restrict__ py,
                                 const double* __restrict__ pz, double* __restrict__ ax,
                                 double* __restrict__ ay, double* __restrict__ az,
@@ -160,15 +161,16 @@ __global__ void k_body_epilogue(const double* __restrict__ px, const double* __r
             NbDwarfDev& d = forest.dwarfs[dj];
             w.dtHalf = 0.5 * d.dt;
             p.time = d.time;
-            if (forest.lmcShift) {                   // LMC runs: this dwarf's LMC and acc_i1
-                p.lmc = d.lmc;
-                if (w.kick) {
-                    const double* sh = forest.lmcShift + 3 * ((size_t) dj * forest.nShift + sc->step + 1);
-                    w.shift[0] = sh[0]; w.shift[1] = sh[1]; w.shift[2] = sh[2];
-                }
-            }
+            // LMC runs: this dwarf's LMC and its reflex acceleration acc_i1 (selects, not
+            // branches: a conditional update of the copies costs the kernel ~70 registers)
+            const bool lmc = forest.lmcShift != nullptr;
+            p.lmc = lmc ? d.lmc : p.lmc;
+            const double* sh = lmc && w.kick
+                ? forest.lmcShift + 3 * ((size_t) dj * forest.nShift + sc->step + 1) : w.shift;
+            const double s0 = sh[0], s1 = sh[1], s2 = sh[2];
+            w.shift[0] = s0; w.shift[1] = s1; w.shift[2] = s2;
         }
-        nb_finish_body(p, w, (unsigned) j, px[j], py[j], pz[j], ax[j], ay[j], az[j], ax, ay, az,
+        nb_finish_body<CAUSTIC>(p, w, (unsigned) j, px[j], py[j], pz[j], ax[j], ay[j], az[j], ax, ay, az,
                        vx, vy, vz);
     }
 }
@@ -180,12 +182,17 @@ void nb_launch_body_epilogue(const double* px, const double* py, const double* p
 {
     if (wp.n <= 0) return;
     const int g = numSMs > 0 ? min((wp.n + 255) / 256, numSMs * 8) : (wp.n + 255) / 256;
-    if (forest)
-        k_body_epilogue<true><<<g, 256, 0, s>>>(px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc,
-                                                *forest);
-    else
-        k_body_epilogue<false><<<g, 256, 0, s>>>(px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc,
-                                                 NbForest{nullptr, nullptr, 0, nullptr, 0});
+    const NbForest f = forest ? *forest : NbForest{nullptr, nullptr, 0, nullptr, 0};
+    const bool caustic = pot.enabled && pot.haloType == NBCUDA_CAUSTIC_HALO;
+#define NB_EPI_ARGS px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc, f
+    if (forest) {
+        if (caustic) k_body_epilogue<true, true><<<g, 256, 0, s>>>(NB_EPI_ARGS);
+        else k_body_epilogue<true, false><<<g, 256, 0, s>>>(NB_EPI_ARGS);
+    } else {
+        if (caustic) k_body_epilogue<false, true><<<g, 256, 0, s>>>(NB_EPI_ARGS);
+        else k_body_epilogue<false, false><<<g, 256, 0, s>>>(NB_EPI_ARGS);
+    }
+#undef NB_EPI_ARGS
     nb_count_launch();
 }
 

@@ -72,6 +72,14 @@ class Halo:
         return h
 
     @staticmethod
+    def caustic(vhalo=0.0, scaleLength=0.0):
+        """Halo.caustic{vhalo, scaleLength}: the field takes the reference's fixed flow tables;
+        the two parameters are carried but unused, as in the reference."""
+        h = _lib.Halo()
+        h.type, h.vhalo, h.scaleLength = _lib.CAUSTIC_HALO, vhalo, scaleLength
+        return h
+
+    @staticmethod
     def triaxial(vhalo, scaleLength, flattenX, flattenY, flattenZ, triaxAngle):
         """Triaxial logarithmic halo; c1..c3 as nbCheckParams derives them
         (nbody/src/nbody_check_params.c:182-194)."""
