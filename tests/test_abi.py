@@ -49,6 +49,43 @@ def test_struct_layouts():
     assert ctypes.sizeof(_lib.TreeInfo) == 8 + 7 * 4 + 4
 
 
+# every struct of the C ABI and its ctypes mirror (field names as in C, but for renames)
+MIRRORS = [("NBodyCudaSpherical", "Spherical"), ("NBodyCudaDisk", "Disk"), ("NBodyCudaHalo", "Halo"),
+           ("NBodyCudaPotential", "Potential"), ("NBodyCudaCtx", "Ctx"),
+           ("NBodyCudaTreeInfo", "TreeInfo"), ("NBodyCudaHistogramParams", "HistParams"),
+           ("NBodyCudaDataHistogram", "DataHist"), ("NBodyCudaRunParams", "RunParams"),
+           ("NBodyCudaRunResult", "RunResult"), ("NBodyCudaPlummerDwarf", "PlummerDwarf"),
+           ("NBodyCudaDwarfComponent", "DwarfComponent"), ("NBodyCudaMixedDwarf", "MixedDwarf"),
+           ("NBodyCudaDwarf", "Dwarf")]
+RENAMED = {"lambda_": "lambda"}
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """sizeof and every field's offset of each C struct (compiled against the header by the C
+    compiler) equal the ctypes mirror's: a field added on one side only fails here."""
+    import subprocess
+    from milkywayathome_client_b200 import _lib
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "nbody_b200.h"', 'int main(void) {']
+    want = []
+    for cname, pyname in MIRRORS:
+        cls = getattr(_lib, pyname)
+        lines.append('printf("%%zu\\n", sizeof(%s));' % cname)
+        want.append(ctypes.sizeof(cls))
+        for f in cls._fields_:
+            lines.append('printf("%%zu\\n", offsetof(%s, %s));' % (cname, RENAMED.get(f[0], f[0])))
+            want.append(getattr(cls, f[0]).offset)
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    r = subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    assert got == want
+
+
 def test_library_built_for_sm100a_only():
     """The shared library carries sm_100a code (no other architecture, no PTX fallback)."""
     from milkywayathome_client_b200 import build
