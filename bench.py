@@ -4,22 +4,31 @@ dwarf (TreeCode, theta 0.5, quadrupoles, Miyamoto-Nagai + Hernquist + logarithmi
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+The input is the sample workunit's two-component Plummer dwarf (for_developers.lua: baryons
+a = 0.2 kpc, M = 12; radius and mass ratios 0.2; half the bodies baryons) sampled on the GPU by
+the library's port of the reference's Eddington-inversion sampler (nbGenerateDwarfCUDA, a fixed
+seed, the same bodies bit for bit on every run), placed on its orbit point (l = 218, b = 53.5,
+r = 28.6 kpc; v = (-156, 79, 107)); dt and eps2 from the reference's formulas.  Both arms step
+the same arrays.
+
 One step = one kick-drift-kick step of the whole dwarf: bounding box, octree build,
 moments, the force walk with the external potential, both leapfrog halves.  The headline
 `value` is the FP64 drop-in form (bit-exact with the reference CPU step), timed on the device
 (CUDA events on the library's stream) with the bodies resident in HBM; `e2e` is the same
 metric through the C ABI with host (pinned) buffers copied in and out every step.  The
 mixed-precision form, the sampled accuracy of both forms against FP64 direct summation, the
-roofline of the walk kernel and the reference CPU baseline are reported alongside.
+roofline of the walk kernel, the CPU-runnable 20,000-body configuration (200 steps), the
+8,388,608-body configuration, the adjoint cost and the batched dwarfs are reported alongside;
+short top-level keys at the end of the line repeat their headline figures.
 
 Multi-GPU (launched under torchrun): one independent dwarf per GPU, no collective on the
 data path ("replicas only": a single Barnes-Hut step does not shard), weak scaling;
 `value` = all ranks' body-updates / the slowest rank's device time.
 
---impl reference: the reference's own CPU code (oracle/_ref, built from its sources;
-the C restatement in oracle/ when that is absent) on this host's cores, on the same workload,
-each step a bounded sample: the full tree build plus the force walk of a random subset of
-bodies, scaled to the whole dwarf.
+--impl reference: the reference's own CPU code (oracle/_ref, built from its sources; the C
+restatement in oracle/ when that is absent) on this host's cores, stepping the same dwarf
+through its stock step (nbGravMap once, then nbStepSystem per step) for the W + K steps the
+line claims, each timed whole; plus the 200-step run of the 20,000-body configuration.
 """
 import argparse
 import json
@@ -38,11 +47,19 @@ METRIC = "body-updates/s N=1M: FP64 vs mixed at stated error; adjoint/forward ti
 UNIT = "body-updates/s"
 N_DEFAULT = 1048576
 THETA_DEFAULT = 0.5
-WORKLOAD = ("two-component Plummer dwarf, N=1,048,576 (half baryons), TreeCode theta=0.5, "
-            "quadrupoles, Miyamoto-Nagai+Hernquist+logarithmic-halo potential, KDK leapfrog")
+SEED_1M, SEED_CONFIG0, SEED_CONFIG2 = 1000, 2000, 3000
+WORKLOAD = ("sample workunit's two-component Plummer dwarf, N=1,048,576 (half baryons), "
+            "TreeCode theta=0.5, quadrupoles, Miyamoto-Nagai+Hernquist+logarithmic-halo "
+            "potential, KDK leapfrog")
 # algorithmic flops per unit of the walk (add/mul/div/sqrt = 1): node visit test 9,
 # body/monopole interaction 18, quadrupole cell 18 + 38 (nbody/src/nbody_grav.c:53-100)
 FLOP_VISIT, FLOP_MONO, FLOP_QUAD = 9, 18, 56
+# compulsory HBM bytes per body of the phases outside the walk, one step, from the kernels'
+# inputs and outputs touched once: drift + bounding box 72 read + 48 written; keys 32 + 12;
+# radix sort 8 passes x (12 read + 12 written); grid gather, run fix and parting depths ~60;
+# prefix sums 8; node records ~1.5 nodes per body x 64; links 1.5 x 8; moments 1.5 x 80;
+# potential + kick 72 read + 48 written
+NONWALK_BYTES_PER_BODY = 120 + 44 + 192 + 60 + 8 + 96 + 12 + 120 + 120
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "walk_traffic.json")
 
 
@@ -55,10 +72,15 @@ def parse_args():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--theta", type=float, default=THETA_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--config0-steps", type=int, default=200,
+                    help="steps of the 20,000-body configuration (0: skip)")
+    ap.add_argument("--config2-n", type=int, default=8388608,
+                    help="bodies of the large configuration (0: skip)")
+    ap.add_argument("--config2-steps", type=int, default=50)
     ap.add_argument("--adjoint-n", type=int, default=131072,
                     help="bodies of the adjoint-cost measurement (0 skips it)")
-    ap.add_argument("--adjoint-steps", type=int, default=64)
+    ap.add_argument("--adjoint-steps", type=int, default=1000)
+    ap.add_argument("--adjoint-warmup-steps", type=int, default=64)
     ap.add_argument("--batch-dwarfs", type=int, default=256,
                     help="dwarfs of the batched workload (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=500)
@@ -71,6 +93,31 @@ def parse_args():
     ap.add_argument("--profile", choices=["fp64", "mixed", "adjoint", "batch"],
                     help="profiling entry: build the dwarf, run two force evaluations, exit")
     return ap.parse_args()
+
+
+def bench_ctx(n, theta, precision="fp64"):
+    from milkywayathome_client_b200 import models
+    from milkywayathome_client_b200.nbody import NBodyCtx
+    cfg = models.dwarf_config(n, theta=theta)
+    return NBodyCtx(potential=models.sample_workunit_potential(), precision=precision, **cfg), cfg
+
+
+def bench_config(n, theta):
+    """The `config` of the JSON line: the same dict in both arms."""
+    _, cfg = bench_ctx(n, theta)
+    return {"workload": WORKLOAD, "n_bodies": n, "theta": theta, "criterion": "TreeCode",
+            "quadrupole": True, "eps2": cfg["eps2"], "dt": cfg["timestep"],
+            "input": "nbGenerateDwarfCUDA (the reference's two-component sampler on the GPU), "
+                     "seed %d, on the orbit point l=218 b=53.5 r=28.6 v=(-156,79,107)" % SEED_1M,
+            "parallelism": "replicas: one independent dwarf per GPU",
+            "l2": "inputs larger than L2: ~%.1fM tree nodes (~%.0f MB) + bodies (~%.0f MB) per "
+                  "step" % (1.5 * n / 1e6, 1.5 * n * 176 / 1e6, n * 120 / 1e6)}
+
+
+def bench_input(n, seed, device=0):
+    """The benchmark dwarf: host arrays pos, vel, mass, type (models.sampled_dwarf)."""
+    from milkywayathome_client_b200 import models
+    return models.sampled_dwarf(n, seed=seed, device=device)
 
 
 # ---------------------------------------------------------------------------------------
@@ -207,68 +254,103 @@ def walk_flops(counts, use_quad=True):
 
 
 # ---------------------------------------------------------------------------------------
-def cpu_baseline_sample(ctx, pos, mass, seconds):
-    """Reference CPU code on this host's cores: tree build + walk of a random body subset,
-    scaled to the whole dwarf.  Returns the cpu_baseline object."""
-    from oracle import bindings as ob
-    n = len(mass)
-    rng = np.random.default_rng(12345)
-    use_ref = ob.ref_available()
-    if use_ref:
-        r = ob.RefState.create(ctx.struct, pos, np.zeros_like(pos), mass)
-        cores = ob.ref().nbref_threads()
+class RefStepper:
+    """The reference's stock step on this host's cores: a reference NBodyState built from the
+    arrays (oracle/_ref: setInitialNBodyState), nbGravMap once, then nbStepSystem per step
+    (nbody/src/nbody.c:182-200 -> nbStepSystemPlain, nbody/src/nbody_plain.c:329-364).  Where
+    the reference build is absent, the oracle's C restatement (or_grav_map + or_step)."""
 
-        def run(idx):
-            rc, tt, tw = r.sample_step(idx)
-            return rc, tt, tw
-    else:
-        cores = ob.oracle().or_threads()
+    def __init__(self, ctx, pos, vel, mass, typ):
+        from oracle import bindings as ob
+        self.ob = ob
+        self.ctx = ctx
+        self.kind = "reference" if ob.ref_available() else "port"
+        self.n = len(mass)
+        if self.kind == "reference":
+            self.r = ob.RefState.create(ctx.struct, pos, vel, mass, typ)
+            self.cores = int(ob.ref().nbref_threads())
+            self.status = int(self.r.gravmap())
+        else:
+            self.cores = int(ob.oracle().or_threads())
+            self.status, self.pos, self.vel, self.acc, self.rsize = ob.steps(
+                ctx.struct, pos, vel, mass, ctx.treeRSize, 0)
+            self.mass = np.ascontiguousarray(mass, dtype=np.float64)
 
-        def run(idx):
-            rc, tt, tw, _ = ob.sample_step(ctx.struct, pos, mass, ctx.treeRSize, idx)
-            return rc, tt, tw
-    # size the subset from a small probe so one sample takes about `seconds`
-    probe = np.sort(rng.choice(n, size=min(n, 2048), replace=False))
-    rc, tt, tw = run(probe)
-    per_body = tw / len(probe)
-    m = int(min(n, max(2048, (seconds - tt) / max(per_body, 1e-9))))
-    idx = np.sort(rng.choice(n, size=m, replace=False))
-    rc, tt, tw = run(idx)
-    step_s = tt + tw * n / m
-    if use_ref:
-        r.close()
-    return {"value": n / step_s, "unit": UNIT, "cores": int(cores),
-            "kind": "reference" if use_ref else "port",
-            "sample": ("one step of the same dwarf: full nbMakeTree (%.2f s, serial in the "
-                       "reference) + nbGravity/nbExtAcceleration for %d random bodies (%.2f s "
-                       "on %d threads) scaled to all %d bodies; leapfrog passes not timed"
-                       % (tt, m, tw, cores, n)),
-            "status": int(rc), "step_seconds_estimate": step_s}
+    def step(self, k=1):
+        """k steps; returns their wall-clock seconds."""
+        import ctypes
+        t0 = time.perf_counter()
+        if self.kind == "reference":
+            self.status |= int(self.r.step(k))
+        else:
+            rs, inc = ctypes.c_double(self.rsize), ctypes.c_int(0)
+            p = lambda a: ctypes.c_void_p(a.ctypes.data)
+            self.status |= int(self.ob.oracle().or_step(
+                ctypes.byref(self.ctx.struct), p(self.pos), p(self.vel), p(self.mass), self.n,
+                ctypes.byref(rs), p(self.acc), k, ctypes.byref(inc)))
+            self.rsize = rs.value
+        return time.perf_counter() - t0
+
+    def close(self):
+        if self.kind == "reference":
+            self.r.close()
 
 
-def adjoint_ratio(n, steps, dev):
+def config0_reference(args, dev):
+    """The 20,000-body configuration's whole run (args.config0_steps steps) on the reference's
+    CPU code, timed without sampling; the same input as the GPU leg."""
+    n0 = 20000
+    pos, vel, mass, typ = bench_input(n0, SEED_CONFIG0, dev)
+    ctx0, _ = bench_ctx(n0, 1.0)
+    ref = RefStepper(ctx0, pos, vel, mass, typ)
+    secs = ref.step(args.config0_steps)
+    ref.close()
+    return {"value": n0 * args.config0_steps / secs, "unit": UNIT, "seconds": secs,
+            "steps": args.config0_steps, "n_bodies": n0, "cores": ref.cores, "kind": ref.kind,
+            "status": ref.status}
+
+
+def cpu_baseline_step(ctx, pos, vel, mass, typ, args, dev):
+    """Reference CPU code on this host's cores on the same dwarf: its initial nbGravMap
+    (untimed), then one whole nbStepSystem step timed -- no sampling, no extrapolation; plus
+    the 20,000-body configuration's whole run.  Returns the cpu_baseline object."""
+    ref = RefStepper(ctx, pos, vel, mass, typ)
+    step_s = ref.step(1)
+    ref.close()
+    out = {"value": len(mass) / step_s, "unit": UNIT, "cores": ref.cores, "kind": ref.kind,
+           "sample": ("one whole step of the same %d-body dwarf (nbStepSystem after the initial "
+                      "nbGravMap, %.2f s on %d threads), not extrapolated"
+                      % (len(mass), step_s, ref.cores)) if ref.kind == "reference" else
+                     ("one whole step of the oracle's C restatement (or_step) on the same dwarf "
+                      "(%.2f s on %d threads)" % (step_s, ref.cores)),
+           "status": ref.status, "step_seconds": step_s}
+    if args.config0_steps > 0:
+        out["config0"] = config0_reference(args, dev)
+    return out
+
+
+def adjoint_ratio(n, steps, warm_steps, dev):
     """Adjoint step / forward step time of the FP64 step with the tree frozen per step, on the
     two-component dwarf at n bodies (checkpoints every 32 steps, recomputation between them).
     Both passes are timed the same way (CUDA events on torch's stream around the whole pass,
-    host sequencing included), on the second of two runs (the first one warms up)."""
+    host sequencing included), on a run of `steps` steps after a warm-up run of `warm_steps`."""
     import torch
-    from milkywayathome_client_b200 import adjoint, models
-    from milkywayathome_client_b200.nbody import NBodyCtx, milky_way_potential
-    pos, vel, mass, _ = models.plummer_plummer_dwarf(n, seed=4242)
-    ctx = NBodyCtx(potential=milky_way_potential(), **models.dwarf_config(n, theta=0.5))
+    from milkywayathome_client_b200 import adjoint
+    pos, vel, mass, _ = bench_input(n, 4242, dev)
+    ctx, _ = bench_ctx(n, 0.5)
     device = torch.device("cuda:%d" % dev)
     t = lambda a: torch.tensor(a, dtype=torch.float64, device=device)
     x0, v0, m = t(pos).requires_grad_(True), t(vel).requires_grad_(True), t(mass).requires_grad_(True)
     dt = t(ctx.timestep).requires_grad_(True)
     w = torch.randn((n, 3), dtype=torch.float64, device=device, generator=torch.Generator(device=device).manual_seed(0))
-    # one untimed run first: its device state (buffers and saved trees) is kept for the next
-    # run, as in an optimisation loop
-    for _ in range(2):
+    # the warm-up run's device state (buffers and saved trees) is kept for the timed run, as in
+    # an optimisation loop
+    for nsteps in (warm_steps, steps):
         stats = {}
-        xN, vN = adjoint.run(ctx, x0, v0, m, dt, steps, every=32, stats=stats)
+        xN, vN = adjoint.run(ctx, x0, v0, m, dt, nsteps, every=32, stats=stats)
         ((xN * w).sum() + (vN * w).sum()).backward()
     adjoint.release_states()
-    return {"n_bodies": n, "steps": steps, "checkpoint_every": 32,
+    return {"n_bodies": n, "steps": steps, "checkpoint_every": 32, "warmup_steps": warm_steps,
             "forward_step_ms": stats["forward_step_ms"], "adjoint_step_ms": stats["adjoint_step_ms"],
             "ratio": stats["adjoint_step_ms"] / stats["forward_step_ms"],
             "parts_device_ms": {k: stats[k] for k in ("forward_step_device_ms",
@@ -289,8 +371,8 @@ def batched_run(args, dist, dev):
     collective on the data path).  Steps run through one captured CUDA graph each, after the
     autotuner picked the walk tuning; the device time of the timed steps is the measure."""
     from milkywayathome_client_b200 import (NBodyBatch, NBodyCtx, HistogramParams,
-                                            data_from_counts, milky_way_potential, models)
-    pot = milky_way_potential()
+                                            data_from_counts, models)
+    pot = models.sample_workunit_potential()          # the CPU-runnable configuration's
     draws = models.dwarf_parameter_draws(args.batch_dwarfs, seed=args.batch_seed)
     mine = draws[dist.rank::dist.world]
     ref_draw = models.dwarf_parameter_draws(1, seed=args.batch_seed + 1)[0]
@@ -356,60 +438,135 @@ def batched_run(args, dist, dev):
 
 
 def run_reference(args, dist):
-    """--impl reference: bounded reference samples on the host, rank 0 only."""
+    """--impl reference: the reference's stock step on the host, rank 0 only."""
     if dist.rank != 0:
         return 0
-    from milkywayathome_client_b200 import models
-    from milkywayathome_client_b200.nbody import NBodyCtx, milky_way_potential
-    from oracle import bindings as ob
-    n = args.n
-    pos, vel, mass, _ = models.plummer_plummer_dwarf(n, seed=1000)
-    ctx = NBodyCtx(potential=milky_way_potential(), **models.dwarf_config(n, theta=args.theta))
-    use_ref = ob.ref_available()
-    rng = np.random.default_rng(777)
-    m = max(2048, n // 64)
-    if use_ref:
-        r = ob.RefState.create(ctx.struct, pos, vel, mass)
-        cores = ob.ref().nbref_threads()
-    else:
-        cores = ob.oracle().or_threads()
-    times = []
-    for k in range(args.warmup + args.steps):
-        idx = np.sort(rng.choice(n, size=m, replace=False))
-        if use_ref:
-            rc, tt, tw = r.sample_step(idx)
-        else:
-            rc, tt, tw, _ = ob.sample_step(ctx.struct, pos, mass, ctx.treeRSize, idx)
-        if k >= args.warmup:
-            times.append(tt + tw * n / m)
+    n, K, W = args.n, args.steps, args.warmup
+    # the same arrays as the GPU arm's rank 0 (generated on the GPU, outside the timed steps)
+    pos, vel, mass, typ = bench_input(n, SEED_1M)
+    ctx, _ = bench_ctx(n, args.theta)
+    ref = RefStepper(ctx, pos, vel, mass, typ)
+    times = [ref.step(1) for _ in range(W + K)][W:]
+    ref.close()
     step_s = float(np.mean(times))
-    value = n / step_s
+    value = n * K / float(np.sum(times))
+    c0 = config0_reference(args, 0) if args.config0_steps > 0 else None
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic: seeded two-component Plummer dwarf",
-        "config": {"workload": WORKLOAD, "n_bodies": n, "theta": args.theta},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(cores),
-                         "kind": "reference" if use_ref else "port",
-                         "sample": ("each step: full nbMakeTree + nbGravity/nbExtAcceleration "
-                                    "for %d random bodies of %d, scaled to the whole dwarf" % (m, n))},
+        "steps": K, "warmup": W, "ms_per_step": step_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: the sample workunit's two-component dwarf (seeded; no dataset)",
+        "config": bench_config(n, args.theta),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.cores, "kind": ref.kind,
+                         "sample": ("none: %d warm-up + %d timed whole steps of the %d-body dwarf "
+                                    "(nbGravMap once, then nbStepSystem per step), each timed "
+                                    "with the host clock" % (W, K, n))},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "status": ref.status,
+        "step_seconds": times,
+        "config0": c0,
+        "config0_value": c0["value"] if c0 else None,
     }
     print(json.dumps(out), flush=True)
     return 0
 
 
 # ---------------------------------------------------------------------------------------
+def form_accuracy(pos, vel, mass, c_cfg, dev, seed=4096):
+    """Relative acceleration error of the FP64 walk, the mixed walk (exact sets) and the mixed
+    group mode against FP64 direct summation, self-gravity only, on a seeded 4,096-body
+    sample."""
+    from milkywayathome_client_b200.nbody import NBodyCtx, NBodyState
+    n = len(mass)
+    rng = np.random.default_rng(seed)
+    sample = np.sort(rng.choice(n, size=min(4096, n), replace=False)).astype(np.int32)
+    c_self = NBodyCtx(potential=None, **c_cfg)
+    rel = {}
+    with NBodyState.create(c_self, pos, vel, mass, device=dev, gravmap=False) as sa:
+        direct = sa.direct_sample(c_cfg["eps2"], sample)
+        cm = c_self.with_precision("mixed")
+        for name, c, exact in (("fp64", c_self, True), ("mixed", cm, True),
+                               ("mixed_group_mode", cm, False)):
+            sa.set_mixed_mode(exact)
+            sa.check("nbGravMap", sa.gravMap(c))
+            a = sa.accels()[sample]
+            rel[name] = np.linalg.norm(a - direct, axis=1) / np.linalg.norm(direct, axis=1)
+    out = {"sample": "4,096 seeded bodies, self-gravity only, vs FP64 direct summation"}
+    for name in ("fp64", "mixed", "mixed_group_mode"):
+        out[name] = {p: float(np.percentile(rel[name], q)) for p, q in
+                     (("p50", 50), ("p90", 90), ("p99", 99), ("max", 100))}
+    for form, tag in (("mixed", "mixed"), ("mixed_group_mode", "group_mode")):
+        for p in ("p50", "p99", "max"):
+            out["%s_added_error_%s_pct" % (tag, p)] = 100.0 * (
+                out[form][p] - out["fp64"][p]) / out["fp64"][p]
+    return out
+
+
+def run_steps_timed(c, pos, vel, mass, dev, warm, steps, exact=True):
+    """A fresh state of the arrays, `warm` untimed steps, then `steps` steps each timed with
+    CUDA events; returns (step ms list, walk ms list, tree info)."""
+    from milkywayathome_client_b200.nbody import NBodyState
+    with NBodyState.create(c, pos, vel, mass, device=dev) as st:
+        st.set_mixed_mode(exact)
+        for _ in range(warm):
+            st.check("nbStepSystem", st.step(c))
+        ms, walk = [], []
+        for _ in range(steps):
+            st.check("nbStepSystem", st.step(c))
+            ms.append(st.step_time_ms())
+            walk.append(st.walk_time_ms()[0])
+        return ms, walk, st.tree_info()
+
+
+def config0_run(args, dist, dev):
+    """The CPU-runnable configuration on the GPU: the sample workunit's dwarf at 20,000 bodies,
+    TreeCode theta = 1.0 with quadrupoles, its whole run of args.config0_steps steps (the
+    reference's dt and eps2), FP64 and mixed, after one warm-up run on another state."""
+    n0, S = 20000, args.config0_steps
+    pos, vel, mass, _ = bench_input(n0, SEED_CONFIG0 + dist.rank, dev)
+    ctx0, _ = bench_ctx(n0, 1.0)
+    out = {"workload": "sample workunit's two-component dwarf, N=20,000, TreeCode theta=1.0, "
+                       "quadrupoles, %d steps (nbGenerateDwarfCUDA seed %d)" % (S, SEED_CONFIG0),
+           "n_bodies": n0, "steps": S}
+    for name, c in (("fp64", ctx0), ("mixed", ctx0.with_precision("mixed"))):
+        run_steps_timed(c, pos, vel, mass, dev, 0, max(args.warmup, 3))
+        ms, _, _ = run_steps_timed(c, pos, vel, mass, dev, 0, S)
+        v, t = replica_throughput(dist, n0, S, sum(ms) / 1e3)
+        out[name] = {"value": v, "unit": UNIT, "ms_per_step": 1e3 * t / S, "run_ms": 1e3 * t}
+    return out
+
+
+def config2_run(args, dist, dev):
+    """The large configuration: the sample workunit's dwarf at args.config2_n bodies, TreeCode
+    theta = 0.5 with quadrupoles, args.config2_steps steps of each form after W warm-up steps;
+    sampled direct-sum error; HBM throughput of the phases outside the walk (their compulsory
+    bytes over their device time)."""
+    n2, S, W = args.config2_n, args.config2_steps, args.warmup
+    pos, vel, mass, _ = bench_input(n2, SEED_CONFIG2 + dist.rank, dev)
+    ctx2, cfg2 = bench_ctx(n2, 0.5)
+    out = {"workload": "sample workunit's two-component dwarf, N=%d, TreeCode theta=0.5, "
+                       "quadrupoles, %d steps (nbGenerateDwarfCUDA seed %d)" % (n2, S, SEED_CONFIG2),
+           "n_bodies": n2, "steps": S}
+    for name, c in (("fp64", ctx2), ("mixed", ctx2.with_precision("mixed"))):
+        ms, walk, info = run_steps_timed(c, pos, vel, mass, dev, W, S)
+        v, t = replica_throughput(dist, n2, S, sum(ms) / 1e3)
+        nonwalk = float(np.mean(ms) - np.mean(walk))
+        out[name] = {"value": v, "unit": UNIT, "ms_per_step": 1e3 * t / S,
+                     "walk_ms": float(np.mean(walk)), "nonwalk_ms": nonwalk,
+                     "nonwalk_hbm_gbs": NONWALK_BYTES_PER_BODY * n2 / (nonwalk * 1e-3) / 1e9}
+        out["tree"] = {"nodes": info.nNodes, "max_depth": info.maxDepth, "rsize": info.rsize}
+    out["mixed_speedup"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["nonwalk_bytes_per_body"] = NONWALK_BYTES_PER_BODY
+    out["accuracy"] = form_accuracy(pos, vel, mass, cfg2, dev)
+    return out
+
+
 def run_ours(args, dist):
-    from milkywayathome_client_b200 import models
-    from milkywayathome_client_b200.nbody import (NBodyCtx, NBodyState, kernel_launches,
-                                                 milky_way_potential, peak_fma_tflops)
+    from milkywayathome_client_b200.nbody import NBodyState, kernel_launches, peak_fma_tflops
     n, K, W = args.n, args.steps, args.warmup
     dev = dist.local
-    pos, vel, mass, _ = models.plummer_plummer_dwarf(n, seed=1000 + dist.rank)
-    cfg = models.dwarf_config(n, theta=args.theta)
-    ctx = NBodyCtx(potential=milky_way_potential(), **cfg)
+    pos, vel, mass, typ = bench_input(n, SEED_1M + dist.rank, dev)
+    ctx, cfg = bench_ctx(n, args.theta)
     ctx_mixed = ctx.with_precision("mixed")
     notes = []
 
@@ -445,32 +602,7 @@ def run_ours(args, dist):
     mean_walk = float(np.mean(walk_ms))
 
     # ---- accuracy against FP64 direct summation on a seeded 4,096-body sample ----
-    rng = np.random.default_rng(4096)
-    sample = np.sort(rng.choice(n, size=min(4096, n), replace=False)).astype(np.int32)
-
-    def form_accuracy(c_cfg):
-        c_self = NBodyCtx(potential=None, **c_cfg)
-        rel = {}
-        with NBodyState.create(c_self, pos, vel, mass, device=dev, gravmap=False) as sa:
-            direct = sa.direct_sample(c_cfg["eps2"], sample)
-            cm = c_self.with_precision("mixed")
-            for name, c, exact in (("fp64", c_self, True), ("mixed", cm, True),
-                                   ("mixed_group_mode", cm, False)):
-                sa.set_mixed_mode(exact)
-                sa.check("nbGravMap", sa.gravMap(c))
-                a = sa.accels()[sample]
-                rel[name] = np.linalg.norm(a - direct, axis=1) / np.linalg.norm(direct, axis=1)
-        out = {"sample": "4,096 seeded bodies, self-gravity only, vs FP64 direct summation"}
-        for name in ("fp64", "mixed", "mixed_group_mode"):
-            out[name] = {p: float(np.percentile(rel[name], q)) for p, q in
-                         (("p50", 50), ("p90", 90), ("p99", 99), ("max", 100))}
-        for form, tag in (("mixed", "mixed"), ("mixed_group_mode", "group_mode")):
-            for p in ("p50", "p99", "max"):
-                out["%s_added_error_%s_pct" % (tag, p)] = 100.0 * (
-                    out[form][p] - out["fp64"][p]) / out["fp64"][p]
-        return out
-
-    accuracy = form_accuracy(cfg)
+    accuracy = form_accuracy(pos, vel, mass, cfg, dev)
 
     # ---- e2e through the C ABI with pinned host buffers ----
     hp = pinned_array((n, 3)); hv = pinned_array((n, 3)); hm = pinned_array((n,))
@@ -535,23 +667,16 @@ def run_ours(args, dist):
     # ---- the configuration's second opening angle: both forms, speed and accuracy ----
     theta2 = None
     if args.theta2 > 0:
-        cfg2 = models.dwarf_config(n, theta=args.theta2)
-        ctx2 = NBodyCtx(potential=milky_way_potential(), **cfg2)
+        ctx2, cfg2 = bench_ctx(n, args.theta2)
         theta2 = {"theta": args.theta2}
         for name, c in (("fp64", ctx2), ("mixed", ctx2.with_precision("mixed"))):
-            with NBodyState.create(c, pos, vel, mass, device=dev) as s2:
-                for _ in range(W):
-                    s2.check("nbStepSystem", s2.step(c))
-                ms = []
-                for _ in range(K):
-                    s2.check("nbStepSystem", s2.step(c))
-                    ms.append(s2.step_time_ms())
+            ms, _, _ = run_steps_timed(c, pos, vel, mass, dev, W, K)
             v2, t2 = replica_throughput(dist, n, K, sum(ms) / 1e3)
             theta2[name] = {"value": v2, "unit": UNIT, "ms_per_step": 1e3 * t2 / K}
         theta2["speedup_mixed_vs_fp64"] = theta2["mixed"]["value"] / theta2["fp64"]["value"]
-        theta2["accuracy"] = form_accuracy(cfg2)
+        theta2["accuracy"] = form_accuracy(pos, vel, mass, cfg2, dev)
 
-    # ---- roofline of the walk kernel (FP64 pipe) ----
+    # ---- roofline of the walk kernels (FP64 pipe; FP32 pipe for the mixed walk) ----
     peak64 = peak_fma_tflops(True, dev)
     peak32 = peak_fma_tflops(False, dev)
     achieved = flops_per_walk / (mean_walk * 1e-3) / 1e12
@@ -572,18 +697,36 @@ def run_ours(args, dist):
                 "interactions_per_body": {"body": counts[0] / n, "cell": counts[1] / n,
                                           "visits": counts[2] / n},
                 "lane_utilisation": counts[2] / (32.0 * max(counts[3], 1))}
+    # the exact-set mixed walk evaluates every body's own FP64 interaction set, so its
+    # algorithmic work is the FP64 walk's count; issued work (list entries x 32 lanes, masked
+    # lanes included) is given beside it
     mixed["roofline"] = {"bound": "fp32", "kernel": "k_walk_mixed",
-                         "achieved": walk_flops(counts_m) / (mixed["walk_ms"] * 1e-3) / 1e12,
+                         "achieved": flops_per_walk / (mixed["walk_ms"] * 1e-3) / 1e12,
                          "peak": peak32, "unit": "TFLOP/s",
-                         "peak_source": "measured FFMA throughput (nbPeakFmaCUDA)"}
+                         "peak_source": "measured FFMA throughput (nbPeakFmaCUDA)",
+                         "flops_per_launch": flops_per_walk,
+                         "issued_flops_per_launch": walk_flops(counts_m)}
     mixed["roofline"]["frac"] = mixed["roofline"]["achieved"] / peak32
-    mixed["roofline"]["lane_utilisation"] = counts_m[2] / (32.0 * max(counts_m[3], 1))
+
+    # ---- the CPU-runnable and the large configurations ----
+    config0 = None
+    if args.config0_steps > 0:
+        try:
+            config0 = config0_run(args, dist, dev)
+        except Exception as e:
+            notes.append("config0 measurement failed: %r" % (e,))
+    config2 = None
+    if args.config2_n > 0:
+        try:
+            config2 = config2_run(args, dist, dev)
+        except Exception as e:
+            notes.append("config2 measurement failed: %r" % (e,))
 
     # ---- adjoint step cost (the adjoint configuration's dwarf) ----
     adj = None
     if args.adjoint_n > 0:
         try:
-            adj = adjoint_ratio(args.adjoint_n, args.adjoint_steps, dev)
+            adj = adjoint_ratio(args.adjoint_n, args.adjoint_steps, args.adjoint_warmup_steps, dev)
         except Exception as e:
             notes.append("adjoint measurement failed: %r" % (e,))
 
@@ -599,7 +742,7 @@ def run_ours(args, dist):
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline_sample(ctx, pos, mass, args.cpu_sample_seconds)
+            cpu = cpu_baseline_step(ctx, pos, vel, mass, typ, args, dev)
         except Exception as e:  # the baseline is reported, never the target
             notes.append("cpu_baseline failed: %r" % (e,))
 
@@ -608,22 +751,39 @@ def run_ours(args, dist):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": K,
             "warmup": W, "ms_per_step": 1e3 * t_dev / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: seeded two-component Plummer dwarf per GPU (no dataset)",
-            "config": {"workload": WORKLOAD, "n_bodies": n, "theta": args.theta,
-                       "criterion": "TreeCode", "quadrupole": True, "eps2": cfg["eps2"],
-                       "dt": cfg["timestep"], "form": "fp64 drop-in (bit-exact with the reference)",
-                       "parallelism": "replicas: one independent dwarf per GPU",
-                       "l2": "inputs larger than L2: %d tree nodes (~%.0f MB) + bodies (~%.0f MB) per step"
-                             % (info.nNodes, info.nNodes * 176 / 1e6, n * 120 / 1e6)},
+            "data": "synthetic: the sample workunit's two-component dwarf per GPU (seeded; no dataset)",
+            "form": "fp64 drop-in (bit-exact with the reference)",
+            "config": bench_config(n, args.theta),
             "roofline": roofline, "mixed": mixed, "accuracy": accuracy, "energy": energy,
             "theta2": theta2, "e2e": e2e,
             "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk, "adjoint": adj,
-            "batched": batched,
+            "batched": batched, "config0": config0, "config2": config2,
             "tree": {"nodes": info.nNodes, "cells": info.cellUsed, "max_depth": info.maxDepth,
                      "rsize": info.rsize},
         }
         if notes:
             out["notes"] = notes
+        # the headline figures of every configuration once more, short, at the end of the line
+        out["summary"] = {
+            "fp64_value": value,
+            "mixed_speedup": mixed["speedup_vs_fp64"],
+            "mixed_added_error_p99_pct": accuracy["mixed_added_error_p99_pct"],
+            "mixed_added_error_max_pct": accuracy["mixed_added_error_max_pct"],
+            "theta1_mixed_speedup": theta2["speedup_mixed_vs_fp64"] if theta2 else None,
+            "walk_fp64_frac": roofline["frac"],
+            "walk_mixed_frac": mixed["roofline"]["frac"],
+            "config0_value": config0["fp64"]["value"] if config0 else None,
+            "config0_reference_value": (cpu["config0"]["value"]
+                                        if cpu and "config0" in cpu else None),
+            "config2_fp64_value": config2["fp64"]["value"] if config2 else None,
+            "config2_mixed_speedup": config2["mixed_speedup"] if config2 else None,
+            "config2_mixed_added_error_p99_pct": (
+                config2["accuracy"]["mixed_added_error_p99_pct"] if config2 else None),
+            "adjoint_ratio": adj["ratio"] if adj else None,
+            "adjoint_steps": adj["steps"] if adj else None,
+            "batched_value": batched["value"] if batched else None,
+            "cpu_baseline_value": cpu["value"] if cpu else None,
+        }
         print(json.dumps(out), flush=True)
     return 0
 
@@ -633,8 +793,8 @@ def run_profile(args):
     --profile adjoint, one force evaluation followed by one force VJP at --adjoint-n bodies)."""
     from milkywayathome_client_b200 import models
     if args.profile == "batch":
-        from milkywayathome_client_b200 import NBodyBatch, NBodyCtx, milky_way_potential
-        pot = milky_way_potential()
+        from milkywayathome_client_b200 import NBodyBatch, NBodyCtx
+        pot = models.sample_workunit_potential()
         draws = models.dwarf_parameter_draws(args.batch_dwarfs, seed=args.batch_seed)
         spec, structs = models.batched_dwarf_structs(draws, pot, seed=args.batch_seed * 1000,
                                                      nsteps=args.batch_steps)
@@ -650,10 +810,9 @@ def run_profile(args):
     if args.profile == "adjoint":
         import torch
         from milkywayathome_client_b200.adjoint import DeviceState
-        from milkywayathome_client_b200.nbody import NBodyCtx, milky_way_potential
         n = args.adjoint_n
-        pos, vel, mass, _ = models.plummer_plummer_dwarf(n, seed=4242)
-        ctx = NBodyCtx(potential=milky_way_potential(), **models.dwarf_config(n, theta=args.theta))
+        pos, vel, mass, _ = bench_input(n, 4242)
+        ctx, _ = bench_ctx(n, args.theta)
         dev = torch.device("cuda:0")
         t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
         ds = DeviceState(n, dev)
@@ -667,10 +826,9 @@ def run_profile(args):
                           "vjp_walk_ms": ds.st.walk_time_ms()[0], "vjp_ms": ds.st.step_time_ms()}))
         ds.close()
         return 0
-    from milkywayathome_client_b200.nbody import NBodyCtx, NBodyState, milky_way_potential
-    pos, vel, mass, _ = models.plummer_plummer_dwarf(args.n, seed=1000)
-    ctx = NBodyCtx(potential=milky_way_potential(), precision=args.profile,
-                   **models.dwarf_config(args.n, theta=args.theta))
+    from milkywayathome_client_b200.nbody import NBodyState
+    pos, vel, mass, _ = bench_input(args.n, SEED_1M)
+    ctx, _ = bench_ctx(args.n, args.theta, precision=args.profile)
     with NBodyState.create(ctx, pos, vel, mass) as st:
         st.check("nbGravMap", st.gravMap(ctx))
         print(json.dumps({"profile": args.profile, "n": args.n, "walk_ms": st.walk_time_ms()[0],

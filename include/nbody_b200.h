@@ -331,6 +331,12 @@ NBodyCudaStatus nbGetLMCCUDA(NBodyCudaState* st, double* pos3, double* vel3);
  * For a batch, set it on the batch's state through nbBatchSetTimeOriginCUDA. */
 NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTime);
 
+/* The step counter of a state resumed from a checkpoint: nbThawState restores st->step from
+ * the checkpoint header (nbody/src/nbody_checkpoint.c:123-130), and nbMarshalBodiesCUDA's
+ * copy-in resets it to 0, so a resumed run sets it after marshalling the bodies in (the
+ * orbiting bar's time and the LMC's reflex accelerations are read at it). */
+NBodyCudaStatus nbSetStepCUDA(NBodyCudaState* st, int step);
+
 /* Mixed-precision walk tuning of a single state (as nbBatchSetTuningCUDA): bodies per walk
  * group (1..64), interaction-list entries per warp (32, 64, 128), walk blocks per SM (0: max). */
 NBodyCudaStatus nbSetMixedTuningCUDA(NBodyCudaState* st, int groupMax, int listCap, int blocksPerSM);
@@ -531,8 +537,10 @@ NBodyCudaStatus nbExtAccelerationCUDA(const NBodyCudaPotential* pot, const doubl
  * NB_NOALLOC_MAX_POINTS (65536) points (3 MiB, held by every device that loads the library
  * until exit); larger n is rejected with NBODY_USER_ERROR.  The first call on a device looks
  * up the array's address (cudaGetSymbolAddress), so make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race.  Same results as
- * nbExtAccelerationCUDA. */
+ * capture.  The address is kept for the life of the process: a device reset
+ * (cudaDeviceReset) unloads the array with the module, and calls after a reset of that
+ * device are not supported.  All calls share the array: calls that overlap on the GPU race.
+ * Same results as nbExtAccelerationCUDA. */
 NBodyCudaStatus nbExtAccelerationNoAllocCUDA(const NBodyCudaPotential* pot, const double* pos,
                                              double* acc, int n, int device);
 

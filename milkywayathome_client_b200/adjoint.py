@@ -325,8 +325,11 @@ def lbr_to_cartesian(l_deg, b_deg, r, sun_gc_dist=SUN_GC_DIST):
 def reverse_orbit(pot, pos, vel, tstop, dt):
     """nbReverseOrbit (nbody/src/nbody_orbit_integrator.c:44-86): leapfrog of the dwarf's
     centre backwards in the external potential for tstop; returns its start position and
-    velocity.  The step count is fixed by the values of tstop and dt (not differentiated)."""
-    nsteps = int(math.floor(float(tstop) / float(dt))) + 1
+    velocity.  The step count is fixed by the values of tstop and dt (a whole number, not
+    differentiated): the gradient with respect to tstop flows only through the step length
+    tstop / nsteps."""
+    value = lambda t: float(t.detach()) if torch.is_tensor(t) else float(t)
+    nsteps = int(math.floor(value(tstop) / value(dt))) + 1
     dtr = tstop / nsteps
     x, v = pos, -vel
     acc = ext_accel_torch(pot, x)

@@ -1640,6 +1640,13 @@ NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTi
     return NBODY_SUCCESS;
 }
 
+NBodyCudaStatus nbSetStepCUDA(NBodyCudaState* st, int step)
+{
+    if (!st || step < 0) return NBODY_USER_ERROR;
+    st->step = step;
+    return NBODY_SUCCESS;
+}
+
 NBodyCudaStatus nbSetTypesCUDA(NBodyCudaState* st, const int* types)
 {
     if (!st) return NBODY_USER_ERROR;

@@ -384,40 +384,39 @@ __global__ void k_ic_sample(const NbIcDwarf* __restrict__ dwarfs, int nD, int n,
     }
 }
 
-// Per (dwarf, component): sums of m x and m v (warp-segmented, one atomic per segment).
-__global__ void k_ic_moments(const NbIcDwarf* __restrict__ dwarfs, int nD, int n,
-                             const double* __restrict__ px, const double* __restrict__ py,
-                             const double* __restrict__ pz, const double* __restrict__ vx,
-                             const double* __restrict__ vy, const double* __restrict__ vz,
-                             const double* __restrict__ mass, double* __restrict__ sums)
+// Per (dwarf, component): sums of m x and m v, one block per component.  Each thread adds its
+// strided share of the component's bodies in index order and the block combines the threads'
+// sums by a fixed tree, so the sums -- and the recentred bodies -- are the same on every run
+// (floating-point atomics would add in arrival order).
+constexpr int kIcMomentThreads = 512;
+
+__global__ void __launch_bounds__(kIcMomentThreads)
+k_ic_moments(const NbIcDwarf* __restrict__ dwarfs, int nD,
+             const double* __restrict__ px, const double* __restrict__ py,
+             const double* __restrict__ pz, const double* __restrict__ vx,
+             const double* __restrict__ vy, const double* __restrict__ vz,
+             const double* __restrict__ mass, double* __restrict__ sums)
 {
-    const int lane = threadIdx.x & 31;
-    const int warpsTotal = (gridDim.x * blockDim.x) >> 5;
-    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n;
-         base += warpsTotal * 32) {
-        const int i = base + lane;
-        const bool valid = i < n;
-        int key = -1;
-        double s[6] = {0, 0, 0, 0, 0, 0};
-        if (valid) {
-            const int dwi = ic_dwarf_of(dwarfs, nD, i);
-            key = 2 * dwi + (i - dwarfs[dwi].first >= dwarfs[dwi].nBaryon);
-            const double mi = mass[i];
-            s[0] = mi * px[i]; s[1] = mi * py[i]; s[2] = mi * pz[i];
-            s[3] = mi * vx[i]; s[4] = mi * vy[i]; s[5] = mi * vz[i];
-        }
-        unsigned pending = __ballot_sync(NB_FULL_MASK, valid);
-        while (pending) {
-            const int leader = __ffs(pending) - 1;
-            const int kl = __shfl_sync(NB_FULL_MASK, key, leader);
-            for (int c = 0; c < 6; ++c) {
-                double v = key == kl ? s[c] : 0.0;
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(NB_FULL_MASK, v, o);
-                if (lane == leader) atomicAdd(&sums[6 * (size_t) kl + c], v);
-            }
-            pending &= ~__ballot_sync(NB_FULL_MASK, key == kl);
-        }
+    __shared__ double part[6][kIcMomentThreads];
+    const int seg = blockIdx.x;                       // 2 * dwarf + (dark component)
+    const NbIcDwarf& d = dwarfs[seg >> 1];
+    const bool dark = seg & 1;
+    const int lo = d.first + (dark ? d.nBaryon : 0);
+    const int hi = dark ? d.first + d.count : d.first + d.nBaryon;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = lo + (int) threadIdx.x; i < hi; i += kIcMomentThreads) {
+        const double mi = mass[i];
+        s[0] += mi * px[i]; s[1] += mi * py[i]; s[2] += mi * pz[i];
+        s[3] += mi * vx[i]; s[4] += mi * vy[i]; s[5] += mi * vz[i];
     }
+    for (int c = 0; c < 6; ++c) part[c][threadIdx.x] = s[c];
+    __syncthreads();
+    for (int w = kIcMomentThreads / 2; w > 0; w >>= 1) {
+        if ((int) threadIdx.x < w)
+            for (int c = 0; c < 6; ++c) part[c][threadIdx.x] += part[c][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) sums[6 * (size_t) seg + threadIdx.x] = part[threadIdx.x][0];
 }
 
 // x - cm + shift, v - cv + shift per component (cm = sum m x / component mass)
@@ -554,7 +553,8 @@ int nb_launch_ic(const NBodyCudaMixedDwarf* host, int nD, const int* firsts, voi
     else
         k_ic_sample<false><<<g, 128, 0, s>>>(dt, nD, n, b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.mass, types, sc);
     const int g2 = min((n + 255) / 256, numSMs * 8);
-    k_ic_moments<<<g2, 256, 0, s>>>(dt, nD, n, b.px, b.py, b.pz, b.vx, b.vy, b.vz, b.mass, scratch);
+    k_ic_moments<<<2 * nD, kIcMomentThreads, 0, s>>>(dt, nD, b.px, b.py, b.pz, b.vx, b.vy, b.vz,
+                                                     b.mass, scratch);
     k_ic_shift<<<g2, 256, 0, s>>>(dt, nD, n, b.px, b.py, b.pz, b.vx, b.vy, b.vz, scratch);
     nb_count_launch(3);
     return 3;

@@ -36,7 +36,9 @@ __global__ void k_ext_scratch(double* __restrict__ scratch, int n, NbPot pot)
     }
 }
 
-// Device address of g_extScratch, looked up once per device with that device current.
+// Device address of g_extScratch, looked up once per device with that device current and kept
+// for the life of the process (a device reset unloads the array; calls after one are not
+// supported).
 static std::mutex g_scratchLock;
 static double* g_scratchPtr[64];
 

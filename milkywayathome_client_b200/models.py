@@ -13,7 +13,9 @@ import math
 
 import numpy as np
 
-PI_4_3 = 4.0 * math.pi / 3.0
+# PI_4_3 of the reference (milkyway/include/milkyway_math_supplemental.h:195), the constant its
+# Lua set-up sees as pi_4_3; 4.0 * math.pi / 3.0 rounds one ulp lower
+PI_4_3 = 4.188790204786390984616857844372670512262892532500141
 SUN_GC_DIST = 8.0   # ctx.sunGCDist default (nbody/include/nbody_defaults.h)
 
 
@@ -29,33 +31,49 @@ def two_component_timestep(mass_l, rscale_l, mass_d, rscale_d):
     mass_enc_l = mass_l * rscale_d ** 3 * (rscale_l ** 2 + rscale_d ** 2) ** (-1.5)
     s1 = rscale_l ** 3 / (mass_enc_d + mass_l)
     s2 = rscale_d ** 3 / (mass_enc_l + mass_d)
-    return (1.0 / 100.0) * math.sqrt(PI_4_3 * min(s1, s2))
+    return (1.0 / 100.0) * (PI_4_3 * min(s1, s2)) ** (1.0 / 2.0)
 
 
 def calculate_virial(a_b, a_d, M_b, M_d, n=100000):
     """nbCalculateVirial (nbody/src/nbody_virial.c:38-103): 5-point Gauss-Legendre on n
-    panels out to 1000 scale radii."""
+    panels out to 1000 scale radii, the terms formed in the reference's operation order and
+    summed one after another as its loop does (numpy's pow stands in for crlibm's pow_rn,
+    so the result may differ from the reference's in the last bits)."""
     w = np.array([0.2369268850561891, 0.4786286704993665, 0.5688888888888889,
                   0.4786286704993665, 0.2369268850561891])
     x = np.array([-0.9061798459386640, -0.5384693101056831, 0.0, 0.5384693101056831,
                   0.9061798459386640])
-    upper = 1000.0 * max(a_b, a_d)
-    width = upper / n
-    a1 = np.arange(n) * width
-    r = (width * x[None, :] / 2.0 + (a1[:, None] + a1[:, None] + width) / 2.0)
-    dens = 3.0 / 4.0 / math.pi * (M_b / a_b ** 3 * (1.0 + r * r / a_b / a_b) ** -2.5 +
-                                  M_d / a_d ** 3 * (1.0 + r * r / a_d / a_d) ** -2.5)
+    upper = 1000.0 * a_b if a_b > a_d else 1000.0 * a_d
+    width = (upper - 0.0) / (n * 1.0)
+    i = np.arange(n, dtype=np.float64)
+    a1 = 0.0 + i * width
+    b1 = 0.0 + (i + 1.0) * width
+    r = width * x[None, :] / 2.0 + ((a1 + b1) / 2.0)[:, None]
+    dens = 3.0 / 4.0 / math.pi * (M_b / a_b ** 3.0 * (1.0 + r * r / a_b / a_b) ** -2.5 +
+                                  M_d / a_d ** 3.0 * (1.0 + r * r / a_d / a_d) ** -2.5)
     integ = 1.0 / 4.0 / math.pi * (M_b / a_b * r * r * (1.0 + r * r / a_b / a_b) ** -0.5 +
                                    M_d / a_d * r * r * (1.0 + r * r / a_d / a_d) ** -0.5)
-    integral = float(np.sum(w[None, :] * dens * integ * width / 2.0))
+    terms = (w[None, :] * dens * integ * width / 2.0).ravel()
+    integral = 0.0
+    for t in terms.tolist():
+        integral += t
     M_tot = M_b + M_d
     return M_tot * M_tot / 16.0 / math.pi / math.pi / integral
 
 
 def calculate_eps2(nbody, a_b, a_d, M_b, M_d):
-    """calculateEps2 (nbody/src/nbody_lua_models.c:158-169)."""
-    eps = calculate_virial(a_b, a_d, M_b, M_d) * 0.98 * nbody ** -0.26
-    return max(eps * eps, np.finfo(np.float64).eps)
+    """calculateEps2 (nbody/src/nbody_lua_models.c:158-169): eps = 0.98 r_v N^-0.26."""
+    eps = calculate_virial(a_b, a_d, M_b, M_d) * 0.98 * float(nbody) ** -0.26
+    eps2 = (eps * eps) / 1.0
+    return eps2 if eps2 > np.finfo(np.float64).eps else float(np.finfo(np.float64).eps)
+
+
+def sample_workunit_potential():
+    """The potential of the two-component sample workunit
+    (nbody/sample_workunits/for_developers.lua:150-162): Hernquist bulge, Miyamoto-Nagai disk
+    and a logarithmic halo of vhalo = 74.61 kpc/Gyr (73 km/s)."""
+    from .nbody import milky_way_potential
+    return milky_way_potential(vhalo=74.61)
 
 
 def lbr_to_cartesian(l_deg, b_deg, r, sun_gc_dist=SUN_GC_DIST):
@@ -131,6 +149,36 @@ def plummer_plummer_dwarf(nbody, seed=0, mass_l=12.0, rscale_l=0.2, light_r_rati
     return pos, vel, mass, typ
 
 
+# the present-day orbit point of the sample workunits' dwarf: (l, b, r) in deg, deg, kpc and
+# the velocity the Lua set-up gives Vector.create
+SAMPLE_ORBIT = ((218.0, 53.5, 28.6), (-156.0, 79.0, 107.0))
+
+
+def sampled_dwarf(nbody, seed, device=0, mass_l=12.0, rscale_l=0.2, light_r_ratio=0.2,
+                  light_mass_ratio=0.2, position=None, velocity=None):
+    """The sample workunit's two-component Plummer dwarf (half baryons) sampled on the GPU by
+    the library's port of the reference's sampler (nbGenerateDwarfCUDA: nbGenerateMixedDwarfCore,
+    nbody/src/nbody_mixeddwarf.c:765-1026, with a counter-based stream per body), recentred and
+    placed on the orbit point (by default SAMPLE_ORBIT, no reverse orbit).  The same seed gives
+    the same bodies bit for bit on every run.  Returns host arrays pos (n,3), vel (n,3),
+    mass (n,) and type (n,): +1 for the baryons (the first nbody // 2), -1 for dark matter."""
+    from .nbody import NBodyState, plummer_dwarf_struct
+    import ctypes
+    if position is None:
+        position = lbr_to_cartesian(*SAMPLE_ORBIT[0])
+    if velocity is None:
+        velocity = np.asarray(SAMPLE_ORBIT[1], dtype=np.float64)
+    d = plummer_dwarf_struct(nbody, seed, None, mass_l, rscale_l, light_r_ratio,
+                             light_mass_ratio, position, velocity)
+    with NBodyState(nbody, device) as st:
+        st.check("nbGenerateDwarf", st.lib.nbGenerateDwarfCUDA(st._h, ctypes.byref(d), 4.0))
+        pos, vel = st.bodies()
+        mass = st.masses()
+    nb = int(d.nbodyBaryon)
+    typ = np.concatenate([np.ones(nb, np.int32), -np.ones(nbody - nb, np.int32)])
+    return pos, vel, mass, typ
+
+
 def dwarf_config(nbody, theta=1.0, criterion="TreeCode", useQuad=True, mass_l=12.0,
                  rscale_l=0.2, light_r_ratio=0.2, light_mass_ratio=0.2):
     """Context settings of the two-component sample workunit at nbody bodies: dt from the
@@ -160,7 +208,8 @@ def reverse_orbits(potential, pos, vel, tstops, dt, device=0):
     """nbReverseOrbit (nbody/src/nbody_orbit_integrator.c:44-86) of many orbit centres at once:
     leapfrog backwards for each tstop with nsteps = floor(tstop / dt) + 1 steps of
     tstop / nsteps, the potential evaluated on the GPU (nbExtAccelerationNoAllocCUDA: one small
-    call per step, no allocation)."""
+    call per step, no allocation; more than 65,536 orbit centres are evaluated in chunks of
+    65,536 per step)."""
     from .nbody import ext_acceleration
     pos = np.array(pos, dtype=np.float64).reshape(-1, 3)
     vel = -np.array(vel, dtype=np.float64).reshape(-1, 3)

@@ -400,6 +400,10 @@ class NBodyState:
         self.check("nbSetTimeOrigin", self.lib.nbSetTimeOriginCUDA(self._h,
                                                                   float(previous_forward_time)))
 
+    def set_step(self, step):
+        """The step counter of a state resumed from a checkpoint (nbSetStepCUDA)."""
+        self.check("nbSetStep", self.lib.nbSetStepCUDA(self._h, int(step)))
+
     # -- marshalling (nbMarshalBodies) --
     def set_bodies(self, pos, vel, mass, treeRSize=4.0):
         pos = np.ascontiguousarray(pos, dtype=np.float64)
@@ -763,16 +767,28 @@ class NBodyBatch:
         return "nbBatch%sCUDA" % name
 
 
+NO_ALLOC_MAX_POINTS = 65536       # the static staging area of nbExtAccelerationNoAllocCUDA
+
+
 def ext_acceleration(potential, pos, device=0, no_alloc=False):
     """nbExtAcceleration (nbody/src/nbody_potential.c:627) at many positions, on the GPU.
-    no_alloc: through nbExtAccelerationNoAllocCUDA (at most 65,536 positions, no device
-    allocation per call: the form for loops of small calls such as orbit integration)."""
+    no_alloc: through nbExtAccelerationNoAllocCUDA (no device allocation per call: the form
+    for loops of small calls such as orbit integration); that entry point takes at most
+    NO_ALLOC_MAX_POINTS (65,536) positions per call, so more positions are evaluated in
+    consecutive chunks of that size."""
     lib = _lib.load()
     pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
     acc = np.empty_like(pos)
-    fn = lib.nbExtAccelerationNoAllocCUDA if no_alloc else lib.nbExtAccelerationCUDA
-    rc = fn(ctypes.byref(potential), _lib.ptr(pos), _lib.ptr(acc), len(pos), device)
-    NBodyState.check("nbExtAcceleration", rc)
+    if not no_alloc:
+        rc = lib.nbExtAccelerationCUDA(ctypes.byref(potential), _lib.ptr(pos), _lib.ptr(acc),
+                                       len(pos), device)
+        NBodyState.check("nbExtAcceleration", rc)
+        return acc
+    for lo in range(0, len(pos), NO_ALLOC_MAX_POINTS):
+        p, a = pos[lo:lo + NO_ALLOC_MAX_POINTS], acc[lo:lo + NO_ALLOC_MAX_POINTS]
+        rc = lib.nbExtAccelerationNoAllocCUDA(ctypes.byref(potential), _lib.ptr(p), _lib.ptr(a),
+                                              len(p), device)
+        NBodyState.check("nbExtAccelerationNoAlloc", rc)
     return acc
 
 

@@ -17,6 +17,9 @@ REF_LIB = os.path.join(HERE, "_ref", "libnbref.so")
 REF_EXE = os.path.join(HERE, "_ref", "milkyway_nbody")
 
 _dp = ctypes.POINTER(ctypes.c_double)
+# the reference's Body record (nbody/include/nbody_types.h:103-125), 96 bytes
+BODY_DTYPE = np.dtype([("pos", "f8", 4), ("next", "u8"), ("mass", "f8"), ("type", "i2"),
+                       ("pad", "i2"), ("id", "u4"), ("pad2", "u8"), ("vel", "f8", 4)])
 _vp = ctypes.c_void_p
 _ip = ctypes.POINTER(ctypes.c_int)
 
@@ -101,6 +104,12 @@ def ref():
             "nbref_ext_accel": (None, [_vp, _vp, _vp, ctypes.c_int]),
             "nbref_sample_step": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _dp, _dp]),
             "nbref_threads": (ctypes.c_int, []),
+            "nbref_handle_set_hist": (None, [_vp, ctypes.c_char_p]),
+            "nbref_state_bodytab": (_vp, [_vp]),
+            "nbref_state_set_progress": (None, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+            "nbref_state_progress": (None, [_vp, _ip, _dp, _ip]),
+            "nbref_write_checkpoint": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_char_p]),
+            "nbref_read_checkpoint": (_vp, [ctypes.c_char_p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -332,6 +341,35 @@ class RefState:
         v = np.ascontiguousarray(velocity, dtype=np.float64).reshape(3)
         sh = np.ascontiguousarray(shift, dtype=np.float64).reshape(-1, 3)
         self.lib.nbref_handle_set_lmc(self.h, _p(p), _p(v), _p(sh), len(sh))
+
+    def set_histogram_file(self, path):
+        """The data histogram the next likelihood() compares with."""
+        self.lib.nbref_handle_set_hist(self.h, path.encode() if path else None)
+
+    def bodytab(self):
+        """The state's Body[] as a numpy record view (96-byte records, the reference's layout):
+        pos, next, mass, type, id, vel."""
+        n = self.nbody
+        buf = (ctypes.c_char * (96 * n)).from_address(self.lib.nbref_state_bodytab(self.h))
+        return np.frombuffer(buf, dtype=BODY_DTYPE, count=n)
+
+    def set_progress(self, step, rsize, tree_incest=0):
+        self.lib.nbref_state_set_progress(self.h, int(step), float(rsize), int(tree_incest))
+
+    def progress(self):
+        """(step, tree root size, treeIncest) of the state."""
+        stp, rs, inc = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+        self.lib.nbref_state_progress(self.h, ctypes.byref(stp), ctypes.byref(rs), ctypes.byref(inc))
+        return stp.value, rs.value, inc.value
+
+    def write_checkpoint(self, path, tmp):
+        rc = self.lib.nbref_write_checkpoint(self.h, path.encode(), tmp.encode())
+        if rc:
+            raise RuntimeError("nbWriteCheckpoint failed: %d" % rc)
+
+    @classmethod
+    def read_checkpoint(cls, path):
+        return cls(ref().nbref_read_checkpoint(path.encode()))
 
     def likelihood(self):
         out = np.zeros(10)

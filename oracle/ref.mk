@@ -10,11 +10,16 @@
 #
 #   make -f oracle/ref.mk REF=/path/to/reference        (run from the repo root)
 #
+# Without REF, the reference checkout is looked for beside this repository (../reference
+# relative to the repository root); a variable MILKYWAY_REFERENCE_SRC in the environment
+# overrides that.
+#
 # Products:
 #   oracle/_ref/milkyway_nbody   the reference executable (golden likelihood runs)
 #   oracle/_ref/libnbref.so      the reference objects + ref_shim.c (ctypes entry points)
 
-REF     ?= /root/reference
+REPO    := $(abspath $(dir $(lastword $(MAKEFILE_LIST)))..)
+REF     ?= $(or $(MILKYWAY_REFERENCE_SRC),$(abspath $(REPO)/../reference))
 OUT     := oracle/_ref
 OBJ     := $(OUT)/obj
 GEN     := $(OUT)/include

@@ -10,7 +10,7 @@
  *   nbCreateHistogram / nbReadHistogram / nbSystemLikelihood (nbody/src/nbody.c:217-397).
  * The mapping between the reference's NBodyCtx and the flat NBodyCudaCtx of
  * include/nbody_b200.h below is the same code a maintainer adds to the reference to call
- * the CUDA library (INTEGRATION.md).
+ * the CUDA library.
  */
 #include "nbody_priv.h"
 #include "nbody.h"
@@ -21,6 +21,7 @@
 #include "nbody_histogram.h"
 #include "nbody_likelihood.h"
 #include "nbody_orbit_integrator.h"
+#include "nbody_checkpoint.h"
 #include "nbody_defaults.h"
 #include "milkyway_util.h"
 #include <crlibm.h>
@@ -538,6 +539,69 @@ int nbref_likelihood(void* hv, double* out)
     free(histogram);
     free(data);
     return 0;
+}
+
+/* Points the handle's likelihood at another data histogram file (nbf.histogramFileName,
+ * which nbReportResults reads when the run ends). */
+void nbref_handle_set_hist(void* hv, const char* histFile)
+{
+    RefHandle* h = (RefHandle*) hv;
+    if (h->fromLua) free(h->nbf.histogramFileName);
+    h->nbf.histogramFileName = histFile ? strdup(histFile) : NULL;
+    h->fromLua = 1;
+}
+
+/* ---- checkpoints (nbWriteCheckpoint / nbReadCheckpoint, nbody/src/nbody_checkpoint.c:597-672) */
+
+/* The state's Body[] (NBCUDA_BODY_STRIDE-byte records): the host table a GPU state marshals
+ * into and out of (nbMarshalBodiesCUDA). */
+void* nbref_state_bodytab(void* hv) { return ((RefHandle*) hv)->st.bodytab; }
+
+/* The step counter, root size and incest flag the checkpoint header records
+ * (nbPrepareWriteCheckpointHeader), as a GPU state reports them. */
+void nbref_state_set_progress(void* hv, int step, double rsize, int treeIncest)
+{
+    RefHandle* h = (RefHandle*) hv;
+    h->st.step = (unsigned int) step;
+    h->st.tree.rsize = rsize;
+    h->st.treeIncest = treeIncest;
+}
+
+void nbref_state_progress(void* hv, int* step, double* rsize, int* treeIncest)
+{
+    RefHandle* h = (RefHandle*) hv;
+    *step = (int) h->st.step;
+    *rsize = h->st.tree.rsize;
+    *treeIncest = h->st.treeIncest;
+}
+
+/* Writes the handle's context and state to checkpointFile through the temporary tmpFile, as
+ * nbWriteCheckpoint does at a checkpoint of the run loop.  Returns nonzero on failure. */
+int nbref_write_checkpoint(void* hv, const char* checkpointFile, const char* tmpFile)
+{
+    RefHandle* h = (RefHandle*) hv;
+    free(h->st.checkpointResolved);
+    h->st.checkpointResolved = NULL;
+    if (nbResolveCheckpoint(&h->st, checkpointFile)) return -1;
+    return nbWriteCheckpointWithTmpFile(&h->ctx, &h->st, tmpFile);
+}
+
+/* A new handle with the context and state read back from checkpointFile (nbReadCheckpoint),
+ * or NULL. */
+void* nbref_read_checkpoint(const char* checkpointFile)
+{
+    static const NBodyState emptyState = EMPTY_NBODYSTATE;
+    static const NBodyCtx emptyCtx = EMPTY_NBODYCTX;
+    RefHandle* h = (RefHandle*) calloc(1, sizeof(RefHandle));
+    h->ctx = emptyCtx;
+    h->st = emptyState;
+    if (nbResolveCheckpoint(&h->st, checkpointFile) || nbReadCheckpoint(&h->ctx, &h->st)) {
+        free(h->st.checkpointResolved);
+        free(h);
+        return NULL;
+    }
+    h->ctx.quietErrors = TRUE;
+    return h;
 }
 
 /* ---- math pins ---- */

@@ -39,7 +39,11 @@ def parse_results(text, model):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    # the reference checkout: the first argument, MILKYWAY_REFERENCE_SRC, or `reference` beside
+    # this repository
+    repo = os.path.dirname(os.path.dirname(HERE))
+    ref = (sys.argv[1] if len(sys.argv) > 1 else
+           os.environ.get("MILKYWAY_REFERENCE_SRC") or os.path.join(os.path.dirname(repo), "reference"))
     tests = os.path.join(ref, "nbody", "tests")
     text = open(os.path.join(tests, "RunTestUnits.lua")).read()
     golden = {

@@ -39,6 +39,24 @@ def test_no_alloc_matches_allocating_entry_point_twice():
         assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
 
 
+def test_no_alloc_leaves_device_memory_unchanged():
+    """The property the entry point exists for: repeated calls take no device memory (the
+    device's free memory, as cudaMemGetInfo reports it, is the same before and after)."""
+    import torch
+    from milkywayathome_client_b200 import _lib, nbody
+    lib = _lib.load()
+    pot = nbody.milky_way_potential()
+    pos = np.random.default_rng(7).normal(scale=15.0, size=(4096, 3))
+    assert _call(lib.nbExtAccelerationNoAllocCUDA, pot, pos)[0] == 0      # set-up call
+    torch.cuda.synchronize(0)
+    free0, _ = torch.cuda.mem_get_info(0)
+    for _ in range(200):
+        assert _call(lib.nbExtAccelerationNoAllocCUDA, pot, pos)[0] == 0
+    torch.cuda.synchronize(0)
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
+
+
 def test_no_alloc_rejects_more_points_than_the_array_holds():
     from milkywayathome_client_b200 import _lib, nbody
     lib = _lib.load()
