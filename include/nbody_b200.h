@@ -269,6 +269,10 @@ typedef struct {                       /* a data histogram as nbReadHistogram re
     int nRange;
     int reserved2;
     const double* emdRange;
+    /* bin centres in beta (nBins entries; needed when betaBins > 1, may be NULL otherwise):
+     * with more than one beta bin each range's EMD is the reference's transportation-simplex
+     * emdCalc over (lambda, beta) with the L2 ground distance */
+    const double* beta;
 } NBodyCudaDataHistogram;
 /* ---- nbRunSystem: the run loop with the best-likelihood scan and the bar's calibration ----
  * The forward evolution of nbody/src/nbody.c:420-520 around nbRunSystemPlain
@@ -543,6 +547,14 @@ NBodyCudaStatus nbExtAccelerationCUDA(const NBodyCudaPotential* pot, const doubl
  * Same results as nbExtAccelerationCUDA. */
 NBodyCudaStatus nbExtAccelerationNoAllocCUDA(const NBodyCudaPotential* pot, const double* pos,
                                              double* acc, int n, int device);
+
+/* emdCalc (nbody/src/nbody_emd.c:1207-1268) on the GPU: the earth mover's distance between two
+ * signatures of (weight, lambda, beta) triples (n1 and n2 of them, host arrays) with the L2
+ * ground distance, by the reference's transportation simplex (the same decisions, so the same
+ * value bit for bit); NaN where the reference returns EMD_INVALID.  The likelihood runs the
+ * same solver on the device for two-dimensional histograms (betaBins > 1). */
+NBodyCudaStatus nbEmdCalcCUDA(const double* sig1, int n1, const double* sig2, int n2,
+                              double* emd, int device);
 
 /* Number of this library's kernel launches issued since load (a launch counter for
  * benchmarks). */

@@ -7,7 +7,7 @@ sm_100a, C ABI in include/nbody_b200.h).  `nbody` mirrors the reference's step i
 formulas and a synthetic dwarf sampler.
 """
 from .nbody import (Disk, Dwarf, Halo, NBodyBatch, NBodyCtx, NBodyError, NBodyState, Potential,
-                    Spherical, ext_acceleration, kernel_launches, milky_way_potential,
+                    Spherical, emd, ext_acceleration, kernel_launches, milky_way_potential,
                     mixed_dwarf_particle_masses, mixed_dwarf_struct)
 from ._lib import status_is_fatal, status_names
 from .histogram import (DataHistogram, HistogramParams, data_from_counts, read_histogram,
@@ -15,6 +15,6 @@ from .histogram import (DataHistogram, HistogramParams, data_from_counts, read_h
 
 __all__ = ["Disk", "Dwarf", "Halo", "NBodyBatch", "NBodyCtx", "NBodyError", "NBodyState", "Potential",
            "Spherical",
-           "ext_acceleration", "kernel_launches", "milky_way_potential", "status_is_fatal",
+           "emd", "ext_acceleration", "kernel_launches", "milky_way_potential", "status_is_fatal",
            "status_names", "DataHistogram", "HistogramParams", "data_from_counts", "write_histogram",
            "read_histogram", "mixed_dwarf_struct", "mixed_dwarf_particle_masses"]

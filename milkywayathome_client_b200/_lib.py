@@ -143,7 +143,8 @@ class DataHist(ctypes.Structure):
                 ("compVariable", ctypes.POINTER(ctypes.c_double) * HIST_COMPONENTS),
                 ("compErr", ctypes.POINTER(ctypes.c_double) * HIST_COMPONENTS),
                 ("nRange", ctypes.c_int), ("reserved2", ctypes.c_int),
-                ("emdRange", ctypes.POINTER(ctypes.c_double))]
+                ("emdRange", ctypes.POINTER(ctypes.c_double)),
+                ("beta", ctypes.POINTER(ctypes.c_double))]
 
 
 class RunParams(ctypes.Structure):
@@ -252,6 +253,7 @@ SIGNATURES = [
     ("nbStepAdjointCUDA", ctypes.c_int, [ctypes.POINTER(Ctx), _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("nbTreeInfoCUDA", ctypes.c_int, [_vp, ctypes.POINTER(TreeInfo)]),
     ("nbGetTreeCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("nbEmdCalcCUDA", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int]),
     ("nbExtAccelerationCUDA", ctypes.c_int,
      [ctypes.POINTER(Potential), _vp, _vp, ctypes.c_int, ctypes.c_int]),
     ("nbExtAccelerationNoAllocCUDA", ctypes.c_int,

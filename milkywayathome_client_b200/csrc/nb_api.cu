@@ -55,6 +55,9 @@ static NBodyCudaStatus nb_cuda_fail(cudaError_t e, const char* what)
         if (e_ != cudaSuccess) return nb_cuda_fail(e_, #call);                \
     } while (0)
 
+// 256-byte rounding of the pieces carved from one device allocation
+static size_t nb_al(size_t x) { return (x + 255) & ~(size_t) 255; }
+
 // ---- small kernels: SoA <-> interleaved / AoS Body ----
 __global__ void k_split_xyz(const double* __restrict__ in, double* __restrict__ x,
                             double* __restrict__ y, double* __restrict__ z, int n)
@@ -82,16 +85,16 @@ __global__ void k_from_bodies(const unsigned char* __restrict__ aos, double* px,
         vz[i] = b[NBCUDA_BODY_VEL_OFFSET / 8 + 2];
     }
 }
-__global__ void k_to_bodies(unsigned char* __restrict__ aos, const double* px, const double* py,
+// positions and velocities, six doubles per body (x y z vx vy vz), for the copy-out of
+// nbMarshalBodiesCUDA, which writes them into the caller's Body records on the host
+__global__ void k_to_posvel(double* __restrict__ out, const double* px, const double* py,
                             const double* pz, const double* vx, const double* vy,
                             const double* vz, int n)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double* b = reinterpret_cast<double*>(aos + (size_t) i * NBCUDA_BODY_STRIDE);
+        double* b = out + 6 * (size_t) i;
         b[0] = px[i]; b[1] = py[i]; b[2] = pz[i];
-        b[NBCUDA_BODY_VEL_OFFSET / 8] = vx[i];
-        b[NBCUDA_BODY_VEL_OFFSET / 8 + 1] = vy[i];
-        b[NBCUDA_BODY_VEL_OFFSET / 8 + 2] = vz[i];
+        b[3] = vx[i]; b[4] = vy[i]; b[5] = vz[i];
     }
 }
 // advanceVelocities alone, for a step whose force evaluation failed (the reference still
@@ -598,10 +601,22 @@ NBodyCudaStatus nbMarshalBodiesCUDA(NBodyCudaState* st, void* bodytab, int nbody
             nb_count_launch();
         }
     } else if (nbody) {
-        k_to_bodies<<<nb_blocks(st, nbody), 256, 0, s>>>(st->aos, b.px, b.py, b.pz, b.vx, b.vy, b.vz,
-                                                          nbody);
+        // only pos and vel of the caller's records change (mass, type, id and the rest of each
+        // record are the caller's): stage them compactly, then scatter on the host
+        k_to_posvel<<<nb_blocks(st, nbody), 256, 0, s>>>((double*) st->aos, b.px, b.py, b.pz,
+                                                          b.vx, b.vy, b.vz, nbody);
         nb_count_launch();
-        NB_CHECK(cudaMemcpyAsync(bodytab, st->aos, bytes, cudaMemcpyDeviceToHost, s));
+        std::vector<double> pv(6 * (size_t) nbody);
+        NB_CHECK(cudaMemcpyAsync(pv.data(), st->aos, pv.size() * sizeof(double),
+                                 cudaMemcpyDeviceToHost, s));
+        NB_CHECK(cudaGetLastError());
+        NB_CHECK(cudaStreamSynchronize(s));
+        unsigned char* rec = (unsigned char*) bodytab;
+        for (size_t i = 0; i < (size_t) nbody; ++i) {
+            memcpy(rec + i * NBCUDA_BODY_STRIDE + NBCUDA_BODY_POS_OFFSET, &pv[6 * i], 3 * sizeof(double));
+            memcpy(rec + i * NBCUDA_BODY_STRIDE + NBCUDA_BODY_VEL_OFFSET, &pv[6 * i + 3], 3 * sizeof(double));
+        }
+        return NBODY_SUCCESS;
     }
     NB_CHECK(cudaGetLastError());
     NB_CHECK(cudaStreamSynchronize(s));
@@ -850,6 +865,33 @@ NBodyCudaStatus nbExtAccelerationCUDA(const NBodyCudaPotential* pot, const doubl
     cudaFree(dp);
     cudaFree(da);
     if (e != cudaSuccess) return nb_cuda_fail(e, "nbExtAccelerationCUDA");
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbEmdCalcCUDA(const double* sig1, int n1, const double* sig2, int n2,
+                              double* emd, int device)
+{
+    if (!emd || n1 < 0 || n2 < 0 || (n1 && !sig1) || (n2 && !sig2)) return NBODY_USER_ERROR;
+    NB_CHECK(cudaSetDevice(device));
+    const int nb = std::max(std::max(n1, n2), 1);
+    const size_t sigBytes = nb_al(24 * (size_t) nb);
+    const size_t bytes = 2 * sigBytes + nb_al(nb_emd_problem_bytes(nb)) + nb_al(8);
+    char* buf = nullptr;
+    NB_CHECK(cudaMalloc((void**) &buf, bytes));
+    double* d1 = (double*) buf;
+    double* d2 = (double*) (buf + sigBytes);
+    double* dOut = (double*) (buf + 2 * sigBytes);
+    char* work = buf + 2 * sigBytes + nb_al(8);
+    cudaError_t e = cudaSuccess;
+    if (n1) e = cudaMemcpy(d1, sig1, 24 * (size_t) n1, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n2) e = cudaMemcpy(d2, sig2, 24 * (size_t) n2, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        nb_launch_emd_direct(d1, n1, d2, n2, work, dOut, 0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(emd, dOut, sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+    if (e != cudaSuccess) return nb_cuda_fail(e, "nbEmdCalcCUDA");
     return NBODY_SUCCESS;
 }
 
@@ -1207,7 +1249,6 @@ static NbHistDev nb_hist_dev(const NBodyCudaHistogramParams* hp)
     return h;
 }
 
-static size_t nb_al(size_t x) { return (x + 255) & ~(size_t) 255; }
 
 static NbLikeFlags nb_like_flags(const NBodyCudaHistogramParams* hp)
 {
@@ -1251,9 +1292,9 @@ static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int
             g_lastError = "data histogram: invalid EMD ranges";
             return NBODY_USER_ERROR;
         }
-        if (hp->betaBins != 1) {
-            g_lastError = "the likelihood is implemented for one beta bin";
-            return NBODY_UNSUPPORTED;
+        if (hp->betaBins > 1 && !data->beta) {
+            g_lastError = "a two-dimensional data histogram needs its beta bin centres";
+            return NBODY_USER_ERROR;
         }
         if ((f.betaDisp && (!data->compVariable[0] || !data->compErr[0])) ||
             (f.velDisp && (!data->compVariable[1] || !data->compErr[1]))) {
@@ -1330,13 +1371,19 @@ static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int
                         nb_al(8 * Dz * NB_HIST_COMPONENTS * 2 * Bz) + nb_al(4 * Bz) +
                         (3 + 2 * NB_HIST_COMPONENTS) * nb_al(8 * Bz) +
                         nb_al(8 * (size_t) (data && data->nRange > 0 ? data->nRange : 0)) + 256;
+    // two-dimensional histograms: one emdCalc problem per dwarf and lambda range
+    const size_t emdProblems = data && hp->betaBins > 1
+        ? Dz * (size_t) (data->nRange > 0 ? data->nRange / 2 : 1) : 0;
+    const size_t emdBytes = emdProblems ? nb_al(nb_emd_problem_bytes(B)) : 0;
+    const size_t needAll = need + (emdProblems ? nb_al(8 * Bz) + nb_al(8 * emdProblems) +
+                                                   emdProblems * emdBytes : 0);
     NB_CHECK(cudaSetDevice(st->device));
-    if (st->histScratchBytes < need) {
+    if (st->histScratchBytes < needAll) {
         cudaFree(st->histScratch);
         st->histScratch = nullptr;
         st->histScratchBytes = 0;
-        NB_CHECK(cudaMalloc((void**) &st->histScratch, need));
-        st->histScratchBytes = need;
+        NB_CHECK(cudaMalloc((void**) &st->histScratch, needAll));
+        st->histScratchBytes = needAll;
     }
     char* cur = st->histScratch;
     auto carve = [&cur](size_t bytes) { char* q = cur; cur += nb_al(bytes); return q; };
@@ -1395,6 +1442,16 @@ static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int
             double* dst = (double*) carve(8 * (size_t) data->nRange);
             cudaMemcpyAsync(dst, data->emdRange, 8 * (size_t) data->nRange, cudaMemcpyHostToDevice, s);
             dh.emdRange = dst;
+        }
+        dh.beta = nullptr;
+        dh.emd2d = nullptr;
+        dh.emdWork = nullptr;
+        dh.emdWorkBytes = 0;
+        if (emdProblems) {
+            dh.beta = up(data->beta);
+            dh.emd2d = (double*) carve(8 * emdProblems);
+            dh.emdWork = carve(emdProblems * emdBytes);
+            dh.emdWorkBytes = emdBytes;
         }
         NB_CHECK(cudaGetLastError());
     }

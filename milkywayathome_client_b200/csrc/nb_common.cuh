@@ -204,7 +204,18 @@ struct NbDataHistDev {
     int betaDispBins;
     int nRange;                     // EMD lambda ranges (0: one over every bin)
     const double* emdRange;
+    const double* beta;             // bin centres in beta (two-dimensional histograms)
+    double* emd2d;                  // betaBins > 1: emdCalc of every (dwarf, range) problem
+    char* emdWork;                  //   and the workspace of each problem,
+    size_t emdWorkBytes;            //   emdWorkBytes apart
 };
+// emdCalc problems of the two-dimensional likelihood: one per dwarf and lambda range.
+int nb_emd_ranges(const NbDataHistDev& dh);
+size_t nb_emd_problem_bytes(int nBins);
+void nb_launch_emd_ranges(const NbHistPlan& p, const NbDataHistDev& dh, cudaStream_t s);
+// emdCalc of two host-given signatures on the device (work: nb_emd_problem_bytes(max(n1, n2))).
+void nb_launch_emd_direct(const double* sig1, int n1, const double* sig2, int n2, char* work,
+                          double* out, cudaStream_t s);
 // Which comparison terms nbSystemLikelihood adds (the reference's st->use* flags).
 struct NbLikeFlags {
     int betaDisp, velDisp, betaComp, vlos, dist, propMot;

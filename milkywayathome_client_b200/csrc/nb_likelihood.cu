@@ -19,6 +19,7 @@
 // and averages equal the reference's bit for bit.  Counts are integers and exact.
 #include "nb_common.cuh"
 #include "nb_crmath.cuh"
+#include "nb_emd.cuh"
 
 #include <math.h>
 
@@ -374,11 +375,144 @@ __device__ double nb_compare(const NbHistPlan& p, const NbDataHistDev& dh, int c
     return nsig / 2.0;
 }
 
-// nbSystemLikelihood (nbody/src/nbody_likelihood.c:155-324), one thread per dwarf, for one
-// beta bin and the default EMD range (the whole histogram): the EMD between two weight sets
-// on the lambda axis with the L2 ground distance of the reference's emdCalc is the 1-D
-// transport cost sum_k |F_sim(k) - F_data(k)| (lambda_{k+1} - lambda_k) over the used bins
-// (nbMatchEMD, nbody/src/nbody_emd.c:1278-1427); nbCostComponent (nbody_mass.c:318-391);
+// ---- the two-dimensional EMD (betaBins > 1): nb_emd.cuh run by one block per problem ----
+constexpr int EMD_THREADS = 256;
+
+// The block as an EMD team: first minimum in (value, index) order and maximum over its
+// threads, by warp shuffles and one shared slot per warp.
+struct NbEmdBlock {
+    NbEmdMin* partM;            // shared, one per warp
+    double* partD;
+    NbEmdMin* resM;             // shared result
+    double* resD;
+    __device__ int rank() const { return (int) threadIdx.x; }
+    __device__ int size() const { return (int) blockDim.x; }
+    __device__ void sync() const { __syncthreads(); }
+    __device__ NbEmdMin argmin(NbEmdMin a) const
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int o = 16; o > 0; o >>= 1) {
+            NbEmdMin b;
+            b.val = __shfl_xor_sync(NB_FULL_MASK, a.val, o);
+            b.idx = __shfl_xor_sync(NB_FULL_MASK, a.idx, o);
+            if (nb_emd_before(b, a)) a = b;
+        }
+        if (lane == 0) partM[warp] = a;
+        __syncthreads();
+        if (warp == 0) {
+            a = lane < (int) (blockDim.x >> 5) ? partM[lane] : NbEmdMin{NB_EMD_INF, -1};
+            for (int o = 16; o > 0; o >>= 1) {
+                NbEmdMin b;
+                b.val = __shfl_xor_sync(NB_FULL_MASK, a.val, o);
+                b.idx = __shfl_xor_sync(NB_FULL_MASK, a.idx, o);
+                if (nb_emd_before(b, a)) a = b;
+            }
+            if (lane == 0) *resM = a;
+        }
+        __syncthreads();
+        return *resM;
+    }
+    __device__ double maxv(double a) const
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(NB_FULL_MASK, a, o));
+        if (lane == 0) partD[warp] = a;
+        __syncthreads();
+        if (warp == 0) {
+            a = lane < (int) (blockDim.x >> 5) ? partD[lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(NB_FULL_MASK, a, o));
+            if (lane == 0) *resD = a;
+        }
+        __syncthreads();
+        return *resD;
+    }
+};
+
+#define NB_EMD_BLOCK_SHARED                                                                  \
+    __shared__ NbEmdScalars sc;                                                              \
+    __shared__ NbEmdMin partM[EMD_THREADS / 32], resM;                                       \
+    __shared__ double partD[EMD_THREADS / 32], resD;                                         \
+    const NbEmdBlock team{partM, partD, &resM, &resD}
+
+__global__ void __launch_bounds__(EMD_THREADS)
+k_emd_direct(const double* __restrict__ sig1, int n1, const double* __restrict__ sig2, int n2,
+             char* __restrict__ work, double* __restrict__ out)
+{
+    NB_EMD_BLOCK_SHARED;
+    const NbEmdWork w = nb_emd_carve(work, n1, n2);
+    const double e = nb_emd_calc(team, sig1, n1, sig2, n2, w, sc);
+    if (threadIdx.x == 0) *out = e;
+}
+
+// nbMatchEMD's emdCalc calls (nbody/src/nbody_emd.c:1332-1402) for two-dimensional histograms,
+// one block per (dwarf, lambda range): the data side -- the used bins whose data-file lambda
+// lies in the range, weight variable n / (the range's rounded counts), at the file's centres
+// -- and the simulated side -- the used bins whose own centre lies in the range, weight
+// (count / n_sim) n_sim / (its rounded counts), at the centres (i + 1/2) size + start --
+// as the reference builds them; the reference passes the data side's bin count for both
+// sides, and so does this (simulated bins beyond their own count weigh nothing).
+__global__ void __launch_bounds__(EMD_THREADS)
+k_emd_ranges(NbHistPlan p, NbDataHistDev dh)
+{
+    NB_EMD_BLOCK_SHARED;
+    __shared__ int nData;
+    const int nProb = dh.nRange > 0 ? dh.nRange / 2 : 1;
+    const int d = blockIdx.x / nProb, r = blockIdx.x % nProb;
+    const int nb = dh.nBins;
+    char* base = dh.emdWork + (size_t) blockIdx.x * dh.emdWorkBytes;
+    double* sigData = (double*) base;
+    double* sigSim = (double*) (base + nb_emd_align(8 * 3 * (size_t) nb));
+    char* work = base + 2 * nb_emd_align(8 * 3 * (size_t) nb);
+    const unsigned* c = p.counts + (size_t) d * nb;
+    const unsigned nSimU = p.inRange[d];
+    const unsigned nDataU = dh.totalNum;
+    if (threadIdx.x == 0) {
+        const bool every = dh.nRange == 0;
+        const double lo = every ? 0.0 : dh.emdRange[2 * r];
+        const double hi = every ? 0.0 : dh.emdRange[2 * r + 1];
+        unsigned simRange = 0, dataRange = 0;
+        for (int j = 0; j < nb; ++j) {
+            if (!dh.useBin[j]) continue;
+            const double simL = ((double) (j / p.h.betaBins) + 0.5) * p.h.lambdaSize + p.h.lambdaStart;
+            if (every || (simL >= lo && simL <= hi))
+                simRange += (unsigned) round(((double) c[j] / (double) nSimU) * (double) nSimU);
+            if (every || (dh.lambda[j] >= lo && dh.lambda[j] <= hi))
+                dataRange += (unsigned) round(dh.variable[j] * (double) nDataU);
+        }
+        int ns = 0, ndat = 0;
+        for (int j = 0; j < nb; ++j) {
+            if (!dh.useBin[j]) continue;
+            const double simL = ((double) (j / p.h.betaBins) + 0.5) * p.h.lambdaSize + p.h.lambdaStart;
+            if (every || (simL >= lo && simL <= hi)) {
+                const double var = (double) c[j] / (double) nSimU;
+                sigSim[3 * ns] = var * (double) nSimU / (1.0 * simRange);
+                sigSim[3 * ns + 1] = simL;
+                sigSim[3 * ns + 2] = ((double) (j % p.h.betaBins) + 0.5) * p.h.betaSize + p.h.betaStart;
+                ++ns;
+            }
+            if (every || (dh.lambda[j] >= lo && dh.lambda[j] <= hi)) {
+                sigData[3 * ndat] = dh.variable[j] * (double) nDataU / (1.0 * dataRange);
+                sigData[3 * ndat + 1] = dh.lambda[j];
+                sigData[3 * ndat + 2] = dh.beta[j];
+                ++ndat;
+            }
+        }
+        for (int k = ns; k < ndat; ++k) sigSim[3 * k] = sigSim[3 * k + 1] = sigSim[3 * k + 2] = 0.0;
+        nData = ndat;
+    }
+    __syncthreads();
+    const int n = nData;
+    const NbEmdWork w = nb_emd_carve(work, n, n);
+    const double e = nb_emd_calc(team, sigData, n, sigSim, n, w, sc);
+    if (threadIdx.x == 0) dh.emd2d[blockIdx.x] = e;
+}
+
+// nbSystemLikelihood (nbody/src/nbody_likelihood.c:155-324), one thread per dwarf.  The EMD
+// per lambda range (nbMatchEMD, nbody/src/nbody_emd.c:1278-1427): with one beta bin the two
+// weight sets lie on the lambda axis and the reference's emdCalc with the L2 ground distance
+// is the 1-D transport cost sum_k |F_sim(k) - F_data(k)| (lambda_{k+1} - lambda_k) over the
+// used bins; with more beta bins each range's emdCalc comes from k_emd_ranges (the
+// transportation simplex of nb_emd.cuh); nbCostComponent (nbody_mass.c:318-391);
 // then the enabled comparisons in the reference's order.
 // out[NB_LIKELIHOOD_TERMS d ..]: likelihood, EMD component, cost component, beta dispersion,
 // velocity dispersion, beta average, line-of-sight velocity, distance, dec and RA proper
@@ -441,14 +575,19 @@ __global__ void k_likelihood(NbHistPlan p, const double* __restrict__ mass,
             }
             double Fs = 0.0, Fd = 0.0, cost = 0.0, prevL = 0.0;
             bool first = true;
-            for (int j = 0; j < nb; ++j) {
-                if (!dh.useBin[j] || !(every || (dh.lambda[j] >= lo && dh.lambda[j] <= hi))) continue;
-                if (!first) cost += fabs(Fs - Fd) * (dh.lambda[j] - prevL);
-                const double var = (double) c[j] / (double) nSimU;
-                Fs += var * (double) nSimU / (1.0 * simRange);
-                Fd += dh.variable[j] * (double) nData / (1.0 * dataRange);
-                prevL = dh.lambda[j];
-                first = false;
+            if (p.h.betaBins > 1) {
+                // the range's emdCalc, solved by k_emd_ranges
+                cost = dh.emd2d[(size_t) d * (nR / 2) + r / 2];
+            } else {
+                for (int j = 0; j < nb; ++j) {
+                    if (!dh.useBin[j] || !(every || (dh.lambda[j] >= lo && dh.lambda[j] <= hi))) continue;
+                    if (!first) cost += fabs(Fs - Fd) * (dh.lambda[j] - prevL);
+                    const double var = (double) c[j] / (double) nSimU;
+                    Fs += var * (double) nSimU / (1.0 * simRange);
+                    Fd += dh.variable[j] * (double) nData / (1.0 * dataRange);
+                    prevL = dh.lambda[j];
+                    first = false;
+                }
             }
             totalRange += dataRange;
             emdSum += cost * ((double) dataRange / (1.0 * nData));
@@ -658,9 +797,30 @@ int nb_launch_hist_plan(const NbHistPlan& p, const double* px, const double* py,
     return launches;
 }
 
+int nb_emd_ranges(const NbDataHistDev& dh) { return dh.nRange > 0 ? dh.nRange / 2 : 1; }
+
+size_t nb_emd_problem_bytes(int nBins)
+{
+    return 2 * nb_emd_align(8 * 3 * (size_t) nBins) + nb_emd_work_bytes(nBins, nBins);
+}
+
+void nb_launch_emd_ranges(const NbHistPlan& p, const NbDataHistDev& dh, cudaStream_t s)
+{
+    k_emd_ranges<<<p.D * nb_emd_ranges(dh), EMD_THREADS, 0, s>>>(p, dh);
+    nb_count_launch();
+}
+
+void nb_launch_emd_direct(const double* sig1, int n1, const double* sig2, int n2, char* work,
+                          double* out, cudaStream_t s)
+{
+    k_emd_direct<<<1, EMD_THREADS, 0, s>>>(sig1, n1, sig2, n2, work, out);
+    nb_count_launch();
+}
+
 void nb_launch_likelihood(const NbHistPlan& p, const double* mass, const int* nbodyOf,
                           const NbDataHistDev& dh, NbLikeFlags f, double* out, cudaStream_t s)
 {
+    if (p.h.betaBins > 1) nb_launch_emd_ranges(p, dh, s);
     k_likelihood<<<(p.D + 127) / 128, 128, 0, s>>>(p, mass, nbodyOf, dh, f, out);
     nb_count_launch();
 }

@@ -122,15 +122,17 @@ class DataHistogram:
         dp = ctypes.POINTER(ctypes.c_double)
         use = np.ascontiguousarray(self.useBin, dtype=np.int32)
         lam = np.ascontiguousarray(self.lambda_, dtype=np.float64)
+        beta = np.ascontiguousarray(self.beta, dtype=np.float64)
         var = np.ascontiguousarray(self.variable, dtype=np.float64)
         err = np.ascontiguousarray(self.err, dtype=np.float64)
-        keep = [use, lam, var, err]
+        keep = [use, lam, beta, var, err]
         d = _lib.DataHist()
         d.nBins = len(var)
         d.totalNum = int(self.totalNum)
         d.massPerParticle = float(self.massPerParticle)
         d.useBin = use.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         d.lambda_ = lam.ctypes.data_as(dp)
+        d.beta = beta.ctypes.data_as(dp)
         d.variable = var.ctypes.data_as(dp)
         d.err = err.ctypes.data_as(dp)
         d.betaDispBins = int(self.betaDispBins)

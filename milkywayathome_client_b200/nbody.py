@@ -792,6 +792,19 @@ def ext_acceleration(potential, pos, device=0, no_alloc=False):
     return acc
 
 
+def emd(sig1, sig2, device=0):
+    """emdCalc (nbody/src/nbody_emd.c:1207-1268) of two signatures, (n, 3) arrays of (weight,
+    lambda, beta) rows, on the GPU (nbEmdCalcCUDA): the reference's transportation simplex with
+    the L2 ground distance; NaN where the reference's is invalid."""
+    lib = _lib.load()
+    a = np.ascontiguousarray(sig1, dtype=np.float64).reshape(-1, 3)
+    b = np.ascontiguousarray(sig2, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros(1)
+    NBodyState.check("nbEmdCalc", lib.nbEmdCalcCUDA(_lib.ptr(a), len(a), _lib.ptr(b), len(b),
+                                                    _lib.ptr(out), device))
+    return float(out[0])
+
+
 def peak_fma_tflops(fp64=True, device=0):
     """Measured DFMA (fp64) or FFMA throughput of the device, TFLOP/s."""
     out = ctypes.c_double()

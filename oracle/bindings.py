@@ -110,6 +110,7 @@ def ref():
             "nbref_state_progress": (None, [_vp, _ip, _dp, _ip]),
             "nbref_write_checkpoint": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_char_p]),
             "nbref_read_checkpoint": (_vp, [ctypes.c_char_p]),
+            "nbref_emd_calc": (ctypes.c_double, [_vp, ctypes.c_uint, _vp, ctypes.c_uint]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -377,6 +378,13 @@ class RefState:
         if rc:
             raise RuntimeError("nbref_likelihood failed: %d" % rc)
         return out
+
+
+def ref_emd(sig1, sig2):
+    """The reference's emdCalc of two (n, 3) signatures of (weight, lambda, beta) rows."""
+    a = np.ascontiguousarray(sig1, dtype=np.float64).reshape(-1, 3)
+    b = np.ascontiguousarray(sig2, dtype=np.float64).reshape(-1, 3)
+    return ref().nbref_emd_calc(_p(a), len(a), _p(b), len(b))
 
 
 def ref_ext_accel(potential, pos):

@@ -22,6 +22,7 @@
 #include "nbody_likelihood.h"
 #include "nbody_orbit_integrator.h"
 #include "nbody_checkpoint.h"
+#include "nbody_emd.h"
 #include "nbody_defaults.h"
 #include "milkyway_util.h"
 #include <crlibm.h>
@@ -602,6 +603,13 @@ void* nbref_read_checkpoint(const char* checkpointFile)
     }
     h->ctx.quietErrors = TRUE;
     return h;
+}
+
+/* The reference's EMD (emdCalc, nbody/src/nbody_emd.c:1207-1268) between two signatures of
+ * (weight, lambda, beta) triples, as nbMatchEMD calls it (no lower bound). */
+double nbref_emd_calc(const double* sig1, unsigned int n1, const double* sig2, unsigned int n2)
+{
+    return emdCalc(sig1, sig2, n1, n2, NULL);
 }
 
 /* ---- math pins ---- */

@@ -8,7 +8,8 @@
 --   orbit and the context fields that differ between the models.
 --   options (optional): "allterms" turns on every comparison of the likelihood (velocity
 --   dispersion, line-of-sight velocity, beta average, distance, proper motions); "bestlike"
---   turns on the best-likelihood scan over the last 5% of the steps.
+--   turns on the best-likelihood scan over the last 5% of the steps; "betaN" (N a number)
+--   gives the histogram N beta bins instead of one (a two-dimensional histogram).
 -- The seed comes from the command line (argSeed), as in the reference tests.
 
 arg = {...}
@@ -19,6 +20,7 @@ local variantName = arg[2] or "5"
 local options = arg[3] or ""
 local allTerms = string.find(options, "allterms") ~= nil
 local bestLike = string.find(options, "bestlike") ~= nil
+local betaBins = tonumber(string.match(options, "beta(%d+)") or "1")
 
 assert(seed ~= nil, "seed argument missing")
 assert(nbody ~= nil, "body count argument missing")
@@ -217,6 +219,6 @@ function makeHistogram()
       lambdaBins  = 34,
       betaStart = -15,
       betaEnd   = 15,
-      betaBins  = 1
+      betaBins  = betaBins
    }
 end

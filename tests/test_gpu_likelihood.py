@@ -172,3 +172,73 @@ def test_batch_likelihood_matches_single_states():
         assert np.array_equal(totals[k], t1[0])
         assert mpp[k] == m1[0]
         assert np.array_equal(out[k], lk, equal_nan=True)
+
+
+# ---- two-dimensional histograms (betaBins > 1): the EMD by the transportation simplex ----
+def _orphan_params_2d(beta_bins, **flags):
+    from milkywayathome_client_b200 import HistogramParams
+    return HistogramParams(phi=128.79, theta=54.39, psi=90.70, lambdaStart=-50.0, lambdaEnd=50.0,
+                           lambdaBins=34, betaStart=-15.0, betaEnd=15.0, betaBins=beta_bins,
+                           sunGCDist=8.0, **flags)
+
+
+def _random_data_2d(params, seed, fill=0.6):
+    """A data histogram over the two-dimensional grid: seeded counts in a fraction of the bins,
+    a few bins unused."""
+    from milkywayathome_client_b200 import data_from_counts
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(1, 40, params.nbins) * (rng.uniform(size=params.nbins) < fill)
+    data = data_from_counts(params, counts, int(counts.sum()) * 3, 2.5e-3)
+    data.useBin[rng.choice(params.nbins, size=3, replace=False)] = 0
+    return data
+
+
+@pytest.mark.parametrize("beta_bins,ranges", [(2, None), (3, None), (5, None),
+                                              (4, "{-40,-10.3,10.3,40}")])
+def test_two_dimensional_likelihood_matches_reference(tmp_path, beta_bins, ranges):
+    """betaBins > 1: each lambda range's EMD is the reference's transportation-simplex emdCalc
+    over (lambda, beta) (nbMatchEMD, nbody/src/nbody_emd.c:1278-1427), solved on the GPU by the
+    same decisions; every likelihood term agrees with the reference's nbSystemLikelihood."""
+    from oracle import bindings as ob
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    from milkywayathome_client_b200 import read_histogram, write_histogram
+    params = _orphan_params_2d(beta_bins)
+    data = _random_data_2d(params, 100 + beta_bins)
+    path = str(tmp_path / "hist2d")
+    write_histogram(path, params, data)
+    if ranges:
+        text = open(path).read()
+        open(path, "w").write(text.replace("betaBins = %d\n" % beta_bins,
+                                           "betaBins = %d\nEMDRange = %s\n" % (beta_bins, ranges)))
+    r, st, _ = _run_case("5", "1024", "886885833", ["beta%d" % beta_bins], hist=path)
+    counts, _, _ = st.histogram(params)
+    assert np.count_nonzero(counts[0]) > 10            # a stream over many (lambda, beta) bins
+    ref = r.likelihood()
+    got = st.likelihood(params, read_histogram(path))[0]
+    st.close()
+    assert np.isfinite(ref[1]) and ref[1] > 0.0
+    _assert_terms(got, ref)
+
+
+def test_emd_on_the_gpu_matches_reference_emdcalc():
+    """nbEmdCalcCUDA (the device solver, one block per problem) against the reference's emdCalc
+    on grid signatures with ties, zero weights and unequal totals: bit for bit."""
+    from oracle import bindings as ob
+    if not ob.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    from milkywayathome_client_b200 import emd
+    rng = np.random.default_rng(77)
+    for k in range(40):
+        lb, bb = int(rng.integers(4, 30)), int(rng.integers(2, 6))
+        li = np.repeat(np.arange(lb), bb)
+        bi = np.tile(np.arange(bb), lb)
+        sig = []
+        for _ in range(2):
+            c = rng.integers(1, 50, lb * bb) * (rng.uniform(size=lb * bb) < 0.5)
+            w = c / max(c.sum(), 1)
+            sig.append(np.stack([w, (li + 0.5) * (300.0 / lb) - 150.0, (bi + 0.5) * (30.0 / bb) - 15.0], 1))
+        if k % 5 == 0:
+            sig[1][:, 0] *= 1.3                          # unequal totals: the dummy node
+        want, got = ob.ref_emd(sig[0], sig[1]), emd(sig[0], sig[1])
+        assert np.float64(got).view(np.uint64) == np.float64(want).view(np.uint64), (k, got, want)
