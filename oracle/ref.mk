@@ -17,6 +17,13 @@
 # Products:
 #   oracle/_ref/milkyway_nbody   the reference executable (golden likelihood runs)
 #   oracle/_ref/libnbref.so      the reference objects + ref_shim.c (ctypes entry points)
+#   oracle/_ref/milkyway_nbody_cuda
+#                                the reference executable with the B200 binding compiled in:
+#                                milkywayathome_client_b200/reference_binding/nbody_cuda.c and
+#                                the reference's nbody.c, nbody_plain.c and nbody_types.c with
+#                                its dispatches added (oracle/apply_cuda_binding.py), linked
+#                                against milkywayathome_client_b200/libnbody_b200.so; it steps
+#                                on the GPU when NBODY_CUDA_DEVICE names one, else on the CPU
 
 REPO    := $(abspath $(dir $(lastword $(MAKEFILE_LIST)))..)
 REF     ?= $(or $(MILKYWAY_REFERENCE_SRC),$(abspath $(REPO)/../reference))
@@ -79,6 +86,12 @@ OBJS := $(addprefix $(OBJ)/crlibm/,$(CRLIBM_SRC:.c=.o)) \
 
 all: $(OUT)/milkyway_nbody $(OUT)/libnbref.so
 
+LIBDIR   := milkywayathome_client_b200
+BIND     := $(LIBDIR)/reference_binding
+CUDA_SRC := $(OUT)/cuda_src
+PATCHED  := nbody.c nbody_plain.c nbody_types.c
+CUDA_OBJS := $(addprefix $(OBJ)/cuda/,$(PATCHED:.c=.o)) $(OBJ)/cuda/nbody_cuda.o
+
 $(GEN)/.stamp: oracle/configure_ref.py
 	python3 oracle/configure_ref.py $(REF) $(GEN)
 	touch $@
@@ -123,7 +136,7 @@ $(OBJ)/nbody/%.o: $(REF)/nbody/src/%.c $(GEN)/.stamp
 
 $(OBJ)/local/%.o: oracle/%.c oracle/ref.mk $(GEN)/.stamp
 	@mkdir -p $(dir $@)
-	$(CC) $(CFLAGS) -I$(REF)/nbody/src -c $< -o $@
+	$(CC) $(CFLAGS) -Iinclude -I$(REF)/nbody/src -c $< -o $@
 
 $(OUT)/milkyway_nbody: $(OBJ)/nbody/main.o $(OBJS)
 	$(CXX) -fopenmp -o $@ $^ -lm -lrt -lpthread -ldl
@@ -133,4 +146,28 @@ $(OUT)/milkyway_nbody: $(OBJ)/nbody/main.o $(OBJS)
 $(OUT)/libnbref.so: $(OBJ)/local/ref_shim.o $(filter-out $(OBJ)/nbody/nbody_grav.o,$(OBJS))
 	$(CXX) -shared -fopenmp -o $@ $^ -lm -lrt -lpthread -ldl
 
-.PHONY: all
+# the reference executable with the B200 binding (needs libnbody_b200.so built first)
+cuda: $(OUT)/milkyway_nbody_cuda
+
+$(CUDA_SRC)/.stamp: oracle/apply_cuda_binding.py $(addprefix $(REF)/nbody/src/,$(PATCHED))
+	python3 oracle/apply_cuda_binding.py $(REF) $(CUDA_SRC)
+	touch $@
+
+$(CUDA_SRC)/%.c: $(CUDA_SRC)/.stamp ;
+
+$(OBJ)/cuda/%.o: $(CUDA_SRC)/%.c $(BIND)/nbody_cuda.h $(GEN)/.stamp
+	@mkdir -p $(dir $@)
+	$(CC) $(CFLAGS) -I$(BIND) -I$(REF)/nbody/src -c $< -o $@
+
+$(OBJ)/cuda/nbody_cuda.o: $(BIND)/nbody_cuda.c $(BIND)/nbody_cuda.h $(BIND)/nbody_cuda_ctx.h \
+                          include/nbody_b200.h $(GEN)/.stamp
+	@mkdir -p $(dir $@)
+	$(CC) $(CFLAGS) -Iinclude -I$(BIND) -c $< -o $@
+
+$(OUT)/milkyway_nbody_cuda: $(OBJ)/nbody/main.o $(CUDA_OBJS) \
+                            $(filter-out $(addprefix $(OBJ)/nbody/,$(PATCHED:.c=.o)),$(OBJS)) \
+                            $(LIBDIR)/libnbody_b200.so
+	$(CXX) -fopenmp -o $@ $(filter %.o,$^) -L$(LIBDIR) -lnbody_b200 \
+	    -Wl,-rpath,'$$ORIGIN/../../$(LIBDIR)' -lm -lrt -lpthread -ldl
+
+.PHONY: all cuda

@@ -8,9 +8,8 @@
  *   nbMakeTree (nbody/src/nbody_tree.c:429), nbExtAcceleration
  *   (nbody/src/nbody_potential.c:627), nbSetup (nbody/src/nbody_lua.c:612),
  *   nbCreateHistogram / nbReadHistogram / nbSystemLikelihood (nbody/src/nbody.c:217-397).
- * The mapping between the reference's NBodyCtx and the flat NBodyCudaCtx of
- * include/nbody_b200.h below is the same code a maintainer adds to the reference to call
- * the CUDA library.
+ * The mapping from the reference's NBodyCtx to the flat NBodyCudaCtx of include/nbody_b200.h
+ * is the binding's own (milkywayathome_client_b200/reference_binding/nbody_cuda_ctx.h).
  */
 #include "nbody_priv.h"
 #include "nbody.h"
@@ -31,6 +30,7 @@
 #include <string.h>
 
 #include "../include/nbody_b200.h"
+#include "../milkywayathome_client_b200/reference_binding/nbody_cuda_ctx.h"
 
 /* The reference's force walk itself (nbGravity and nbMapForceBody are file-static in
  * nbody/src/nbody_grav.c): compiled here from that source so that a bounded sample of the
@@ -107,53 +107,8 @@ void nbref_ctx_from_flat(NBodyCtx* ctx, const NBodyCudaCtx* c)
     ctx->coulomb_log = c->coulombLog;
 }
 
-void nbref_ctx_to_flat(NBodyCudaCtx* c, const NBodyCtx* ctx)
-{
-    memset(c, 0, sizeof *c);
-    c->eps2 = ctx->eps2;
-    c->theta = ctx->theta;
-    c->timestep = ctx->timestep;
-    c->treeRSize = ctx->treeRSize;
-    c->criterion = (int) ctx->criterion;
-    c->useQuad = ctx->useQuad;
-    c->allowIncest = ctx->allowIncest;
-    c->potentialType = (int) ctx->potentialType;
-    c->precision = NBCUDA_PRECISION_FP64;
-    c->pot.sphere.type = ctx->pot.sphere[0].type;
-    c->pot.sphere.mass = ctx->pot.sphere[0].mass;
-    c->pot.sphere.scale = ctx->pot.sphere[0].scale;
-    c->pot.disk.type = ctx->pot.disk.type;
-    c->pot.disk.mass = ctx->pot.disk.mass;
-    c->pot.disk.scaleLength = ctx->pot.disk.scaleLength;
-    c->pot.disk.scaleHeight = ctx->pot.disk.scaleHeight;
-    c->pot.disk.patternSpeed = ctx->pot.disk.patternSpeed;
-    c->pot.disk.startAngle = ctx->pot.disk.startAngle;
-    c->pot.disk2.type = ctx->pot.disk2.type;
-    c->pot.disk2.mass = ctx->pot.disk2.mass;
-    c->pot.disk2.scaleLength = ctx->pot.disk2.scaleLength;
-    c->pot.disk2.scaleHeight = ctx->pot.disk2.scaleHeight;
-    c->pot.disk2.patternSpeed = ctx->pot.disk2.patternSpeed;
-    c->pot.disk2.startAngle = ctx->pot.disk2.startAngle;
-    c->pot.halo.type = ctx->pot.halo.type;
-    c->pot.halo.vhalo = ctx->pot.halo.vhalo;
-    c->pot.halo.scaleLength = ctx->pot.halo.scaleLength;
-    c->pot.halo.flattenZ = ctx->pot.halo.flattenZ;
-    c->pot.halo.flattenY = ctx->pot.halo.flattenY;
-    c->pot.halo.flattenX = ctx->pot.halo.flattenX;
-    c->pot.halo.triaxAngle = ctx->pot.halo.triaxAngle;
-    c->pot.halo.c1 = ctx->pot.halo.c1;
-    c->pot.halo.c2 = ctx->pot.halo.c2;
-    c->pot.halo.c3 = ctx->pot.halo.c3;
-    c->pot.halo.mass = ctx->pot.halo.mass;
-    c->pot.halo.gamma = ctx->pot.halo.gamma;
-    c->pot.halo.lambda = ctx->pot.halo.lambda;
-    c->pot.halo.rho0 = ctx->pot.halo.rho0;
-    c->lmc = (int) ctx->LMC;
-    c->lmcDynaFric = (int) ctx->LMCDynaFric;
-    c->lmcMass = ctx->LMCmass;
-    c->lmcScale = ctx->LMCscale;
-    c->coulombLog = ctx->coulomb_log;
-}
+/* the binding's own mapping (milkywayathome_client_b200/reference_binding/nbody_cuda_ctx.h) */
+void nbref_ctx_to_flat(NBodyCudaCtx* c, const NBodyCtx* ctx) { nbCudaCtxFromNBodyCtx(c, ctx); }
 
 /* ---- states built from arrays ---- */
 void* nbref_state_new(const NBodyCudaCtx* c, const double* pos, const double* vel,
