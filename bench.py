@@ -90,7 +90,7 @@ def parse_args():
                     help="steps of the energy-drift run of both forms (0: skip)")
     ap.add_argument("--theta2", type=float, default=1.0,
                     help="second opening angle measured for both forms (0: skip)")
-    ap.add_argument("--profile", choices=["fp64", "mixed", "adjoint", "batch"],
+    ap.add_argument("--profile", choices=["fp64", "mixed", "adjoint", "batch", "config0"],
                     help="profiling entry: build the dwarf, run two force evaluations, exit")
     return ap.parse_args()
 
@@ -806,6 +806,18 @@ def run_profile(args):
             bt.check("nbBatchRunSteps", bt.run_steps(ctx, 2, graph=False))
             print(json.dumps({"profile": "batch", "dwarfs": len(spec), "bodies": bt.nbody,
                               "step_ms": bt.step_time_ms()}))
+        return 0
+    if args.profile == "config0":
+        # the 20,000-body configuration: a few whole steps (launch lists of the small case)
+        from milkywayathome_client_b200.nbody import NBodyState
+        pos, vel, mass, _ = bench_input(20000, SEED_CONFIG0)
+        ctx, _ = bench_ctx(20000, 1.0)
+        with NBodyState.create(ctx, pos, vel, mass) as st:
+            ms = []
+            for _ in range(5):
+                st.check("nbStepSystem", st.step(ctx))
+                ms.append(st.step_time_ms())
+            print(json.dumps({"profile": "config0", "n": 20000, "step_ms": ms}))
         return 0
     if args.profile == "adjoint":
         import torch

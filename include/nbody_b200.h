@@ -341,6 +341,14 @@ NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTi
  * orbiting bar's time and the LMC's reflex accelerations are read at it). */
 NBodyCudaStatus nbSetStepCUDA(NBodyCudaState* st, int step);
 
+/* Whether nbStepSystemCUDA / nbRunStepsCUDA replay a step as one captured CUDA graph (enable
+ * != 0, the default): a step's ~60 kernels are captured once per context, node capacity and
+ * tuning and then launched as one graph, which removes the launch gaps that dominate small
+ * systems (tens of thousands of bodies); the kernels, their order and so the results are the
+ * same either way.  Steps with an orbiting bar or an LMC (whose per-step values are kernel
+ * arguments) and counted evaluations are always launched directly. */
+NBodyCudaStatus nbSetStepGraphCUDA(NBodyCudaState* st, int enable);
+
 /* Mixed-precision walk tuning of a single state (as nbBatchSetTuningCUDA): bodies per walk
  * group (1..64), interaction-list entries per warp (32, 64, 128), walk blocks per SM (0: max). */
 NBodyCudaStatus nbSetMixedTuningCUDA(NBodyCudaState* st, int groupMax, int listCap, int blocksPerSM);

@@ -220,6 +220,7 @@ SIGNATURES = [
     ("nbSetTypesCUDA", ctypes.c_int, [_vp, _vp]),
     ("nbSetTimeOriginCUDA", ctypes.c_int, [_vp, ctypes.c_double]),
     ("nbSetStepCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nbSetStepGraphCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbSetMixedTuningCUDA", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("nbBatchSetTimeOriginCUDA", ctypes.c_int, [_vp, ctypes.c_double]),
     ("nbGenerateDwarfCUDA", ctypes.c_int, [_vp, ctypes.POINTER(PlummerDwarf), ctypes.c_double]),

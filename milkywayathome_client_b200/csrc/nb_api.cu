@@ -167,6 +167,16 @@ struct NBodyCudaState {
     std::vector<double> lmcShift;       // shiftByLMC: 3 doubles per step
     NbSlot runStart;                    // nbRunSystemCUDA: the initial state of the runs
     NbBestDev* best = nullptr;          // nbRunSystemCUDA: device best-likelihood record
+    // the step replayed as one captured CUDA graph (nb_force, tree criteria without an orbiting
+    // bar or an LMC): the graph, what it was captured for, and the pinned per-evaluation
+    // scalars its first copy uploads
+    cudaGraphExec_t stepGraph = nullptr;
+    NBodyCudaCtx stepGraphCtx{};
+    int stepGraphDrift = -1, stepGraphKick = -1, stepGraphCap = -1;
+    int stepGraphMx[4] = {0, 0, 0, 0};
+    unsigned long long stepGraphLaunches = 0;
+    int useStepGraph = 1;
+    NbScalars* scInit = nullptr;
     double* keepPos = nullptr;          // bodies at the best likelihood (3n each)
     double* keepVel = nullptr;
     int haveKeep = 0;
@@ -180,8 +190,16 @@ static cudaError_t nb_alloc(T** p, size_t count)
     return cudaMalloc((void**) p, count * sizeof(T));
 }
 
+static void nb_drop_step_graph(NBodyCudaState* st)
+{
+    if (st->stepGraph) cudaGraphExecDestroy(st->stepGraph);
+    st->stepGraph = nullptr;
+    st->stepGraphCap = -1;
+}
+
 static void nb_free_nodes(NBodyCudaState* st)
 {
+    nb_drop_step_graph(st);             // its kernels hold the node arrays' addresses
     NbTreeBuffers& b = st->b;
     cudaFree(b.nodePM); cudaFree(b.nodeCrit); cudaFree(b.nodeLink); cudaFree(b.nodeQuad);
     cudaFree(b.nodeDepth); cudaFree(b.parent); cudaFree(b.nchild); cudaFree(b.arrive);
@@ -282,6 +300,7 @@ static void nb_free_all(NBodyCudaState* st)
     cudaFree(st->keepVel);
     st->keepPos = st->keepVel = nullptr;
     if (st->scHost) cudaFreeHost(st->scHost);
+    if (st->scInit) cudaFreeHost(st->scInit);
     if (st->ev0) cudaEventDestroy(st->ev0);
     if (st->ev1) cudaEventDestroy(st->ev1);
     if (st->evS) cudaEventDestroy(st->evS);
@@ -367,8 +386,11 @@ static int nb_blocks(NBodyCudaState* st, int n)
     return g < cap ? g : cap;
 }
 
-// One force evaluation; drift/kick select the fused halves of the leapfrog.
-static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int drift, int kick)
+// One force evaluation; drift/kick select the fused halves of the leapfrog.  allowGraph: the
+// evaluation may be replayed from a captured CUDA graph (the same kernels in the same order,
+// launched as one graph instead of ~60 launches; used for whole steps).
+static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int drift, int kick,
+                                bool allowGraph = false)
 {
     std::string why;
     NBodyCudaStatus rc = nb_check_ctx(ctx, why);
@@ -418,62 +440,105 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
                                ctx->lmcDynaFric, ctx->coulombLog, s);
     }
 
-    for (int attempt = 0; attempt < 4; ++attempt) {
-        // reset per-evaluation device scalars (keep rsize)
-        NbScalars init{};
-        init.rsize = st->rsize;
-        init.capNodes = st->capNodes;
-        NB_CHECK(cudaMemcpyAsync(b.sc, &init, sizeof init, cudaMemcpyHostToDevice, s));
-        NB_CHECK(cudaEventRecord(st->evS, s));
-        st->walkLaunches = 0;
+    if (mixed) {
+        if (!st->mx.stacks) {
+            // stacks for the largest persistent grid any list capacity allows
+            int mxb = 0;
+            for (int cap : {32, 64, 128})
+                for (int gm : {32, 64})
+                    mxb = std::max(mxb, nb_mixed_walk_blocks(st->numSMs, cap, gm));
+            NB_CHECK(nb_alloc(&st->mx.stacks, nb_mixed_stack_ints(mxb)));
+        }
+        const int fit = nb_mixed_walk_blocks(st->numSMs, st->mixListCap, st->mixGroupMax) / st->numSMs;
+        const int per = st->mixBlocksPerSM > 0 ? std::min(st->mixBlocksPerSM, fit) : fit;
+        st->mx.walkBlocks = std::max(1, per) * st->numSMs;
+        st->mx.groupMax = st->mixGroupMax;
+        st->mx.listCap = st->mixListCap;
+        st->mx.exact = st->mixExact;
+    }
+    // The device work of the evaluation, enqueued without host synchronisation: the scalars
+    // from the pinned st->scInit, the tree or the direct sum, the walk, the scalars back into
+    // st->scHost.  capturing: inside a stream capture (events become graph nodes).
+    auto enqueue = [&](bool capturing) {
+        auto rec = [&](cudaEvent_t ev) {
+            if (capturing) cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal);
+            else cudaEventRecord(ev, s);
+        };
+        cudaMemcpyAsync(b.sc, st->scInit, sizeof(NbScalars), cudaMemcpyHostToDevice, s);
+        rec(st->evS);
         if (ctx->criterion == NBCUDA_EXACT) {
             if (drift) {
                 // advancePosVel without the tree: reuse the bounding-box pass for the drift
                 nb_launch_drift_only(b, n, ctx->timestep, st->numSMs, s, shift0);
             }
-            NB_CHECK(cudaEventRecord(st->ev0, s));
+            rec(st->ev0);
             nb_launch_direct_fp64(b.px, b.py, b.pz, b.mass, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp,
                                   pot, b.sc, s);
-            NB_CHECK(cudaEventRecord(st->ev1, s));
-            st->walkLaunches = 1;
-            st->haveTree = 0;
+            rec(st->ev1);
         } else {
             nb_build_tree(b, n, ctx->criterion, ctx->theta, ctx->useQuad, drift, ctx->timestep,
                           st->numSMs, s, shift0);
             nb_link_and_moments(b, n, st->capNodes, ctx->criterion, ctx->theta, ctx->useQuad, s);
-            NB_CHECK(cudaEventRecord(st->ev0, s));
-            if (mixed) {
-                if (!st->mx.stacks) {
-                    // stacks for the largest persistent grid any list capacity allows
-                    int mxb = 0;
-                    for (int cap : {32, 64, 128})
-                        for (int gm : {32, 64})
-                            mxb = std::max(mxb, nb_mixed_walk_blocks(st->numSMs, cap, gm));
-                    NB_CHECK(nb_alloc(&st->mx.stacks, nb_mixed_stack_ints(mxb)));
-                }
-                {
-                    const int fit = nb_mixed_walk_blocks(st->numSMs, st->mixListCap,
-                                                         st->mixGroupMax) / st->numSMs;
-                    const int per = st->mixBlocksPerSM > 0 ? std::min(st->mixBlocksPerSM, fit) : fit;
-                    st->mx.walkBlocks = std::max(1, per) * st->numSMs;
-                    st->mx.groupMax = st->mixGroupMax;
-                    st->mx.listCap = st->mixListCap;
-                    st->mx.exact = st->mixExact;
-                }
+            rec(st->ev0);
+            if (mixed)
                 nb_launch_walk_mixed(b, st->mx, st->capNodes, wp, pot, st->counting != 0,
                                      st->numSMs, s);
-            }
             else
                 nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px,
                                     b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
-                                    st->counting != 0, s, b.walkRec, st->capNodes);
-            NB_CHECK(cudaEventRecord(st->ev1, s));
-            st->walkLaunches = 1;
-            st->haveTree = 1;
+                                    st->counting != 0, s, b.walkRec, b.bodyNode, st->capNodes);
+            rec(st->ev1);
         }
-        NB_CHECK(cudaEventRecord(st->evE, s));
+        rec(st->evE);
+        cudaMemcpyAsync(st->scHost, b.sc, sizeof(NbScalars), cudaMemcpyDeviceToHost, s);
+    };
+    // the orbiting bar's time and an LMC's reflex accelerations change every step and are
+    // kernel arguments: those evaluations are launched directly
+    const bool graphable = allowGraph && st->useStepGraph && ctx->criterion != NBCUDA_EXACT &&
+                           !lmc && !st->counting && ctx->pot.disk.type != NBCUDA_ORBITING_BAR &&
+                           ctx->pot.disk2.type != NBCUDA_ORBITING_BAR;
+
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        // reset per-evaluation device scalars (keep rsize)
+        *st->scInit = NbScalars{};
+        st->scInit->rsize = st->rsize;
+        st->scInit->capNodes = st->capNodes;
+        st->walkLaunches = 1;
+        if (graphable) {
+            const int mxKey[4] = {mixed ? st->mx.walkBlocks : 0, mixed ? st->mx.groupMax : 0,
+                                  mixed ? st->mx.listCap : 0, mixed ? st->mx.exact : 0};
+            const bool same = st->stepGraph && st->stepGraphDrift == drift &&
+                              st->stepGraphKick == kick && st->stepGraphCap == st->capNodes &&
+                              std::memcmp(st->stepGraphMx, mxKey, sizeof mxKey) == 0 &&
+                              std::memcmp(&st->stepGraphCtx, ctx, sizeof *ctx) == 0;
+            if (!same) {
+                nb_drop_step_graph(st);
+                const unsigned long long l0 = g_launches.load();
+                cudaGraph_t g = nullptr;
+                NB_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                enqueue(true);
+                cudaError_t e = cudaStreamEndCapture(s, &g);
+                if (e == cudaSuccess) e = cudaGraphInstantiate(&st->stepGraph, g, 0);
+                if (g) cudaGraphDestroy(g);
+                if (e != cudaSuccess) {
+                    st->stepGraph = nullptr;
+                    return nb_cuda_fail(e, "step graph capture");
+                }
+                st->stepGraphLaunches = g_launches.load() - l0;
+                st->stepGraphCtx = *ctx;
+                st->stepGraphDrift = drift;
+                st->stepGraphKick = kick;
+                st->stepGraphCap = st->capNodes;
+                std::memcpy(st->stepGraphMx, mxKey, sizeof mxKey);
+            } else {
+                nb_count_launch((int) st->stepGraphLaunches);
+            }
+            NB_CHECK(cudaGraphLaunch(st->stepGraph, s));
+        } else {
+            enqueue(false);
+        }
+        st->haveTree = ctx->criterion != NBCUDA_EXACT;
         NB_CHECK(cudaGetLastError());
-        NB_CHECK(cudaMemcpyAsync(st->scHost, b.sc, sizeof(NbScalars), cudaMemcpyDeviceToHost, s));
         NB_CHECK(cudaStreamSynchronize(s));
         NbScalars& h = *st->scHost;
         st->rsize = h.rsize;
@@ -540,6 +605,7 @@ NBodyCudaStatus nbInitCUDA(NBodyCudaState** out, int device, int nbody)
     if (e == cudaSuccess) e = cudaEventCreate(&st->evS);
     if (e == cudaSuccess) e = cudaEventCreate(&st->evE);
     if (e == cudaSuccess) e = cudaMallocHost((void**) &st->scHost, sizeof(NbScalars));
+    if (e == cudaSuccess) e = cudaMallocHost((void**) &st->scInit, sizeof(NbScalars));
     if (e == cudaSuccess) e = cudaMalloc((void**) &st->b.sc, sizeof(NbScalars));
     if (e != cudaSuccess) rc = nb_cuda_fail(e, "nbInitCUDA");
     if (!rc) rc = nb_alloc_bodies(st, nbody);
@@ -731,7 +797,7 @@ NBodyCudaStatus nbGravMapCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st)
 NBodyCudaStatus nbStepSystemCUDA(const NBodyCudaCtx* ctx, NBodyCudaState* st)
 {
     if (!st) return NBODY_USER_ERROR;
-    NBodyCudaStatus rc = nb_force(ctx, st, 1, 1);
+    NBodyCudaStatus rc = nb_force(ctx, st, 1, 1, true);
     if (!(rc & (NBODY_USER_ERROR | NBODY_UNSUPPORTED | NBODY_CUDA_ERROR))) st->step++;
     return rc;
 }
@@ -1697,6 +1763,14 @@ NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTi
     return NBODY_SUCCESS;
 }
 
+NBodyCudaStatus nbSetStepGraphCUDA(NBodyCudaState* st, int enable)
+{
+    if (!st) return NBODY_USER_ERROR;
+    st->useStepGraph = enable != 0;
+    if (!enable) nb_drop_step_graph(st);
+    return NBODY_SUCCESS;
+}
+
 NBodyCudaStatus nbSetStepCUDA(NBodyCudaState* st, int step)
 {
     if (!st || step < 0) return NBODY_USER_ERROR;
@@ -1960,7 +2034,7 @@ static int nb_batch_enqueue(NBodyCudaBatch* bt, const NBodyCudaCtx* ctx, int dri
     } else {
         nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px, b.py,
                             b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc, false, s,
-                            b.walkRec, st->capNodes, &f);
+                            b.walkRec, b.bodyNode, st->capNodes, &f);
         launches += 1;
     }
     cudaEventRecord(st->ev1, s);

@@ -400,6 +400,10 @@ class NBodyState:
         self.check("nbSetTimeOrigin", self.lib.nbSetTimeOriginCUDA(self._h,
                                                                   float(previous_forward_time)))
 
+    def set_step_graph(self, enable=True):
+        """Whole steps replayed as one captured CUDA graph (nbSetStepGraphCUDA; the default)."""
+        self.check("nbSetStepGraph", self.lib.nbSetStepGraphCUDA(self._h, int(bool(enable))))
+
     def set_step(self, step):
         """The step counter of a state resumed from a checkpoint (nbSetStepCUDA)."""
         self.check("nbSetStep", self.lib.nbSetStepCUDA(self._h, int(step)))

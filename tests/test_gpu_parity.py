@@ -330,3 +330,21 @@ def test_mixed_flags_test_particles_as_incest():
     ctx = make_ctx(len(mass), theta=0.6, allowIncest=True, precision="mixed")
     with _gpu_state(ctx, pos, vel, mass) as st:
         assert st.gravMap(ctx) == (1 << 24)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_step_graph_equals_direct_launches(dwarf_small, precision):
+    """Whole steps are replayed as one captured CUDA graph by default (nbSetStepGraphCUDA); the
+    same steps launched kernel by kernel give the same bodies and accelerations bit for bit."""
+    from milkywayathome_client_b200 import NBodyState
+    pos, vel, mass, _ = dwarf_small
+    ctx = make_ctx(len(mass), theta=0.7, precision=precision)
+    with NBodyState.create(ctx, pos, vel, mass) as a, NBodyState.create(ctx, pos, vel, mass) as b:
+        b.set_step_graph(False)
+        for k in range(8):
+            assert a.step(ctx) == 0 and b.step(ctx) == 0
+        assert a.run_steps(ctx, 5) == 0 and b.run_steps(ctx, 5) == 0
+        pa, va = a.bodies()
+        pb, vb = b.bodies()
+        assert bits_equal(pa, pb) and bits_equal(va, vb) and bits_equal(a.accels(), b.accels())
+        assert a.step_count == b.step_count == 13
