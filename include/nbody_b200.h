@@ -263,7 +263,10 @@ typedef struct {                       /* a data histogram as nbReadHistogram re
     const double* compErr[NBODY_CUDA_HIST_COMPONENTS];
     /* the lambda ranges of the EMD ("EMDRange = {start, end, ...}", the values as strtof
      * parses them, params.EMDRange of nbody/src/nbody_histogram.c:1547-1561): nRange values,
-     * pairs of inclusive bounds; nRange 0: one range over every bin (the file's default).  The
+     * pairs of inclusive bounds; nRange 0: the range nbReadHistogram gives a file without that
+     * line (nbody/src/nbody_histogram.c:1563-1567) -- every bin with one beta bin; with more
+     * beta bins the lambdas of bins 0 and lambdaBins - 1 in lambda-major order bound it, i.e.
+     * the first 1/betaBins of the lambda axis, as the reference compares.  The
      * EMD is taken per range over its used bins, each renormalised, weighted by the range's
      * share of the data counts (nbMatchEMD, nbody/src/nbody_emd.c:1332-1402). */
     int nRange;

@@ -1428,6 +1428,22 @@ static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int
     chunkFirst[D] = (int) chunks.size();
     if (first != n) { g_lastError = "dwarf sizes do not add up to the body count"; return NBODY_USER_ERROR; }
     p.nChunks = (int) chunks.size();
+    // A data file without an EMDRange line gets the range nbReadHistogram sets
+    // (nbody/src/nbody_histogram.c:1563-1567): data[0].lambda and data[lambdaBins - 1].lambda,
+    // each widened by half the lambda spacing of data[0] and data[1].  With one beta bin that is
+    // every bin (one range over all used bins, nRange 0 below).  With more beta bins data[1]
+    // shares data[0]'s lambda and data[lambdaBins - 1] is the (lambdaBins - 1)-th bin in
+    // lambda-major order, so the range is [first lambda, the lambda of that bin]: the first
+    // 1/betaBins of the lambda axis; the reference compares only that part, and so does this.
+    double defaultRange[2] = {0.0, 0.0};
+    const bool twoDimDefault = data && hp->betaBins > 1 && data->nRange == 0 && B >= 2;
+    if (twoDimDefault) {
+        const double half = (data->lambda[1] - data->lambda[0]) / 2;
+        defaultRange[0] = data->lambda[0] - half;
+        defaultRange[1] = data->lambda[hp->lambdaBins - 1] + half;
+    }
+    const int nRangeUsed = twoDimDefault ? 2 : (data ? data->nRange : 0);
+    const double* rangeUsed = twoDimDefault ? defaultRange : (data ? data->emdRange : nullptr);
     const size_t Dz = (size_t) D, Bz = (size_t) B, nz = (size_t) n, nq = (size_t) p.h.nq;
     const size_t QDB = std::max<size_t>(nq, 1) * Dz * Bz;
     const size_t need = nb_al(4 * Dz * Bz) + 4 * nb_al(4 * Dz) + nb_al(4 * nz) +
@@ -1436,10 +1452,10 @@ static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int
                         5 * nb_al(8 * QDB) + nb_al(4 * Dz) + nb_al(8 * NB_LIKELIHOOD_TERMS * Dz) +
                         nb_al(8 * Dz * NB_HIST_COMPONENTS * 2 * Bz) + nb_al(4 * Bz) +
                         (3 + 2 * NB_HIST_COMPONENTS) * nb_al(8 * Bz) +
-                        nb_al(8 * (size_t) (data && data->nRange > 0 ? data->nRange : 0)) + 256;
+                        nb_al(8 * (size_t) (data && nRangeUsed > 0 ? nRangeUsed : 0)) + 256;
     // two-dimensional histograms: one emdCalc problem per dwarf and lambda range
     const size_t emdProblems = data && hp->betaBins > 1
-        ? Dz * (size_t) (data->nRange > 0 ? data->nRange / 2 : 1) : 0;
+        ? Dz * (size_t) (nRangeUsed > 0 ? nRangeUsed / 2 : 1) : 0;
     const size_t emdBytes = emdProblems ? nb_al(nb_emd_problem_bytes(B)) : 0;
     const size_t needAll = need + (emdProblems ? nb_al(8 * Bz) + nb_al(8 * emdProblems) +
                                                    emdProblems * emdBytes : 0);
@@ -1502,11 +1518,12 @@ static NBodyCudaStatus nb_hist_prepare(NBodyCudaState* st, const std::vector<int
         dh.totalNum = data->totalNum;
         dh.nBins = B;
         dh.betaDispBins = data->betaDispBins;
-        dh.nRange = data->nRange;
+        dh.nRange = nRangeUsed;
         dh.emdRange = nullptr;
-        if (data->nRange > 0) {
-            double* dst = (double*) carve(8 * (size_t) data->nRange);
-            cudaMemcpyAsync(dst, data->emdRange, 8 * (size_t) data->nRange, cudaMemcpyHostToDevice, s);
+        if (nRangeUsed > 0) {
+            double* dst = (double*) carve(8 * (size_t) nRangeUsed);
+            // pageable source: the copy has read it when the call returns
+            cudaMemcpyAsync(dst, rangeUsed, 8 * (size_t) nRangeUsed, cudaMemcpyHostToDevice, s);
             dh.emdRange = dst;
         }
         dh.beta = nullptr;

@@ -111,6 +111,8 @@ def ref():
             "nbref_write_checkpoint": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_char_p]),
             "nbref_read_checkpoint": (_vp, [ctypes.c_char_p]),
             "nbref_emd_calc": (ctypes.c_double, [_vp, ctypes.c_uint, _vp, ctypes.c_uint]),
+            "nbref_histogram": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp,
+                                               ctypes.POINTER(ctypes.c_uint)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -371,6 +373,19 @@ class RefState:
     @classmethod
     def read_checkpoint(cls, path):
         return cls(ref().nbref_read_checkpoint(path.encode()))
+
+    def histogram(self):
+        """The reference's counts histogram of the state: dict of lambda, beta, variable,
+        rawCount (per bin) and totalNum."""
+        cap = 1 << 16
+        lam, beta, var = np.zeros(cap), np.zeros(cap), np.zeros(cap)
+        raw = np.zeros(cap, np.uint32)
+        tot = ctypes.c_uint()
+        n = self.lib.nbref_histogram(self.h, cap, _p(lam), _p(beta), _p(var), _p(raw), ctypes.byref(tot))
+        if n < 0:
+            raise RuntimeError("nbref_histogram failed: %d" % n)
+        return dict(lambda_=lam[:n], beta=beta[:n], variable=var[:n], rawCount=raw[:n],
+                    totalNum=tot.value)
 
     def likelihood(self):
         out = np.zeros(10)

@@ -567,6 +567,35 @@ double nbref_emd_calc(const double* sig1, unsigned int n1, const double* sig2, u
     return emdCalc(sig1, sig2, n1, n2, NULL);
 }
 
+/* The reference's own counts histogram of the state (nbCreateHistogram, histogram 0): per bin
+ * its lambda and beta centres, normalised count, raw count and useBin; returns the bin count
+ * (cap: the arrays' length) and the histogram's totalNum. */
+int nbref_histogram(void* hv, int cap, double* lambda, double* beta, double* variable,
+                    unsigned int* rawCount, unsigned int* totalNum)
+{
+    RefHandle* h = (RefHandle*) hv;
+    HistogramParams hp;
+    NBodyLikelihoodMethod method;
+    MainStruct* hist;
+    NBodyHistogram* h0;
+    int k, n;
+    if (nbGetLikelihoodInfo(&h->nbf, &hp, &method)) return -1;
+    hist = nbCreateHistogram(&h->ctx, &h->st, &hp);
+    if (!hist) return -2;
+    h0 = hist->histograms[0];
+    n = (int) (h0->lambdaBins * h0->betaBins);
+    for (k = 0; k < n && k < cap; ++k) {
+        lambda[k] = h0->data[k].lambda;
+        beta[k] = h0->data[k].beta;
+        variable[k] = h0->data[k].variable;
+        rawCount[k] = h0->data[k].rawCount;
+    }
+    *totalNum = h0->totalNum;
+    for (k = 0; k < 8; ++k) free(hist->histograms[k]);
+    free(hist);
+    return n;
+}
+
 /* ---- math pins ---- */
 double nbref_pow_rn(double x, double y) { return pow_rn(x, y); }
 double nbref_log_rn(double x) { return log_rn(x); }
