@@ -176,8 +176,7 @@ __device__ __forceinline__ double nb_warp_sum_transposed(double (&r)[V], int lan
 
 // Node adjoints: nodeBar[k*10 + 0..2] = CoM, [3] = mass, [4..9] = quadrupole.
 __global__ void __launch_bounds__(128, 5)
-k_walk_vjp(const double4* __restrict__ head, const double2* __restrict__ aux,
-           const double2* __restrict__ quad,
+k_walk_vjp(const double4* __restrict__ rec,
            const unsigned int* __restrict__ order, const double* __restrict__ px,
            const double* __restrict__ py, const double* __restrict__ pz,
            const double* __restrict__ abar, double* __restrict__ xbar,
@@ -199,9 +198,9 @@ k_walk_vjp(const double4* __restrict__ head, const double2* __restrict__ aux,
         const int q = __reduce_min_sync(NB_FULL_MASK, ptr);
         if (q >= end) break;
         const bool active = ptr == q;
-        // the FP64 walk's node data: {CoM, mass}, {rcrit2, links}, the cell's quadrupole
-        const double4 nd = head[q];
-        const double2 r1 = aux[q];
+        // the FP64 walk's packed record: {CoM, mass}, {rcrit2, links, Qxx, Qxy}, {Qxz .. Qzz}
+        const double4 nd = rec[3 * (size_t) q];
+        const double4 r1 = rec[3 * (size_t) q + 1];
         const long long word = __double_as_longlong(r1.y);
         const int2 link = make_int2((int) (unsigned) (word & 0xffffffffll), (int) (word >> 32));
         const bool isBody = link.y >= 0;
@@ -214,12 +213,9 @@ k_walk_vjp(const double4* __restrict__ head, const double2* __restrict__ aux,
                 ptr = link.x;
                 inter = !(isBody && (unsigned) link.y == j);
                 if (inter) {
-                    double2 q0 = make_double2(0.0, 0.0), q1 = q0, q2 = q0;
-                    if (useQuad && !isBody) {
-                        const double2* Q = quad + 3 * (size_t) (-link.y - 1);
-                        q0 = Q[0]; q1 = Q[1]; q2 = Q[2];
-                    }
-                    v = nb_interaction_vjp(dx, dy, dz, nd.w, q0.x, q0.y, q1.x, q1.y, q2.x, q2.y,
+                    double4 r2 = make_double4(0.0, 0.0, 0.0, 0.0);
+                    if (useQuad && !isBody) r2 = rec[3 * (size_t) q + 2];
+                    v = nb_interaction_vjp(dx, dy, dz, nd.w, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w,
                                            useQuad && !isBody, wp.eps2, abx, aby, abz);
                     gx -= v.rx; gy -= v.ry; gz -= v.rz;
                 }
@@ -390,11 +386,8 @@ void nb_launch_vjp(NbTreeBuffers& b, double* nodeBar, int capNodes, int maxDepth
     const int warps = (n + 31) / 32;
     cudaEventRecord(walkStart, s);
     // packed records from the (possibly restored) tree arrays
-    nb_launch_pack_walk(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.bodyNode, b.walkRec,
-                        capNodes, b.sc, s);
-    const NbWalkNodes wn = nb_walk_nodes(b.walkRec, capNodes);
-    k_walk_vjp<<<(warps * 32 + 127) / 128, 128, 0, s>>>(wn.head, wn.aux, wn.quad, b.sort.idxA,
-                                                        b.px, b.py, b.pz,
+    nb_launch_pack_walk(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.walkRec, capNodes, b.sc, s);
+    k_walk_vjp<<<(warps * 32 + 127) / 128, 128, 0, s>>>(b.walkRec, b.sort.idxA, b.px, b.py, b.pz,
                                                         abar, xbar, nodeBar, wp, pot, b.sc);
     cudaEventRecord(walkEnd, s);
     const int g = min((capNodes + 255) / 256, numSMs * 16);

@@ -486,7 +486,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
             else
                 nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px,
                                     b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
-                                    st->counting != 0, s, b.walkRec, b.bodyNode, st->capNodes);
+                                    st->counting != 0, s, b.walkRec, st->capNodes);
             rec(st->ev1);
         }
         rec(st->evE);
@@ -2051,7 +2051,7 @@ static int nb_batch_enqueue(NBodyCudaBatch* bt, const NBodyCudaCtx* ctx, int dri
     } else {
         nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px, b.py,
                             b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc, false, s,
-                            b.walkRec, b.bodyNode, st->capNodes, &f);
+                            b.walkRec, st->capNodes, &f);
         launches += 1;
     }
     cudaEventRecord(st->ev1, s);

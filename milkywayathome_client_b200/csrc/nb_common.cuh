@@ -272,7 +272,7 @@ struct NbTreeBuffers {
     double4* nodePM; double* nodeCrit; int2* nodeLink; double* nodeQuad;
     int *nodeDepth, *parent, *nchild, *arrive;
     int2* nodeRange;   // first and last sorted body of every node's subtree
-    double4* walkRec;  // 3 per node of room: the FP64 walks' node data (NbWalkNodes)
+    double4* walkRec;  // 3 per node: the FP64 walk's packed node records
     NbScalars* sc;
 };
 
@@ -292,31 +292,10 @@ struct NbMixedBuffers {
 int nb_mixed_walk_blocks(int numSMs, int listCap = 0, int groupMax = 32);
 size_t nb_mixed_stack_ints(int blocks);
 
-// The FP64 walks' node data, carved from an allocation of 3 double4 per node of capacity:
-//   head[q] = {CoM, mass} of every node (32 B);
-//   aux[q]  = {rcrit2, the links as one 64-bit word: Next(q) in the low half, in the high half
-//              the body's index for a body (>= 0) or -(its cell slot + 1) for a cell} (16 B);
-//   quad[3 c .. 3 c + 2] = {Qxx, Qxy}, {Qxz, Qyy}, {Qyz, Qzz} of cell slot c (48 B), where
-//              c = q - (bodies before q in walk order): cells only, densely numbered.
-// Bodies, two thirds of the nodes, take 48 bytes instead of a 96-byte record with empty
-// quadrupole slots, so the data a walk touches (~99 MB at N = 1M) is two thirds of what it was.
-struct NbWalkNodes {
-    double4* head;
-    double2* aux;
-    double2* quad;
-};
-__host__ __device__ inline NbWalkNodes nb_walk_nodes(double4* rec, int capNodes)
-{
-    NbWalkNodes w;
-    w.head = rec;
-    w.aux = reinterpret_cast<double2*>(rec + capNodes);
-    w.quad = w.aux + capNodes;
-    return w;
-}
-// Fills NbWalkNodes from the tree arrays (bodyNode: walk-order node of every sorted tree body).
+// The FP64 walks' packed node records (3 double4 per node) from the tree arrays.
 void nb_launch_pack_walk(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
-                         const double* nodeQuad, const int* bodyNode, double4* rec, int capNodes,
-                         const NbScalars* sc, cudaStream_t s);
+                         const double* nodeQuad, double4* rec, int capNodes, const NbScalars* sc,
+                         cudaStream_t s);
 
 // The walks (forest != nullptr: one tree per dwarf, see NbForest).
 void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
@@ -324,8 +303,7 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
                          const double* py, const double* pz, double* ax, double* ay, double* az,
                          double* vx, double* vy, double* vz, const NbWalkParams& wp,
                          const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s,
-                         double4* walkRec, const int* bodyNode, int capNodes,
-                         const NbForest* forest = nullptr);
+                         double4* walkRec, int capNodes, const NbForest* forest = nullptr);
 void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int capNodes,
                           const NbWalkParams& wp, const NbPot& pot, bool count, int numSMs,
                           cudaStream_t s, const NbForest* forest = nullptr);

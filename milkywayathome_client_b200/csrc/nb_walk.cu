@@ -18,44 +18,31 @@ constexpr int WALK_THREADS = 128;
 // FOREST: the nodes hold one tree per dwarf (batched dwarfs); each lane walks its own
 // dwarf's tree, [rootNode, rootEnd), with that dwarf's softening and time step.  A warp whose
 // 32 bodies straddle two dwarfs visits the union of both walks, each lane its own.
-// The walk reads the node data of NbWalkNodes (k_pack_walk): per visit the node's head
-// {CoM, mass} and aux {rcrit2, links}, and for an accepted cell with quadrupoles its
-// quadrupole from the dense cell array.
+// The walk reads one packed record per node (k_pack_walk): 96 bytes, three double4 --
+// {CoM, mass}, {rcrit2, Next and body index as one 64-bit word, Qxx, Qxy},
+// {Qxz, Qyy, Qyz, Qzz} -- so a visit touches one record instead of four arrays.
 __global__ void k_pack_walk(const double4* __restrict__ nodePM, const double* __restrict__ nodeCrit,
                             const int2* __restrict__ nodeLink, const double* __restrict__ nodeQuad,
-                            const int* __restrict__ bodyNode, NbWalkNodes w,
-                            const NbScalars* __restrict__ sc)
+                            double4* __restrict__ rec, const NbScalars* __restrict__ sc)
 {
     if (nb_failed(sc)) return;
-    const int nNodes = sc->nNodes, m = sc->nTree;
+    const int nNodes = sc->nNodes;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nNodes; k += gridDim.x * blockDim.x) {
         const int2 l = nodeLink[k];
-        int hiWord = l.y;
-        if (l.y < 0) {
-            // cell slot: k minus the tree bodies before it (bodyNode increases with the sorted
-            // index, so that count is a lower bound)
-            int lo = 0, hi = m;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (bodyNode[mid] < k) lo = mid + 1; else hi = mid;
-            }
-            const int c = k - lo;
-            hiWord = -(c + 1);
-            const double* Q = nodeQuad + 6 * (size_t) k;
-            w.quad[3 * (size_t) c] = make_double2(Q[0], Q[1]);
-            w.quad[3 * (size_t) c + 1] = make_double2(Q[2], Q[3]);
-            w.quad[3 * (size_t) c + 2] = make_double2(Q[4], Q[5]);
-        }
-        const long long word = (long long) (unsigned) l.x | ((long long) hiWord << 32);
-        w.head[k] = nodePM[k];
-        w.aux[k] = make_double2(nodeCrit[k], __longlong_as_double(word));
+        const long long word = (long long) (unsigned) l.x | ((long long) l.y << 32);
+        const double* Q = nodeQuad + 6 * (size_t) k;
+        const bool body = l.y >= 0;
+        rec[3 * (size_t) k] = nodePM[k];
+        rec[3 * (size_t) k + 1] = make_double4(nodeCrit[k], __longlong_as_double(word),
+                                               body ? 0.0 : Q[0], body ? 0.0 : Q[1]);
+        rec[3 * (size_t) k + 2] = body ? make_double4(0.0, 0.0, 0.0, 0.0)
+                                       : make_double4(Q[2], Q[3], Q[4], Q[5]);
     }
 }
 
 template <bool COUNT, bool FOREST>
 __global__ void __launch_bounds__(WALK_THREADS)
-k_walk_fp64(const double4* __restrict__ head, const double2* __restrict__ aux,
-            const double2* __restrict__ quad,
+k_walk_fp64(const double4* __restrict__ rec,
             const unsigned int* __restrict__ order, const double* __restrict__ px,
             const double* __restrict__ py, const double* __restrict__ pz,
             double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
@@ -90,8 +77,8 @@ k_walk_fp64(const double4* __restrict__ head, const double2* __restrict__ aux,
         if (q >= end) break;
         if (COUNT) ++cSteps;
         if (ptr != q) continue;
-        const double4 nd = head[q];
-        const double2 r1 = aux[q];
+        const double4 nd = rec[3 * (size_t) q];
+        const double4 r1 = rec[3 * (size_t) q + 1];
         const long long word = __double_as_longlong(r1.y);
         const int2 link = make_int2((int) (unsigned) (word & 0xffffffffll), (int) (word >> 32));
         const double dx = nd.x - x0, dy = nd.y - y0, dz = nd.z - z0;
@@ -110,9 +97,8 @@ k_walk_fp64(const double4* __restrict__ head, const double2* __restrict__ aux,
             accy = accy + mor3 * dy;
             accz = accz + mor3 * dz;
             if (useQuad && !isBody) {
-                const double2* Q = quad + 3 * (size_t) (-link.y - 1);
-                const double2 q0 = Q[0], q1 = Q[1], q2 = Q[2];
-                const double qxx = q0.x, qxy = q0.y, qxz = q1.x, qyy = q1.y, qyz = q2.x, qzz = q2.y;
+                const double4 r2 = rec[3 * (size_t) q + 2];
+                const double qxx = r1.z, qxy = r1.w, qxz = r2.x, qyy = r2.y, qyz = r2.z, qzz = r2.w;
                 const double qdx = qxx * dx + qxy * dy + qxz * dz;
                 const double qdy = qxy * dx + qyy * dy + qyz * dz;
                 const double qdz = qxz * dx + qyz * dy + qzz * dz;
@@ -373,11 +359,11 @@ void nb_launch_body_epilogue(const double* px, const double* py, const double* p
                              int numSMs, cudaStream_t s, const NbForest* forest);
 
 void nb_launch_pack_walk(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
-                         const double* nodeQuad, const int* bodyNode, double4* rec, int capNodes,
-                         const NbScalars* sc, cudaStream_t s)
+                         const double* nodeQuad, double4* rec, int capNodes, const NbScalars* sc,
+                         cudaStream_t s)
 {
-    k_pack_walk<<<min((capNodes + 255) / 256, 4096), 256, 0, s>>>(
-        nodePM, nodeCrit, nodeLink, nodeQuad, bodyNode, nb_walk_nodes(rec, capNodes), sc);
+    k_pack_walk<<<min((capNodes + 255) / 256, 4096), 256, 0, s>>>(nodePM, nodeCrit, nodeLink,
+                                                                  nodeQuad, rec, sc);
     nb_count_launch();
 }
 
@@ -386,16 +372,14 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
                          const double* py, const double* pz, double* ax, double* ay, double* az,
                          double* vx, double* vy, double* vz, const NbWalkParams& wp,
                          const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s,
-                         double4* walkRec, const int* bodyNode, int capNodes,
-                         const NbForest* forest)
+                         double4* walkRec, int capNodes, const NbForest* forest)
 {
     const int warps = (wp.n + 31) / 32;
     const int blocks = (warps * 32 + WALK_THREADS - 1) / WALK_THREADS;
     if (blocks <= 0) return;
-    nb_launch_pack_walk(nodePM, nodeCrit, nodeLink, nodeQuad, bodyNode, walkRec, capNodes, sc, s);
+    nb_launch_pack_walk(nodePM, nodeCrit, nodeLink, nodeQuad, walkRec, capNodes, sc, s);
     const NbForest f = forest ? *forest : NbForest{nullptr, nullptr, 0};
-    const NbWalkNodes wn = nb_walk_nodes(walkRec, capNodes);
-#define NB_WALK_ARGS wn.head, wn.aux, wn.quad, order, px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc, f
+#define NB_WALK_ARGS walkRec, order, px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc, f
     if (forest) {
         if (count) k_walk_fp64<true, true><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
         else k_walk_fp64<false, true><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
