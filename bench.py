@@ -48,6 +48,7 @@ UNIT = "body-updates/s"
 N_DEFAULT = 1048576
 THETA_DEFAULT = 0.5
 SEED_1M, SEED_CONFIG0, SEED_CONFIG2 = 1000, 2000, 3000
+WALK_FORM = -1          # the FP64 walk's form (nbSetWalkFormCUDA): -1 chosen by timing
 WORKLOAD = ("sample workunit's two-component Plummer dwarf, N=1,048,576 (half baryons), "
             "TreeCode theta=0.5, quadrupoles, Miyamoto-Nagai+Hernquist+logarithmic-halo "
             "potential, KDK leapfrog")
@@ -90,6 +91,8 @@ def parse_args():
                     help="steps of the energy-drift run of both forms (0: skip)")
     ap.add_argument("--theta2", type=float, default=1.0,
                     help="second opening angle measured for both forms (0: skip)")
+    ap.add_argument("--walk-form", choices=["auto", "union", "lanes"], default="auto",
+                    help="the FP64 walk: chosen by timing (default), warp union or per lane")
     ap.add_argument("--profile", choices=["fp64", "mixed", "adjoint", "batch", "config0"],
                     help="profiling entry: build the dwarf, run two force evaluations, exit")
     return ap.parse_args()
@@ -506,7 +509,10 @@ def run_steps_timed(c, pos, vel, mass, dev, warm, steps, exact=True):
     """A fresh state of the arrays, `warm` untimed steps, then `steps` steps each timed with
     CUDA events; returns (step ms list, walk ms list, tree info)."""
     from milkywayathome_client_b200.nbody import NBodyState
-    with NBodyState.create(c, pos, vel, mass, device=dev) as st:
+    with NBodyState(len(mass), dev) as st:
+        st.set_walk_form(WALK_FORM)
+        st.set_bodies(pos, vel, mass, c.treeRSize)
+        st.check("nbGravMap", st.gravMap(c))
         st.set_mixed_mode(exact)
         for _ in range(warm):
             st.check("nbStepSystem", st.step(c))
@@ -571,15 +577,18 @@ def run_ours(args, dist):
     notes = []
 
     def timed_run(c, exact=True):
-        st = NBodyState.create(c, pos, vel, mass, device=dev)
+        st = NBodyState(n, dev)
+        st.set_walk_form(WALK_FORM)
+        st.set_bodies(pos, vel, mass, c.treeRSize)
+        st.check("nbGravMap", st.gravMap(c))
         st.set_mixed_mode(exact)
+        for _ in range(W):              # the automatic walk form is chosen here
+            st.check("nbStepSystem", st.step(c))
+        # the interaction counts of the walk in use (a force evaluation at the same positions)
         st.set_counting(True)
         st.check("nbGravMap", st.gravMap(c))
         counts = st.walk_stats()
         st.set_counting(False)
-        st.check("nbGravMap", st.gravMap(c))
-        for _ in range(W):
-            st.check("nbStepSystem", st.step(c))
         dist.barrier()
         l0 = kernel_launches()
         clocks = ClockSampler(dev)
@@ -593,6 +602,7 @@ def run_ours(args, dist):
         launches = kernel_launches() - l0
         dist.barrier()
         info = st.tree_info()
+        info.walkForm = st.walk_form()
         return st, counts, step_ms, walk_ms, launches, clk, info
 
     # ---- FP64 drop-in (headline) ----
@@ -696,7 +706,8 @@ def run_ours(args, dist):
                 "flops_per_launch": flops_per_walk, "walk_ms": mean_walk,
                 "interactions_per_body": {"body": counts[0] / n, "cell": counts[1] / n,
                                           "visits": counts[2] / n},
-                "lane_utilisation": counts[2] / (32.0 * max(counts[3], 1))}
+                "lane_utilisation": counts[2] / (32.0 * max(counts[3], 1)),
+                "walk_form": {0: "warp union", 1: "per lane"}.get(info.walkForm, "undecided")}
     # the exact-set mixed walk evaluates every body's own FP64 interaction set, so its
     # algorithmic work is the FP64 walk's count; issued work (list entries x 32 lanes, masked
     # lanes included) is given beside it
@@ -812,7 +823,10 @@ def run_profile(args):
         from milkywayathome_client_b200.nbody import NBodyState
         pos, vel, mass, _ = bench_input(20000, SEED_CONFIG0)
         ctx, _ = bench_ctx(20000, 1.0)
-        with NBodyState.create(ctx, pos, vel, mass) as st:
+        with NBodyState(20000, 0) as st:
+            st.set_walk_form(WALK_FORM)
+            st.set_bodies(pos, vel, mass, ctx.treeRSize)
+            st.check("nbGravMap", st.gravMap(ctx))
             ms = []
             for _ in range(5):
                 st.check("nbStepSystem", st.step(ctx))
@@ -841,7 +855,10 @@ def run_profile(args):
     from milkywayathome_client_b200.nbody import NBodyState
     pos, vel, mass, _ = bench_input(args.n, SEED_1M)
     ctx, _ = bench_ctx(args.n, args.theta, precision=args.profile)
-    with NBodyState.create(ctx, pos, vel, mass) as st:
+    with NBodyState(args.n, 0) as st:
+        st.set_walk_form(WALK_FORM if WALK_FORM >= 0 else 0)
+        st.set_bodies(pos, vel, mass, ctx.treeRSize)
+        st.check("nbGravMap", st.gravMap(ctx))
         st.check("nbGravMap", st.gravMap(ctx))
         print(json.dumps({"profile": args.profile, "n": args.n, "walk_ms": st.walk_time_ms()[0],
                           "step_ms": st.step_time_ms()}))
@@ -850,6 +867,8 @@ def run_profile(args):
 
 def main():
     args = parse_args()
+    global WALK_FORM
+    WALK_FORM = {"auto": -1, "union": 0, "lanes": 1}[args.walk_form]
     if args.impl == "reference":
         # the reference arm is host-only: rank 0 runs it, other ranks exit without work
         os.environ.setdefault("WORLD_SIZE", "1")

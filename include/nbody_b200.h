@@ -352,6 +352,19 @@ NBodyCudaStatus nbSetStepCUDA(NBodyCudaState* st, int step);
  * arguments) and counted evaluations are always launched directly. */
 NBodyCudaStatus nbSetStepGraphCUDA(NBodyCudaState* st, int enable);
 
+/* The FP64 force walk's form: 0 walks the union of a warp's 32 tree paths node by node (the
+ * lanes whose path holds the node doing it); 1 walks every body's path in its own lane (a
+ * lane idles only once its walk is over; per-lane loads instead of one broadcast per node);
+ * -1 (the default) times the first uncounted FP64 tree evaluation with the union walk and
+ * the second per lane and keeps the faster (longer walks, theta 0.5 at 1M bodies, favour the
+ * union; shorter ones, theta 1.0 or small systems, the lanes).  Every form gives every body
+ * exactly its CPU walk -- same nodes, same order, same sums: the accelerations are the same
+ * bit for bit.  A batch walks the union unless its state's form is set to 1; the force
+ * adjoint always walks the union (it reduces each node's adjoints over the warp).
+ * nbGetWalkFormCUDA reports the form in use (-1 while undecided). */
+NBodyCudaStatus nbSetWalkFormCUDA(NBodyCudaState* st, int form);
+NBodyCudaStatus nbGetWalkFormCUDA(NBodyCudaState* st, int* form);
+
 /* Mixed-precision walk tuning of a single state (as nbBatchSetTuningCUDA): bodies per walk
  * group (1..64), interaction-list entries per warp (32, 64, 128), walk blocks per SM (0: max). */
 NBodyCudaStatus nbSetMixedTuningCUDA(NBodyCudaState* st, int groupMax, int listCap, int blocksPerSM);

@@ -221,6 +221,8 @@ SIGNATURES = [
     ("nbSetTimeOriginCUDA", ctypes.c_int, [_vp, ctypes.c_double]),
     ("nbSetStepCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbSetStepGraphCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nbSetWalkFormCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nbGetWalkFormCUDA", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     ("nbSetMixedTuningCUDA", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("nbBatchSetTimeOriginCUDA", ctypes.c_int, [_vp, ctypes.c_double]),
     ("nbGenerateDwarfCUDA", ctypes.c_int, [_vp, ctypes.POINTER(PlummerDwarf), ctypes.c_double]),

@@ -176,7 +176,13 @@ struct NBodyCudaState {
     int stepGraphMx[4] = {0, 0, 0, 0};
     unsigned long long stepGraphLaunches = 0;
     int useStepGraph = 1;
+    int stepGraphLanes = -1;
     NbScalars* scInit = nullptr;
+    // the FP64 walk's form (nbSetWalkFormCUDA): -1 chooses by timing -- the first uncounted
+    // FP64 tree evaluation walks the warp union, the second per lane, the faster one is kept
+    int walkForm = -1;
+    int walkFormChosen = -1;
+    float walkFormMs[2] = {-1.0f, -1.0f};
     double* keepPos = nullptr;          // bodies at the best likelihood (3n each)
     double* keepVel = nullptr;
     int haveKeep = 0;
@@ -456,6 +462,15 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
         st->mx.listCap = st->mixListCap;
         st->mx.exact = st->mixExact;
     }
+    // the FP64 walk's form for this evaluation (its timing decides the automatic choice)
+    const bool fp64Tree = !mixed && ctx->criterion != NBCUDA_EXACT;
+    int lanes = 0;
+    bool tuning = false;
+    if (fp64Tree) {
+        if (st->walkForm >= 0) lanes = st->walkForm;
+        else if (st->walkFormChosen >= 0) lanes = st->walkFormChosen;
+        else { lanes = st->walkFormMs[0] < 0.0f ? 0 : 1; tuning = !st->counting; }
+    }
     // The device work of the evaluation, enqueued without host synchronisation: the scalars
     // from the pinned st->scInit, the tree or the direct sum, the walk, the scalars back into
     // st->scHost.  capturing: inside a stream capture (events become graph nodes).
@@ -486,7 +501,8 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
             else
                 nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px,
                                     b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
-                                    st->counting != 0, s, b.walkRec, st->capNodes);
+                                    st->counting != 0, s, b.walkRec, st->capNodes, nullptr,
+                                    lanes != 0);
             rec(st->ev1);
         }
         rec(st->evE);
@@ -509,6 +525,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
                                   mixed ? st->mx.listCap : 0, mixed ? st->mx.exact : 0};
             const bool same = st->stepGraph && st->stepGraphDrift == drift &&
                               st->stepGraphKick == kick && st->stepGraphCap == st->capNodes &&
+                              st->stepGraphLanes == lanes &&
                               std::memcmp(st->stepGraphMx, mxKey, sizeof mxKey) == 0 &&
                               std::memcmp(&st->stepGraphCtx, ctx, sizeof *ctx) == 0;
             if (!same) {
@@ -529,6 +546,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
                 st->stepGraphDrift = drift;
                 st->stepGraphKick = kick;
                 st->stepGraphCap = st->capNodes;
+                st->stepGraphLanes = lanes;
                 std::memcpy(st->stepGraphMx, mxKey, sizeof mxKey);
             } else {
                 nb_count_launch((int) st->stepGraphLaunches);
@@ -553,6 +571,11 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, st->ev0, st->ev1);
         st->walkMs = ms;
+        if (tuning && !(h.status & ~(int) NBODY_STATUS_WARNINGS_MASK)) {
+            st->walkFormMs[lanes] = ms;
+            if (st->walkFormMs[0] >= 0.0f && st->walkFormMs[1] >= 0.0f)
+                st->walkFormChosen = st->walkFormMs[1] < st->walkFormMs[0] ? 1 : 0;
+        }
         ms = 0.0f;
         cudaEventElapsedTime(&ms, st->evS, st->evE);
         st->stepMs = ms;
@@ -1780,6 +1803,22 @@ NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTi
     return NBODY_SUCCESS;
 }
 
+NBodyCudaStatus nbSetWalkFormCUDA(NBodyCudaState* st, int form)
+{
+    if (!st || form < -1 || form > 1) return NBODY_USER_ERROR;
+    st->walkForm = form;
+    st->walkFormChosen = -1;
+    st->walkFormMs[0] = st->walkFormMs[1] = -1.0f;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbGetWalkFormCUDA(NBodyCudaState* st, int* form)
+{
+    if (!st || !form) return NBODY_USER_ERROR;
+    *form = st->walkForm >= 0 ? st->walkForm : st->walkFormChosen;
+    return NBODY_SUCCESS;
+}
+
 NBodyCudaStatus nbSetStepGraphCUDA(NBodyCudaState* st, int enable)
 {
     if (!st) return NBODY_USER_ERROR;
@@ -2051,7 +2090,7 @@ static int nb_batch_enqueue(NBodyCudaBatch* bt, const NBodyCudaCtx* ctx, int dri
     } else {
         nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px, b.py,
                             b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc, false, s,
-                            b.walkRec, st->capNodes, &f);
+                            b.walkRec, st->capNodes, &f, st->walkForm == 1);
         launches += 1;
     }
     cudaEventRecord(st->ev1, s);

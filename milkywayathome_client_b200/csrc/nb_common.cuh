@@ -303,7 +303,8 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
                          const double* py, const double* pz, double* ax, double* ay, double* az,
                          double* vx, double* vy, double* vz, const NbWalkParams& wp,
                          const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s,
-                         double4* walkRec, int capNodes, const NbForest* forest = nullptr);
+                         double4* walkRec, int capNodes, const NbForest* forest = nullptr,
+                         bool lanes = false);
 void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int capNodes,
                           const NbWalkParams& wp, const NbPot& pot, bool count, int numSMs,
                           cudaStream_t s, const NbForest* forest = nullptr);

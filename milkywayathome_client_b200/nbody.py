@@ -400,6 +400,17 @@ class NBodyState:
         self.check("nbSetTimeOrigin", self.lib.nbSetTimeOriginCUDA(self._h,
                                                                   float(previous_forward_time)))
 
+    def set_walk_form(self, form=-1):
+        """The FP64 walk's form (nbSetWalkFormCUDA): 0 warp union, 1 per lane, -1 chosen by
+        timing the first two evaluations; the accelerations are the same bit for bit."""
+        self.check("nbSetWalkForm", self.lib.nbSetWalkFormCUDA(self._h, int(form)))
+
+    def walk_form(self):
+        """The FP64 walk form in use (-1 while the automatic choice is undecided)."""
+        f = ctypes.c_int()
+        self.check("nbGetWalkForm", self.lib.nbGetWalkFormCUDA(self._h, ctypes.byref(f)))
+        return f.value
+
     def set_step_graph(self, enable=True):
         """Whole steps replayed as one captured CUDA graph (nbSetStepGraphCUDA; the default)."""
         self.check("nbSetStepGraph", self.lib.nbSetStepGraphCUDA(self._h, int(bool(enable))))

@@ -348,3 +348,37 @@ def test_step_graph_equals_direct_launches(dwarf_small, precision):
         pb, vb = b.bodies()
         assert bits_equal(pa, pb) and bits_equal(va, vb) and bits_equal(a.accels(), b.accels())
         assert a.step_count == b.step_count == 13
+
+
+@pytest.mark.parametrize("cfg", [dict(theta=0.5, criterion="TreeCode", useQuad=True),
+                                 dict(theta=1.0, criterion="SW93", useQuad=True),
+                                 dict(theta=0.7, criterion="TreeCode", useQuad=False)],
+                         ids=lambda c: "%s-%g-q%d" % (c["criterion"], c["theta"], c["useQuad"]))
+def test_union_and_per_lane_walks_are_bit_equal(dwarf_small, cfg):
+    """The FP64 walk's forms (nbSetWalkFormCUDA): the warp-union walk, per-lane walks and the
+    automatic choice between them all give each body its CPU walk -- the oracle's
+    accelerations bit for bit, and the same interaction counts."""
+    from oracle import bindings as ob
+    pos, vel, mass, _ = dwarf_small
+    ctx = make_ctx(len(mass), **cfg)
+    rc, acc, _, _, cnt = ob.grav_map(ctx.struct, pos, mass, ctx.treeRSize, counts=True)
+    steps = {}
+    for form in (0, 1):
+        with _gpu_state(ctx, pos, vel, mass) as st:
+            st.set_walk_form(form)
+            st.set_counting(True)
+            assert st.gravMap(ctx) == rc == 0
+            stats = st.walk_stats()
+            assert bits_equal(st.accels(), acc), form
+            assert tuple(stats[:3]) == tuple(cnt), form
+            steps[form] = stats[3]
+            assert st.walk_form() == form
+    # the per-lane walk runs fewer warp iterations than the union walk
+    assert steps[1] < steps[0]
+    # automatic: the first two evaluations time both forms, then one is kept
+    with _gpu_state(ctx, pos, vel, mass) as st:
+        assert st.walk_form() == -1
+        for _ in range(3):
+            assert st.gravMap(ctx) == 0
+            assert bits_equal(st.accels(), acc)
+        assert st.walk_form() in (0, 1)
