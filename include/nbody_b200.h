@@ -355,9 +355,10 @@ NBodyCudaStatus nbSetStepGraphCUDA(NBodyCudaState* st, int enable);
 /* The FP64 force walk's form: 0 walks the union of a warp's 32 tree paths node by node (the
  * lanes whose path holds the node doing it); 1 walks every body's path in its own lane (a
  * lane idles only once its walk is over; per-lane loads instead of one broadcast per node);
- * -1 (the default) times the first uncounted FP64 tree evaluation with the union walk and
- * the second per lane and keeps the faster (longer walks, theta 0.5 at 1M bodies, favour the
- * union; shorter ones, theta 1.0 or small systems, the lanes).  Every form gives every body
+ * -1 (the default) alternates the two forms over a state's first four uncounted FP64 tree
+ * evaluations, times the third (union) and fourth (per lane) -- the first launch of each
+ * kernel also loads it -- and keeps the faster (longer walks, theta 0.5 at 1M bodies, favour
+ * the union; shorter ones, theta 1.0 or small systems, the lanes).  Every form gives every body
  * exactly its CPU walk -- same nodes, same order, same sums: the accelerations are the same
  * bit for bit.  A batch walks the union unless its state's form is set to 1; the force
  * adjoint always walks the union (it reduces each node's adjoints over the warp).

@@ -178,10 +178,12 @@ struct NBodyCudaState {
     int useStepGraph = 1;
     int stepGraphLanes = -1;
     NbScalars* scInit = nullptr;
-    // the FP64 walk's form (nbSetWalkFormCUDA): -1 chooses by timing -- the first uncounted
-    // FP64 tree evaluation walks the warp union, the second per lane, the faster one is kept
+    // the FP64 walk's form (nbSetWalkFormCUDA): -1 chooses by timing -- the first four
+    // uncounted FP64 tree evaluations alternate the warp union and per-lane walks, the last two
+    // (past each kernel's first launch, which also loads it) are timed, the faster form is kept
     int walkForm = -1;
     int walkFormChosen = -1;
+    int walkTuneStep = 0;
     float walkFormMs[2] = {-1.0f, -1.0f};
     double* keepPos = nullptr;          // bodies at the best likelihood (3n each)
     double* keepVel = nullptr;
@@ -469,7 +471,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
     if (fp64Tree) {
         if (st->walkForm >= 0) lanes = st->walkForm;
         else if (st->walkFormChosen >= 0) lanes = st->walkFormChosen;
-        else { lanes = st->walkFormMs[0] < 0.0f ? 0 : 1; tuning = !st->counting; }
+        else { lanes = st->walkTuneStep & 1; tuning = !st->counting; }
     }
     // The device work of the evaluation, enqueued without host synchronisation: the scalars
     // from the pinned st->scInit, the tree or the direct sum, the walk, the scalars back into
@@ -572,7 +574,8 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
         cudaEventElapsedTime(&ms, st->ev0, st->ev1);
         st->walkMs = ms;
         if (tuning && !(h.status & ~(int) NBODY_STATUS_WARNINGS_MASK)) {
-            st->walkFormMs[lanes] = ms;
+            if (st->walkTuneStep >= 2) st->walkFormMs[lanes] = ms;
+            ++st->walkTuneStep;
             if (st->walkFormMs[0] >= 0.0f && st->walkFormMs[1] >= 0.0f)
                 st->walkFormChosen = st->walkFormMs[1] < st->walkFormMs[0] ? 1 : 0;
         }
@@ -1808,6 +1811,7 @@ NBodyCudaStatus nbSetWalkFormCUDA(NBodyCudaState* st, int form)
     if (!st || form < -1 || form > 1) return NBODY_USER_ERROR;
     st->walkForm = form;
     st->walkFormChosen = -1;
+    st->walkTuneStep = 0;
     st->walkFormMs[0] = st->walkFormMs[1] = -1.0f;
     return NBODY_SUCCESS;
 }

@@ -402,7 +402,7 @@ class NBodyState:
 
     def set_walk_form(self, form=-1):
         """The FP64 walk's form (nbSetWalkFormCUDA): 0 warp union, 1 per lane, -1 chosen by
-        timing the first two evaluations; the accelerations are the same bit for bit."""
+        timing the third and fourth evaluations; the accelerations are the same bit for bit."""
         self.check("nbSetWalkForm", self.lib.nbSetWalkFormCUDA(self._h, int(form)))
 
     def walk_form(self):
