@@ -52,24 +52,26 @@ __global__ void k_pack_f32(const double4* __restrict__ nodePM, const double* __r
         // bodies carry an rcrit2 of -inf, so the acceptance test needs no body branch
         const float crit = isBody ? __int_as_float(0xff800000) : __double2float_rn(nodeCrit[k]);
         nodeHi[k] = make_float4(hx, hy, hz, crit);
-        nodeLo[k] = make_float4(lx, ly, lz, __double2float_rn(p.w));
-        if (!isBody) {
+        if (isBody) {
+            nodeLo[k] = make_float4(lx, ly, lz, __double2float_rn(p.w));
+        } else {
+            // a cell's slot c = k minus the tree bodies before it (they are the sorted bodies
+            // below its first one): the cells' quadrupoles, masses and child lists are stored
+            // densely by slot, and lo.w carries the slot (the mass is in the slot's record)
+            const int c = k - nodeRange[k].x;
+            nodeLo[k] = make_float4(lx, ly, lz, __int_as_float(c));
             // the children of a cell: k+1, then Next() up to Next(k) (threadTree order)
             int ch[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
             const int stop = nodeLink[k].x;
-            int c = k + 1;
-            for (int m = 0; m < 8 && c < stop; ++m) { ch[m] = c; c = nodeLink[c].x; }
-            child8[2 * (size_t) k] = make_int4(ch[0], ch[1], ch[2], ch[3]);
-            child8[2 * (size_t) k + 1] = make_int4(ch[4], ch[5], ch[6], ch[7]);
-        }
-        const double* Q = nodeQuad + 6 * (size_t) k;
-        if (isBody) {
-            nodeQ32[2 * (size_t) k] = make_float4(0.f, 0.f, 0.f, 0.f);
-            nodeQ32[2 * (size_t) k + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
-        } else {
-            nodeQ32[2 * (size_t) k] = make_float4(__double2float_rn(Q[0]), __double2float_rn(Q[1]),
+            int kc = k + 1;
+            for (int m = 0; m < 8 && kc < stop; ++m) { ch[m] = kc; kc = nodeLink[kc].x; }
+            child8[2 * (size_t) c] = make_int4(ch[0], ch[1], ch[2], ch[3]);
+            child8[2 * (size_t) c + 1] = make_int4(ch[4], ch[5], ch[6], ch[7]);
+            const double* Q = nodeQuad + 6 * (size_t) k;
+            nodeQ32[2 * (size_t) c] = make_float4(__double2float_rn(Q[0]), __double2float_rn(Q[1]),
                                                   __double2float_rn(Q[2]), __double2float_rn(Q[3]));
-            nodeQ32[2 * (size_t) k + 1] = make_float4(__double2float_rn(Q[4]), __double2float_rn(Q[5]), 0.f, 0.f);
+            nodeQ32[2 * (size_t) c + 1] = make_float4(__double2float_rn(Q[4]), __double2float_rn(Q[5]),
+                                                      __double2float_rn(p.w), 0.f);
         }
     }
 }
@@ -431,7 +433,8 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
             }
             const bool addCell = accCell || (EXACT && boundary && anyUse);
             int4 c0 = make_int4(-1, -1, -1, -1), c1 = c0;
-            if (openCell) { c0 = child8[2 * (size_t) k]; c1 = child8[2 * (size_t) k + 1]; }
+            const size_t cs = (size_t) __float_as_int(lo.w);     // a cell's slot
+            if (openCell) { c0 = child8[2 * cs]; c1 = child8[2 * cs + 1]; }
             const unsigned bodyMask = __ballot_sync(NB_FULL_MASK, isBody);
             const unsigned cellMask = __ballot_sync(NB_FULL_MASK, addCell);
             if (COUNT) {
@@ -471,8 +474,8 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
             }
             if (addCell) {
                 const int e = nC + __popc(cellMask & ltMask);
-                const float4 qa = nodeQ32[2 * (size_t) k], qb = nodeQ32[2 * (size_t) k + 1];
-                cells.a[e] = rel;
+                const float4 qa = nodeQ32[2 * cs], qb = nodeQ32[2 * cs + 1];
+                cells.a[e] = make_float4(rel.x, rel.y, rel.z, qb.z);   // the cell's mass
                 cells.b[e] = qa;
                 cells.c[e] = qb;
                 if (EXACT)
