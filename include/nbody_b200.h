@@ -353,16 +353,15 @@ NBodyCudaStatus nbSetStepCUDA(NBodyCudaState* st, int step);
 NBodyCudaStatus nbSetStepGraphCUDA(NBodyCudaState* st, int enable);
 
 /* The FP64 force walk's form: 0 walks the union of a warp's 32 tree paths node by node (the
- * lanes whose path holds the node doing it); 1 walks every body's path in its own lane (a
- * lane idles only once its walk is over; per-lane loads instead of one broadcast per node);
- * -1 (the default) alternates the two forms over a state's first four uncounted FP64 tree
- * evaluations, times the third (union) and fourth (per lane) -- the first launch of each
- * kernel also loads it -- and keeps the faster (longer walks, theta 0.5 at 1M bodies, favour
- * the union; shorter ones, theta 1.0 or small systems, the lanes).  Every form gives every body
- * exactly its CPU walk -- same nodes, same order, same sums: the accelerations are the same
- * bit for bit.  A batch walks the union unless its state's form is set to 1; the force
- * adjoint always walks the union (it reduces each node's adjoints over the warp).
- * nbGetWalkFormCUDA reports the form in use (-1 while undecided). */
+ * lanes whose path holds the node doing it, one broadcast load per node); 1 walks every body's
+ * path in its own lane (a lane idles only once its walk is over; per-lane loads).
+ * -1 (the default) cycles twice through the candidate forms over a state's first uncounted
+ * FP64 tree evaluations, times the second round (the first launch of each kernel also loads
+ * it) and keeps the fastest.  Every form gives every body exactly its CPU walk -- same nodes,
+ * same order, same sums: the accelerations are the same bit for bit.  A batch walks the union
+ * unless its form is set to 1 (nbBatchSetWalkFormCUDA); the force adjoint always walks the union
+ * (it reduces each node's adjoints over the warp).  nbGetWalkFormCUDA reports the form in use
+ * (-1 while undecided). */
 NBodyCudaStatus nbSetWalkFormCUDA(NBodyCudaState* st, int form);
 NBodyCudaStatus nbGetWalkFormCUDA(NBodyCudaState* st, int* form);
 
@@ -493,6 +492,10 @@ NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* batch, int groupMax, int li
                                      int blocksPerSM);
 /* as nbSetMixedModeCUDA, for every dwarf of the batch */
 NBodyCudaStatus nbBatchSetMixedModeCUDA(NBodyCudaBatch* batch, int exactSet);
+/* The FP64 walk's form for every dwarf of the batch, as nbSetWalkFormCUDA but without the
+ * automatic choice: 0 (the default) the warp union, 1 per lane (a warp may span two dwarfs;
+ * each lane walks only its own dwarf's tree). */
+NBodyCudaStatus nbBatchSetWalkFormCUDA(NBodyCudaBatch* batch, int form);
 NBodyCudaStatus nbBatchGetTuningCUDA(NBodyCudaBatch* batch, int* groupMax, int* listCap,
                                      int* blocksPerSM);
 /* autotuner of the mixed walk on the batch's current state: times every candidate tuning

@@ -250,6 +250,7 @@ SIGNATURES = [
     ("nbSetLMCCUDA", ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int]),
     ("nbGetLMCCUDA", ctypes.c_int, [_vp, _vp, _vp]),
     ("nbBatchSetMixedModeCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nbBatchSetWalkFormCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbSaveStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbRestoreStateCUDA", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nbReleaseStatesCUDA", ctypes.c_int, [_vp]),

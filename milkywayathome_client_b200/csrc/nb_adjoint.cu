@@ -199,8 +199,8 @@ k_walk_vjp(const double4* __restrict__ rec,
         if (q >= end) break;
         const bool active = ptr == q;
         // the FP64 walk's packed record: {CoM, mass}, {rcrit2, links, Qxx, Qxy}, {Qxz .. Qzz}
-        const double4 nd = rec[3 * (size_t) q];
-        const double4 r1 = rec[3 * (size_t) q + 1];
+        const double4 nd = nb_ld32(rec + 3 * (size_t) q);
+        const double4 r1 = nb_ld32(rec + 3 * (size_t) q + 1);
         const long long word = __double_as_longlong(r1.y);
         const int2 link = make_int2((int) (unsigned) (word & 0xffffffffll), (int) (word >> 32));
         const bool isBody = link.y >= 0;
@@ -214,7 +214,7 @@ k_walk_vjp(const double4* __restrict__ rec,
                 inter = !(isBody && (unsigned) link.y == j);
                 if (inter) {
                     double4 r2 = make_double4(0.0, 0.0, 0.0, 0.0);
-                    if (useQuad && !isBody) r2 = rec[3 * (size_t) q + 2];
+                    if (useQuad && !isBody) r2 = nb_ld32(rec + 3 * (size_t) q + 2);
                     v = nb_interaction_vjp(dx, dy, dz, nd.w, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w,
                                            useQuad && !isBody, wp.eps2, abx, aby, abz);
                     gx -= v.rx; gy -= v.ry; gz -= v.rz;

@@ -128,6 +128,11 @@ struct NbSlot {
     double lmc[6] = {0, 0, 0, 0, 0, 0};   // the LMC's position and velocity (LMC runs)
 };
 
+// The FP64 walk forms the automatic choice times (nbSetWalkFormCUDA): 0 the warp union,
+// 1 the walk per lane.
+static const int kWalkTuneForms[] = {0, 1};
+static const int kWalkTuneN = (int) (sizeof kWalkTuneForms / sizeof kWalkTuneForms[0]);
+
 struct NBodyCudaState {
     int device = 0;
     int nbody = 0;
@@ -176,15 +181,15 @@ struct NBodyCudaState {
     int stepGraphMx[4] = {0, 0, 0, 0};
     unsigned long long stepGraphLaunches = 0;
     int useStepGraph = 1;
-    int stepGraphLanes = -1;
+    int stepGraphForm = -1;
     NbScalars* scInit = nullptr;
-    // the FP64 walk's form (nbSetWalkFormCUDA): -1 chooses by timing -- the first four
-    // uncounted FP64 tree evaluations alternate the warp union and per-lane walks, the last two
-    // (past each kernel's first launch, which also loads it) are timed, the faster form is kept
+    // the FP64 walk's form (nbSetWalkFormCUDA): -1 chooses by timing -- the first 2C uncounted
+    // FP64 tree evaluations cycle twice through the C candidate forms, the second round (past
+    // each kernel's first launch, which also loads it) is timed, the fastest form is kept
     int walkForm = -1;
     int walkFormChosen = -1;
     int walkTuneStep = 0;
-    float walkFormMs[2] = {-1.0f, -1.0f};
+    float walkFormMs[8] = {-1.0f, -1.0f, -1.0f, -1.0f, -1.0f, -1.0f, -1.0f, -1.0f};
     double* keepPos = nullptr;          // bodies at the best likelihood (3n each)
     double* keepVel = nullptr;
     int haveKeep = 0;
@@ -466,12 +471,12 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
     }
     // the FP64 walk's form for this evaluation (its timing decides the automatic choice)
     const bool fp64Tree = !mixed && ctx->criterion != NBCUDA_EXACT;
-    int lanes = 0;
+    int form = 0;
     bool tuning = false;
     if (fp64Tree) {
-        if (st->walkForm >= 0) lanes = st->walkForm;
-        else if (st->walkFormChosen >= 0) lanes = st->walkFormChosen;
-        else { lanes = st->walkTuneStep & 1; tuning = !st->counting; }
+        if (st->walkForm >= 0) form = st->walkForm;
+        else if (st->walkFormChosen >= 0) form = st->walkFormChosen;
+        else { form = kWalkTuneForms[st->walkTuneStep % kWalkTuneN]; tuning = !st->counting; }
     }
     // The device work of the evaluation, enqueued without host synchronisation: the scalars
     // from the pinned st->scInit, the tree or the direct sum, the walk, the scalars back into
@@ -504,7 +509,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
                 nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px,
                                     b.py, b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc,
                                     st->counting != 0, s, b.walkRec, st->capNodes, nullptr,
-                                    lanes != 0);
+                                    form);
             rec(st->ev1);
         }
         rec(st->evE);
@@ -527,7 +532,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
                                   mixed ? st->mx.listCap : 0, mixed ? st->mx.exact : 0};
             const bool same = st->stepGraph && st->stepGraphDrift == drift &&
                               st->stepGraphKick == kick && st->stepGraphCap == st->capNodes &&
-                              st->stepGraphLanes == lanes &&
+                              st->stepGraphForm == form &&
                               std::memcmp(st->stepGraphMx, mxKey, sizeof mxKey) == 0 &&
                               std::memcmp(&st->stepGraphCtx, ctx, sizeof *ctx) == 0;
             if (!same) {
@@ -548,7 +553,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
                 st->stepGraphDrift = drift;
                 st->stepGraphKick = kick;
                 st->stepGraphCap = st->capNodes;
-                st->stepGraphLanes = lanes;
+                st->stepGraphForm = form;
                 std::memcpy(st->stepGraphMx, mxKey, sizeof mxKey);
             } else {
                 nb_count_launch((int) st->stepGraphLaunches);
@@ -574,10 +579,14 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
         cudaEventElapsedTime(&ms, st->ev0, st->ev1);
         st->walkMs = ms;
         if (tuning && !(h.status & ~(int) NBODY_STATUS_WARNINGS_MASK)) {
-            if (st->walkTuneStep >= 2) st->walkFormMs[lanes] = ms;
-            ++st->walkTuneStep;
-            if (st->walkFormMs[0] >= 0.0f && st->walkFormMs[1] >= 0.0f)
-                st->walkFormChosen = st->walkFormMs[1] < st->walkFormMs[0] ? 1 : 0;
+            const int c = st->walkTuneStep % kWalkTuneN;
+            if (st->walkTuneStep >= kWalkTuneN) st->walkFormMs[c] = ms;
+            if (++st->walkTuneStep == 2 * kWalkTuneN) {
+                int best = 0;
+                for (int k = 1; k < kWalkTuneN; ++k)
+                    if (st->walkFormMs[k] < st->walkFormMs[best]) best = k;
+                st->walkFormChosen = kWalkTuneForms[best];
+            }
         }
         ms = 0.0f;
         cudaEventElapsedTime(&ms, st->evS, st->evE);
@@ -1812,7 +1821,7 @@ NBodyCudaStatus nbSetWalkFormCUDA(NBodyCudaState* st, int form)
     st->walkForm = form;
     st->walkFormChosen = -1;
     st->walkTuneStep = 0;
-    st->walkFormMs[0] = st->walkFormMs[1] = -1.0f;
+    for (float& ms : st->walkFormMs) ms = -1.0f;
     return NBODY_SUCCESS;
 }
 
@@ -2094,7 +2103,7 @@ static int nb_batch_enqueue(NBodyCudaBatch* bt, const NBodyCudaCtx* ctx, int dri
     } else {
         nb_launch_walk_fp64(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeQuad, b.sort.idxA, b.px, b.py,
                             b.pz, b.ax, b.ay, b.az, b.vx, b.vy, b.vz, wp, pot, b.sc, false, s,
-                            b.walkRec, st->capNodes, &f, st->walkForm == 1);
+                            b.walkRec, st->capNodes, &f, st->walkForm > 0 ? st->walkForm : 0);
         launches += 1;
     }
     cudaEventRecord(st->ev1, s);
@@ -2399,6 +2408,14 @@ NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* bt, int groupMax, int listC
     bt->tune.groupMax = groupMax;
     bt->tune.listCap = listCap;
     bt->tune.blocksPerSM = blocksPerSM;
+    return NBODY_SUCCESS;
+}
+
+NBodyCudaStatus nbBatchSetWalkFormCUDA(NBodyCudaBatch* bt, int form)
+{
+    if (!bt || form < 0 || form > 1) return NBODY_USER_ERROR;
+    bt->st->walkForm = form;
+    nb_batch_drop_graph(bt);            // the captured step holds the walk kernel
     return NBODY_SUCCESS;
 }
 

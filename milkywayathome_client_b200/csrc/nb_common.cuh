@@ -114,6 +114,18 @@ __device__ __forceinline__ bool nb_failed(const NbScalars* sc)
     return (*(volatile const int*) &sc->status & ~(int) NBODY_STATUS_WARNINGS_MASK) != 0;
 }
 
+// One 32-byte read-only load of a 32-byte-aligned double4 (ld.global.nc.v4.f64, sm_100).
+// double4 itself is only 16-byte aligned, so a plain load of one is two 16-byte requests that
+// each count the same sector; this is one request, one sector per lane.  For buffers a kernel
+// only reads.
+__device__ __forceinline__ double4 nb_ld32(const double4* p)
+{
+    double4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+    return r;
+}
+
 // ---- batched dwarfs: a forest of independent trees in one set of arrays ----
 // Dwarf d owns bodies [first, first + count) (input order and sorted order alike: the sort
 // orders by dwarf first) and the nodes [rootNode, rootEnd) in walk order.
@@ -297,14 +309,15 @@ void nb_launch_pack_walk(const double4* nodePM, const double* nodeCrit, const in
                          const double* nodeQuad, double4* rec, int capNodes, const NbScalars* sc,
                          cudaStream_t s);
 
-// The walks (forest != nullptr: one tree per dwarf, see NbForest).
+// The walks (forest != nullptr: one tree per dwarf, see NbForest).  form: the FP64 walk's
+// form, 0 the warp-union walk, 1 the walk per lane.
 void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const int2* nodeLink,
                          const double* nodeQuad, const unsigned* order, const double* px,
                          const double* py, const double* pz, double* ax, double* ay, double* az,
                          double* vx, double* vy, double* vz, const NbWalkParams& wp,
                          const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s,
                          double4* walkRec, int capNodes, const NbForest* forest = nullptr,
-                         bool lanes = false);
+                         int form = 0);
 void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int capNodes,
                           const NbWalkParams& wp, const NbPot& pot, bool count, int numSMs,
                           cudaStream_t s, const NbForest* forest = nullptr);

@@ -120,8 +120,8 @@ __device__ __forceinline__ void nb_acc_if(unsigned tk, float s, float dx, float 
         : "+f"(fx), "+f"(fy), "+f"(fz)
         : "r"(tk), "f"(s), "f"(dx), "f"(dy), "f"(dz));
 }
-// f += phiQ d - dr5inv qd under the predicate (the quadrupole term of a masked cell)
-__device__ __forceinline__ void nb_acc_quad_if(unsigned tk, float phiQ, float dx, float dy,
+// f += s d - dr5inv qd under the predicate (a masked cell's monopole and quadrupole terms)
+__device__ __forceinline__ void nb_acc_quad_if(unsigned tk, float sr, float dx, float dy,
                                                float dz, float ndr5, float qx, float qy, float qz,
                                                float& fx, float& fy, float& fz)
 {
@@ -130,7 +130,7 @@ __device__ __forceinline__ void nb_acc_quad_if(unsigned tk, float phiQ, float dx
         "@p fma.rn.f32 %1, %8, %10, %1;\n\t@p fma.rn.f32 %1, %4, %6, %1;\n\t"
         "@p fma.rn.f32 %2, %8, %11, %2;\n\t@p fma.rn.f32 %2, %4, %7, %2;\n\t}"
         : "+f"(fx), "+f"(fy), "+f"(fz)
-        : "r"(tk), "f"(phiQ), "f"(dx), "f"(dy), "f"(dz), "f"(ndr5), "f"(qx), "f"(qy), "f"(qz));
+        : "r"(tk), "f"(sr), "f"(dx), "f"(dy), "f"(dz), "f"(ndr5), "f"(qx), "f"(qy), "f"(qz));
 }
 
 // MASKED (the exact-set walk): lanes outside an entry's use mask skip its accumulation.
@@ -175,30 +175,32 @@ __device__ __forceinline__ void nb_eval_cells(const CellList<LIST_CAP>& list, in
             const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
             const float rinv = rsqrtf(r2);
             const float rinv2 = rinv * rinv;
-            const float mor3 = a.w * rinv * rinv2;
-            if (MASKED) {
-                nb_acc_if(tk, mor3, dx, dy, dz, f[q][0], f[q][1], f[q][2]);
-            } else {
-                f[q][0] = fmaf(mor3, dx, f[q][0]);
-                f[q][1] = fmaf(mor3, dy, f[q][1]);
-                f[q][2] = fmaf(mor3, dz, f[q][2]);
-            }
+            const float rinv3 = rinv * rinv2;
+            const float mor3 = a.w * rinv3;
             if (useQuad) {
                 const float qxx = b.x, qxy = b.y, qxz = b.z, qyy = b.w, qyz = c.x, qzz = c.y;
                 const float qdx = fmaf(qxz, dz, fmaf(qxy, dy, qxx * dx));
                 const float qdy = fmaf(qyz, dz, fmaf(qyy, dy, qxy * dx));
                 const float qdz = fmaf(qzz, dz, fmaf(qyz, dy, qxz * dx));
                 const float drQdr = fmaf(qdz, dz, fmaf(qdy, dy, qdx * dx));
-                const float dr5inv = rinv2 * rinv2 * rinv;
-                const float phiQ = 2.5f * dr5inv * drQdr * rinv2;
+                const float dr5inv = rinv3 * rinv2;
+                // the monopole's and the quadrupole's radial terms in one factor:
+                // f += (m r^-3 + 2.5 (r.Q.r) r^-7) r - r^-5 Q.r
+                const float sr = fmaf(2.5f * drQdr * rinv2, dr5inv, mor3);
                 if (MASKED) {
-                    nb_acc_quad_if(tk, phiQ, dx, dy, dz, -dr5inv, qdx, qdy, qdz, f[q][0], f[q][1],
+                    nb_acc_quad_if(tk, sr, dx, dy, dz, -dr5inv, qdx, qdy, qdz, f[q][0], f[q][1],
                                    f[q][2]);
                 } else {
-                    f[q][0] = fmaf(phiQ, dx, fmaf(-dr5inv, qdx, f[q][0]));
-                    f[q][1] = fmaf(phiQ, dy, fmaf(-dr5inv, qdy, f[q][1]));
-                    f[q][2] = fmaf(phiQ, dz, fmaf(-dr5inv, qdz, f[q][2]));
+                    f[q][0] = fmaf(sr, dx, fmaf(-dr5inv, qdx, f[q][0]));
+                    f[q][1] = fmaf(sr, dy, fmaf(-dr5inv, qdy, f[q][1]));
+                    f[q][2] = fmaf(sr, dz, fmaf(-dr5inv, qdz, f[q][2]));
                 }
+            } else if (MASKED) {
+                nb_acc_if(tk, mor3, dx, dy, dz, f[q][0], f[q][1], f[q][2]);
+            } else {
+                f[q][0] = fmaf(mor3, dx, f[q][0]);
+                f[q][1] = fmaf(mor3, dy, f[q][1]);
+                f[q][2] = fmaf(mor3, dz, f[q][2]);
             }
         }
     }

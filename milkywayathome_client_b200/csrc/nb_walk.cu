@@ -77,8 +77,8 @@ k_walk_fp64(const double4* __restrict__ rec,
         if (q >= end) break;
         if (COUNT) ++cSteps;
         if (ptr != q) continue;
-        const double4 nd = rec[3 * (size_t) q];
-        const double4 r1 = rec[3 * (size_t) q + 1];
+        const double4 nd = nb_ld32(rec + 3 * (size_t) q);
+        const double4 r1 = nb_ld32(rec + 3 * (size_t) q + 1);
         const long long word = __double_as_longlong(r1.y);
         const int2 link = make_int2((int) (unsigned) (word & 0xffffffffll), (int) (word >> 32));
         const double dx = nd.x - x0, dy = nd.y - y0, dz = nd.z - z0;
@@ -97,7 +97,7 @@ k_walk_fp64(const double4* __restrict__ rec,
             accy = accy + mor3 * dy;
             accz = accz + mor3 * dz;
             if (useQuad && !isBody) {
-                const double4 r2 = rec[3 * (size_t) q + 2];
+                const double4 r2 = nb_ld32(rec + 3 * (size_t) q + 2);
                 const double qxx = r1.z, qxy = r1.w, qxz = r2.x, qyy = r2.y, qyz = r2.z, qzz = r2.w;
                 const double qdx = qxx * dx + qxy * dy + qxz * dz;
                 const double qdy = qxy * dx + qyy * dy + qyz * dz;
@@ -142,12 +142,14 @@ k_walk_fp64(const double4* __restrict__ rec,
 
 // The same walk with every lane on its own path (no warp union): each iteration every lane
 // that has not finished takes the next node of its own walk (a per-lane gather of the node
-// record instead of one broadcast), so a lane is idle only when its walk is over.  Each lane
-// still meets exactly its CPU walk's nodes in the CPU's order and sums the same terms in the
-// same order.  Bodies consecutive in path order have walks of similar length, so the warp runs
-// about as many iterations as its longest walk, while the union walk runs one iteration per
-// node any of its lanes visits: on the 131k-body dwarf at theta 0.5, 0.96 of the lane slots
-// do work against 0.70 in the union walk (a CPU count over the oracle's tree).
+// record, one 32-byte load per sector, instead of one broadcast), so a lane is idle only when
+// its walk is over.  Each lane still meets exactly its CPU walk's nodes in the CPU's order and
+// sums the same terms in the same order.  Bodies consecutive in path order have walks of
+// similar length, so the warp runs about as many iterations as its longest walk, while the
+// union walk runs one iteration per node any of its lanes visits: on the 131k-body dwarf at
+// theta 0.5, 0.96 of the lane slots do work against 0.70 in the union walk (a CPU count over
+// the oracle's tree).  Walks in groups of 2 to 16 lanes (the union of each group's paths) were
+// measured between the two and slower than both.
 template <bool COUNT, bool FOREST>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk_fp64_lanes(const double4* __restrict__ rec,
@@ -186,8 +188,8 @@ k_walk_fp64_lanes(const double4* __restrict__ rec,
         if (COUNT) ++cSteps;
         if (!active) continue;
         const int q = ptr;
-        const double4 nd = rec[3 * (size_t) q];
-        const double4 r1 = rec[3 * (size_t) q + 1];
+        const double4 nd = nb_ld32(rec + 3 * (size_t) q);
+        const double4 r1 = nb_ld32(rec + 3 * (size_t) q + 1);
         const long long word = __double_as_longlong(r1.y);
         const int2 link = make_int2((int) (unsigned) (word & 0xffffffffll), (int) (word >> 32));
         const double dx = nd.x - x0, dy = nd.y - y0, dz = nd.z - z0;
@@ -206,7 +208,7 @@ k_walk_fp64_lanes(const double4* __restrict__ rec,
             accy = accy + mor3 * dy;
             accz = accz + mor3 * dz;
             if (useQuad && !isBody) {
-                const double4 r2 = rec[3 * (size_t) q + 2];
+                const double4 r2 = nb_ld32(rec + 3 * (size_t) q + 2);
                 const double qxx = r1.z, qxy = r1.w, qxz = r2.x, qyy = r2.y, qyz = r2.z, qzz = r2.w;
                 const double qdx = qxx * dx + qxy * dy + qxz * dz;
                 const double qdy = qxy * dx + qyy * dy + qyz * dz;
@@ -481,7 +483,7 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
                          const double* py, const double* pz, double* ax, double* ay, double* az,
                          double* vx, double* vy, double* vz, const NbWalkParams& wp,
                          const NbPot& pot, NbScalars* sc, bool count, cudaStream_t s,
-                         double4* walkRec, int capNodes, const NbForest* forest, bool lanes)
+                         double4* walkRec, int capNodes, const NbForest* forest, int form)
 {
     const int warps = (wp.n + 31) / 32;
     const int blocks = (warps * 32 + WALK_THREADS - 1) / WALK_THREADS;
@@ -491,7 +493,7 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
 #define NB_WALK_ARGS walkRec, order, px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc, f
 #define NB_LANES_ARGS walkRec, order, px, py, pz, ax, ay, az, wp, sc, f
     if (forest) {
-        if (lanes) {
+        if (form == 1) {
             if (count) k_walk_fp64_lanes<true, true><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
             else k_walk_fp64_lanes<false, true><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
         } else {
@@ -499,7 +501,7 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
             else k_walk_fp64<false, true><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
         }
     } else {
-        if (lanes) {
+        if (form == 1) {
             if (count) k_walk_fp64_lanes<true, false><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
             else k_walk_fp64_lanes<false, false><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
         } else {

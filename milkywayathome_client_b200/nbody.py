@@ -401,8 +401,8 @@ class NBodyState:
                                                                   float(previous_forward_time)))
 
     def set_walk_form(self, form=-1):
-        """The FP64 walk's form (nbSetWalkFormCUDA): 0 warp union, 1 per lane, -1 chosen by
-        timing the third and fourth evaluations; the accelerations are the same bit for bit."""
+        """The FP64 walk's form (nbSetWalkFormCUDA): 0 the warp union, 1 per lane, -1 chosen by
+        timing both over the first evaluations; the accelerations are the same bit for bit."""
         self.check("nbSetWalkForm", self.lib.nbSetWalkFormCUDA(self._h, int(form)))
 
     def walk_form(self):
@@ -688,6 +688,11 @@ class NBodyBatch:
     def set_tuning(self, group_max=32, list_cap=64, blocks_per_sm=0):
         self.check("nbBatchSetTuningCUDA", self.lib.nbBatchSetTuningCUDA(
             self._h, int(group_max), int(list_cap), int(blocks_per_sm)))
+
+    def set_walk_form(self, form=0):
+        """nbBatchSetWalkFormCUDA: the FP64 walk's form for every dwarf (0 warp union, 1 per
+        lane); the accelerations are the same bit for bit."""
+        self.check("nbBatchSetWalkFormCUDA", self.lib.nbBatchSetWalkFormCUDA(self._h, int(form)))
 
     def set_mixed_mode(self, exact=True):
         """nbBatchSetMixedModeCUDA: as NBodyState.set_mixed_mode for every dwarf."""

@@ -50,12 +50,14 @@ def _run_single(pot, dwarfs, precision, steps):
     return res
 
 
-def _run_batch(pot, dwarfs, precision, steps, graph):
+def _run_batch(pot, dwarfs, precision, steps, graph, walk_form=0):
     from milkywayathome_client_b200 import NBodyBatch, NBodyCtx
     cfg0 = dwarfs[0][3]
     ctx = NBodyCtx(potential=pot, precision=precision, **cfg0)
     spec = [(len(m), cfg["eps2"], cfg["timestep"], 4.0) for _, _, m, cfg in dwarfs]
     with NBodyBatch(spec) as bt:
+        if walk_form:
+            bt.set_walk_form(walk_form)
         bt.set_bodies(np.concatenate([d[0] for d in dwarfs]), np.concatenate([d[1] for d in dwarfs]),
                       np.concatenate([d[2] for d in dwarfs]))
         bt.check("nbBatchGravMap", bt.gravMap(ctx))
@@ -72,13 +74,15 @@ def _run_batch(pot, dwarfs, precision, steps, graph):
     return out, status, root, nodes
 
 
-@pytest.mark.parametrize("graph", [False, True])
-def test_fp64_batch_matches_single_dwarfs_bit_for_bit(graph):
+@pytest.mark.parametrize("graph,walk_form", [(False, 0), (True, 0), (False, 1), (True, 1)])
+def test_fp64_batch_matches_single_dwarfs_bit_for_bit(graph, walk_form):
+    """Both FP64 walk forms; with the walk per lane a warp that spans two dwarfs has each lane
+    walk its own dwarf's tree."""
     from milkywayathome_client_b200 import milky_way_potential
     dwarfs = _batch_dwarfs()
     pot = milky_way_potential()
     want = _run_single(pot, dwarfs, "fp64", 4)
-    got, status, root, nodes = _run_batch(pot, dwarfs, "fp64", 4, graph)
+    got, status, root, nodes = _run_batch(pot, dwarfs, "fp64", 4, graph, walk_form)
     assert np.all(status == 0)
     assert root[0] == 0 and np.all(np.diff(root) == nodes[:-1])
     for k, (w, g) in enumerate(zip(want, got)):

@@ -375,7 +375,7 @@ def test_union_and_per_lane_walks_are_bit_equal(dwarf_small, cfg):
             assert st.walk_form() == form
     # the per-lane walk runs fewer warp iterations than the union walk
     assert steps[1] < steps[0]
-    # automatic: the first four evaluations alternate both forms, then one is kept
+    # automatic: the first evaluations cycle twice through the candidates, then one is kept
     with _gpu_state(ctx, pos, vel, mass) as st:
         assert st.walk_form() == -1
         for _ in range(5):
