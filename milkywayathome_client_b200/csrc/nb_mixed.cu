@@ -99,11 +99,11 @@ constexpr int NB_GROUP_STACK = 16384;     // >= 256 x 63 + 32
 // entry as broadcasts.  Positions are stored relative to the walking group's centre (FP32):
 // the lane that appends an entry forms (hi - centre) + lo once, so an interaction costs each
 // body one subtraction per coordinate.  Cell entry: {rel, mass} {qxx, qxy, qxz, qyy}
-// {qyz, qzz, -, -}; body entry: {rel, mass}.
-// use[q][e]: the lanes whose body q takes entry e (all lanes, except in the exact-set walk).
+// {qyz, qzz, use[0], use[1]}; body entry: {rel, mass} and use[q][e].
+// use[q]: the lanes whose body q takes the entry (all lanes, except in the exact-set walk); a
+// cell entry carries its masks as the bits of its third record's last two floats.
 template <int LIST_CAP> struct CellList {
     float4 a[LIST_CAP], b[LIST_CAP], c[LIST_CAP];
-    unsigned use[2][LIST_CAP];
 };
 template <int LIST_CAP> struct BodyList { float4 a[LIST_CAP]; unsigned use[2][LIST_CAP]; };
 
@@ -167,10 +167,11 @@ __device__ __forceinline__ void nb_eval_cells(const CellList<LIST_CAP>& list, in
     for (int e = 0; e < n; ++e) {
         const float4 a = list.a[e];
         float4 b = make_float4(0.f, 0.f, 0.f, 0.f), c = b;
-        if (useQuad) { b = list.b[e]; c = list.c[e]; }
+        if (useQuad) b = list.b[e];
+        if (useQuad || MASKED) c = list.c[e];
 #pragma unroll
         for (int q = 0; q < BPL; ++q) {
-            const unsigned tk = MASKED ? list.use[q][e] & (1u << lane) : 1u;
+            const unsigned tk = MASKED ? __float_as_uint(q == 0 ? c.z : c.w) & (1u << lane) : 1u;
             const float dx = a.x - rb[q][0], dy = a.y - rb[q][1], dz = a.z - rb[q][2];
             const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
             const float rinv = rsqrtf(r2);
@@ -479,9 +480,8 @@ k_walk_mixed(const float4* __restrict__ nodeHi, const float4* __restrict__ nodeL
                 const float4 qa = nodeQ32[2 * cs], qb = nodeQ32[2 * cs + 1];
                 cells.a[e] = make_float4(rel.x, rel.y, rel.z, qb.z);   // the cell's mass
                 cells.b[e] = qa;
-                cells.c[e] = qb;
-                if (EXACT)
-                    for (int q = 0; q < BPL; ++q) cells.use[q][e] = use[q];
+                cells.c[e] = make_float4(qb.x, qb.y, EXACT ? __uint_as_float(use[0]) : 0.f,
+                                         EXACT && BPL > 1 ? __uint_as_float(use[BPL - 1]) : 0.f);
             }
             nB += __popc(bodyMask);
             nC += __popc(cellMask);
