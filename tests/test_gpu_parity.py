@@ -382,3 +382,20 @@ def test_union_and_per_lane_walks_are_bit_equal(dwarf_small, cfg):
             assert st.gravMap(ctx) == 0
             assert bits_equal(st.accels(), acc)
         assert st.walk_form() in (0, 1)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_negative_mass_bodies(dwarf_small, form):
+    """Bodies of negative mass (nothing in the reference forbids them): the tree, its moments
+    and both walk forms still give the oracle's status and accelerations bit for bit."""
+    from oracle import bindings as ob
+    pos, vel, mass, _ = dwarf_small
+    mass = mass.copy()
+    mass[::97] *= -0.5
+    ctx = make_ctx(len(mass), theta=0.6, allowIncest=True)
+    rc, acc, _, _ = ob.grav_map(ctx.struct, pos, mass, ctx.treeRSize)
+    with _gpu_state(ctx, pos, vel, mass) as st:
+        st.set_walk_form(form)
+        assert st.gravMap(ctx) == rc
+        if rc == 0:
+            assert bits_equal(st.accels(), acc)
