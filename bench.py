@@ -695,11 +695,14 @@ def run_ours(args, dist):
         try:
             with open(PROFILE_TRAFFIC) as f:
                 prof = json.load(f)
-            per_body = prof["fp64_walk"]["dram_bytes"] / prof["fp64_walk"]["n_bodies"]
+            rec = prof["fp64_walk_lanes" if info.walkForm == 1 else "fp64_walk"]
+            per_body = rec["dram_bytes"] / rec["n_bodies"]
             traffic = per_body * n
         except (OSError, KeyError, ValueError):
             traffic = None
-    roofline = {"bound": "fp64", "kernel": "k_walk_fp64", "achieved": achieved,
+    roofline = {"bound": "fp64",
+                "kernel": "k_walk_fp64_lanes" if info.walkForm == 1 else "k_walk_fp64",
+                "achieved": achieved,
                 "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
                 "traffic": traffic,
                 "peak_source": "measured DFMA throughput on this GPU (nbPeakFmaCUDA, in this run)",
