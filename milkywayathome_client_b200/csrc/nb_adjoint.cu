@@ -175,7 +175,10 @@ __device__ __forceinline__ double nb_warp_sum_transposed(double (&r)[V], int lan
 }
 
 // Node adjoints: nodeBar[k*10 + 0..2] = CoM, [3] = mass, [4..9] = quadrupole.
-__global__ void __launch_bounds__(128, 5)
+// Seven resident blocks of 128 (72 registers, a few spilled): 28 warps per SM, so the
+// 131,072-body dwarf's 4,096 warps run in one wave on 148 SMs (5 blocks, 96 registers: 1.4
+// waves and a 6 % slower walk).
+__global__ void __launch_bounds__(128, 7)
 k_walk_vjp(const double4* __restrict__ rec,
            const unsigned int* __restrict__ order, const double* __restrict__ px,
            const double* __restrict__ py, const double* __restrict__ pz,
