@@ -131,9 +131,6 @@ struct NbSlot {
 // The FP64 walk forms the automatic choice times (nbSetWalkFormCUDA): 0 the warp union,
 // 1 the walk per lane.
 static const int kWalkTuneForms[] = {0, 1};
-// Levels of the moment pass beyond the depth the previous tree reached (a deeper tree redoes
-// its evaluation with more).
-#define NB_LEVEL_MARGIN 3
 static const int kWalkTuneN = (int) (sizeof kWalkTuneForms / sizeof kWalkTuneForms[0]);
 
 struct NBodyCudaState {
@@ -189,10 +186,6 @@ struct NBodyCudaState {
     // the FP64 walk's form (nbSetWalkFormCUDA): -1 chooses by timing -- the first 2C uncounted
     // FP64 tree evaluations cycle twice through the C candidate forms, the second round (past
     // each kernel's first launch, which also loads it) is timed, the fastest form is kept
-    // moment levels launched per evaluation (0: the climbing pass; set from the tree depth the
-    // last evaluation found, with a margin, and raised whenever a tree grows deeper)
-    int momentLevels = 0;
-    int stepGraphLevels = -1;
     int walkForm = -1;
     int walkFormChosen = -1;
     int walkTuneStep = 0;
@@ -224,9 +217,6 @@ static void nb_free_nodes(NBodyCudaState* st)
     cudaFree(b.nodePM); cudaFree(b.nodeCrit); cudaFree(b.nodeLink); cudaFree(b.nodeQuad);
     cudaFree(b.nodeDepth); cudaFree(b.parent); cudaFree(b.nchild); cudaFree(b.arrive);
     cudaFree(b.nodeRange); b.nodeRange = nullptr;
-    cudaFree(b.childList); cudaFree(b.cellRank); cudaFree(b.cellsByDepth);
-    cudaFree(b.depthCount); cudaFree(b.depthOff);
-    b.childList = b.cellRank = b.cellsByDepth = b.depthCount = b.depthOff = nullptr;
     cudaFree(b.walkRec); b.walkRec = nullptr;
     cudaFree(st->mx.groups);
     cudaFree(st->mx.hi); cudaFree(st->mx.lo); cudaFree(st->mx.q32); cudaFree(st->mx.child8);
@@ -253,11 +243,6 @@ static NBodyCudaStatus nb_alloc_nodes(NBodyCudaState* st, int cap)
     NB_CHECK(nb_alloc(&b.nchild, cap));
     NB_CHECK(nb_alloc(&b.arrive, cap));
     NB_CHECK(nb_alloc(&b.nodeRange, cap));
-    NB_CHECK(nb_alloc(&b.childList, 8 * (size_t) cap));
-    NB_CHECK(nb_alloc(&b.cellRank, cap));
-    NB_CHECK(nb_alloc(&b.cellsByDepth, cap));
-    NB_CHECK(nb_alloc(&b.depthCount, NB_MAX_LEVELS));
-    NB_CHECK(nb_alloc(&b.depthOff, NB_MAX_LEVELS + 1));
     NB_CHECK(nb_alloc(&b.walkRec, 3 * (size_t) cap));
     NB_CHECK(nb_alloc(&st->mx.groups, cap));
     NB_CHECK(nb_alloc(&st->mx.hi, cap));
@@ -515,8 +500,7 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
         } else {
             nb_build_tree(b, n, ctx->criterion, ctx->theta, ctx->useQuad, drift, ctx->timestep,
                           st->numSMs, s, shift0);
-            nb_link_and_moments(b, n, st->capNodes, ctx->criterion, ctx->theta, ctx->useQuad, s,
-                                st->momentLevels, st->numSMs);
+            nb_link_and_moments(b, n, st->capNodes, ctx->criterion, ctx->theta, ctx->useQuad, s);
             rec(st->ev0);
             if (mixed)
                 nb_launch_walk_mixed(b, st->mx, st->capNodes, wp, pot, st->counting != 0,
@@ -549,7 +533,6 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
             const bool same = st->stepGraph && st->stepGraphDrift == drift &&
                               st->stepGraphKick == kick && st->stepGraphCap == st->capNodes &&
                               st->stepGraphForm == form &&
-                              st->stepGraphLevels == st->momentLevels &&
                               std::memcmp(st->stepGraphMx, mxKey, sizeof mxKey) == 0 &&
                               std::memcmp(&st->stepGraphCtx, ctx, sizeof *ctx) == 0;
             if (!same) {
@@ -571,7 +554,6 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
                 st->stepGraphKick = kick;
                 st->stepGraphCap = st->capNodes;
                 st->stepGraphForm = form;
-                st->stepGraphLevels = st->momentLevels;
                 std::memcpy(st->stepGraphMx, mxKey, sizeof mxKey);
             } else {
                 nb_count_launch((int) st->stepGraphLaunches);
@@ -585,12 +567,6 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
         NB_CHECK(cudaStreamSynchronize(s));
         NbScalars& h = *st->scHost;
         st->rsize = h.rsize;
-        if (h.status & NB_STATUS_LEVEL_REDO) {
-            // the tree grew deeper than the moment levels launched: redo with more
-            st->momentLevels = h.maxDepth + 1 + NB_LEVEL_MARGIN;
-            drift = 0;
-            continue;
-        }
         if (h.status & NBODY_CELL_OVERFLOW_ERROR) {
             // grow the node arrays and redo this evaluation (positions already drifted)
             int need = h.neededNodes + h.neededNodes / 4 + 64;
@@ -598,12 +574,6 @@ static NBodyCudaStatus nb_force(const NBodyCudaCtx* ctx, NBodyCudaState* st, int
             if (rc) return rc;
             drift = 0;
             continue;
-        }
-        if (ctx->criterion != NBCUDA_EXACT) {
-            // the depth this tree reached sets the moment levels of the next evaluations
-            const int want = h.maxDepth + 1 + NB_LEVEL_MARGIN;
-            if (st->momentLevels == 0 || st->momentLevels > want + NB_LEVEL_MARGIN)
-                st->momentLevels = want;
         }
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, st->ev0, st->ev1);

@@ -23,10 +23,6 @@
 // integer on this grid and `mid <= pos` (nbody/src/nbody_tree.c:42-49) is an exact
 // integer comparison.
 #define NB_GRID_LEVELS 62
-#define NB_MAX_LEVELS 64          // cell depths are below NB_GRID_LEVELS
-// Internal status bit (the reference's NBODY_RESERVED_ERROR_3, never returned): the tree is
-// deeper than the level-synchronous moment pass was launched for; the evaluation is redone.
-#define NB_STATUS_LEVEL_REDO (1 << 22)
 #define NB_KEY_LEVELS 21          // levels in the 63-bit sort key
 #define NB_MASSLESS_KEY 0xffffffffffffffffull
 
@@ -51,7 +47,6 @@ struct NbScalars {
     int nGroups;                    // walk groups formed for the mixed walk
     int step;                       // batched dwarfs: steps taken (the bar's time)
     double timeOrigin;              // batched dwarfs: the bar's time origin
-    int levelOverflow;              // a cell deeper than the moment levels launched for
 };
 
 // Potential parameters in constant-friendly POD form.
@@ -289,9 +284,6 @@ struct NbTreeBuffers {
     double4* nodePM; double* nodeCrit; int2* nodeLink; double* nodeQuad;
     int *nodeDepth, *parent, *nchild, *arrive;
     int2* nodeRange;   // first and last sorted body of every node's subtree
-    // level-synchronous moments: each cell's children (8 per node, -1 = none), its rank among
-    // the cells of its depth, the cells grouped by depth, and per-depth counts and offsets
-    int *childList, *cellRank, *cellsByDepth, *depthCount, *depthOff;
     double4* walkRec;  // 3 per node: the FP64 walk's packed node records
     NbScalars* sc;
 };
@@ -332,12 +324,8 @@ void nb_launch_walk_mixed(const NbTreeBuffers& b, const NbMixedBuffers& m, int c
 
 void nb_build_tree(NbTreeBuffers& b, int n, int criterion, double theta, int useQuad, int drift,
                    double dt, int numSMs, cudaStream_t s, const double* shift = nullptr);
-// Parents and child lists, then the moments bottom-up.  levels > 0: level-synchronous, one
-// launch per depth from levels - 1 to 0 (sc->levelOverflow is raised, and nothing computed, if
-// a cell is deeper; the caller redoes the evaluation with more levels); levels == 0: one
-// launch in which each cell's last-arriving child computes it.
 void nb_link_and_moments(NbTreeBuffers& b, int n, int capNodes, int criterion, double theta,
-                         int useQuad, cudaStream_t s, int levels = 0, int numSMs = 0);
+                         int useQuad, cudaStream_t s);
 void nb_launch_drift_only(NbTreeBuffers& b, int n, double dt, int numSMs, cudaStream_t s,
                           const double* shift = nullptr);
 // One half of the LMC's step (nb_lmc.cu): phase 0 drifts and kicks, phase 1 kicks; shift is

@@ -23,7 +23,6 @@
 //      bottom-up: the last child to finish (atomic arrival counter) computes its parent,
 //      reading the children in octant order as hackCofM does (:386-424).  No thread ever
 //      waits on another.
-#include <algorithm>
 #include "nb_common.cuh"
 #include "nb_tree_util.cuh"
 #include <cfloat>
@@ -198,10 +197,8 @@ __device__ __forceinline__ int nb_cells_before_body(const int* cum, int i, int m
 }
 
 // Total node count; checks the capacity.
-__global__ void k_count_nodes(const int* __restrict__ cum, int* __restrict__ depthCount,
-                              NbScalars* __restrict__ sc)
+__global__ void k_count_nodes(const int* __restrict__ cum, NbScalars* __restrict__ sc)
 {
-    for (int d = 0; d < NB_MAX_LEVELS; ++d) depthCount[d] = 0;
     if (nb_failed(sc)) return;
     const int m = sc->nTree;
     const int cells = m <= 1 ? 1 : cum[m - 2];
@@ -304,78 +301,26 @@ __global__ void k_emit_cells(const long long* __restrict__ gx, const long long* 
     }
 }
 
-// Parent pointers and child counts from Next() (children of cell c: c+1, then Next()).  With a
-// child list (level-synchronous moments): each cell's children in that order (-1 after the
-// last) and the cell's rank among the cells of its depth (warp-aggregated counts per depth).
-__global__ void k_link_children(const int2* __restrict__ nodeLink, const int* __restrict__ nodeDepth,
-                                int* __restrict__ parent, int* __restrict__ nchild,
-                                int* __restrict__ arrive, int* __restrict__ childList,
-                                int* __restrict__ depthCount, int* __restrict__ cellRank,
+// Parent pointers and child counts from Next() (children of cell c: c+1, then Next()).
+__global__ void k_link_children(const int2* __restrict__ nodeLink, int* __restrict__ parent,
+                                int* __restrict__ nchild, int* __restrict__ arrive,
                                 NbScalars* __restrict__ sc)
 {
     if (nb_failed(sc)) return;
     const int nNodes = sc->nNodes;
-    const int lane = threadIdx.x & 31;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nNodes; c += gridDim.x * blockDim.x) {
         if (c == 0) parent[0] = -1;
         const int2 l = nodeLink[c];
-        const bool cell = l.y < 0;
-        if (cell) {
-            int k = c + 1, count = 0;
-            while (k < l.x) {
-                parent[k] = c;
-                if (childList && count < 8) childList[8 * (size_t) c + count] = k;
-                ++count;
-                k = nodeLink[k].x;
-            }
-            if (childList)
-                for (int r = count; r < 8; ++r) childList[8 * (size_t) c + r] = -1;
-            nchild[c] = count;
-            arrive[c] = 0;
+        if (l.y >= 0) continue;            // body
+        int k = c + 1, count = 0;
+        while (k < l.x) {
+            parent[k] = c;
+            ++count;
+            k = nodeLink[k].x;
         }
-        if (childList) {
-            const int d = cell ? nodeDepth[c] : -1;
-            const unsigned act = __activemask();
-            const unsigned same = __match_any_sync(act, d);
-            if (cell) {
-                const int leader = __ffs(same) - 1;
-                int base = 0;
-                if (lane == leader) base = atomicAdd(&depthCount[d], __popc(same));
-                base = __shfl_sync(same, base, leader);
-                cellRank[c] = base + __popc(same & ((1u << lane) - 1u));
-            }
-        }
+        nchild[c] = count;
+        arrive[c] = 0;
     }
-}
-
-// Offsets of the depth groups (one thread).
-__global__ void k_depth_offsets(const int* __restrict__ depthCount, int* __restrict__ depthOff,
-                                int levels, NbScalars* __restrict__ sc)
-{
-    if (nb_failed(sc)) return;
-    int acc = 0;
-    for (int d = 0; d < NB_MAX_LEVELS; ++d) {
-        depthOff[d] = acc;
-        acc += depthCount[d];
-    }
-    depthOff[NB_MAX_LEVELS] = acc;
-    // a deeper tree than the levels launched for: stop this evaluation (the status bit stops
-    // every later kernel) and let the host redo it with more levels
-    if (sc->maxDepth >= levels) {
-        sc->levelOverflow = 1;
-        nb_raise(sc, NB_STATUS_LEVEL_REDO);
-    }
-}
-
-// Every cell into its depth group, at its rank.
-__global__ void k_depth_place(const int2* __restrict__ nodeLink, const int* __restrict__ nodeDepth,
-                              const int* __restrict__ cellRank, const int* __restrict__ depthOff,
-                              int* __restrict__ cellsByDepth, NbScalars* __restrict__ sc)
-{
-    if (nb_failed(sc)) return;
-    const int nNodes = sc->nNodes;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nNodes; c += gridDim.x * blockDim.x)
-        if (nodeLink[c].y < 0) cellsByDepth[depthOff[nodeDepth[c]] + cellRank[c]] = c;
 }
 
 // ---------------------------------------------------------------------------------
@@ -457,106 +402,6 @@ __global__ void k_moments(double4* __restrict__ nodePM, double* __restrict__ nod
     if (structErr) nb_raise(sc, NBODY_TREE_STRUCTURE_ERROR);
 }
 
-// One depth of the moments, level-synchronous: hackCofM, findRCrit, nbCheckTreeStructure and
-// hackQuad of every cell at depth D, whose children the launches for the deeper levels have
-// already summarised.  Eight lanes per cell, one child each, so a cell's child records are read
-// at once instead of along the Next chain; every sum still runs in child (octant) order, over
-// the eight lanes' values by shuffles, with the climbing kernel's expressions.
-__global__ void __launch_bounds__(256)
-k_moments_level(int D, const int* __restrict__ cellsByDepth, const int* __restrict__ depthOff,
-                const int* __restrict__ childList, double4* __restrict__ nodePM,
-                double* __restrict__ nodeCrit, const int2* __restrict__ nodeLink,
-                double* __restrict__ nodeQuad, int criterion, double theta, int useQuad,
-                NbScalars* __restrict__ sc)
-{
-    if (nb_failed(sc)) return;
-    const int lo = depthOff[D], hi = depthOff[D + 1];
-    const int lane = threadIdx.x & 31, r = lane & 7, g0 = lane & ~7;
-    const double rsize = sc->rsize;
-    double psize = rsize;
-    for (int d = 0; d < D; ++d) psize *= 0.5;
-    const int warp = (int) ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int warps = (int) ((gridDim.x * blockDim.x) >> 5);
-    int structErr = 0;
-    for (int p0 = lo + 4 * warp; p0 < hi; p0 += 4 * warps) {      // the same p0 on all lanes
-        const int p = p0 + (lane >> 3);
-        const bool has = p < hi;
-        const int c = has ? cellsByDepth[p] : -1;
-        const int k = has ? childList[8 * (size_t) c + r] : -1;
-        double4 q = make_double4(0.0, 0.0, 0.0, 0.0);
-        bool kCell = false;
-        if (k >= 0) {
-            q = nodePM[k];
-            kCell = nodeLink[k].y < 0;
-        }
-        const unsigned present = (__ballot_sync(NB_FULL_MASK, k >= 0) >> g0) & 0xffu;
-        const double4 geo = has ? nodePM[c] : make_double4(0.0, 0.0, 0.0, 0.0);
-        // hackCofM (:394-424)
-        const double wx = q.w * q.x, wy = q.w * q.y, wz = q.w * q.z;
-        double M = 0.0, cmx = 0.0, cmy = 0.0, cmz = 0.0;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const double mj = __shfl_sync(NB_FULL_MASK, q.w, g0 + j);
-            const double xj = __shfl_sync(NB_FULL_MASK, wx, g0 + j);
-            const double yj = __shfl_sync(NB_FULL_MASK, wy, g0 + j);
-            const double zj = __shfl_sync(NB_FULL_MASK, wz, g0 + j);
-            if (present & (1u << j)) {
-                M = M + mj;
-                cmx = cmx + xj;
-                cmy = cmy + yj;
-                cmz = cmz + zj;
-            }
-        }
-        if (M > 0.0) { cmx = cmx / M; cmy = cmy / M; cmz = cmz / M; }
-        else { cmx = geo.x; cmy = geo.y; cmz = geo.z; }
-        // nbCheckTreeStructure (:345-380)
-        const double h = 0.5 * psize;
-        if (has && r == 0 &&
-            (cmx < geo.x - h || cmx > geo.x + h || cmy < geo.y - h || cmy > geo.y + h ||
-             cmz < geo.z - h || cmz > geo.z + h))
-            structErr = 1;
-        // hackQuad (:70-121): each lane its child's term, summed in child order
-        double qs[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        if (useQuad) {
-            double t[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            if (k >= 0) {
-                const double dx = q.x - cmx, dy = q.y - cmy, dz = q.z - cmz;
-                const double drsq = dz * dz + (dy * dy + dx * dx);
-                const double mq = q.w;
-                t[0] = mq * (3.0 * (dx * dx) - drsq);
-                t[1] = mq * (3.0 * (dx * dy));
-                t[2] = mq * (3.0 * (dx * dz));
-                t[3] = mq * (3.0 * (dy * dy) - drsq);
-                t[4] = mq * (3.0 * (dy * dz));
-                t[5] = mq * (3.0 * (dz * dz) - drsq);
-                if (kCell) {
-                    const double* Q = nodeQuad + 6 * (size_t) k;
-#pragma unroll
-                    for (int e = 0; e < 6; ++e) t[e] = t[e] + Q[e];
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-#pragma unroll
-                for (int e = 0; e < 6; ++e) {
-                    const double v = __shfl_sync(NB_FULL_MASK, t[e], g0 + j);
-                    if (present & (1u << j)) qs[e] = qs[e] + v;
-                }
-            }
-        }
-        if (has && r == 0) {
-            nodeCrit[c] = nb_find_rcrit2(criterion, theta, rsize, geo.x, geo.y, geo.z,
-                                         cmx, cmy, cmz, psize);
-            // without quadrupoles the record reads as zero (as the restated CPU tree does)
-            double* Q = nodeQuad + 6 * (size_t) c;
-#pragma unroll
-            for (int e = 0; e < 6; ++e) Q[e] = qs[e];
-            nodePM[c] = make_double4(cmx, cmy, cmz, M);
-        }
-    }
-    if (structErr) nb_raise(sc, NBODY_TREE_STRUCTURE_ERROR);
-}
-
 // ---------------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------------
@@ -595,7 +440,7 @@ void nb_build_tree(NbTreeBuffers& b, int n, int criterion, double theta, int use
     // cum = inclusive prefix sum of owned-cell counts over boundaries [0, n-2] (the kernels
     // only read the first m-1 entries; entries past m-2 hold stale counts and are unused)
     if (n > 1) nb_inclusive_scan(b.cum, n - 1, b.scanTmp, s);
-    k_count_nodes<<<1, 1, 0, s>>>(b.cum, b.depthCount, b.sc);
+    k_count_nodes<<<1, 1, 0, s>>>(b.cum, b.sc);
     k_emit_bodies<<<g, T, 0, s>>>(b.px, b.py, b.pz, b.mass, b.sort.idxA, b.delta, b.cum, b.nodePM,
                                   b.nodeCrit, b.nodeLink, b.nodeDepth, b.bodyNode, b.nodeRange, b.sc);
     k_emit_cells<<<g, T, 0, s>>>(b.gx, b.gy, b.gz, b.delta, b.cum, b.nodePM, b.nodeCrit,
@@ -605,37 +450,15 @@ void nb_build_tree(NbTreeBuffers& b, int n, int criterion, double theta, int use
 }
 
 void nb_link_and_moments(NbTreeBuffers& b, int n, int capNodes, int criterion, double theta,
-                         int useQuad, cudaStream_t s, int levels, int numSMs)
+                         int useQuad, cudaStream_t s)
 {
     const int T = 256;
     const int gNodes = nb_grid_for(capNodes, T, 1 << 20);
-    if (levels <= 0) {
-        const int g = nb_grid_for(n, T, 1 << 20);
-        k_link_children<<<gNodes, T, 0, s>>>(b.nodeLink, b.nodeDepth, b.parent, b.nchild, b.arrive,
-                                             nullptr, nullptr, nullptr, b.sc);
-        k_moments<<<g, T, 0, s>>>(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeDepth, b.nodeQuad,
-                                  b.parent, b.nchild, b.arrive, b.bodyNode, criterion, theta,
-                                  useQuad, b.sc);
-        nb_count_launch(2);
-        return;
-    }
-    levels = std::min(levels, NB_MAX_LEVELS);
-    k_link_children<<<gNodes, T, 0, s>>>(b.nodeLink, b.nodeDepth, b.parent, b.nchild, b.arrive,
-                                         b.childList, b.depthCount, b.cellRank, b.sc);
-    k_depth_offsets<<<1, 1, 0, s>>>(b.depthCount, b.depthOff, levels, b.sc);
-    k_depth_place<<<gNodes, T, 0, s>>>(b.nodeLink, b.nodeDepth, b.cellRank, b.depthOff,
-                                       b.cellsByDepth, b.sc);
-    const long long cap = numSMs > 0 ? 8LL * numSMs : 1184;
-    for (int D = levels - 1; D >= 0; --D) {
-        // at most 8^D cells at depth D, 32 per block and pass
-        const long long most = D < 10 ? std::min(1LL << (3 * D), (long long) capNodes)
-                                      : (long long) capNodes;
-        const int blocks = (int) std::max(1LL, std::min(cap, (most + 31) / 32));
-        k_moments_level<<<blocks, T, 0, s>>>(D, b.cellsByDepth, b.depthOff, b.childList, b.nodePM,
-                                             b.nodeCrit, b.nodeLink, b.nodeQuad, criterion, theta,
-                                             useQuad, b.sc);
-    }
-    nb_count_launch(3 + levels);
+    const int g = nb_grid_for(n, T, 1 << 20);
+    k_link_children<<<gNodes, T, 0, s>>>(b.nodeLink, b.parent, b.nchild, b.arrive, b.sc);
+    k_moments<<<g, T, 0, s>>>(b.nodePM, b.nodeCrit, b.nodeLink, b.nodeDepth, b.nodeQuad, b.parent,
+                              b.nchild, b.arrive, b.bodyNode, criterion, theta, useQuad, b.sc);
+    nb_count_launch(2);
 }
 
 void nb_launch_drift_only(NbTreeBuffers& b, int n, double dt, int numSMs, cudaStream_t s,

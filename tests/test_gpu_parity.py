@@ -399,54 +399,3 @@ def test_negative_mass_bodies(dwarf_small, form):
         assert st.gravMap(ctx) == rc
         if rc == 0:
             assert bits_equal(st.accels(), acc)
-
-
-@pytest.mark.parametrize("cfg", CONFIGS, ids=lambda c: "%s-%g-q%d" % (c["criterion"], c["theta"], c["useQuad"]))
-def test_level_synchronous_moments_bitexact(dwarf_small, cfg):
-    """From a state's second force evaluation on, the moments run level by level (one launch
-    per depth, eight lanes per cell); the tree they leave -- centres of mass, masses, rcrit2,
-    quadrupoles -- and the accelerations equal the oracle's bit for bit."""
-    from oracle import bindings as ob
-    pos, vel, mass, _ = dwarf_small
-    ctx = make_ctx(len(mass), **cfg)
-    want = ob.tree(ctx.struct, pos, mass, ctx.treeRSize)
-    rc, acc, _, _ = ob.grav_map(ctx.struct, pos, mass, ctx.treeRSize)
-    with _gpu_state(ctx, pos, vel, mass) as st:
-        assert st.gravMap(ctx) == rc == 0          # the first evaluation sets the levels
-        st.set_bodies(pos, vel, mass, ctx.treeRSize)
-        assert st.gravMap(ctx) == 0
-        got = st.tree()
-        assert bits_equal(st.accels(), acc)
-    for k in TREE_KEYS:
-        if k in ("next", "body", "depth"):
-            assert np.array_equal(got[k], want[k]), k
-        else:
-            assert bits_equal(got[k], want[k]), k
-
-
-def test_deeper_tree_redoes_the_level_moments(dwarf_small):
-    """A tree that grows deeper than the moment levels launched (two bodies 1e-9 apart after a
-    shallow tree) is redone with more levels: tree and accelerations still equal the oracle's."""
-    from oracle import bindings as ob
-    pos, vel, mass, _ = dwarf_small
-    ctx = make_ctx(len(mass), theta=0.5)
-    deep = pos.copy()
-    deep[1] = deep[0] + 1e-9
-    want = ob.tree(ctx.struct, deep, mass, ctx.treeRSize)
-    rc, acc, _, _ = ob.grav_map(ctx.struct, deep, mass, ctx.treeRSize)
-    assert rc == 0 and want["maxDepth"] > 25
-    with _gpu_state(ctx, pos, vel, mass) as st:
-        assert st.gravMap(ctx) == 0
-        assert st.gravMap(ctx) == 0
-        shallow = st.tree_info().maxDepth
-        assert shallow < 20
-        st.set_bodies(deep, vel, mass, ctx.treeRSize)
-        assert st.gravMap(ctx) == 0
-        assert st.tree_info().maxDepth == want["maxDepth"]
-        got = st.tree()
-        assert bits_equal(st.accels(), acc)
-    for k in TREE_KEYS:
-        if k in ("next", "body", "depth"):
-            assert np.array_equal(got[k], want[k]), k
-        else:
-            assert bits_equal(got[k], want[k]), k
