@@ -242,10 +242,13 @@ k_walk_vjp(const double4* __restrict__ rec,
                     for (int c = 0; c < 6; ++c) atomicAdd(nb + 4 + c, v.q[c]);
             }
         } else if (interMask && cellQ) {
-            double r[16] = {v.rx, v.ry, v.rz, v.m, v.q[0], v.q[1], v.q[2], v.q[3], v.q[4], v.q[5],
-                            0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            const double sum = nb_warp_sum_transposed<16>(r, lane);
-            if ((lane & 1) == 0 && (lane >> 1) < 10) atomicAdd(nb + (lane >> 1), sum);
+            // ten values as eight plus two (14 shuffles, against 16 for ten padded to sixteen)
+            double r8[8] = {v.rx, v.ry, v.rz, v.m, v.q[0], v.q[1], v.q[2], v.q[3]};
+            double r2[2] = {v.q[4], v.q[5]};
+            const double s8 = nb_warp_sum_transposed<8>(r8, lane);
+            const double s2 = nb_warp_sum_transposed<2>(r2, lane);
+            if ((lane & 3) == 0) atomicAdd(nb + (lane >> 2), s8);
+            if ((lane & 15) == 0) atomicAdd(nb + 8 + (lane >> 4), s2);
         } else if (interMask) {
             double r[4] = {v.rx, v.ry, v.rz, v.m};
             const double sum = nb_warp_sum_transposed<4>(r, lane);
