@@ -5,11 +5,14 @@
 // Walk (nbGravity, nbody/src/nbody_grav.c:42-124).  One warp walks for 32 bodies that are
 // consecutive in octree-path order.  Every lane keeps its own position in the reference's
 // stackless walk: at node q it accepts (interacts, then jumps to Next(q)) if q is a body or
-// |dr|^2 >= rcrit2(q), otherwise it opens q (goes to More(q) = q + 1 in walk order).  The warp
-// visits the smallest pending node of its lanes, so each lane sees exactly the nodes of its
-// own CPU walk, in the CPU's order, and accumulates the same terms in the same order; the
-// node records are read once per warp visit (uniform address).  FP64-pipe bound: a monopole
-// interaction is 18 flops + sqrt + 2 divisions, a quadrupole cell adds 38 flops + 2 divisions.
+// |dr|^2 >= rcrit2(q), otherwise it opens q (goes to More(q) = q + 1 in walk order).  Two
+// forms: the warp-union walk (k_walk_fp64) visits the smallest pending node of its lanes, each
+// node record read once per warp visit (uniform address); the per-lane walk
+// (k_walk_fp64_lanes) lets each lane take its own next node every iteration.  Either way each
+// lane sees exactly the nodes of its own CPU walk, in the CPU's order, and accumulates the same
+// terms in the same order.  A monopole interaction is 18 flops + sqrt + 2 divisions, a
+// quadrupole cell adds 38 flops + 2 divisions: the FP64 pipe (and, per lane, the L1 data pipe
+// that gathers the records) bounds the walk.
 #include "nb_common.cuh"
 #include "nb_potential.cuh"
 
