@@ -91,8 +91,10 @@ def parse_args():
                     help="steps of the energy-drift run of both forms (0: skip)")
     ap.add_argument("--theta2", type=float, default=1.0,
                     help="second opening angle measured for both forms (0: skip)")
-    ap.add_argument("--walk-form", choices=["auto", "union", "lanes"], default="auto",
-                    help="the FP64 walk: chosen by timing (default), warp union or per lane")
+    ap.add_argument("--walk-form", choices=["auto", "union", "lanes", "prefetch"],
+                    default="auto",
+                    help="the FP64 walk: chosen by timing (default), warp union, per lane, or "
+                         "per lane loading the next record early")
     ap.add_argument("--profile", choices=["fp64", "mixed", "adjoint", "batch", "config0"],
                     help="profiling entry: build the dwarf, run two force evaluations, exit")
     return ap.parse_args()
@@ -505,6 +507,22 @@ def form_accuracy(pos, vel, mass, c_cfg, dev, seed=4096):
     return out
 
 
+WALK_FORM_NAMES = {0: "warp union", 1: "per lane", 2: "per lane, next record loaded early"}
+
+
+def settle_walk_form(st, c):
+    """Untimed force evaluations at the current positions (each recomputes the same
+    accelerations) until the FP64 walk's automatic form choice is made, so that no timed step
+    runs a candidate form; a no-op for the mixed form and once a form is set."""
+    from milkywayathome_client_b200 import _lib
+    if c.precision != _lib.PRECISION_FP64 or c.criterion == _lib.EXACT:
+        return                          # only FP64 tree walks choose a form
+    for _ in range(8):
+        if st.walk_form() >= 0:
+            return
+        st.check("nbGravMap", st.gravMap(c))
+
+
 def run_steps_timed(c, pos, vel, mass, dev, warm, steps, exact=True):
     """A fresh state of the arrays, `warm` untimed steps, then `steps` steps each timed with
     CUDA events; returns (step ms list, walk ms list, tree info)."""
@@ -516,6 +534,8 @@ def run_steps_timed(c, pos, vel, mass, dev, warm, steps, exact=True):
         st.set_mixed_mode(exact)
         for _ in range(warm):
             st.check("nbStepSystem", st.step(c))
+        if warm:
+            settle_walk_form(st, c)
         ms, walk = [], []
         for _ in range(steps):
             st.check("nbStepSystem", st.step(c))
@@ -584,6 +604,7 @@ def run_ours(args, dist):
         st.set_mixed_mode(exact)
         for _ in range(W):              # the automatic walk form is chosen here
             st.check("nbStepSystem", st.step(c))
+        settle_walk_form(st, c)
         # the interaction counts of the walk in use (a force evaluation at the same positions)
         st.set_counting(True)
         st.check("nbGravMap", st.gravMap(c))
@@ -695,13 +716,13 @@ def run_ours(args, dist):
         try:
             with open(PROFILE_TRAFFIC) as f:
                 prof = json.load(f)
-            rec = prof["fp64_walk_lanes" if info.walkForm == 1 else "fp64_walk"]
+            rec = prof["fp64_walk_lanes" if info.walkForm >= 1 else "fp64_walk"]
             per_body = rec["dram_bytes"] / rec["n_bodies"]
             traffic = per_body * n
         except (OSError, KeyError, ValueError):
             traffic = None
     roofline = {"bound": "fp64",
-                "kernel": "k_walk_fp64_lanes" if info.walkForm == 1 else "k_walk_fp64",
+                "kernel": "k_walk_fp64_lanes" if info.walkForm >= 1 else "k_walk_fp64",
                 "achieved": achieved,
                 "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
                 "traffic": traffic,
@@ -710,7 +731,7 @@ def run_ours(args, dist):
                 "interactions_per_body": {"body": counts[0] / n, "cell": counts[1] / n,
                                           "visits": counts[2] / n},
                 "lane_utilisation": counts[2] / (32.0 * max(counts[3], 1)),
-                "walk_form": {0: "warp union", 1: "per lane"}.get(info.walkForm, "undecided")}
+                "walk_form": WALK_FORM_NAMES.get(info.walkForm, "undecided")}
     # the exact-set mixed walk evaluates every body's own FP64 interaction set, so its
     # algorithmic work is the FP64 walk's count; issued work (list entries x 32 lanes, masked
     # lanes included) is given beside it
@@ -871,7 +892,7 @@ def run_profile(args):
 def main():
     args = parse_args()
     global WALK_FORM
-    WALK_FORM = {"auto": -1, "union": 0, "lanes": 1}[args.walk_form]
+    WALK_FORM = {"auto": -1, "union": 0, "lanes": 1, "prefetch": 2}[args.walk_form]
     if args.impl == "reference":
         # the reference arm is host-only: rank 0 runs it, other ranks exit without work
         os.environ.setdefault("WORLD_SIZE", "1")

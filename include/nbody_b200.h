@@ -354,14 +354,16 @@ NBodyCudaStatus nbSetStepGraphCUDA(NBodyCudaState* st, int enable);
 
 /* The FP64 force walk's form: 0 walks the union of a warp's 32 tree paths node by node (the
  * lanes whose path holds the node doing it, one broadcast load per node); 1 walks every body's
- * path in its own lane (a lane idles only once its walk is over; per-lane loads).
- * -1 (the default) cycles twice through the candidate forms over a state's first uncounted
- * FP64 tree evaluations, times the second round (the first launch of each kernel also loads
- * it) and keeps the fastest.  Every form gives every body exactly its CPU walk -- same nodes,
- * same order, same sums: the accelerations are the same bit for bit.  A batch walks the union
- * unless its form is set to 1 (nbBatchSetWalkFormCUDA); the force adjoint always walks the union
- * (it reduces each node's adjoints over the warp).  nbGetWalkFormCUDA reports the form in use
- * (-1 while undecided). */
+ * path in its own lane (a lane idles only once its walk is over; per-lane loads); 2 is the
+ * per-lane walk that loads the next node's record as soon as the opening test has chosen it,
+ * overlapping that load with the current node's arithmetic (more registers: faster for small
+ * systems, slower at a million bodies).  -1 (the default) cycles twice through the three
+ * forms over a state's first six uncounted FP64 tree evaluations, times the second round (the
+ * first launch of each kernel also loads it) and keeps the fastest.  Every form gives every
+ * body exactly its CPU walk -- same nodes, same order, same sums: the accelerations are the
+ * same bit for bit.  A batch walks the union unless its form is set (nbBatchSetWalkFormCUDA);
+ * the force adjoint always walks the union (it reduces each node's adjoints over the warp).
+ * nbGetWalkFormCUDA reports the form in use (-1 while undecided). */
 NBodyCudaStatus nbSetWalkFormCUDA(NBodyCudaState* st, int form);
 NBodyCudaStatus nbGetWalkFormCUDA(NBodyCudaState* st, int* form);
 
@@ -493,8 +495,8 @@ NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* batch, int groupMax, int li
 /* as nbSetMixedModeCUDA, for every dwarf of the batch */
 NBodyCudaStatus nbBatchSetMixedModeCUDA(NBodyCudaBatch* batch, int exactSet);
 /* The FP64 walk's form for every dwarf of the batch, as nbSetWalkFormCUDA but without the
- * automatic choice: 0 (the default) the warp union, 1 per lane (a warp may span two dwarfs;
- * each lane walks only its own dwarf's tree). */
+ * automatic choice: 0 (the default) the warp union, 1 per lane, 2 per lane with the next
+ * record loaded early (a warp may span two dwarfs; each lane walks only its own dwarf's tree). */
 NBodyCudaStatus nbBatchSetWalkFormCUDA(NBodyCudaBatch* batch, int form);
 NBodyCudaStatus nbBatchGetTuningCUDA(NBodyCudaBatch* batch, int* groupMax, int* listCap,
                                      int* blocksPerSM);

@@ -129,8 +129,8 @@ struct NbSlot {
 };
 
 // The FP64 walk forms the automatic choice times (nbSetWalkFormCUDA): 0 the warp union,
-// 1 the walk per lane.
-static const int kWalkTuneForms[] = {0, 1};
+// 1 the walk per lane, 2 the walk per lane that loads the next node's record early.
+static const int kWalkTuneForms[] = {0, 1, 2};
 static const int kWalkTuneN = (int) (sizeof kWalkTuneForms / sizeof kWalkTuneForms[0]);
 
 struct NBodyCudaState {
@@ -1817,7 +1817,7 @@ NBodyCudaStatus nbSetTimeOriginCUDA(NBodyCudaState* st, double previousForwardTi
 
 NBodyCudaStatus nbSetWalkFormCUDA(NBodyCudaState* st, int form)
 {
-    if (!st || form < -1 || form > 1) return NBODY_USER_ERROR;
+    if (!st || form < -1 || form > 2) return NBODY_USER_ERROR;
     st->walkForm = form;
     st->walkFormChosen = -1;
     st->walkTuneStep = 0;
@@ -2413,7 +2413,7 @@ NBodyCudaStatus nbBatchSetTuningCUDA(NBodyCudaBatch* bt, int groupMax, int listC
 
 NBodyCudaStatus nbBatchSetWalkFormCUDA(NBodyCudaBatch* bt, int form)
 {
-    if (!bt || form < 0 || form > 1) return NBODY_USER_ERROR;
+    if (!bt || form < 0 || form > 2) return NBODY_USER_ERROR;
     bt->st->walkForm = form;
     nb_batch_drop_graph(bt);            // the captured step holds the walk kernel
     return NBODY_SUCCESS;

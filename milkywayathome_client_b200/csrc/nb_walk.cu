@@ -153,7 +153,7 @@ k_walk_fp64(const double4* __restrict__ rec,
 // theta 0.5, 0.96 of the lane slots do work against 0.70 in the union walk (a CPU count over
 // the oracle's tree).  Walks in groups of 2 to 16 lanes (the union of each group's paths) were
 // measured between the two and slower than both.
-template <bool COUNT, bool FOREST>
+template <bool COUNT, bool FOREST, bool PREFETCH>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk_fp64_lanes(const double4* __restrict__ rec,
                   const unsigned int* __restrict__ order, const double* __restrict__ px,
@@ -183,6 +183,15 @@ k_walk_fp64_lanes(const double4* __restrict__ rec,
     double accx = 0.0, accy = 0.0, accz = 0.0;
     bool metSelf = false;
     unsigned long long cVisit = 0, cBB = 0, cBC = 0, cSteps = 0;
+    // PREFETCH: the next node's record is loaded as soon as the opening test has chosen it,
+    // before this node's terms are computed, so its latency overlaps the FP64 arithmetic (72
+    // registers against 56: it pays where few warps are resident, tens of thousands of bodies,
+    // and costs at a million, where other warps already hide the latency)
+    double4 nd = make_double4(0.0, 0.0, 0.0, 0.0), r1 = nd;
+    if (PREFETCH && ptr < myEnd) {
+        nd = nb_ld32(rec + 3 * (size_t) ptr);
+        r1 = nb_ld32(rec + 3 * (size_t) ptr + 1);
+    }
     for (;;) {
         // every lane takes part in the vote of every iteration (a finished lane idles in the
         // loop), and the warp leaves the loop together when all its walks are over
@@ -191,17 +200,25 @@ k_walk_fp64_lanes(const double4* __restrict__ rec,
         if (COUNT) ++cSteps;
         if (!active) continue;
         const int q = ptr;
-        const double4 nd = nb_ld32(rec + 3 * (size_t) q);
-        const double4 r1 = nb_ld32(rec + 3 * (size_t) q + 1);
+        if (!PREFETCH) {
+            nd = nb_ld32(rec + 3 * (size_t) q);
+            r1 = nb_ld32(rec + 3 * (size_t) q + 1);
+        }
         const long long word = __double_as_longlong(r1.y);
         const int2 link = make_int2((int) (unsigned) (word & 0xffffffffll), (int) (word >> 32));
         const double dx = nd.x - x0, dy = nd.y - y0, dz = nd.z - z0;
         double drSq = dz * dz + (dy * dy + dx * dx);
         const bool isBody = link.y >= 0;
         if (COUNT) ++cVisit;
-        if (isBody || drSq >= r1.x) {
-            ptr = link.x;
-            if (isBody && (unsigned) link.y == j) { metSelf = true; continue; }
+        const bool accept = isBody || drSq >= r1.x;
+        ptr = accept ? link.x : q + 1;
+        double4 ndNext = nd, r1Next = r1;
+        if (PREFETCH && ptr < myEnd) {
+            ndNext = nb_ld32(rec + 3 * (size_t) ptr);
+            r1Next = nb_ld32(rec + 3 * (size_t) ptr + 1);
+        }
+        if (accept && isBody && (unsigned) link.y == j) metSelf = true;
+        else if (accept) {
             if (COUNT) { if (isBody) ++cBB; else ++cBC; }
             drSq = drSq + eps2;
             const double drab = sqrt(drSq);
@@ -226,9 +243,8 @@ k_walk_fp64_lanes(const double4* __restrict__ rec,
                 accy = accy - dr5inv * qdy;
                 accz = accz - dr5inv * qdz;
             }
-        } else {
-            ptr = q + 1;
         }
+        if (PREFETCH) { nd = ndNext; r1 = r1Next; }
     }
     if (COUNT) {
         // every lane counted the warp's iterations alike
@@ -496,17 +512,23 @@ void nb_launch_walk_fp64(const double4* nodePM, const double* nodeCrit, const in
 #define NB_WALK_ARGS walkRec, order, px, py, pz, ax, ay, az, vx, vy, vz, wp, pot, sc, f
 #define NB_LANES_ARGS walkRec, order, px, py, pz, ax, ay, az, wp, sc, f
     if (forest) {
-        if (form == 1) {
-            if (count) k_walk_fp64_lanes<true, true><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
-            else k_walk_fp64_lanes<false, true><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
+        if (form == 2) {
+            if (count) k_walk_fp64_lanes<true, true, true><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
+            else k_walk_fp64_lanes<false, true, true><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
+        } else if (form == 1) {
+            if (count) k_walk_fp64_lanes<true, true, false><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
+            else k_walk_fp64_lanes<false, true, false><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
         } else {
             if (count) k_walk_fp64<true, true><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
             else k_walk_fp64<false, true><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
         }
     } else {
-        if (form == 1) {
-            if (count) k_walk_fp64_lanes<true, false><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
-            else k_walk_fp64_lanes<false, false><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
+        if (form == 2) {
+            if (count) k_walk_fp64_lanes<true, false, true><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
+            else k_walk_fp64_lanes<false, false, true><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
+        } else if (form == 1) {
+            if (count) k_walk_fp64_lanes<true, false, false><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
+            else k_walk_fp64_lanes<false, false, false><<<blocks, WALK_THREADS, 0, s>>>(NB_LANES_ARGS);
         } else {
             if (count) k_walk_fp64<true, false><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);
             else k_walk_fp64<false, false><<<blocks, WALK_THREADS, 0, s>>>(NB_WALK_ARGS);

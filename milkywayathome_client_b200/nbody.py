@@ -401,8 +401,9 @@ class NBodyState:
                                                                   float(previous_forward_time)))
 
     def set_walk_form(self, form=-1):
-        """The FP64 walk's form (nbSetWalkFormCUDA): 0 the warp union, 1 per lane, -1 chosen by
-        timing both over the first evaluations; the accelerations are the same bit for bit."""
+        """The FP64 walk's form (nbSetWalkFormCUDA): 0 the warp union, 1 per lane, 2 per lane
+        with the next node's record loaded early, -1 chosen by timing the three over the first
+        evaluations; the accelerations are the same bit for bit."""
         self.check("nbSetWalkForm", self.lib.nbSetWalkFormCUDA(self._h, int(form)))
 
     def walk_form(self):
@@ -691,7 +692,8 @@ class NBodyBatch:
 
     def set_walk_form(self, form=0):
         """nbBatchSetWalkFormCUDA: the FP64 walk's form for every dwarf (0 warp union, 1 per
-        lane); the accelerations are the same bit for bit."""
+        lane, 2 per lane loading the next record early); the accelerations are the same bit
+        for bit."""
         self.check("nbBatchSetWalkFormCUDA", self.lib.nbBatchSetWalkFormCUDA(self._h, int(form)))
 
     def set_mixed_mode(self, exact=True):

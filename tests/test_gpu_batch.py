@@ -74,9 +74,10 @@ def _run_batch(pot, dwarfs, precision, steps, graph, walk_form=0):
     return out, status, root, nodes
 
 
-@pytest.mark.parametrize("graph,walk_form", [(False, 0), (True, 0), (False, 1), (True, 1)])
+@pytest.mark.parametrize("graph,walk_form", [(False, 0), (True, 0), (False, 1), (True, 1),
+                                             (True, 2)])
 def test_fp64_batch_matches_single_dwarfs_bit_for_bit(graph, walk_form):
-    """Both FP64 walk forms; with the walk per lane a warp that spans two dwarfs has each lane
+    """Every FP64 walk form; with the walks per lane a warp that spans two dwarfs has each lane
     walk its own dwarf's tree."""
     from milkywayathome_client_b200 import milky_way_potential
     dwarfs = _batch_dwarfs()
