@@ -2,7 +2,7 @@
 own code -- nbGravMap once, then whole nbStepSystem steps -- with no sampling: after k steps
 its state is the reference's after k steps, and the C restatement it falls back to (where the
 reference build is absent) lands on the same state bit for bit.  Both arms print the same
-`config`.  CPU only."""
+`config`.  The timed arm settles the FP64 walk's automatic form before timing.  CPU only."""
 import os
 import sys
 
@@ -60,3 +60,42 @@ def test_both_arms_print_the_same_config():
     b = bench.bench_config(1048576, 0.5)
     assert a == b and a["n_bodies"] == 1048576 and a["theta"] == 0.5
     assert a["eps2"] == bench.bench_ctx(1048576, 0.5)[0].eps2
+
+
+class _FakeState:
+    """Stands in for NBodyState: the walk form is chosen after `decide_after` evaluations."""
+
+    def __init__(self, decide_after):
+        self.evaluations = 0
+        self.decide_after = decide_after
+
+    def walk_form(self):
+        return 1 if self.evaluations >= self.decide_after else -1
+
+    def gravMap(self, ctx):
+        self.evaluations += 1
+        return 0
+
+    def check(self, what, rc):
+        assert rc == 0, what
+
+
+def test_walk_form_is_settled_before_timed_steps():
+    """bench settles the FP64 walk's automatic form with untimed force evaluations, only for
+    FP64 tree walks, and never loops past its bound."""
+    import bench
+    from milkywayathome_client_b200 import NBodyCtx, models
+    ctx = NBodyCtx(potential=models.sample_workunit_potential(), **models.dwarf_config(4096))
+    st = _FakeState(decide_after=2)
+    bench.settle_walk_form(st, ctx)
+    assert st.evaluations == 2 and st.walk_form() == 1
+    st = _FakeState(decide_after=0)
+    bench.settle_walk_form(st, ctx)
+    assert st.evaluations == 0
+    st = _FakeState(decide_after=100)
+    bench.settle_walk_form(st, ctx)
+    assert st.evaluations == 8
+    st = _FakeState(decide_after=2)
+    bench.settle_walk_form(st, ctx.with_precision("mixed"))
+    assert st.evaluations == 0
+    assert set(bench.WALK_FORM_NAMES) == {0, 1, 2}
